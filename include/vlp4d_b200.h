@@ -1,0 +1,159 @@
+/* vlp4d_b200 — C ABI of the B200 (sm_100a) implementation of the vlp4d
+ * semi-Lagrangian hot path from yasahi-hpc/P3-miniapps.
+ *
+ * Every entry point replaces one function of the reference's single-process
+ * CUDA variant (miniapps/vlp4d/thrust); the citation in each comment is the
+ * reference interface it stands in for.  The C++ layer in
+ * p3-miniapps_b200/cpp/vlp4d_api.hpp re-exports these under the reference's
+ * own C++ signatures (Advection::advect_1D_x(Config*, const RealView4D&, ...)).
+ *
+ * Conventions
+ * - The distribution function f is a caller-owned DEVICE buffer of
+ *   nx*ny*nvx*nvy elements in the reference's layout_left order: element
+ *   (ix, iy, ivx, ivy) sits at ix + nx*(iy + ny*(ivx + nvx*ivy))
+ *   (miniapps/vlp4d/thrust/types.hpp:13,33).  Its element type is fixed per
+ *   context: VLP4D_F64 (double, as the reference) or VLP4D_F32 (float
+ *   storage; displacements, weights' derivation, rho accumulation, the field
+ *   solve and diagnostics stay FP64).
+ * - 2D fields (rho/phi, Ex, Ey) are FP64 nx*ny device arrays owned by the
+ *   context, index ix + nx*iy (miniapps/vlp4d/thrust/efield.hpp:13-16).
+ * - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *   stream).  All calls are stream-ordered and asynchronous unless stated;
+ *   none allocates device memory after vlp4d_ctx_create.
+ * - Every function returns VLP4D_OK (0) or an error code; none exits the
+ *   process (the reference's SafeCudaCall exits, lib/Cuda_Helper.hpp:8-16).
+ *   vlp4d_last_error() gives a message for the calling thread.
+ * - A context is not thread-safe; use one context per host thread/stream.
+ */
+#ifndef VLP4D_B200_H
+#define VLP4D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VLP4D_OK 0
+#define VLP4D_ERR_INVALID_ARG 1
+#define VLP4D_ERR_CUDA 2
+#define VLP4D_ERR_UNSUPPORTED 3
+#define VLP4D_ERR_NO_DEVICE 4
+#define VLP4D_ERR_IO 5
+
+#define VLP4D_F64 0
+#define VLP4D_F32 1
+
+/* Field selectors for vlp4d_field_ptr. */
+#define VLP4D_FIELD_RHO 0 /* rho before field_poisson, phi after it (the
+                             reference's irfft2 writes phi into rho_,
+                             miniapps/vlp4d/thrust/efield.cpp:102) */
+#define VLP4D_FIELD_EX 1
+#define VLP4D_FIELD_EY 2
+
+/* Initial conditions for vlp4d_init_case.  2/5/10/20 are the reference's
+ * testcases (miniapps/vlp4d/thrust/init.cpp:118-285); 110/120 are the
+ * perturbed Maxwellians of the benchmark configurations:
+ *   110: (1 + amp cos(k x) + amp cos(k y)) M(vx) M(vy)
+ *   120: (1 + amp cos(k x) + amp cos(k y)) 0.5[M(vx-u) + M(vx+u)] M(vy)
+ * with M the unit Maxwellian exp(-v^2/2)/sqrt(2 pi). */
+#define VLP4D_IC_CYL02 2
+#define VLP4D_IC_CYL05 5
+#define VLP4D_IC_SLD10 10
+#define VLP4D_IC_TSI20 20
+#define VLP4D_IC_LANDAU_SUM 110
+#define VLP4D_IC_TWO_STREAM 120
+
+/* Mirrors the reference's Domain (miniapps/vlp4d/thrust/config.hpp:8-20);
+ * dx is derived as (max - min) / n (init.cpp:77-79). */
+typedef struct vlp4d_domain {
+  int32_t nxmax[4];   /* nx, ny, nvx, nvy */
+  double min_phy[4];
+  double max_phy[4];
+  double dt;
+  int32_t nbiter;     /* number of steps; the diagnostic history holds nbiter+1 entries */
+  int32_t ifreq;
+  int32_t idcase;     /* field_poisson branch: 2, 6, 10, 20 or other (field.cpp:48-76) */
+  int32_t fxvx;
+} vlp4d_domain;
+
+typedef struct vlp4d_ctx vlp4d_ctx;
+
+/* Parses a reference input deck (values after each ':' in the fixed order of
+ * docs/vlp4d.md:55-86), as import() does (miniapps/vlp4d/thrust/init.cpp:12-82). */
+int vlp4d_read_deck(const char *path, vlp4d_domain *out);
+
+/* Allocates the Efield/Diags equivalents on the current CUDA device:
+ * replaces `new Efield(conf, {nx, ny})` (efield.cpp:5-37, including the
+ * cuFFT plans of lib/Cuda_FFT.hpp:83-159) and `new Diags(conf)`
+ * (diags.cpp:6-11). */
+int vlp4d_ctx_create(const vlp4d_domain *dom, int dtype, vlp4d_ctx **out);
+int vlp4d_ctx_destroy(vlp4d_ctx *ctx);
+const char *vlp4d_last_error(void);
+int vlp4d_ctx_dtype(const vlp4d_ctx *ctx);
+
+/* Device pointer of a context-owned FP64 nx*ny field (VLP4D_FIELD_*). */
+int vlp4d_field_ptr(vlp4d_ctx *ctx, int which, double **dev_ptr);
+
+/* Fills f with an initial condition (initcase, init.cpp:118-141). */
+int vlp4d_init_case(vlp4d_ctx *ctx, void *f, int ic, double amp, double k, double u, void *stream);
+
+/* Advection::advect_1D_x / _y (miniapps/vlp4d/thrust/advection.hpp:336-360):
+ * 1D Lagrange-5 shift along x by dt*vx, along y by dt*vy.  fn and fnp1 must
+ * not overlap. */
+int vlp4d_advect_x(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream);
+int vlp4d_advect_y(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream);
+/* Advection::advect_1D_vx / _vy (advection.hpp:362-386): shift along vx by
+ * dt*Ex(x,y), along vy by dt*Ey(x,y), reading the context's Ex/Ey. */
+int vlp4d_advect_vx(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream);
+int vlp4d_advect_vy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream);
+
+/* Fused pairs of the Strang sequence (timestep.hpp:17-28 and :43-58):
+ * advect_1D_x then advect_1D_y in one pass, and advect_1D_vx then
+ * advect_1D_vy in one pass.  Equal to the 1D sequence up to FP rounding. */
+int vlp4d_advect_xy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream);
+int vlp4d_advect_vxvy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream);
+
+/* field_rho (miniapps/vlp4d/thrust/field.cpp:6-32): rho = dvx*dvy*sum_v f. */
+int vlp4d_field_rho(vlp4d_ctx *ctx, const void *fn, void *stream);
+/* field_poisson (field.cpp:34-82 -> efield.cpp:43-105): rho -= 1 for cases
+ * 10/20, FP64 2D FFT solve; rho then holds phi. */
+int vlp4d_field_poisson(vlp4d_ctx *ctx, void *stream);
+/* Diags::compute (diags.cpp:13-55) for iteration `iter` (0..nbiter): energy
+ * log(sqrt(sum|E|^2 dx dy)) and mass sum(rho)*dx*dy, kept on the device. */
+int vlp4d_diags_compute(vlp4d_ctx *ctx, int iter, void *stream);
+/* Synchronous read of the diagnostic history entries [0, count). */
+int vlp4d_diags_read(vlp4d_ctx *ctx, double *nrj, double *mass, int count);
+/* Diags::save (diags.cpp:57-68): "t nrj mass" per iteration into `path`. */
+int vlp4d_diags_save(vlp4d_ctx *ctx, const char *path);
+
+/* onetimestep (miniapps/vlp4d/thrust/timestep.hpp:14-67) as three fused
+ * passes: x/y half step with the rho moment in its epilogue, the field solve
+ * and diagnostic `iter`, the vx/vy full step, the x/y half step.  fn holds
+ * the state before and after; fnp1 is scratch of the same size. */
+int vlp4d_step(vlp4d_ctx *ctx, void *fn, void *fnp1, int iter, void *stream);
+
+/* The time loop of main() (miniapps/vlp4d/thrust/vlp4d.cpp:55-73) with host
+ * buffers: copies f0 (host, nx*ny*nvx*nvy elements of the context's dtype)
+ * into fn, runs the initial field solve + diagnostic 0 and `nsteps` steps,
+ * copies the final f back into f_out (host; may be NULL) and the
+ * diagnostic history into nrj/mass (host, nsteps+1 entries each; may be
+ * NULL).  Synchronous. */
+int vlp4d_run(vlp4d_ctx *ctx, const void *f0_host, void *f_out_host, int nsteps, double *nrj,
+              double *mass, void *fn, void *fnp1, void *stream);
+
+/* Advection::print_fxvx (advection.hpp:388-411): the (x, vx) slice at iy=0,
+ * ivy=nvy/2 as CSV into `path`.  Synchronous. */
+int vlp4d_print_fxvx(vlp4d_ctx *ctx, const void *fn, const char *path);
+
+/* Impl::Transpose::forward/backward (lib/Cuda_Transpose.hpp:38-46):
+ * out-of-place transpose of a (rows x cols) column-major matrix of
+ * elements of `elem_size` bytes (4, 8 or 16). */
+int vlp4d_transpose(const void *in, void *out, int rows, int cols, int elem_size, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VLP4D_B200_H */

@@ -1,0 +1,274 @@
+// Advection kernels of the vlp4d step: stencil tables and the generic
+// (any-shape) sweeps.  The bandwidth-optimised plane and v-slab kernels live
+// in advect_plane.cu and advect_vslab.cu and fall back to these when a shape
+// is outside what they support.
+//
+// Reference: miniapps/vlp4d/thrust/advection.hpp:77-386 (four functors run
+// by kernel_for_each_left over (ix, iy, ivx) with a serial ivy loop,
+// lib/thrust/Cuda_Parallel_For.hpp:37-45).
+#include <vector>
+
+#include "internal.cuh"
+
+namespace vlp4d {
+
+namespace {
+
+// FP32 copy of a line's weights: the five smallest are rounded, the largest
+// is set so that the six FP32 weights sum to 1 as closely as FP32 allows.
+// Constants are then advected without a per-line gain, which would otherwise
+// accumulate coherently over the steps of a run.
+__host__ __device__ inline void weights_to_f32(const double w[6], float wf[6]) {
+  int kmax = 0;
+  for (int k = 1; k < 6; ++k)
+    if (fabs(w[k]) > fabs(w[kmax])) kmax = k;
+  double s = 0.0;
+  for (int k = 0; k < 6; ++k) {
+    if (k == kmax) continue;
+    wf[k] = (float)w[k];
+    s += (double)wf[k];
+  }
+  wf[kmax] = (float)(1.0 - s);
+}
+
+// One v-line per (ix, iy): displacement dt*E(ix, iy) (advection.hpp:243, 306).
+__global__ void k_build_vtable(const double *__restrict__ e, int lines, double dt, double hmin, double hmax,
+                               int n, int *__restrict__ m, double *__restrict__ w, float *__restrict__ wf) {
+  const int line = blockIdx.x * blockDim.x + threadIdx.x;
+  if (line >= lines) return;
+  const LineStencil s = line_stencil(__dmul_rn(dt, e[line]), hmin, hmax, n);
+  m[line] = s.m;
+  float f[6];
+  weights_to_f32(s.w, f);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    w[6 * line + k] = s.w[k];
+    wf[6 * line + k] = f[k];
+  }
+}
+
+template <typename T>
+struct Weights;
+template <>
+struct Weights<double> {
+  static __device__ __forceinline__ const double *get(const StencilTable &t) { return t.w; }
+};
+template <>
+struct Weights<float> {
+  static __device__ __forceinline__ const float *get(const StencilTable &t) { return t.wf; }
+};
+
+// Generic 1D sweep along dimension DIM: one thread per output cell, taps
+// gathered through L1/L2.  Any extents (including n < 6, where the stencil
+// wraps more than once).
+template <typename T, int DIM>
+__global__ void k_advect_generic(const T *__restrict__ fn, T *__restrict__ fnp1, int nx, int ny, int nvx,
+                                 int nvy, StencilTable tab) {
+  const long long nxy = (long long)nx * ny;
+  const long long total = nxy * nvx * nvy;
+  const T *__restrict__ w = Weights<T>::get(tab);
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(idx % nx);
+    long long r = idx / nx;
+    const int iy = (int)(r % ny);
+    r /= ny;
+    const int ivx = (int)(r % nvx);
+    const int ivy = (int)(r / nvx);
+    int line, n, i;
+    long long stride;
+    if (DIM == 0) { line = ivx; n = nx; i = ix; stride = 1; }
+    else if (DIM == 1) { line = ivy; n = ny; i = iy; stride = nx; }
+    else if (DIM == 2) { line = ix + nx * iy; n = nvx; i = ivx; stride = nxy; }
+    else { line = ix + nx * iy; n = nvy; i = ivy; stride = nxy * nvx; }
+    const long long base = idx - (long long)i * stride;
+    int j = i + tab.m[line];
+    if (j >= n) j -= n;
+    T acc = T(0);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      acc = fma(w[6 * line + k], fn[base + (long long)j * stride], acc);
+      if (++j == n) j = 0;
+    }
+    fnp1[idx] = acc;
+  }
+}
+
+// Generic fused pair: the tensor product of two 1D stencils (x then y, or
+// vx then vy).  out = sum_j wb_j * (sum_k wa_k * f[a+k, b+j]); the inner sum
+// is the first sweep, evaluated for the six rows the second sweep needs.
+template <typename T, bool V>
+__global__ void k_advect_pair_generic(const T *__restrict__ fn, T *__restrict__ fnp1, int nx, int ny, int nvx,
+                                      int nvy, StencilTable ta, StencilTable tb) {
+  const long long nxy = (long long)nx * ny;
+  const long long total = nxy * nvx * nvy;
+  const T *__restrict__ wa = Weights<T>::get(ta);
+  const T *__restrict__ wb = Weights<T>::get(tb);
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(idx % nx);
+    long long r = idx / nx;
+    const int iy = (int)(r % ny);
+    r /= ny;
+    const int ivx = (int)(r % nvx);
+    const int ivy = (int)(r / nvx);
+    int la, lb, na, nb, ia, ib;
+    long long sa, sb;
+    if (!V) { la = ivx; lb = ivy; na = nx; nb = ny; ia = ix; ib = iy; sa = 1; sb = nx; }
+    else { la = lb = ix + nx * iy; na = nvx; nb = nvy; ia = ivx; ib = ivy; sa = nxy; sb = nxy * nvx; }
+    const long long base = idx - (long long)ia * sa - (long long)ib * sb;
+    int jb = ib + tb.m[lb];
+    if (jb >= nb) jb -= nb;
+    const int ja0 = (ia + ta.m[la]) >= na ? ia + ta.m[la] - na : ia + ta.m[la];
+    T out = T(0);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      int ja = ja0;
+      T acc = T(0);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        acc = fma(wa[6 * la + k], fn[base + (long long)ja * sa + (long long)jb * sb], acc);
+        if (++ja == na) ja = 0;
+      }
+      out = fma(wb[6 * lb + q], acc, out);
+      if (++jb == nb) jb = 0;
+    }
+    fnp1[idx] = out;
+  }
+}
+
+int alloc_table(StencilTable &t, int lines) {
+  if (t.m && t.lines >= lines) return VLP4D_OK;
+  cudaFree(t.m);
+  cudaFree(t.w);
+  cudaFree(t.wf);
+  t.m = nullptr; t.w = nullptr; t.wf = nullptr;
+  VLP4D_CUDA_TRY(cudaMalloc(&t.m, sizeof(int) * lines));
+  VLP4D_CUDA_TRY(cudaMalloc(&t.w, sizeof(double) * 6 * lines));
+  VLP4D_CUDA_TRY(cudaMalloc(&t.wf, sizeof(float) * 6 * lines));
+  t.lines = lines;
+  t.valid = false;
+  return VLP4D_OK;
+}
+
+int grid_for(long long total, int threads, int sms) {
+  long long blocks = (total + threads - 1) / threads;
+  const long long cap = (long long)sms * 16;
+  return (int)(blocks < cap ? blocks : cap);
+}
+
+}  // namespace
+
+// x lines (dim 0) are indexed by ivx with displacement dt*vx; y lines
+// (dim 1) by ivy with dt*vy (advection.hpp:113-115, 178-181).  Built on the
+// host with the same non-contracted FP64 arithmetic as the device code and
+// uploaded; two slots per dimension cache dt/2 and dt of a Strang step.
+int ensure_xy_table(vlp4d_ctx *c, int dim, double dt, StencilTable **out, cudaStream_t s) {
+  StencilTable *slots = dim == 0 ? c->tab_x : c->tab_y;
+  for (int i = 0; i < 2; ++i)
+    if (slots[i].valid && slots[i].dt == dt) {
+      slots[i].stamp = ++c->table_clock;
+      *out = &slots[i];
+      return VLP4D_OK;
+    }
+  // Replace an empty slot, else the least recently used one.
+  int pick = !slots[0].valid ? 0 : (!slots[1].valid ? 1 : (slots[0].stamp <= slots[1].stamp ? 0 : 1));
+  StencilTable *t = &slots[pick];
+  t->valid = false;
+  const int vdim = dim == 0 ? 2 : 3;
+  const int lines = c->g.n[vdim];
+  int rc = alloc_table(*t, lines);
+  if (rc) return rc;
+  std::vector<int> hm(lines);
+  std::vector<double> hw(6 * (size_t)lines);
+  std::vector<float> hwf(6 * (size_t)lines);
+  for (int l = 0; l < lines; ++l) {
+    const double v = c->g.minp[vdim] + l * c->g.dx[vdim];
+    const double disp = dt * v;
+    const LineStencil st = line_stencil(disp, c->g.minp[dim], c->g.maxp[dim], c->g.n[dim]);
+    hm[l] = st.m;
+    float f[6];
+    weights_to_f32(st.w, f);
+    for (int k = 0; k < 6; ++k) {
+      hw[6 * l + k] = st.w[k];
+      hwf[6 * l + k] = f[k];
+    }
+  }
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(t->m, hm.data(), sizeof(int) * lines, cudaMemcpyHostToDevice, s));
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(t->w, hw.data(), sizeof(double) * 6 * lines, cudaMemcpyHostToDevice, s));
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(t->wf, hwf.data(), sizeof(float) * 6 * lines, cudaMemcpyHostToDevice, s));
+  // The host vectors die at return; make sure the copies have consumed them.
+  VLP4D_CUDA_TRY(cudaStreamSynchronize(s));
+  t->dt = dt;
+  t->valid = true;
+  t->stamp = ++c->table_clock;
+  *out = t;
+  return VLP4D_OK;
+}
+
+int build_v_tables(vlp4d_ctx *c, double dt, bool vx, bool vy, cudaStream_t s) {
+  const int lines = (int)c->g.nxy();
+  const int threads = 256, blocks = (lines + threads - 1) / threads;
+  if (vx) {
+    int rc = alloc_table(c->tab_vx, lines);
+    if (rc) return rc;
+    k_build_vtable<<<blocks, threads, 0, s>>>(c->ex, lines, dt, c->g.minp[2], c->g.maxp[2], c->g.n[2],
+                                               c->tab_vx.m, c->tab_vx.w, c->tab_vx.wf);
+    VLP4D_LAUNCH_CHECK();
+    c->tab_vx.valid = true;
+  }
+  if (vy) {
+    int rc = alloc_table(c->tab_vy, lines);
+    if (rc) return rc;
+    k_build_vtable<<<blocks, threads, 0, s>>>(c->ey, lines, dt, c->g.minp[3], c->g.maxp[3], c->g.n[3],
+                                               c->tab_vy.m, c->tab_vy.w, c->tab_vy.wf);
+    VLP4D_LAUNCH_CHECK();
+    c->tab_vy.valid = true;
+  }
+  return VLP4D_OK;
+}
+
+int launch_advect_generic(vlp4d_ctx *c, int dim, const void *fn, void *fnp1, const StencilTable *t,
+                          cudaStream_t s) {
+  const int threads = 256;
+  const int blocks = grid_for(c->g.cells(), threads, c->num_sms);
+  const int *n = c->g.n;
+#define VLP4D_GEN(T, D)                                                                              \
+  k_advect_generic<T, D><<<blocks, threads, 0, s>>>((const T *)fn, (T *)fnp1, n[0], n[1], n[2], n[3], *t)
+  if (c->dtype == VLP4D_F64) {
+    switch (dim) {
+      case 0: VLP4D_GEN(double, 0); break;
+      case 1: VLP4D_GEN(double, 1); break;
+      case 2: VLP4D_GEN(double, 2); break;
+      default: VLP4D_GEN(double, 3); break;
+    }
+  } else {
+    switch (dim) {
+      case 0: VLP4D_GEN(float, 0); break;
+      case 1: VLP4D_GEN(float, 1); break;
+      case 2: VLP4D_GEN(float, 2); break;
+      default: VLP4D_GEN(float, 3); break;
+    }
+  }
+#undef VLP4D_GEN
+  VLP4D_LAUNCH_CHECK();
+  return VLP4D_OK;
+}
+
+int launch_advect_pair_generic(vlp4d_ctx *c, bool v, const void *fn, void *fnp1, const StencilTable *ta,
+                               const StencilTable *tb, cudaStream_t s) {
+  const int threads = 256;
+  const int blocks = grid_for(c->g.cells(), threads, c->num_sms);
+  const int *n = c->g.n;
+  if (c->dtype == VLP4D_F64) {
+    if (v) k_advect_pair_generic<double, true><<<blocks, threads, 0, s>>>((const double *)fn, (double *)fnp1, n[0], n[1], n[2], n[3], *ta, *tb);
+    else k_advect_pair_generic<double, false><<<blocks, threads, 0, s>>>((const double *)fn, (double *)fnp1, n[0], n[1], n[2], n[3], *ta, *tb);
+  } else {
+    if (v) k_advect_pair_generic<float, true><<<blocks, threads, 0, s>>>((const float *)fn, (float *)fnp1, n[0], n[1], n[2], n[3], *ta, *tb);
+    else k_advect_pair_generic<float, false><<<blocks, threads, 0, s>>>((const float *)fn, (float *)fnp1, n[0], n[1], n[2], n[3], *ta, *tb);
+  }
+  VLP4D_LAUNCH_CHECK();
+  return VLP4D_OK;
+}
+
+}  // namespace vlp4d

@@ -1,0 +1,441 @@
+// The extern "C" entry points of libvlp4d_b200 (include/vlp4d_b200.h).
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <utility>
+
+#include "internal.cuh"
+
+namespace vlp4d {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+namespace {
+
+int fail(int code, const std::string &msg) {
+  set_error(msg);
+  return code;
+}
+
+bool finite(double v) { return std::isfinite(v); }
+
+int validate_domain(const vlp4d_domain *d) {
+  if (!d) return fail(VLP4D_ERR_INVALID_ARG, "domain is NULL");
+  long long cells = 1;
+  for (int i = 0; i < 4; ++i) {
+    if (d->nxmax[i] < 1) return fail(VLP4D_ERR_INVALID_ARG, "nxmax[" + std::to_string(i) + "] < 1");
+    if (!finite(d->min_phy[i]) || !finite(d->max_phy[i]) || !(d->max_phy[i] > d->min_phy[i]))
+      return fail(VLP4D_ERR_INVALID_ARG, "max_phy[" + std::to_string(i) + "] must exceed min_phy");
+    cells *= d->nxmax[i];
+    if (cells > (1LL << 40)) return fail(VLP4D_ERR_INVALID_ARG, "grid too large");
+  }
+  if ((long long)d->nxmax[0] * d->nxmax[1] >= (1LL << 31))
+    return fail(VLP4D_ERR_INVALID_ARG, "nx*ny must be below 2^31");
+  if (!finite(d->dt)) return fail(VLP4D_ERR_INVALID_ARG, "dt is not finite");
+  if (d->nbiter < 0) return fail(VLP4D_ERR_INVALID_ARG, "nbiter < 0");
+  return VLP4D_OK;
+}
+
+cudaStream_t as_stream(void *s) { return (cudaStream_t)s; }
+
+int check_ctx(const vlp4d_ctx *c) {
+  if (!c) return fail(VLP4D_ERR_INVALID_ARG, "context is NULL");
+  return VLP4D_OK;
+}
+
+int check_pair(const void *a, const void *b) {
+  if (!a || !b) return fail(VLP4D_ERR_INVALID_ARG, "f buffer is NULL");
+  if (a == b) return fail(VLP4D_ERR_INVALID_ARG, "fn and fnp1 must be different buffers");
+  return VLP4D_OK;
+}
+
+void free_ctx(vlp4d_ctx *c) {
+  if (!c) return;
+  if (c->plans) {
+    cufftDestroy(c->plan_fwd);
+    cufftDestroy(c->plan_bwd);
+  }
+  cudaFree(c->rho);
+  cudaFree(c->ex);
+  cudaFree(c->ey);
+  cudaFree(c->rho_hat);
+  cudaFree(c->ex_hat);
+  cudaFree(c->ey_hat);
+  cudaFree(c->nrj);
+  cudaFree(c->mass);
+  cudaFree(c->rho_part);
+  for (StencilTable *t : {&c->tab_x[0], &c->tab_x[1], &c->tab_y[0], &c->tab_y[1], &c->tab_vx, &c->tab_vy}) {
+    cudaFree(t->m);
+    cudaFree(t->w);
+    cudaFree(t->wf);
+  }
+  if (c->h_diag) cudaFreeHost(c->h_diag);
+  delete c;
+}
+
+// Skips to the next ':' as the reference's import() does (init.cpp:35-38),
+// returning false at end of file instead of looping forever.
+bool skip_to_colon(FILE *f) {
+  int ch;
+  do {
+    ch = fgetc(f);
+    if (ch == EOF) return false;
+  } while (ch != ':');
+  return true;
+}
+
+}  // namespace
+}  // namespace vlp4d
+
+using namespace vlp4d;
+
+extern "C" {
+
+const char *vlp4d_last_error(void) { return g_last_error.c_str(); }
+
+int vlp4d_read_deck(const char *path, vlp4d_domain *out) {
+  if (!path || !out) return fail(VLP4D_ERR_INVALID_ARG, "NULL argument");
+  FILE *f = fopen(path, "r");
+  if (!f) return fail(VLP4D_ERR_IO, std::string("cannot open deck ") + path);
+  vlp4d_domain d;
+  memset(&d, 0, sizeof(d));
+  bool ok = true;
+  for (int i = 0; i < 4 && ok; ++i) ok = skip_to_colon(f) && fscanf(f, " %d\n", &d.nxmax[i]) == 1;
+  for (int i = 0; i < 4 && ok; ++i) {
+    ok = skip_to_colon(f) && fscanf(f, " %le\n", &d.min_phy[i]) == 1;
+    ok = ok && skip_to_colon(f) && fscanf(f, " %le\n", &d.max_phy[i]) == 1;
+  }
+  char idcase[8] = {0};
+  ok = ok && skip_to_colon(f) && fgets(idcase, 7, f) != nullptr;
+  ok = ok && skip_to_colon(f) && fscanf(f, " %le\n", &d.dt) == 1;
+  ok = ok && skip_to_colon(f) && fscanf(f, " %d\n", &d.nbiter) == 1;
+  ok = ok && skip_to_colon(f) && fscanf(f, " %d\n", &d.ifreq) == 1;
+  ok = ok && skip_to_colon(f) && fscanf(f, " %d\n", &d.fxvx) == 1;
+  fclose(f);
+  if (!ok) return fail(VLP4D_ERR_IO, std::string("malformed deck ") + path);
+  d.idcase = atoi(idcase);
+  *out = d;
+  return VLP4D_OK;
+}
+
+int vlp4d_ctx_create(const vlp4d_domain *dom, int dtype, vlp4d_ctx **out) {
+  if (!out) return fail(VLP4D_ERR_INVALID_ARG, "out is NULL");
+  *out = nullptr;
+  int rc = validate_domain(dom);
+  if (rc) return rc;
+  if (dtype != VLP4D_F64 && dtype != VLP4D_F32) return fail(VLP4D_ERR_INVALID_ARG, "dtype must be F64 or F32");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+    cudaGetLastError();
+    return fail(VLP4D_ERR_NO_DEVICE, "no CUDA device");
+  }
+  vlp4d_ctx *c = new vlp4d_ctx();
+  c->dom = *dom;
+  c->dtype = dtype;
+  c->elem = dtype == VLP4D_F64 ? sizeof(double) : sizeof(float);
+  for (int i = 0; i < 4; ++i) {
+    c->g.n[i] = dom->nxmax[i];
+    c->g.minp[i] = dom->min_phy[i];
+    c->g.maxp[i] = dom->max_phy[i];
+    c->g.dx[i] = (dom->max_phy[i] - dom->min_phy[i]) / dom->nxmax[i];  // init.cpp:77-79
+  }
+  auto bail = [&](int code) {
+    free_ctx(c);
+    return code;
+  };
+  if (cudaGetDevice(&c->device) != cudaSuccess) return bail(fail(VLP4D_ERR_CUDA, "cudaGetDevice failed"));
+  if (cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess)
+    return bail(fail(VLP4D_ERR_CUDA, "cudaDeviceGetAttribute failed"));
+  const long long nxy = c->g.nxy();
+  const int nx1h = c->g.n[0] / 2 + 1;
+  const size_t nh = (size_t)nx1h * c->g.n[1];
+#define CTX_ALLOC(ptr, bytes)                                                                \
+  do {                                                                                       \
+    cudaError_t e_ = cudaMalloc(&(ptr), (bytes));                                            \
+    if (e_ != cudaSuccess) return bail(fail(VLP4D_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e_))); \
+  } while (0)
+  CTX_ALLOC(c->rho, sizeof(double) * nxy);
+  CTX_ALLOC(c->ex, sizeof(double) * nxy);
+  CTX_ALLOC(c->ey, sizeof(double) * nxy);
+  CTX_ALLOC(c->rho_hat, sizeof(cufftDoubleComplex) * nh);
+  CTX_ALLOC(c->ex_hat, sizeof(cufftDoubleComplex) * nh);
+  CTX_ALLOC(c->ey_hat, sizeof(cufftDoubleComplex) * nh);
+  c->hist_len = dom->nbiter + 1;
+  CTX_ALLOC(c->nrj, sizeof(double) * c->hist_len);
+  CTX_ALLOC(c->mass, sizeof(double) * c->hist_len);
+  // Enough (column block, plane group) blocks to fill the GPU a few times.
+  long long groups = ((long long)c->num_sms * 8 * 256 + nxy - 1) / nxy;
+  if (groups > c->g.nv()) groups = c->g.nv();
+  if (groups > 1024) groups = 1024;
+  if (groups < 1) groups = 1;
+  c->rho_groups = (int)groups;
+  CTX_ALLOC(c->rho_part, sizeof(double) * nxy * (size_t)c->rho_groups);
+#undef CTX_ALLOC
+  if (cudaMemset(c->rho, 0, sizeof(double) * nxy) != cudaSuccess ||
+      cudaMemset(c->ex, 0, sizeof(double) * nxy) != cudaSuccess ||
+      cudaMemset(c->ey, 0, sizeof(double) * nxy) != cudaSuccess ||
+      cudaMemset(c->nrj, 0, sizeof(double) * c->hist_len) != cudaSuccess ||
+      cudaMemset(c->mass, 0, sizeof(double) * c->hist_len) != cudaSuccess)
+    return bail(fail(VLP4D_ERR_CUDA, "cudaMemset failed"));
+  // lib/Cuda_FFT.hpp:108-114: cufftPlan2d(nx2 = ny, nx1 = nx) on x-fastest data.
+  if (cufftPlan2d(&c->plan_fwd, c->g.n[1], c->g.n[0], CUFFT_D2Z) != CUFFT_SUCCESS)
+    return bail(fail(VLP4D_ERR_CUDA, "cufftPlan2d D2Z failed"));
+  if (cufftPlan2d(&c->plan_bwd, c->g.n[1], c->g.n[0], CUFFT_Z2D) != CUFFT_SUCCESS) {
+    cufftDestroy(c->plan_fwd);
+    return bail(fail(VLP4D_ERR_CUDA, "cufftPlan2d Z2D failed"));
+  }
+  c->plans = true;
+  if (cudaMallocHost(&c->h_diag, sizeof(double) * 2 * c->hist_len) != cudaSuccess)
+    return bail(fail(VLP4D_ERR_CUDA, "cudaMallocHost failed"));
+  *out = c;
+  return VLP4D_OK;
+}
+
+int vlp4d_ctx_destroy(vlp4d_ctx *ctx) {
+  if (!ctx) return VLP4D_OK;
+  free_ctx(ctx);
+  return VLP4D_OK;
+}
+
+int vlp4d_ctx_dtype(const vlp4d_ctx *ctx) { return ctx ? ctx->dtype : -1; }
+
+int vlp4d_field_ptr(vlp4d_ctx *ctx, int which, double **dev_ptr) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (!dev_ptr) return fail(VLP4D_ERR_INVALID_ARG, "dev_ptr is NULL");
+  switch (which) {
+    case VLP4D_FIELD_RHO: *dev_ptr = ctx->rho; break;
+    case VLP4D_FIELD_EX: *dev_ptr = ctx->ex; break;
+    case VLP4D_FIELD_EY: *dev_ptr = ctx->ey; break;
+    default: return fail(VLP4D_ERR_INVALID_ARG, "unknown field");
+  }
+  return VLP4D_OK;
+}
+
+int vlp4d_init_case(vlp4d_ctx *ctx, void *f, int ic, double amp, double k, double u, void *stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (!f) return fail(VLP4D_ERR_INVALID_ARG, "f is NULL");
+  switch (ic) {
+    case VLP4D_IC_CYL02: case VLP4D_IC_CYL05: case VLP4D_IC_SLD10: case VLP4D_IC_TSI20:
+    case VLP4D_IC_LANDAU_SUM: case VLP4D_IC_TWO_STREAM: break;
+    default: return fail(VLP4D_ERR_INVALID_ARG, "unknown initial condition");  // init.cpp:135-138 aborts
+  }
+  return launch_init_case(ctx, f, ic, amp, k, u, as_stream(stream));
+}
+
+static int advect_1d(vlp4d_ctx *ctx, int dim, const void *fn, void *fnp1, double dt, void *stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if ((rc = check_pair(fn, fnp1))) return rc;
+  if (!std::isfinite(dt)) return fail(VLP4D_ERR_INVALID_ARG, "dt is not finite");
+  cudaStream_t s = as_stream(stream);
+  StencilTable *t = nullptr;
+  if (dim < 2) {
+    if ((rc = ensure_xy_table(ctx, dim, dt, &t, s))) return rc;
+    if (xy_fused_supported(ctx))
+      return launch_advect_xy(ctx, fn, fnp1, dim == 0 ? t : nullptr, dim == 1 ? t : nullptr, dim == 0, dim == 1,
+                              false, s);
+    return launch_advect_generic(ctx, dim, fn, fnp1, t, s);
+  }
+  if ((rc = build_v_tables(ctx, dt, dim == 2, dim == 3, s))) return rc;
+  if (vv_fused_supported(ctx)) return launch_advect_vxvy(ctx, fn, fnp1, dim == 2, dim == 3, s);
+  return launch_advect_generic(ctx, dim, fn, fnp1, dim == 2 ? &ctx->tab_vx : &ctx->tab_vy, s);
+}
+
+int vlp4d_advect_x(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream) {
+  return advect_1d(ctx, 0, fn, fnp1, dt, stream);
+}
+int vlp4d_advect_y(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream) {
+  return advect_1d(ctx, 1, fn, fnp1, dt, stream);
+}
+int vlp4d_advect_vx(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream) {
+  return advect_1d(ctx, 2, fn, fnp1, dt, stream);
+}
+int vlp4d_advect_vy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream) {
+  return advect_1d(ctx, 3, fn, fnp1, dt, stream);
+}
+
+static int advect_xy_impl(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, bool with_rho, cudaStream_t s) {
+  StencilTable *tx = nullptr, *ty = nullptr;
+  int rc;
+  if ((rc = ensure_xy_table(ctx, 0, dt, &tx, s))) return rc;
+  if ((rc = ensure_xy_table(ctx, 1, dt, &ty, s))) return rc;
+  if (xy_fused_supported(ctx)) return launch_advect_xy(ctx, fn, fnp1, tx, ty, true, true, with_rho, s);
+  if ((rc = launch_advect_pair_generic(ctx, false, fn, fnp1, tx, ty, s))) return rc;
+  return with_rho ? launch_field_rho(ctx, fnp1, s) : VLP4D_OK;
+}
+
+static int advect_vxvy_impl(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, cudaStream_t s) {
+  int rc;
+  if ((rc = build_v_tables(ctx, dt, true, true, s))) return rc;
+  if (vv_fused_supported(ctx)) return launch_advect_vxvy(ctx, fn, fnp1, true, true, s);
+  return launch_advect_pair_generic(ctx, true, fn, fnp1, &ctx->tab_vx, &ctx->tab_vy, s);
+}
+
+int vlp4d_advect_xy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if ((rc = check_pair(fn, fnp1))) return rc;
+  if (!std::isfinite(dt)) return fail(VLP4D_ERR_INVALID_ARG, "dt is not finite");
+  return advect_xy_impl(ctx, fn, fnp1, dt, false, as_stream(stream));
+}
+
+int vlp4d_advect_vxvy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if ((rc = check_pair(fn, fnp1))) return rc;
+  if (!std::isfinite(dt)) return fail(VLP4D_ERR_INVALID_ARG, "dt is not finite");
+  return advect_vxvy_impl(ctx, fn, fnp1, dt, as_stream(stream));
+}
+
+int vlp4d_field_rho(vlp4d_ctx *ctx, const void *fn, void *stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (!fn) return fail(VLP4D_ERR_INVALID_ARG, "fn is NULL");
+  return launch_field_rho(ctx, fn, as_stream(stream));
+}
+
+int vlp4d_field_poisson(vlp4d_ctx *ctx, void *stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  return launch_field_poisson(ctx, as_stream(stream));
+}
+
+int vlp4d_diags_compute(vlp4d_ctx *ctx, int iter, void *stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  // diags.cpp:17 asserts 0 <= iter <= nbiter.
+  if (iter < 0 || iter >= ctx->hist_len) return fail(VLP4D_ERR_INVALID_ARG, "iter outside [0, nbiter]");
+  return launch_diags(ctx, iter, as_stream(stream));
+}
+
+int vlp4d_diags_read(vlp4d_ctx *ctx, double *nrj, double *mass, int count) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (count < 0 || count > ctx->hist_len) return fail(VLP4D_ERR_INVALID_ARG, "count outside [0, nbiter+1]");
+  VLP4D_CUDA_TRY(cudaDeviceSynchronize());
+  if (nrj) VLP4D_CUDA_TRY(cudaMemcpy(nrj, ctx->nrj, sizeof(double) * count, cudaMemcpyDeviceToHost));
+  if (mass) VLP4D_CUDA_TRY(cudaMemcpy(mass, ctx->mass, sizeof(double) * count, cudaMemcpyDeviceToHost));
+  return VLP4D_OK;
+}
+
+int vlp4d_diags_save(vlp4d_ctx *ctx, const char *path) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (!path) return fail(VLP4D_ERR_INVALID_ARG, "path is NULL");
+  const int n = ctx->hist_len;
+  double *buf = (double *)malloc(sizeof(double) * 2 * n);
+  if ((rc = vlp4d_diags_read(ctx, buf, buf + n, n))) {
+    free(buf);
+    return rc;
+  }
+  FILE *f = fopen(path, "w");
+  if (!f) {
+    free(buf);
+    return fail(VLP4D_ERR_IO, std::string("cannot write ") + path);
+  }
+  for (int it = 0; it < n; ++it)  // diags.cpp:64-65
+    fprintf(f, "%17.13e %17.13e %17.13e\n", it * ctx->dom.dt, buf[it], buf[n + it]);
+  fclose(f);
+  free(buf);
+  return VLP4D_OK;
+}
+
+int vlp4d_step(vlp4d_ctx *ctx, void *f_state, void *f_next, int iter, void *stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if ((rc = check_pair(f_state, f_next))) return rc;
+  if (iter < 0 || iter >= ctx->hist_len) return fail(VLP4D_ERR_INVALID_ARG, "iter outside [0, nbiter]");
+  cudaStream_t s = as_stream(stream);
+  const double dt = ctx->dom.dt;
+  // timestep.hpp:17-28: x(dt/2), y(dt/2) and the moment of the result.
+  if ((rc = advect_xy_impl(ctx, f_state, f_next, 0.5 * dt, true, s))) return rc;
+  // timestep.hpp:30-38: field solve and the mid-step diagnostic.
+  if ((rc = launch_field_poisson(ctx, s))) return rc;
+  if ((rc = launch_diags(ctx, iter, s))) return rc;
+  // timestep.hpp:40-48: vx(dt), vy(dt).
+  if ((rc = advect_vxvy_impl(ctx, f_next, f_state, dt, s))) return rc;
+  // timestep.hpp:50-58: x(dt/2), y(dt/2).
+  return advect_xy_impl(ctx, f_state, f_next, 0.5 * dt, false, s);
+}
+
+int vlp4d_run(vlp4d_ctx *ctx, const void *f0_host, void *f_out_host, int nsteps, double *nrj, double *mass,
+              void *fn, void *fnp1, void *stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if ((rc = check_pair(fn, fnp1))) return rc;
+  if (!f0_host) return fail(VLP4D_ERR_INVALID_ARG, "f0_host is NULL");
+  if (nsteps < 0 || nsteps >= ctx->hist_len) return fail(VLP4D_ERR_INVALID_ARG, "nsteps outside [0, nbiter]");
+  cudaStream_t s = as_stream(stream);
+  const size_t bytes = (size_t)ctx->g.cells() * ctx->elem;
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(fn, f0_host, bytes, cudaMemcpyHostToDevice, s));
+  // vlp4d.cpp:58-61: initial moment, field and diagnostic 0.
+  if ((rc = launch_field_rho(ctx, fn, s))) return rc;
+  if ((rc = launch_field_poisson(ctx, s))) return rc;
+  if ((rc = launch_diags(ctx, 0, s))) return rc;
+  void *cur = fn, *nxt = fnp1;
+  for (int it = 1; it <= nsteps; ++it) {
+    if ((rc = vlp4d_step(ctx, cur, nxt, it, stream))) return rc;
+    std::swap(cur, nxt);
+  }
+  if (nrj || mass) {
+    VLP4D_CUDA_TRY(cudaMemcpyAsync(ctx->h_diag, ctx->nrj, sizeof(double) * (nsteps + 1), cudaMemcpyDeviceToHost, s));
+    VLP4D_CUDA_TRY(cudaMemcpyAsync(ctx->h_diag + ctx->hist_len, ctx->mass, sizeof(double) * (nsteps + 1),
+                                   cudaMemcpyDeviceToHost, s));
+  }
+  if (f_out_host) VLP4D_CUDA_TRY(cudaMemcpyAsync(f_out_host, cur, bytes, cudaMemcpyDeviceToHost, s));
+  VLP4D_CUDA_TRY(cudaStreamSynchronize(s));
+  if (nrj) memcpy(nrj, ctx->h_diag, sizeof(double) * (nsteps + 1));
+  if (mass) memcpy(mass, ctx->h_diag + ctx->hist_len, sizeof(double) * (nsteps + 1));
+  // Leave the final state in fn, as the reference's loop does.
+  if (cur != fn) VLP4D_CUDA_TRY(cudaMemcpyAsync(fn, cur, bytes, cudaMemcpyDeviceToDevice, s));
+  VLP4D_CUDA_TRY(cudaStreamSynchronize(s));
+  return VLP4D_OK;
+}
+
+int vlp4d_print_fxvx(vlp4d_ctx *ctx, const void *fn, const char *path) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (!fn || !path) return fail(VLP4D_ERR_INVALID_ARG, "NULL argument");
+  const int nx = ctx->g.n[0], nvx = ctx->g.n[2];
+  const int ivy = ctx->g.n[3] / 2;  // advection.hpp:394-395
+  const size_t e = ctx->elem;
+  const size_t row_pitch = (size_t)ctx->g.nxy() * e;  // consecutive ivx at iy = 0
+  const char *base = (const char *)fn + (size_t)ivy * nvx * row_pitch;
+  char *h = (char *)malloc((size_t)nx * nvx * e);
+  cudaError_t err = cudaMemcpy2D(h, (size_t)nx * e, base, row_pitch, (size_t)nx * e, nvx, cudaMemcpyDeviceToHost);
+  if (err != cudaSuccess) {
+    free(h);
+    return fail(VLP4D_ERR_CUDA, std::string("cudaMemcpy2D: ") + cudaGetErrorString(err));
+  }
+  FILE *f = fopen(path, "w");
+  if (!f) {
+    free(h);
+    return fail(VLP4D_ERR_IO, std::string("cannot write ") + path);
+  }
+  for (int ivx = 0; ivx < nvx; ++ivx)
+    for (int ix = 0; ix < nx; ++ix) {
+      const size_t i = (size_t)ivx * nx + ix;
+      const double v = ctx->dtype == VLP4D_F64 ? ((const double *)h)[i] : (double)((const float *)h)[i];
+      fprintf(f, ix == nx - 1 ? "%20.13le\n" : "%20.13le, ", v);
+    }
+  fclose(f);
+  free(h);
+  return VLP4D_OK;
+}
+
+int vlp4d_transpose(const void *in, void *out, int rows, int cols, int elem_size, void *stream) {
+  if (!in || !out) return fail(VLP4D_ERR_INVALID_ARG, "NULL buffer");
+  if (rows < 1 || cols < 1) return fail(VLP4D_ERR_INVALID_ARG, "rows and cols must be positive");
+  if (elem_size != 4 && elem_size != 8 && elem_size != 16)
+    return fail(VLP4D_ERR_INVALID_ARG, "elem_size must be 4, 8 or 16");
+  if (in == out) return fail(VLP4D_ERR_INVALID_ARG, "transpose is out of place");
+  return launch_transpose(in, out, rows, cols, elem_size, as_stream(stream));
+}
+
+}  // extern "C"

@@ -1,0 +1,291 @@
+// Velocity moment, FP64 field solve, diagnostics, initial conditions and the
+// 2D transpose of the vlp4d hot path.
+//
+// References: field_rho (miniapps/vlp4d/thrust/field.cpp:6-32),
+// field_poisson (field.cpp:34-82) -> Efield::solve_poisson_fftw
+// (efield.cpp:43-105) on cuFFT plans (lib/Cuda_FFT.hpp:83-183),
+// Diags::compute (diags.cpp:13-55), initcase (init.cpp:118-285),
+// Impl::Transpose (lib/Cuda_Transpose.hpp:18-136).
+#include "internal.cuh"
+
+namespace vlp4d {
+
+namespace {
+
+// ---- field_rho: deterministic two-level sum over the (vx, vy) planes.
+// Stage 1: block (chunk of columns, group of planes) -> partial[group][ixy].
+// Stage 2: rho[ixy] = (sum over groups) * dvx * dvy.
+template <typename T>
+__global__ void k_rho_partial(const T *__restrict__ f, double *__restrict__ part, long long nxy, long long nv,
+                              int groups) {
+  const long long ixy = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int g = blockIdx.y;
+  if (ixy >= nxy) return;
+  const long long v0 = nv * g / groups, v1 = nv * (g + 1) / groups;
+  double s = 0.0;
+  const T *p = f + ixy + v0 * nxy;
+#pragma unroll 8
+  for (long long v = v0; v < v1; ++v, p += nxy) s += (double)__ldg(p);
+  part[(long long)g * nxy + ixy] = s;
+}
+
+__global__ void k_rho_finish(const double *__restrict__ part, double *__restrict__ rho, long long nxy, int groups,
+                             double dvx, double dvy) {
+  const long long ixy = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (ixy >= nxy) return;
+  double s = 0.0;
+  for (int g = 0; g < groups; ++g) s += part[(long long)g * nxy + ixy];
+  rho[ixy] = s * dvx * dvy;  // field.cpp:23 (sum * dvx * dvy)
+}
+
+// ---- field_poisson pieces.
+__global__ void k_rho_minus_one(double *__restrict__ rho, long long n) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) rho[i] -= 1.;
+}
+
+// field.cpp:48-63 (thrust variant): analytic fields of cases 2 and 6.
+__global__ void k_analytic_field(double *__restrict__ ex, double *__restrict__ ey, int nx, int ny, int idcase,
+                                 double minx, double miny, double dx, double dy) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nx * ny) return;
+  const int ix = i % nx, iy = i / nx;
+  if (idcase == 2) {
+    ex[i] = -(minx + ix * dx);
+    ey[i] = 0.;
+  } else {
+    ey[i] = -(miny + iy * dy);
+    ex[i] = 0.;
+  }
+}
+
+// efield.cpp:68-99 with the filter of efield.cpp:27-33: for every (kx, ky)
+//   ex_hat = -i kx/k^2 rho_hat / (nx*ny), ey_hat = -i ky/k^2 rho_hat / (nx*ny),
+//   rho_hat = rho_hat / k^2 / (nx*ny);  ky = 0 uses filter(kx) (0 at kx = 0),
+//   ky takes the negative branch for ix2 >= ny/2+1.
+__global__ void k_poisson_solve(cufftDoubleComplex *__restrict__ rho_hat, cufftDoubleComplex *__restrict__ ex_hat,
+                                cufftDoubleComplex *__restrict__ ey_hat, int nx1h, int nx2, double kx0,
+                                double ky0, double normcoeff) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nx1h * nx2) return;
+  const int ix1 = i % nx1h, ix2 = i / nx1h;
+  const int nx2h = nx2 / 2 + 1;
+  const double kx = ix1 * kx0;
+  const cufftDoubleComplex r = rho_hat[i];
+  cufftDoubleComplex e1, e2, r1;
+  if (ix2 == 0) {
+    const double filt = ix1 == 0 ? 0. : 1. / (kx * kx);
+    e1.x = __dmul_rn(__dmul_rn(__dmul_rn(kx, r.y), filt), normcoeff);
+    e1.y = __dmul_rn(__dmul_rn(__dmul_rn(-kx, r.x), filt), normcoeff);
+    e2.x = 0.;
+    e2.y = 0.;
+    r1.x = __dmul_rn(__dmul_rn(r.x, filt), normcoeff);
+    r1.y = __dmul_rn(__dmul_rn(r.y, filt), normcoeff);
+  } else {
+    const double ky = (ix2 < nx2h ? ix2 : ix2 - nx2) * ky0;
+    const double k2 = __dadd_rn(__dmul_rn(kx, kx), __dmul_rn(ky, ky));
+    const double cx = -(kx / k2), cy = -(ky / k2);
+    e1.x = __dmul_rn(-cx * r.y, normcoeff);
+    e1.y = __dmul_rn(cx * r.x, normcoeff);
+    e2.x = __dmul_rn(-cy * r.y, normcoeff);
+    e2.y = __dmul_rn(cy * r.x, normcoeff);
+    r1.x = __dmul_rn(r.x / k2, normcoeff);
+    r1.y = __dmul_rn(r.y / k2, normcoeff);
+  }
+  ex_hat[i] = e1;
+  ey_hat[i] = e2;
+  rho_hat[i] = r1;
+}
+
+// ---- Diags::compute: Kahan-compensated FP64 sums of rho and |E|^2 in one
+// block, fixed order (deterministic).  diags.cpp:31-52 (OpenMP variant's
+// mass formula sum*dx*dy; the thrust variant's `*= dx + dy` is a typo).
+__device__ __forceinline__ void kahan_add(double &sum, double &c, double x) {
+  const double y = x - c;
+  const double t = sum + y;
+  c = (t - sum) - y;
+  sum = t;
+}
+
+__global__ void k_diags(const double *__restrict__ rho, const double *__restrict__ ex, const double *__restrict__ ey,
+                        long long n, double dx, double dy, double *__restrict__ nrj_hist,
+                        double *__restrict__ mass_hist, int iter) {
+  double sm = 0., cm = 0., se = 0., ce = 0.;
+  for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+    kahan_add(sm, cm, rho[i]);
+    const double a = ex[i], b = ey[i];
+    kahan_add(se, ce, __dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)));
+  }
+  sm -= cm;
+  se -= ce;
+  for (int o = 16; o > 0; o >>= 1) {
+    sm += __shfl_down_sync(0xffffffffu, sm, o);
+    se += __shfl_down_sync(0xffffffffu, se, o);
+  }
+  __shared__ double wm[32], we[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) { wm[warp] = sm; we[warp] = se; }
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    sm = lane < nw ? wm[lane] : 0.;
+    se = lane < nw ? we[lane] : 0.;
+    for (int o = 16; o > 0; o >>= 1) {
+      sm += __shfl_down_sync(0xffffffffu, sm, o);
+      se += __shfl_down_sync(0xffffffffu, se, o);
+    }
+    if (lane == 0) {
+      double e = sqrt(se * dx * dy);
+      e = e > 1.e-30 ? log(e) : -1.e9;
+      nrj_hist[iter] = e;
+      mass_hist[iter] = sm * dx * dy;
+    }
+  }
+}
+
+// ---- initcase.
+template <typename T>
+__global__ void k_init_case(T *__restrict__ f, Grid g, int ic, double amp, double k, double u) {
+  const long long total = g.cells();
+  const double PI = 3.14159265358979323846;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(idx % g.n[0]);
+    long long r = idx / g.n[0];
+    const int iy = (int)(r % g.n[1]);
+    r /= g.n[1];
+    const int ivx = (int)(r % g.n[2]);
+    const int ivy = (int)(r / g.n[2]);
+    const double x = g.minp[0] + ix * g.dx[0];
+    const double y = g.minp[1] + iy * g.dx[1];
+    const double vx = g.minp[2] + ivx * g.dx[2];
+    const double vy = g.minp[3] + ivy * g.dx[3];
+    double val = 0.;
+    if (ic == VLP4D_IC_SLD10) {  // init.cpp:234-256
+      val = (1. / (2 * PI)) * exp(-0.5 * (vx * vx + vy * vy)) * (1 + 0.05 * (cos(0.5 * x) * cos(0.5 * y)));
+    } else if (ic == VLP4D_IC_TSI20) {  // init.cpp:258-285
+      const double xi = 0.90, alpha = 0.05;
+      val = (1 + alpha * (cos(0.5 * x))) * 1 / (2 * PI) * ((2 - 2 * xi) / (3 - 2 * xi)) *
+            (1 + .5 * vx * vx / (1 - xi)) * exp(-.5 * (vx * vx + vy * vy));
+    } else if (ic == VLP4D_IC_CYL02 || ic == VLP4D_IC_CYL05) {  // init.cpp:143-232
+      const double PERIOD = 0.5 * PI, AMPLI = 4, cc = 0.50 * (6. / 16.), rc = 0.50 * (4. / 16.);
+      const double xx = ic == VLP4D_IC_CYL02 ? x : y, vv = ic == VLP4D_IC_CYL02 ? vx : vy;
+      double hv = 0.0, hx = 0.0;
+      if ((vv <= cc + rc) && (vv >= cc - rc)) hv = cos(PERIOD * ((vv - cc) / rc));
+      else if ((vv <= -cc + rc) && (vv >= -cc - rc)) hv = -cos(PERIOD * ((vv + cc) / rc));
+      if ((xx <= cc + rc) && (xx >= cc - rc)) hx = cos(PERIOD * ((xx - cc) / rc));
+      else if ((xx <= -cc + rc) && (xx >= -cc - rc)) hx = -cos(PERIOD * ((xx + cc) / rc));
+      val = AMPLI * hx * hv;
+    } else if (ic == VLP4D_IC_LANDAU_SUM) {
+      val = (1. + amp * cos(k * x) + amp * cos(k * y)) * (exp(-0.5 * (vx * vx + vy * vy)) / (2 * PI));
+    } else if (ic == VLP4D_IC_TWO_STREAM) {
+      const double s = 1. / sqrt(2 * PI);
+      const double mvy = s * exp(-0.5 * vy * vy);
+      const double mb = 0.5 * (s * exp(-0.5 * (vx - u) * (vx - u)) + s * exp(-0.5 * (vx + u) * (vx + u)));
+      val = (1. + amp * cos(k * x) + amp * cos(k * y)) * mb * mvy;
+    }
+    f[idx] = (T)val;
+  }
+}
+
+// ---- 2D transpose (column-major rows x cols -> cols x rows) through a
+// padded 32x32 shared tile: both the read and the write are coalesced.
+template <typename E>
+__global__ void k_transpose(const E *__restrict__ in, E *__restrict__ out, int rows, int cols) {
+  __shared__ E tile[32][33];
+  const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int r = r0 + threadIdx.x, c = c0 + j;
+    if (r < rows && c < cols) tile[j][threadIdx.x] = in[(long long)c * rows + r];
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int c = c0 + threadIdx.x, r = r0 + j;
+    if (r < rows && c < cols) out[(long long)r * cols + c] = tile[threadIdx.x][j];
+  }
+}
+
+}  // namespace
+
+int launch_field_rho(vlp4d_ctx *c, const void *fn, cudaStream_t s) {
+  const long long nxy = c->g.nxy(), nv = c->g.nv();
+  const int threads = 256;
+  const int groups = c->rho_groups;
+  dim3 grid((unsigned)((nxy + threads - 1) / threads), (unsigned)groups);
+  if (c->dtype == VLP4D_F64)
+    k_rho_partial<double><<<grid, threads, 0, s>>>((const double *)fn, c->rho_part, nxy, nv, groups);
+  else
+    k_rho_partial<float><<<grid, threads, 0, s>>>((const float *)fn, c->rho_part, nxy, nv, groups);
+  VLP4D_LAUNCH_CHECK();
+  return launch_rho_finish(c, groups, s);
+}
+
+int launch_rho_finish(vlp4d_ctx *c, int groups, cudaStream_t s) {
+  const long long nxy = c->g.nxy();
+  const int threads = 256;
+  k_rho_finish<<<(unsigned)((nxy + threads - 1) / threads), threads, 0, s>>>(c->rho_part, c->rho, nxy, groups,
+                                                                              c->g.dx[2], c->g.dx[3]);
+  VLP4D_LAUNCH_CHECK();
+  return VLP4D_OK;
+}
+
+int launch_field_poisson(vlp4d_ctx *c, cudaStream_t s) {
+  const int nx = c->g.n[0], ny = c->g.n[1];
+  const long long n2 = (long long)nx * ny;
+  const int threads = 256;
+  const int idcase = c->dom.idcase;
+  if (idcase == 2 || idcase == 6) {
+    k_analytic_field<<<(unsigned)((n2 + threads - 1) / threads), threads, 0, s>>>(
+        c->ex, c->ey, nx, ny, idcase, c->g.minp[0], c->g.minp[1], c->g.dx[0], c->g.dx[1]);
+    VLP4D_LAUNCH_CHECK();
+    return VLP4D_OK;
+  }
+  if (idcase == 10 || idcase == 20) {
+    k_rho_minus_one<<<(unsigned)((n2 + threads - 1) / threads), threads, 0, s>>>(c->rho, n2);
+    VLP4D_LAUNCH_CHECK();
+  }
+  VLP4D_CUFFT_TRY(cufftSetStream(c->plan_fwd, s));
+  VLP4D_CUFFT_TRY(cufftSetStream(c->plan_bwd, s));
+  VLP4D_CUFFT_TRY(cufftExecD2Z(c->plan_fwd, c->rho, c->rho_hat));
+  const int nx1h = nx / 2 + 1;
+  const double kx0 = 2 * M_PI / c->g.maxp[0];  // efield.cpp:44-45: 2*pi / maxPhy
+  const double ky0 = 2 * M_PI / c->g.maxp[1];
+  const double normcoeff = 1.0 / (double)(nx * ny);
+  const int nh = nx1h * ny;
+  k_poisson_solve<<<(nh + threads - 1) / threads, threads, 0, s>>>(c->rho_hat, c->ex_hat, c->ey_hat, nx1h, ny, kx0,
+                                                                    ky0, normcoeff);
+  VLP4D_LAUNCH_CHECK();
+  VLP4D_CUFFT_TRY(cufftExecZ2D(c->plan_bwd, c->rho_hat, c->rho));
+  VLP4D_CUFFT_TRY(cufftExecZ2D(c->plan_bwd, c->ex_hat, c->ex));
+  VLP4D_CUFFT_TRY(cufftExecZ2D(c->plan_bwd, c->ey_hat, c->ey));
+  return VLP4D_OK;
+}
+
+int launch_diags(vlp4d_ctx *c, int iter, cudaStream_t s) {
+  k_diags<<<1, 1024, 0, s>>>(c->rho, c->ex, c->ey, c->g.nxy(), c->g.dx[0], c->g.dx[1], c->nrj, c->mass, iter);
+  VLP4D_LAUNCH_CHECK();
+  return VLP4D_OK;
+}
+
+int launch_init_case(vlp4d_ctx *c, void *f, int ic, double amp, double k, double u, cudaStream_t s) {
+  const int threads = 256;
+  long long blocks = (c->g.cells() + threads - 1) / threads;
+  if (blocks > (long long)c->num_sms * 32) blocks = (long long)c->num_sms * 32;
+  if (c->dtype == VLP4D_F64)
+    k_init_case<double><<<(unsigned)blocks, threads, 0, s>>>((double *)f, c->g, ic, amp, k, u);
+  else
+    k_init_case<float><<<(unsigned)blocks, threads, 0, s>>>((float *)f, c->g, ic, amp, k, u);
+  VLP4D_LAUNCH_CHECK();
+  return VLP4D_OK;
+}
+
+int launch_transpose(const void *in, void *out, int rows, int cols, int elem, cudaStream_t s) {
+  dim3 block(32, 8), grid((rows + 31) / 32, (cols + 31) / 32);
+  if (elem == 4) k_transpose<float><<<grid, block, 0, s>>>((const float *)in, (float *)out, rows, cols);
+  else if (elem == 8) k_transpose<double><<<grid, block, 0, s>>>((const double *)in, (double *)out, rows, cols);
+  else k_transpose<double2><<<grid, block, 0, s>>>((const double2 *)in, (double2 *)out, rows, cols);
+  VLP4D_LAUNCH_CHECK();
+  return VLP4D_OK;
+}
+
+}  // namespace vlp4d

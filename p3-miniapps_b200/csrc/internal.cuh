@@ -1,0 +1,127 @@
+// Internal declarations shared by the translation units of libvlp4d_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "../../include/vlp4d_b200.h"
+#include "lagrange.cuh"
+
+namespace vlp4d {
+
+constexpr int kNumSMs = 148;  // B200; the launchers read the real count from the device
+
+// Thread-local last error message (vlp4d_last_error).
+void set_error(const std::string &msg);
+
+#define VLP4D_CUDA_TRY(expr)                                                                   \
+  do {                                                                                         \
+    cudaError_t _e = (expr);                                                                   \
+    if (_e != cudaSuccess) {                                                                   \
+      ::vlp4d::set_error(std::string(#expr) + ": " + cudaGetErrorString(_e));                  \
+      return VLP4D_ERR_CUDA;                                                                   \
+    }                                                                                          \
+  } while (0)
+
+#define VLP4D_CUFFT_TRY(expr)                                                                  \
+  do {                                                                                         \
+    cufftResult _r = (expr);                                                                   \
+    if (_r != CUFFT_SUCCESS) {                                                                 \
+      ::vlp4d::set_error(std::string(#expr) + ": cufft error " + std::to_string((int)_r));     \
+      return VLP4D_ERR_CUDA;                                                                   \
+    }                                                                                          \
+  } while (0)
+
+#define VLP4D_LAUNCH_CHECK()                                                                   \
+  do {                                                                                         \
+    cudaError_t _e = cudaGetLastError();                                                       \
+    if (_e != cudaSuccess) {                                                                   \
+      ::vlp4d::set_error(std::string("kernel launch: ") + cudaGetErrorString(_e));             \
+      return VLP4D_ERR_CUDA;                                                                   \
+    }                                                                                          \
+  } while (0)
+
+// Geometry of one run, in the reference's Domain terms.
+struct Grid {
+  int n[4];          // nx, ny, nvx, nvy
+  double minp[4], maxp[4], dx[4];
+  __host__ __device__ long long nxy() const { return (long long)n[0] * n[1]; }
+  __host__ __device__ long long nv() const { return (long long)n[2] * n[3]; }
+  __host__ __device__ long long cells() const { return nxy() * nv(); }
+};
+
+// Device-side line stencil tables, one entry per swept line.
+//   m[line] : tap offset, w[6*line + k] : weights (FP64 and an FP32 copy).
+struct StencilTable {
+  int *m = nullptr;
+  double *w = nullptr;
+  float *wf = nullptr;
+  int lines = 0;
+  double dt = 0.0;  // the dt the table was built for (host-built tables only)
+  bool valid = false;
+  unsigned long long stamp = 0;  // last use, for slot replacement
+};
+
+}  // namespace vlp4d
+
+struct vlp4d_ctx {
+  vlp4d::Grid g;
+  vlp4d_domain dom;
+  int dtype;           // VLP4D_F64 / VLP4D_F32
+  int device;
+  int num_sms;
+  size_t elem;         // sizeof element of f
+
+  // Efield equivalents (FP64, nx*ny).
+  double *rho = nullptr, *ex = nullptr, *ey = nullptr;
+  // Spectral work arrays ((nx/2+1)*ny complex).
+  cufftDoubleComplex *rho_hat = nullptr, *ex_hat = nullptr, *ey_hat = nullptr;
+  cufftHandle plan_fwd = 0, plan_bwd = 0;
+  bool plans = false;
+
+  // Diagnostics history (nbiter+1 entries each) and the reduction scratch.
+  double *nrj = nullptr, *mass = nullptr;
+  int hist_len = 0;
+
+  // Rho reduction partials: rho_groups x nxy FP64.
+  double *rho_part = nullptr;
+  int rho_groups = 0;
+
+  // Stencil tables: x/y lines for the two dt values of a Strang step (built
+  // on the host and uploaded once), v lines rebuilt from E on the device.
+  vlp4d::StencilTable tab_x[2], tab_y[2];
+  vlp4d::StencilTable tab_vx, tab_vy;
+  unsigned long long table_clock = 0;
+
+  // Pinned host staging for vlp4d_run's per-step diagnostic read-back.
+  double *h_diag = nullptr;
+};
+
+namespace vlp4d {
+
+// advect.cu
+int ensure_xy_table(vlp4d_ctx *c, int dim, double dt, StencilTable **out, cudaStream_t s);
+int build_v_tables(vlp4d_ctx *c, double dt, bool vx, bool vy, cudaStream_t s);
+int launch_advect_generic(vlp4d_ctx *c, int dim, const void *fn, void *fnp1, const StencilTable *t,
+                          cudaStream_t s);
+int launch_advect_pair_generic(vlp4d_ctx *c, bool v, const void *fn, void *fnp1, const StencilTable *ta,
+                               const StencilTable *tb, cudaStream_t s);
+int launch_advect_xy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *tx,
+                     const StencilTable *ty, bool do_x, bool do_y, bool with_rho, cudaStream_t s);
+int launch_advect_vxvy(vlp4d_ctx *c, const void *fn, void *fnp1, bool do_vx, bool do_vy, cudaStream_t s);
+bool xy_fused_supported(const vlp4d_ctx *c);
+bool vv_fused_supported(const vlp4d_ctx *c);
+
+// field.cu
+int launch_field_rho(vlp4d_ctx *c, const void *fn, cudaStream_t s);
+int launch_rho_finish(vlp4d_ctx *c, int groups, cudaStream_t s);
+int launch_field_poisson(vlp4d_ctx *c, cudaStream_t s);
+int launch_diags(vlp4d_ctx *c, int iter, cudaStream_t s);
+int launch_init_case(vlp4d_ctx *c, void *f, int ic, double amp, double k, double u, cudaStream_t s);
+int launch_transpose(const void *in, void *out, int rows, int cols, int elem, cudaStream_t s);
+
+}  // namespace vlp4d

@@ -1,0 +1,299 @@
+"""ctypes binding of libvlp4d_b200 (include/vlp4d_b200.h) over torch CUDA tensors.
+
+Tests and bench.py drive the CUDA library through this module; it adds no
+computation of its own.  Device memory and streams come from PyTorch; every
+call passes raw device pointers and a cudaStream_t through the C ABI.  If the
+library is missing the import-time load raises: there is no CPU fallback.
+
+Arrays use the reference's layout_left order, which for a C-ordered torch
+tensor means shape (nvy, nvx, ny, nx) for f and (ny, nx) for 2D fields.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Optional, Sequence
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libvlp4d_b200.so"
+
+OK, ERR_INVALID_ARG, ERR_CUDA, ERR_UNSUPPORTED, ERR_NO_DEVICE, ERR_IO = 0, 1, 2, 3, 4, 5
+F64, F32 = 0, 1
+FIELD_RHO, FIELD_EX, FIELD_EY = 0, 1, 2
+IC_CYL02, IC_CYL05, IC_SLD10, IC_TSI20, IC_LANDAU_SUM, IC_TWO_STREAM = 2, 5, 10, 20, 110, 120
+
+# Every symbol include/vlp4d_b200.h declares.
+EXPORTS = (
+    "vlp4d_read_deck", "vlp4d_ctx_create", "vlp4d_ctx_destroy", "vlp4d_last_error", "vlp4d_ctx_dtype",
+    "vlp4d_field_ptr", "vlp4d_init_case", "vlp4d_advect_x", "vlp4d_advect_y", "vlp4d_advect_vx",
+    "vlp4d_advect_vy", "vlp4d_advect_xy", "vlp4d_advect_vxvy", "vlp4d_field_rho", "vlp4d_field_poisson",
+    "vlp4d_diags_compute", "vlp4d_diags_read", "vlp4d_diags_save", "vlp4d_step", "vlp4d_run",
+    "vlp4d_print_fxvx", "vlp4d_transpose",
+)
+
+
+class Vlp4dError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"vlp4d error {code}: {msg}")
+        self.code = code
+
+
+class CDomain(C.Structure):
+    _fields_ = [
+        ("nxmax", C.c_int32 * 4),
+        ("min_phy", C.c_double * 4),
+        ("max_phy", C.c_double * 4),
+        ("dt", C.c_double),
+        ("nbiter", C.c_int32),
+        ("ifreq", C.c_int32),
+        ("idcase", C.c_int32),
+        ("fxvx", C.c_int32),
+    ]
+
+
+_lib = None
+
+
+def build() -> None:
+    """Compile libvlp4d_b200.so in-tree (nvcc, sm_100a)."""
+    import subprocess
+
+    subprocess.run(["make", "-s", "-C", str(HERE), "lib"], check=True)
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C {HERE}` (no CPU fallback)")
+        L = C.CDLL(str(LIB_PATH))
+        vp, dp, i, d = C.c_void_p, C.POINTER(C.c_double), C.c_int, C.c_double
+        L.vlp4d_last_error.restype = C.c_char_p
+        L.vlp4d_read_deck.argtypes = [C.c_char_p, C.POINTER(CDomain)]
+        L.vlp4d_ctx_create.argtypes = [C.POINTER(CDomain), i, C.POINTER(vp)]
+        L.vlp4d_ctx_destroy.argtypes = [vp]
+        L.vlp4d_ctx_dtype.argtypes = [vp]
+        L.vlp4d_field_ptr.argtypes = [vp, i, C.POINTER(vp)]
+        L.vlp4d_init_case.argtypes = [vp, vp, i, d, d, d, vp]
+        for n in ("vlp4d_advect_x", "vlp4d_advect_y", "vlp4d_advect_vx", "vlp4d_advect_vy", "vlp4d_advect_xy",
+                  "vlp4d_advect_vxvy"):
+            getattr(L, n).argtypes = [vp, vp, vp, d, vp]
+        L.vlp4d_field_rho.argtypes = [vp, vp, vp]
+        L.vlp4d_field_poisson.argtypes = [vp, vp]
+        L.vlp4d_diags_compute.argtypes = [vp, i, vp]
+        L.vlp4d_diags_read.argtypes = [vp, dp, dp, i]
+        L.vlp4d_diags_save.argtypes = [vp, C.c_char_p]
+        L.vlp4d_step.argtypes = [vp, vp, vp, i, vp]
+        L.vlp4d_run.argtypes = [vp, vp, vp, i, dp, dp, vp, vp, vp]
+        L.vlp4d_print_fxvx.argtypes = [vp, vp, C.c_char_p]
+        L.vlp4d_transpose.argtypes = [vp, vp, i, i, i, vp]
+        for n in EXPORTS:
+            if n != "vlp4d_last_error":
+                getattr(L, n).restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != OK:
+        msg = lib().vlp4d_last_error()
+        raise Vlp4dError(rc, msg.decode() if msg else "")
+
+
+@dataclass
+class Domain:
+    """The reference's Domain (miniapps/vlp4d/thrust/config.hpp:8-20)."""
+
+    nxmax: Sequence[int]
+    min_phy: Sequence[float]
+    max_phy: Sequence[float]
+    dt: float
+    nbiter: int = 1
+    idcase: int = 10
+    ifreq: int = 1
+    fxvx: int = 0
+
+    @property
+    def dx(self):
+        return tuple((self.max_phy[i] - self.min_phy[i]) / self.nxmax[i] for i in range(4))
+
+    @property
+    def shape4(self):
+        nx, ny, nvx, nvy = self.nxmax
+        return (nvy, nvx, ny, nx)
+
+    @property
+    def shape2(self):
+        return (self.nxmax[1], self.nxmax[0])
+
+    @property
+    def cells(self) -> int:
+        return int(math.prod(self.nxmax))
+
+    def to_c(self) -> CDomain:
+        c = CDomain()
+        for k in range(4):
+            c.nxmax[k] = int(self.nxmax[k])
+            c.min_phy[k] = float(self.min_phy[k])
+            c.max_phy[k] = float(self.max_phy[k])
+        c.dt, c.nbiter, c.idcase, c.ifreq, c.fxvx = float(self.dt), int(self.nbiter), int(self.idcase), int(self.ifreq), int(self.fxvx)
+        return c
+
+    @classmethod
+    def from_deck(cls, path: str) -> "Domain":
+        c = CDomain()
+        _check(lib().vlp4d_read_deck(str(path).encode(), C.byref(c)))
+        return cls(list(c.nxmax), list(c.min_phy), list(c.max_phy), c.dt, c.nbiter, c.idcase, c.ifreq, c.fxvx)
+
+
+def landau_domain(n, dt=0.125, nbiter=1, L=4 * math.pi, vmax=6.0, idcase=10) -> Domain:
+    """Landau-damping geometry of the benchmark configurations: x, y in [0, L), v in [-vmax, vmax)."""
+    if isinstance(n, int):
+        n = (n, n, n, n)
+    return Domain(list(n), [0.0, 0.0, -vmax, -vmax], [L, L, vmax, vmax], dt, nbiter, idcase)
+
+
+class _DevArray:
+    """Minimal __cuda_array_interface__ wrapper so torch can view a library-owned buffer."""
+
+    def __init__(self, ptr: int, shape, typestr: str):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+def _stream_ptr(stream) -> Optional[int]:
+    import torch
+
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return stream.cuda_stream
+
+
+class Context:
+    """A vlp4d_ctx: the Efield + Diags state of one run on the current device."""
+
+    def __init__(self, dom: Domain, dtype: str = "f64"):
+        import torch
+
+        self.dom = dom
+        self.dtype_code = F64 if dtype in ("f64", "float64", torch.float64) else F32
+        self.torch_dtype = torch.float64 if self.dtype_code == F64 else torch.float32
+        self._c = dom.to_c()
+        h = C.c_void_p()
+        _check(lib().vlp4d_ctx_create(C.byref(self._c), self.dtype_code, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().vlp4d_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- buffers
+    def empty_f(self):
+        import torch
+
+        return torch.empty(self.dom.shape4, dtype=self.torch_dtype, device="cuda")
+
+    def _f(self, t):
+        import torch
+
+        if not (t.is_cuda and t.dtype == self.torch_dtype and t.is_contiguous() and t.numel() == self.dom.cells):
+            raise ValueError(f"f must be a contiguous CUDA {self.torch_dtype} tensor of {self.dom.cells} elements")
+        return C.c_void_p(t.data_ptr())
+
+    def field(self, which: int):
+        """Torch view (no copy) of the context-owned FP64 (ny, nx) field."""
+        import torch
+
+        p = C.c_void_p()
+        _check(lib().vlp4d_field_ptr(self.h, which, C.byref(p)))
+        return torch.as_tensor(_DevArray(p.value, self.dom.shape2, "<f8"), device="cuda")
+
+    rho = property(lambda self: self.field(FIELD_RHO))
+    ex = property(lambda self: self.field(FIELD_EX))
+    ey = property(lambda self: self.field(FIELD_EY))
+
+    # -- entry points (one per C function)
+    def init_case(self, f, ic=IC_LANDAU_SUM, amp=0.05, k=0.5, u=2.4, stream=None):
+        _check(lib().vlp4d_init_case(self.h, self._f(f), ic, amp, k, u, _stream_ptr(stream)))
+
+    def advect_x(self, fn, fnp1, dt, stream=None):
+        _check(lib().vlp4d_advect_x(self.h, self._f(fn), self._f(fnp1), dt, _stream_ptr(stream)))
+
+    def advect_y(self, fn, fnp1, dt, stream=None):
+        _check(lib().vlp4d_advect_y(self.h, self._f(fn), self._f(fnp1), dt, _stream_ptr(stream)))
+
+    def advect_vx(self, fn, fnp1, dt, stream=None):
+        _check(lib().vlp4d_advect_vx(self.h, self._f(fn), self._f(fnp1), dt, _stream_ptr(stream)))
+
+    def advect_vy(self, fn, fnp1, dt, stream=None):
+        _check(lib().vlp4d_advect_vy(self.h, self._f(fn), self._f(fnp1), dt, _stream_ptr(stream)))
+
+    def advect_xy(self, fn, fnp1, dt, stream=None):
+        _check(lib().vlp4d_advect_xy(self.h, self._f(fn), self._f(fnp1), dt, _stream_ptr(stream)))
+
+    def advect_vxvy(self, fn, fnp1, dt, stream=None):
+        _check(lib().vlp4d_advect_vxvy(self.h, self._f(fn), self._f(fnp1), dt, _stream_ptr(stream)))
+
+    def field_rho(self, fn, stream=None):
+        _check(lib().vlp4d_field_rho(self.h, self._f(fn), _stream_ptr(stream)))
+
+    def field_poisson(self, stream=None):
+        _check(lib().vlp4d_field_poisson(self.h, _stream_ptr(stream)))
+
+    def diags_compute(self, it, stream=None):
+        _check(lib().vlp4d_diags_compute(self.h, it, _stream_ptr(stream)))
+
+    def diags_read(self, count=None):
+        import numpy as np
+
+        count = self.dom.nbiter + 1 if count is None else count
+        nrj = (C.c_double * max(count, 1))()
+        mass = (C.c_double * max(count, 1))()
+        _check(lib().vlp4d_diags_read(self.h, nrj, mass, count))
+        return np.array(nrj[:count]), np.array(mass[:count])
+
+    def diags_save(self, path):
+        _check(lib().vlp4d_diags_save(self.h, str(path).encode()))
+
+    def step(self, f_state, f_next, it, stream=None):
+        """One fused Strang step: reads f_state, writes the new state into f_next (f_state becomes scratch)."""
+        _check(lib().vlp4d_step(self.h, self._f(f_state), self._f(f_next), it, _stream_ptr(stream)))
+
+    def run(self, f0_host, nsteps, fn, fnp1, f_out_host=None, stream=None):
+        """vlp4d_run with host buffers (torch CPU tensors, ideally pinned). Returns (nrj, mass) numpy arrays."""
+        import numpy as np
+
+        if f0_host.is_cuda or f0_host.dtype != self.torch_dtype or not f0_host.is_contiguous():
+            raise ValueError("f0_host must be a contiguous CPU tensor of the context dtype")
+        nrj = (C.c_double * (nsteps + 1))()
+        mass = (C.c_double * (nsteps + 1))()
+        out_ptr = C.c_void_p(f_out_host.data_ptr()) if f_out_host is not None else None
+        _check(lib().vlp4d_run(self.h, C.c_void_p(f0_host.data_ptr()), out_ptr, nsteps, nrj, mass, self._f(fn),
+                               self._f(fnp1), _stream_ptr(stream)))
+        return np.array(nrj[:]), np.array(mass[:])
+
+    def print_fxvx(self, fn, path):
+        _check(lib().vlp4d_print_fxvx(self.h, self._f(fn), str(path).encode()))
+
+
+def transpose(a, out, stream=None):
+    """Impl::Transpose::forward on a column-major (rows, cols) matrix held as a C-ordered (cols, rows) tensor."""
+    cols, rows = a.shape
+    _check(lib().vlp4d_transpose(C.c_void_p(a.data_ptr()), C.c_void_p(out.data_ptr()), rows, cols,
+                                 a.element_size(), _stream_ptr(stream)))
