@@ -1,0 +1,431 @@
+"""Benchmark of the vlp4d hot path on B200: Landau damping at 128^4.
+
+Workload (one "step" = one Strang time step, timestep.hpp:14-67 of the
+reference, as three fused passes + the FP64 field solve and diagnostic):
+Landau damping with the sum-form initial condition
+(1 + 0.05 cos(0.5x) + 0.05 cos(0.5y)) M(vx) M(vy) on x, y in [0, 4pi),
+v in [-6, 6), 128^4 cells, dt = 0.1.  f is stored in FP32 (the headline)
+and, for the FP32-vs-FP64 error and the FP64 throughput, also in FP64.
+Inputs are synthetic (the initial condition); f (1.07 GB FP32) is larger
+than the 126 MB L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+One process per GPU; N > 1 runs N independent replicas (a single run does
+not shard) timed as the max over ranks.  `--impl reference` times the
+reference's own OpenMP CPU build (oracle/_ref) on the host cores instead.
+Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+N_GRID = 128
+DT = 0.1
+L_BOX = 4 * math.pi
+VMAX = 6.0
+METRIC = "Gcell-updates/s"
+WORKLOAD = "Landau damping 128^4, dt 0.1, sum-form IC (amp 0.05, k 0.5), Strang step"
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--n", type=int, default=N_GRID, help="cells per dimension (default 128)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end runs")
+    return ap.parse_args(argv)
+
+
+# ---------------------------------------------------------------- ranks
+class Ranks:
+    """torch.distributed plumbing for barriers and max-over-ranks timing only."""
+
+    def __init__(self, world: int, backend: str = "nccl"):
+        self.world = world
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.dist = None
+        if world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+            self.dist = dist
+        self.backend = backend
+
+    def _tensor(self, x):
+        import torch
+
+        dev = "cuda" if self.backend == "nccl" else "cpu"
+        return torch.tensor([float(x)], dtype=torch.float64, device=dev)
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.dist:
+            return float(x)
+        t = self._tensor(x)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist:
+            self.dist.destroy_process_group()
+
+
+def aggregate(seconds_max: float, cells: int, steps: int, world: int) -> dict:
+    """Whole-job throughput: all replicas' cell updates over the slowest rank's time."""
+    return {
+        "value": cells * steps * world / seconds_max / 1e9,
+        "ms_per_step": seconds_max * 1e3 / steps,
+    }
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during timed regions."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"vlp4d_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        self.path.unlink(missing_ok=True)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max((float(r[3]) for r in rows if r[3].replace(".", "").isdigit()), default=None)}
+
+
+def measured_hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- GPU arm
+def _events(torch):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def time_calls(torch, stream, fn, reps):
+    """Mean device time (s) of `fn()` over `reps` calls, events on `stream`."""
+    e0, e1 = _events(torch)
+    fn()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / reps
+
+
+def gpu_arm(args, ranks):
+    import torch
+
+    import __graft_entry__ as ge
+
+    pkg = ge.load_package()
+    v = pkg.vlp4d
+    torch.cuda.set_device(ranks.local_rank)
+    dev = torch.device("cuda", ranks.local_rank)
+    stream = torch.cuda.current_stream(dev)
+    K, W = args.steps, max(args.warmup, 3)
+    n = args.n
+    dom = pkg.landau_domain(n, dt=DT, nbiter=W + K + 2, L=L_BOX, vmax=VMAX)
+    cells = dom.cells
+    sampler = ClockSampler(ranks.local_rank)
+    try:
+        uuid = str(torch.cuda.get_device_properties(dev).uuid)
+        sampler.index = "GPU-" + uuid if not uuid.startswith("GPU-") else uuid
+    except Exception:
+        pass
+    out = {"stages": {}}
+    sampler.start()
+
+    per_dtype = {}
+    for dtype in ("f32", "f64"):
+        with pkg.Context(dom, dtype) as ctx:
+            fa, fb = ctx.empty_f(), ctx.empty_f()
+            ctx.init_case(fa, v.IC_LANDAU_SUM, 0.05, 0.5)
+            ctx.field_rho(fa)
+            ctx.field_poisson()
+            ctx.diags_compute(0)
+            cur, nxt = fa, fb
+            for it in range(1, W + 1):
+                ctx.step(cur, nxt, it)
+                cur, nxt = nxt, cur
+            torch.cuda.synchronize()
+            ranks.barrier()
+            torch.cuda.synchronize()
+            launches0 = v.kernel_launches()
+            e0, e1 = _events(torch)
+            e0.record(stream)
+            for it in range(W + 1, W + K + 1):
+                ctx.step(cur, nxt, it)
+                cur, nxt = nxt, cur
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ranks.barrier()
+            secs = e0.elapsed_time(e1) / 1e3
+            launches = v.kernel_launches() - launches0
+            ctx.check()
+            tmax = ranks.max(secs)
+            rec = aggregate(tmax, cells, K, ranks.world)
+            rec["launches"] = launches
+            # Stage timings: the reference's timer labels (timer.hpp:51-59) plus the fused passes.
+            reps = 10
+            st = {}
+            st["advec1D_x"] = time_calls(torch, stream, lambda: ctx.advect_x(cur, nxt, 0.5 * DT), reps)
+            st["advec1D_y"] = time_calls(torch, stream, lambda: ctx.advect_y(cur, nxt, 0.5 * DT), reps)
+            st["advec1D_vx"] = time_calls(torch, stream, lambda: ctx.advect_vx(cur, nxt, DT), reps)
+            st["advec1D_vy"] = time_calls(torch, stream, lambda: ctx.advect_vy(cur, nxt, DT), reps)
+            st["advect_xy"] = time_calls(torch, stream, lambda: ctx.advect_xy(cur, nxt, 0.5 * DT), reps)
+            st["advect_vxvy"] = time_calls(torch, stream, lambda: ctx.advect_vxvy(cur, nxt, DT), reps)
+            st["field"] = time_calls(torch, stream, lambda: ctx.field_rho(cur), reps)
+            st["Fourier"] = time_calls(torch, stream, lambda: ctx.field_poisson(), reps)
+            st["diag"] = time_calls(torch, stream, lambda: ctx.diags_compute(1), reps)
+            ctx.check()
+            elem = 4 if dtype == "f32" else 8
+            rw = 2.0 * cells * elem
+            rec["stages"] = {
+                k: {"ms": t * 1e3,
+                    "gbs": ((cells * elem if k == "field" else rw) / t / 1e9) if k not in ("Fourier", "diag") else None}
+                for k, t in st.items()}
+            per_dtype[dtype] = rec
+            del fa, fb, cur, nxt
+            torch.cuda.empty_cache()
+
+    clocks = sampler.stop()
+
+    # Roofline of the dominant kernel: the fused x/y plane pass (two of the
+    # three passes of a step).  Algorithmic bytes per launch: f read once +
+    # written once.
+    peak, peak_kind = measured_hbm_peak()
+    f32 = per_dtype["f32"]
+    t_xy = f32["stages"]["advect_xy"]["ms"] / 1e3
+    t_vv = f32["stages"]["advect_vxvy"]["ms"] / 1e3
+    dominant = "advect_xy (k_plane, fused x+y half step)" if 2 * t_xy >= t_vv else "advect_vxvy (k_vslab)"
+    t_dom = t_xy if 2 * t_xy >= t_vv else t_vv
+    achieved = 2.0 * cells * 4 / t_dom / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        try:
+            traffic = json.loads(tf.read_text()).get("plane_f32_128" if "xy" in dominant else "vslab_f32_128")
+        except ValueError:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": dominant, "peak_kind": peak_kind,
+                "bytes_per_launch": 2 * cells * 4,
+                "step_frac": (6.0 * cells * 4 / (f32["ms_per_step"] / 1e3) / 1e9) / peak}
+
+    # End to end through the C ABI with host buffers (vlp4d_run): H2D of the
+    # initial f from pinned memory, the initial solve, K steps, D2H of the
+    # diagnostic history and of the final f.  Also yields the FP32 vs FP64 error.
+    e2e = None
+    err = {}
+    if not args.no_e2e:
+        finals = {}
+        histories = {}
+        e2e_vals = {}
+        for dtype in ("f32", "f64"):
+            tdt = torch.float32 if dtype == "f32" else torch.float64
+            with pkg.Context(dom, dtype) as ctx:
+                fa, fb = ctx.empty_f(), ctx.empty_f()
+                ctx.init_case(fa, v.IC_LANDAU_SUM, 0.05, 0.5)
+                h0 = torch.empty(dom.shape4, dtype=tdt, pin_memory=True)
+                h0.copy_(fa)
+                hout = torch.empty(dom.shape4, dtype=tdt, pin_memory=True)
+                torch.cuda.synchronize()
+                ranks.barrier()
+                e0, e1 = _events(torch)
+                e0.record(stream)
+                nrj, mass = ctx.run(h0, K, fa, fb, f_out_host=hout)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                secs = ranks.max(e0.elapsed_time(e1) / 1e3)
+                e2e_vals[dtype] = cells * K * ranks.world / secs / 1e9
+                histories[dtype] = nrj
+                finals[dtype] = fa.double() if dtype == "f64" else fa.clone()
+                fbytes = cells * h0.element_size()
+                if dtype == "f32":
+                    e2e = {"value": e2e_vals["f32"], "unit": METRIC,
+                           "h2d_bytes_per_step": fbytes / K, "d2h_bytes_per_step": (fbytes + 16 * (K + 1)) / K,
+                           "seconds": secs, "api": "vlp4d_run (C ABI, pinned host buffers)"}
+                del fa, fb, h0, hout
+                torch.cuda.empty_cache()
+        import numpy as np
+
+        w32 = np.exp(2 * histories["f32"])
+        w64 = np.exp(2 * histories["f64"])
+        rel = np.abs(w32 - w64) / w64
+        df = (finals["f32"].double() - finals["f64"]).abs().max().item()
+        err = {"steps": K, "energy_rel_max": float(rel.max()), "energy_rel_final": float(rel[-1]),
+               "energy_abs_max_over_wmax": float(np.abs(w32 - w64).max() / w64.max()),
+               "f_maxabs": df, "f_max": finals["f64"].abs().max().item(),
+               "e2e_f64": e2e_vals["f64"]}
+        del finals
+        torch.cuda.empty_cache()
+
+    rec = per_dtype["f32"]
+    line = {
+        "metric": METRIC, "value": rec["value"], "unit": METRIC, "n_gpus": ranks.world, "steps": K, "warmup": W,
+        "ms_per_step": rec["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (Landau initial condition computed on the device)",
+        "config": {"workload": WORKLOAD, "grid": [n] * 4, "dt": DT, "storage": "f32 f, f64 fields/diagnostics",
+                   "parallelism": f"replicas x{ranks.world}" if ranks.world > 1 else "single GPU",
+                   "l2": "f (%.2f GB) larger than L2, no flush" % (cells * 4 / 1e9)},
+        "roofline": roofline, "e2e": e2e, "gpu_launches": rec["launches"], "clocks": clocks,
+        "f64": {"value": per_dtype["f64"]["value"], "ms_per_step": per_dtype["f64"]["ms_per_step"],
+                "speedup_f32_over_f64": rec["value"] / per_dtype["f64"]["value"],
+                "published_a100_stdpar_f64": 7.19,
+                "stages": per_dtype["f64"]["stages"]},
+        "stages": rec["stages"], "error_f32_vs_f64": err,
+    }
+    return line
+
+
+# ---------------------------------------------------------------- CPU reference
+def landau_f0_numpy(n):
+    """The benchmark initial condition on the host, FP64, layout_left order."""
+    import numpy as np
+
+    dx = L_BOX / n
+    dv = 2 * VMAX / n
+    x = np.arange(n) * dx
+    v = -VMAX + np.arange(n) * dv
+    s = 1.0 + 0.05 * np.cos(0.5 * x)[None, :] + 0.05 * np.cos(0.5 * x)[:, None]  # (iy, ix)
+    m = np.exp(-0.5 * v * v) / math.sqrt(2 * math.pi)
+    out = np.empty((n, n, n, n))
+    for ivy in range(n):
+        out[ivy] = (m[ivy] * m)[:, None, None] * s[None, :, :]
+    return out
+
+
+def reference_cpu(n, max_steps, budget_s):
+    """Times the reference's own OpenMP build (oracle/_ref) on this host:
+    full Strang steps on the whole grid, one untimed step first, then up to
+    max_steps timed steps while the total stays within budget_s."""
+    sys.path.insert(0, str(ROOT))
+    from oracle.oracle import Reference
+
+    if not Reference.available():
+        return None
+    ref = Reference((n, n, n, n), (0.0, 0.0, -VMAX, -VMAX), (L_BOX, L_BOX, VMAX, VMAX), DT,
+                    nbiter=max_steps + 2, idcase=10)
+    f0 = landau_f0_numpy(n)
+    ref.set_f(0, f0)
+    del f0
+    threads = int(ref.L.ref_max_threads())
+    ref.onetimestep(1)  # first touch of fnp1 and the FFT buffers
+    times = []
+    for it in range(max_steps):
+        t0 = time.perf_counter()
+        ref.onetimestep(2 + it)
+        times.append(time.perf_counter() - t0)
+        if sum(times) > budget_s:
+            break
+    ref.close()
+    secs = sum(times)
+    return {"value": n ** 4 * len(times) / secs / 1e9, "unit": METRIC, "cores": threads, "kind": "reference",
+            "steps": len(times), "seconds": secs,
+            "sample": f"{len(times)} full Strang steps of the {n}^4 grid (after 1 untimed step), "
+                      f"reference OpenMP build miniapps/vlp4d/openmp, FP64, OMP_NUM_THREADS={threads}"}
+
+
+def _set_omp_env():
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    os.environ.setdefault("OMP_PROC_BIND", "true")
+
+
+def reference_arm(args):
+    _set_omp_env()
+    budget = 150.0
+    res = reference_cpu(args.n, max(args.steps, 1), budget)
+    if res is None:
+        return {"impl": "reference", "unavailable": "oracle/_ref/libvlp4d_ref.so (the reference's OpenMP build) is absent"}
+    ms = res["seconds"] * 1e3 / res["steps"]
+    return {
+        "impl": "reference", "metric": METRIC, "value": res["value"], "unit": METRIC, "n_gpus": args.gpus,
+        "steps": res["steps"], "warmup": 1, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (Landau initial condition)",
+        "config": {"workload": WORKLOAD, "grid": [args.n] * 4, "dt": DT, "storage": "f64 (reference)",
+                   "requested_steps": args.steps},
+        "cpu_baseline": res,
+        "e2e": {"value": res["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    world = int(os.environ.get("WORLD_SIZE", args.gpus))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(reference_arm(args)), flush=True)
+        return 0
+    ranks = Ranks(world)
+    try:
+        line = gpu_arm(args, ranks)
+        if rank == 0 and world == 1:
+            _set_omp_env()
+            line["cpu_baseline"] = reference_cpu(args.n, 3, 20.0) or {
+                "value": None, "unit": METRIC, "cores": 0, "kind": "reference", "sample": "oracle/_ref absent"}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        ranks.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -41,6 +41,7 @@ extern "C" {
 #define VLP4D_ERR_UNSUPPORTED 3
 #define VLP4D_ERR_NO_DEVICE 4
 #define VLP4D_ERR_IO 5
+#define VLP4D_ERR_TIMEOUT 6 /* a kernel's bounded wait for an async copy ran out */
 
 #define VLP4D_F64 0
 #define VLP4D_F32 1
@@ -92,6 +93,10 @@ int vlp4d_ctx_create(const vlp4d_domain *dom, int dtype, vlp4d_ctx **out);
 int vlp4d_ctx_destroy(vlp4d_ctx *ctx);
 const char *vlp4d_last_error(void);
 int vlp4d_ctx_dtype(const vlp4d_ctx *ctx);
+/* Number of this library's own kernel launches so far in the process
+ * (library kernels such as cuFFT's are not counted).  No counterpart in the
+ * reference; used to account for launches in benchmarks. */
+unsigned long long vlp4d_kernel_launches(void);
 
 /* Device pointer of a context-owned FP64 nx*ny field (VLP4D_FIELD_*). */
 int vlp4d_field_ptr(vlp4d_ctx *ctx, int which, double **dev_ptr);
@@ -123,16 +128,27 @@ int vlp4d_field_poisson(vlp4d_ctx *ctx, void *stream);
 /* Diags::compute (diags.cpp:13-55) for iteration `iter` (0..nbiter): energy
  * log(sqrt(sum|E|^2 dx dy)) and mass sum(rho)*dx*dy, kept on the device. */
 int vlp4d_diags_compute(vlp4d_ctx *ctx, int iter, void *stream);
-/* Synchronous read of the diagnostic history entries [0, count). */
+/* Synchronises the device and reports VLP4D_ERR_TIMEOUT if a fused kernel
+ * gave up waiting for one of its asynchronous copies since the last check
+ * (the kernel then exits early instead of hanging; its outputs are not
+ * valid).  The reference has no counterpart: its launches are unchecked. */
+int vlp4d_check(vlp4d_ctx *ctx);
+
+/* Synchronous read of the diagnostic history entries [0, count); includes
+ * vlp4d_check. */
 int vlp4d_diags_read(vlp4d_ctx *ctx, double *nrj, double *mass, int count);
 /* Diags::save (diags.cpp:57-68): "t nrj mass" per iteration into `path`. */
 int vlp4d_diags_save(vlp4d_ctx *ctx, const char *path);
 
 /* onetimestep (miniapps/vlp4d/thrust/timestep.hpp:14-67) as three fused
  * passes: x/y half step with the rho moment in its epilogue, the field solve
- * and diagnostic `iter`, the vx/vy full step, the x/y half step.  fn holds
- * the state before and after; fnp1 is scratch of the same size. */
-int vlp4d_step(vlp4d_ctx *ctx, void *fn, void *fnp1, int iter, void *stream);
+ * and diagnostic `iter`, the vx/vy full step, the x/y half step.  Reads the
+ * state from f_state and writes the advanced state into f_next; f_state is
+ * used as scratch and holds no meaningful data afterwards, so callers swap
+ * the two pointers between steps.  (The reference's six 1D sweeps ping-pong
+ * an even number of times and end in fn; three passes end in the other
+ * buffer.) */
+int vlp4d_step(vlp4d_ctx *ctx, void *f_state, void *f_next, int iter, void *stream);
 
 /* The time loop of main() (miniapps/vlp4d/thrust/vlp4d.cpp:55-73) with host
  * buffers: copies f0 (host, nx*ny*nvx*nvy elements of the context's dtype)

@@ -9,26 +9,16 @@
 #include <vector>
 
 #include "internal.cuh"
+#include "stencil.cuh"
 
 namespace vlp4d {
 
 namespace {
 
-// FP32 copy of a line's weights: the five smallest are rounded, the largest
-// is set so that the six FP32 weights sum to 1 as closely as FP32 allows.
-// Constants are then advected without a per-line gain, which would otherwise
-// accumulate coherently over the steps of a run.
+// FP32 copy of a line's weights (used by the FP32-storage difference form,
+// stencil.cuh, which never reads the centre weight w[2]).
 __host__ __device__ inline void weights_to_f32(const double w[6], float wf[6]) {
-  int kmax = 0;
-  for (int k = 1; k < 6; ++k)
-    if (fabs(w[k]) > fabs(w[kmax])) kmax = k;
-  double s = 0.0;
-  for (int k = 0; k < 6; ++k) {
-    if (k == kmax) continue;
-    wf[k] = (float)w[k];
-    s += (double)wf[k];
-  }
-  wf[kmax] = (float)(1.0 - s);
+  for (int k = 0; k < 6; ++k) wf[k] = (float)w[k];
 }
 
 // One v-line per (ix, iy): displacement dt*E(ix, iy) (advection.hpp:243, 306).
@@ -47,17 +37,6 @@ __global__ void k_build_vtable(const double *__restrict__ e, int lines, double d
   }
 }
 
-template <typename T>
-struct Weights;
-template <>
-struct Weights<double> {
-  static __device__ __forceinline__ const double *get(const StencilTable &t) { return t.w; }
-};
-template <>
-struct Weights<float> {
-  static __device__ __forceinline__ const float *get(const StencilTable &t) { return t.wf; }
-};
-
 // Generic 1D sweep along dimension DIM: one thread per output cell, taps
 // gathered through L1/L2.  Any extents (including n < 6, where the stencil
 // wraps more than once).
@@ -66,7 +45,7 @@ __global__ void k_advect_generic(const T *__restrict__ fn, T *__restrict__ fnp1,
                                  int nvy, StencilTable tab) {
   const long long nxy = (long long)nx * ny;
   const long long total = nxy * nvx * nvy;
-  const T *__restrict__ w = Weights<T>::get(tab);
+  const T *__restrict__ w = WeightsOf<T>::get(tab);
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
        idx += (long long)gridDim.x * blockDim.x) {
     const int ix = (int)(idx % nx);
@@ -84,13 +63,14 @@ __global__ void k_advect_generic(const T *__restrict__ fn, T *__restrict__ fnp1,
     const long long base = idx - (long long)i * stride;
     int j = i + tab.m[line];
     if (j >= n) j -= n;
-    T acc = T(0);
+    T tap[6], wl[6];
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-      acc = fma(w[6 * line + k], fn[base + (long long)j * stride], acc);
+      tap[k] = fn[base + (long long)j * stride];
       if (++j == n) j = 0;
     }
-    fnp1[idx] = acc;
+    load_weights(w, line, wl);
+    fnp1[idx] = interp6(wl, tap[0], tap[1], tap[2], tap[3], tap[4], tap[5]);
   }
 }
 
@@ -102,8 +82,8 @@ __global__ void k_advect_pair_generic(const T *__restrict__ fn, T *__restrict__ 
                                       int nvy, StencilTable ta, StencilTable tb) {
   const long long nxy = (long long)nx * ny;
   const long long total = nxy * nvx * nvy;
-  const T *__restrict__ wa = Weights<T>::get(ta);
-  const T *__restrict__ wb = Weights<T>::get(tb);
+  const T *__restrict__ wa = WeightsOf<T>::get(ta);
+  const T *__restrict__ wb = WeightsOf<T>::get(tb);
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
        idx += (long long)gridDim.x * blockDim.x) {
     const int ix = (int)(idx % nx);
@@ -120,20 +100,22 @@ __global__ void k_advect_pair_generic(const T *__restrict__ fn, T *__restrict__ 
     int jb = ib + tb.m[lb];
     if (jb >= nb) jb -= nb;
     const int ja0 = (ia + ta.m[la]) >= na ? ia + ta.m[la] - na : ia + ta.m[la];
-    T out = T(0);
+    T wla[6], wlb[6], row[6];
+    load_weights(wa, la, wla);
+    load_weights(wb, lb, wlb);
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
       int ja = ja0;
-      T acc = T(0);
+      T tap[6];
 #pragma unroll
       for (int k = 0; k < 6; ++k) {
-        acc = fma(wa[6 * la + k], fn[base + (long long)ja * sa + (long long)jb * sb], acc);
+        tap[k] = fn[base + (long long)ja * sa + (long long)jb * sb];
         if (++ja == na) ja = 0;
       }
-      out = fma(wb[6 * lb + q], acc, out);
+      row[q] = interp6(wla, tap[0], tap[1], tap[2], tap[3], tap[4], tap[5]);
       if (++jb == nb) jb = 0;
     }
-    fnp1[idx] = out;
+    fnp1[idx] = interp6(wlb, row[0], row[1], row[2], row[3], row[4], row[5]);
   }
 }
 

@@ -1,0 +1,327 @@
+// Fused vx/vy advection pass over column chunks.
+//
+// Replaces advect_1D_vx followed by advect_1D_vy (miniapps/vlp4d/thrust/
+// advection.hpp:203-328, run back to back in timestep.hpp:40-48).
+//
+// For a fixed spatial point (ix, iy) both velocity shifts are constant
+// (dt*Ex(ix,iy) and dt*Ey(ix,iy)), so each "column" ixy = ix + nx*iy has one
+// vx stencil and one vy stencil, read from the device-built line tables.  A
+// work item is a chunk of C consecutive columns (C*elem = 128 bytes) and a
+// segment of Q output vy rows.  The kernel streams "slabs" f[ixy0:ixy0+C,
+// :, ivy] (C x nvx elements, one 3D TMA tile, layout [ivx][c]) through a
+// `stages`-deep mbarrier pipeline, in vy order starting at the smallest
+// vy offset of the chunk.  Each thread owns one column and V consecutive vx:
+// it applies the vx stencil to every slab (taps from shared memory; the bank
+// depends only on the column, so per-column offsets never conflict), keeps
+// the last six vx-swept rows in registers and emits output row ivy once the
+// six rows ivy+o..ivy+o+5 of its own column's vy offset o are in the window.
+// Stores of a warp cover C consecutive columns: 128 contiguous bytes.
+#include <cudaTypedefs.h>
+
+#include "internal.cuh"
+#include "stencil.cuh"
+#include "tma.cuh"
+
+namespace vlp4d {
+
+namespace {
+
+constexpr int kBarBytes = 128;
+constexpr int kMaxStages = 12;
+
+struct VslabArgs {
+  void *fout;
+  int nxy, nvx, nvy;
+  int C;      // columns per chunk
+  int Q;      // output vy rows per item (divides nvy)
+  int nseg;   // nvy / Q
+  long long nitems;
+  int stages;
+  StencilTable tvx, tvy;
+  const int2 *span;  // per chunk: (min, max) signed vy offset of its columns
+  int *err;
+};
+
+// Signed form of a tap offset m in [0, n): the shift in cells, in (-n/2, n/2].
+__device__ __forceinline__ int signed_offset(int m, int n) { return m > n / 2 ? m - n : m; }
+
+template <typename T, bool DVX, bool DVY, int V>
+__global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorMap tin, VslabArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  // Tensor-copy destinations on a 128-byte boundary whatever the base
+  // alignment of dynamic shared memory (the launch adds 128 bytes of slack).
+  unsigned char *smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  const int C = a.C, nvx = a.nvx, nvy = a.nvy, S = a.stages;
+  const size_t slab_elems = (size_t)C * nvx;
+  const uint32_t slab_bytes = (uint32_t)(slab_elems * sizeof(T));
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+  T *slabs = reinterpret_cast<T *>(smem + kBarBytes);
+  const int col = threadIdx.x % C;
+  const int vx0 = (threadIdx.x / C) * V;
+
+  // Slab count and first vy row of an item.
+  auto item_range = [&](long long item, int &cnt, int &start, int &cc) {
+    cc = (int)(item / a.nseg);
+    const int sg = (int)(item % a.nseg);
+    if (DVY) {
+      const int2 sp = a.span[cc];
+      cnt = a.Q + (sp.y - sp.x) + 5;
+      start = sg * a.Q + sp.x;
+    } else {
+      cnt = a.Q;
+      start = sg * a.Q;
+    }
+  };
+
+  // Producer cursor (meaningful in thread 0 only).
+  long long p_item = blockIdx.x, p_k = 0;
+  int p_t = 0, p_cnt = 0, p_start = 0, p_cc = 0;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+    mbar_fence_init();
+    if (p_item < a.nitems) item_range(p_item, p_cnt, p_start, p_cc);
+  }
+  __syncthreads();
+
+  auto issue_next = [&]() {
+    if (p_item >= a.nitems) return;
+    int row = (p_start + p_t) % nvy;
+    if (row < 0) row += nvy;
+    const int slot = (int)(p_k % S);
+    mbar_arrive_expect_tx(&bars[slot], slab_bytes);
+    tensor_load_3d(slabs + (size_t)slot * slab_elems, &tin, p_cc * C, 0, row, &bars[slot]);
+    ++p_k;
+    if (++p_t == p_cnt) {
+      p_t = 0;
+      p_item += gridDim.x;
+      if (p_item < a.nitems) item_range(p_item, p_cnt, p_start, p_cc);
+    }
+  };
+  if (threadIdx.x == 0)
+    for (int s = 0; s < S; ++s) issue_next();
+
+  const long long vstride = a.nxy;                      // consecutive ivx
+  const long long ystride = (long long)a.nxy * nvx;     // consecutive ivy
+  long long k = 0;                                      // slabs consumed
+  for (long long item = blockIdx.x; item < a.nitems; item += gridDim.x) {
+    int cnt, start, cc;
+    item_range(item, cnt, start, cc);
+    const int sg = (int)(item % a.nseg);
+    const long long ixy = (long long)cc * C + col;
+    T wvx[6], wvy[6];
+    int mvx = 0, lag0 = 0;
+    if (DVX) {
+      mvx = __ldg(a.tvx.m + ixy);
+      load_weights(WeightsOf<T>::get(a.tvx), ixy, wvx);
+    }
+    if (DVY) {
+      lag0 = 5 + signed_offset(__ldg(a.tvy.m + ixy), nvy) - a.span[cc].x;
+      load_weights(WeightsOf<T>::get(a.tvy), ixy, wvy);
+    }
+    T *outc = static_cast<T *>(a.fout) + ixy + vstride * vx0 + ystride * (long long)sg * a.Q;
+    T win[6][V];
+#pragma unroll
+    for (int j = 0; j < 6; ++j)
+#pragma unroll
+      for (int i = 0; i < V; ++i) win[j][i] = T(0);
+
+    for (int t = 0; t < cnt; ++t, ++k) {
+      const int slot = (int)(k % S);
+      const bool ok = mbar_wait_bounded(&bars[slot], (uint32_t)((k / S) & 1));
+      const T *sl = slabs + (size_t)slot * slab_elems;  // [ivx][c]
+      T tmp[V];
+      if (DVX) {
+        int j = vx0 + mvx;
+        if (j >= nvx) j -= nvx;
+        T tap[V + 5];
+#pragma unroll
+        for (int q = 0; q < V + 5; ++q) {
+          tap[q] = sl[(size_t)j * C + col];
+          if (++j == nvx) j = 0;
+        }
+#pragma unroll
+        for (int i = 0; i < V; ++i) tmp[i] = interp6(wvx, tap[i], tap[i + 1], tap[i + 2], tap[i + 3], tap[i + 4], tap[i + 5]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < V; ++i) tmp[i] = sl[(size_t)(vx0 + i) * C + col];
+      }
+      if (DVY) {
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+          win[0][i] = win[1][i]; win[1][i] = win[2][i]; win[2][i] = win[3][i];
+          win[3][i] = win[4][i]; win[4][i] = win[5][i]; win[5][i] = tmp[i];
+        }
+        const int e = t - lag0;
+        if (e >= 0 && e < a.Q) {
+          T *o = outc + ystride * e;
+#pragma unroll
+          for (int i = 0; i < V; ++i)
+            o[vstride * i] = interp6(wvy, win[0][i], win[1][i], win[2][i], win[3][i], win[4][i], win[5][i]);
+        }
+      } else {
+        T *o = outc + ystride * t;
+#pragma unroll
+        for (int i = 0; i < V; ++i) o[vstride * i] = tmp[i];
+      }
+      // The slot is free once every thread is here.
+      if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) {
+          atomicExch(a.err, 1);
+          for (long long q = k; q < p_k; ++q) mbar_wait_bounded(&bars[q % S], (uint32_t)((q / S) & 1));
+        }
+        __syncthreads();
+        return;
+      }
+      if (threadIdx.x == 0) issue_next();
+    }
+  }
+}
+
+// Per column chunk of C columns: smallest and largest signed vy offset.
+__global__ void k_vspan(const int *__restrict__ mvy, int nchunks, int C, int nvy, int2 *__restrict__ span) {
+  const int cc = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cc >= nchunks) return;
+  int lo = 1 << 30, hi = -(1 << 30);
+  for (int c = 0; c < C; ++c) {
+    const int o = signed_offset(mvy[(long long)cc * C + c], nvy);
+    lo = o < lo ? o : lo;
+    hi = o > hi ? o : hi;
+  }
+  span[cc] = make_int2(lo, hi);
+}
+
+}  // namespace
+}  // namespace vlp4d
+
+namespace vlp4d {
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    else
+      cudaGetLastError();
+  }
+  return fn;
+}
+
+int env_int(const char *name, int dflt) {
+  const char *v = getenv(name);
+  return v && *v ? atoi(v) : dflt;
+}
+
+struct VslabCfg {
+  int C = 0, V = 0, Q = 0, stages = 0, threads = 0;
+  size_t smem = 0;
+};
+
+// C*elem = 128 bytes per slab row (64 when nvx > 128), V vx per thread,
+// 512 threads.  Q = 32 output rows per item keeps the item count a
+// comfortable multiple of the SM count at 128^4; VLP4D_VSLAB_Q and
+// VLP4D_VSLAB_STAGES override for tuning sweeps.
+bool vslab_config(const vlp4d_ctx *c, VslabCfg &cfg) {
+  const long long nxy = c->g.nxy();
+  const int nvx = c->g.n[2], nvy = c->g.n[3];
+  const bool f32 = c->dtype == VLP4D_F32;
+  if (nvx < 8 || nvx > 256) return false;
+  if (f32) {
+    cfg.V = 8;
+    cfg.C = nvx <= 128 ? 32 : 16;
+  } else {
+    cfg.V = 4;
+    cfg.C = nvx <= 128 ? 16 : 8;
+  }
+  if (nvx % cfg.V || nxy % cfg.C) return false;
+  cfg.threads = cfg.C * (nvx / cfg.V);
+  if (cfg.threads > 512 || cfg.threads < 32) return false;
+  int Q = env_int("VLP4D_VSLAB_Q", 32);
+  if (Q > nvy) Q = nvy;
+  while (Q > 1 && nvy % Q) --Q;
+  cfg.Q = Q;
+  cfg.stages = env_int("VLP4D_VSLAB_STAGES", 6);
+  if (cfg.stages < 2 || cfg.stages > kMaxStages) return false;
+  cfg.smem = 128 + kBarBytes + (size_t)cfg.stages * cfg.C * nvx * c->elem;
+  return cfg.smem <= 200 * 1024;
+}
+
+template <typename T, bool DVX, bool DVY, int V>
+int run_vslab(vlp4d_ctx *c, const CUtensorMap &map, const VslabArgs &args, const VslabCfg &cfg, cudaStream_t s) {
+  auto kern = k_vslab<T, DVX, DVY, V>;
+  VLP4D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
+  int per_sm = 0;
+  VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, cfg.threads, cfg.smem));
+  if (per_sm < 1) return VLP4D_ERR_UNSUPPORTED;
+  long long grid = (long long)per_sm * c->num_sms;
+  if (grid > args.nitems) grid = args.nitems;
+  kern<<<(unsigned)grid, cfg.threads, cfg.smem, s>>>(map, args);
+  VLP4D_LAUNCH_CHECK();
+  return VLP4D_OK;
+}
+
+}  // namespace
+
+int launch_advect_vxvy(vlp4d_ctx *c, const void *fn, void *fnp1, bool do_vx, bool do_vy, cudaStream_t s) {
+  if (!c->fused) return VLP4D_ERR_UNSUPPORTED;
+  if (((uintptr_t)fn & 15) || ((uintptr_t)fnp1 & 15)) return VLP4D_ERR_UNSUPPORTED;
+  if (!do_vx && !do_vy) return VLP4D_ERR_UNSUPPORTED;
+  VslabCfg cfg;
+  if (!vslab_config(c, cfg)) return VLP4D_ERR_UNSUPPORTED;
+  PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+  if (!encode) return VLP4D_ERR_UNSUPPORTED;
+  const long long nxy = c->g.nxy();
+  const int nvx = c->g.n[2], nvy = c->g.n[3];
+  const size_t elem = c->elem;
+  const int nchunks = (int)(nxy / cfg.C);
+  if (do_vy && nchunks > c->vspan_cap) return VLP4D_ERR_UNSUPPORTED;
+
+  CUtensorMap map;
+  cuuint64_t dims[3] = {(cuuint64_t)nxy, (cuuint64_t)nvx, (cuuint64_t)nvy};
+  cuuint64_t strides[2] = {(cuuint64_t)(nxy * elem), (cuuint64_t)(nxy * nvx * elem)};
+  cuuint32_t box[3] = {(cuuint32_t)cfg.C, (cuuint32_t)nvx, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = encode(&map, elem == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                      const_cast<void *>(fn), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return VLP4D_ERR_UNSUPPORTED;
+
+  if (do_vy) {
+    k_vspan<<<(nchunks + 127) / 128, 128, 0, s>>>(c->tab_vy.m, nchunks, cfg.C, nvy, c->vspan);
+    VLP4D_LAUNCH_CHECK();
+  }
+  VslabArgs a;
+  a.fout = fnp1;
+  a.nxy = (int)nxy;
+  a.nvx = nvx;
+  a.nvy = nvy;
+  a.C = cfg.C;
+  a.Q = cfg.Q;
+  a.nseg = nvy / cfg.Q;
+  a.nitems = (long long)nchunks * a.nseg;
+  a.stages = cfg.stages;
+  if (do_vx) a.tvx = c->tab_vx;
+  if (do_vy) a.tvy = c->tab_vy;
+  a.span = c->vspan;
+  a.err = c->d_err;
+#define VLP4D_VS(T, DVX, DVY, V) return run_vslab<T, DVX, DVY, V>(c, map, a, cfg, s)
+  if (c->dtype == VLP4D_F64) {
+    if (do_vx && do_vy) VLP4D_VS(double, true, true, 4);
+    if (do_vx) VLP4D_VS(double, true, false, 4);
+    VLP4D_VS(double, false, true, 4);
+  } else {
+    if (do_vx && do_vy) VLP4D_VS(float, true, true, 8);
+    if (do_vx) VLP4D_VS(float, true, false, 8);
+    VLP4D_VS(float, false, true, 8);
+  }
+#undef VLP4D_VS
+}
+
+}  // namespace vlp4d

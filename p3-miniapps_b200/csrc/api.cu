@@ -5,6 +5,7 @@
 #include <cstring>
 #include <string>
 #include <utility>
+#include <atomic>
 
 #include "internal.cuh"
 
@@ -14,6 +15,10 @@ static thread_local std::string g_last_error;
 
 void set_error(const std::string &msg) { g_last_error = msg; }
 
+static std::atomic<unsigned long long> g_launches{0};
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
 namespace {
 
 int fail(int code, const std::string &msg) {
@@ -22,6 +27,12 @@ int fail(int code, const std::string &msg) {
 }
 
 bool finite(double v) { return std::isfinite(v); }
+
+// Fallback policy after a fused launcher declined a shape.
+int fused_declined(const vlp4d_ctx *c) {
+  if (c->fused_only) return fail(VLP4D_ERR_UNSUPPORTED, "fused kernel unavailable for this shape (VLP4D_KERNELS=fused)");
+  return VLP4D_OK;
+}
 
 int validate_domain(const vlp4d_domain *d) {
   if (!d) return fail(VLP4D_ERR_INVALID_ARG, "domain is NULL");
@@ -68,6 +79,8 @@ void free_ctx(vlp4d_ctx *c) {
   cudaFree(c->nrj);
   cudaFree(c->mass);
   cudaFree(c->rho_part);
+  cudaFree(c->d_err);
+  cudaFree(c->vspan);
   for (StencilTable *t : {&c->tab_x[0], &c->tab_x[1], &c->tab_y[0], &c->tab_y[1], &c->tab_vx, &c->tab_vy}) {
     cudaFree(t->m);
     cudaFree(t->w);
@@ -96,6 +109,8 @@ using namespace vlp4d;
 extern "C" {
 
 const char *vlp4d_last_error(void) { return g_last_error.c_str(); }
+
+unsigned long long vlp4d_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
 
 int vlp4d_read_deck(const char *path, vlp4d_domain *out) {
   if (!path || !out) return fail(VLP4D_ERR_INVALID_ARG, "NULL argument");
@@ -173,13 +188,28 @@ int vlp4d_ctx_create(const vlp4d_domain *dom, int dtype, vlp4d_ctx **out) {
   if (groups > 1024) groups = 1024;
   if (groups < 1) groups = 1;
   c->rho_groups = (int)groups;
-  CTX_ALLOC(c->rho_part, sizeof(double) * nxy * (size_t)c->rho_groups);
+  // The fused x/y pass writes one partial per plane group (up to two CTAs
+  // per SM); bounded so the partials stay below 256 MB.
+  long long fused_groups = 2LL * c->num_sms;
+  const long long cap = (256LL << 20) / ((long long)sizeof(double) * nxy);
+  if (fused_groups > cap) fused_groups = cap;
+  c->rho_part_groups = (int)(fused_groups > groups ? fused_groups : groups);
+  CTX_ALLOC(c->rho_part, sizeof(double) * nxy * (size_t)c->rho_part_groups);
+  CTX_ALLOC(c->d_err, sizeof(int));
+  c->vspan_cap = (int)(nxy / 8 + 1);
+  CTX_ALLOC(c->vspan, sizeof(int2) * (size_t)c->vspan_cap);
+  {
+    const char *k = getenv("VLP4D_KERNELS");
+    c->fused = !(k && strcmp(k, "generic") == 0);
+    c->fused_only = k && strcmp(k, "fused") == 0;
+  }
 #undef CTX_ALLOC
   if (cudaMemset(c->rho, 0, sizeof(double) * nxy) != cudaSuccess ||
       cudaMemset(c->ex, 0, sizeof(double) * nxy) != cudaSuccess ||
       cudaMemset(c->ey, 0, sizeof(double) * nxy) != cudaSuccess ||
       cudaMemset(c->nrj, 0, sizeof(double) * c->hist_len) != cudaSuccess ||
-      cudaMemset(c->mass, 0, sizeof(double) * c->hist_len) != cudaSuccess)
+      cudaMemset(c->mass, 0, sizeof(double) * c->hist_len) != cudaSuccess ||
+      cudaMemset(c->d_err, 0, sizeof(int)) != cudaSuccess)
     return bail(fail(VLP4D_ERR_CUDA, "cudaMemset failed"));
   // lib/Cuda_FFT.hpp:108-114: cufftPlan2d(nx2 = ny, nx1 = nx) on x-fastest data.
   if (cufftPlan2d(&c->plan_fwd, c->g.n[1], c->g.n[0], CUFFT_D2Z) != CUFFT_SUCCESS)
@@ -237,13 +267,16 @@ static int advect_1d(vlp4d_ctx *ctx, int dim, const void *fn, void *fnp1, double
   StencilTable *t = nullptr;
   if (dim < 2) {
     if ((rc = ensure_xy_table(ctx, dim, dt, &t, s))) return rc;
-    if (xy_fused_supported(ctx))
-      return launch_advect_xy(ctx, fn, fnp1, dim == 0 ? t : nullptr, dim == 1 ? t : nullptr, dim == 0, dim == 1,
-                              false, s);
+    rc = launch_advect_xy(ctx, fn, fnp1, dim == 0 ? t : nullptr, dim == 1 ? t : nullptr, dim == 0, dim == 1,
+                          false, s);
+    if (rc != VLP4D_ERR_UNSUPPORTED) return rc;
+    if ((rc = fused_declined(ctx))) return rc;
     return launch_advect_generic(ctx, dim, fn, fnp1, t, s);
   }
   if ((rc = build_v_tables(ctx, dt, dim == 2, dim == 3, s))) return rc;
-  if (vv_fused_supported(ctx)) return launch_advect_vxvy(ctx, fn, fnp1, dim == 2, dim == 3, s);
+  rc = launch_advect_vxvy(ctx, fn, fnp1, dim == 2, dim == 3, s);
+  if (rc != VLP4D_ERR_UNSUPPORTED) return rc;
+  if ((rc = fused_declined(ctx))) return rc;
   return launch_advect_generic(ctx, dim, fn, fnp1, dim == 2 ? &ctx->tab_vx : &ctx->tab_vy, s);
 }
 
@@ -265,7 +298,9 @@ static int advect_xy_impl(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt,
   int rc;
   if ((rc = ensure_xy_table(ctx, 0, dt, &tx, s))) return rc;
   if ((rc = ensure_xy_table(ctx, 1, dt, &ty, s))) return rc;
-  if (xy_fused_supported(ctx)) return launch_advect_xy(ctx, fn, fnp1, tx, ty, true, true, with_rho, s);
+  rc = launch_advect_xy(ctx, fn, fnp1, tx, ty, true, true, with_rho, s);
+  if (rc != VLP4D_ERR_UNSUPPORTED) return rc;
+  if ((rc = fused_declined(ctx))) return rc;
   if ((rc = launch_advect_pair_generic(ctx, false, fn, fnp1, tx, ty, s))) return rc;
   return with_rho ? launch_field_rho(ctx, fnp1, s) : VLP4D_OK;
 }
@@ -273,7 +308,9 @@ static int advect_xy_impl(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt,
 static int advect_vxvy_impl(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, cudaStream_t s) {
   int rc;
   if ((rc = build_v_tables(ctx, dt, true, true, s))) return rc;
-  if (vv_fused_supported(ctx)) return launch_advect_vxvy(ctx, fn, fnp1, true, true, s);
+  rc = launch_advect_vxvy(ctx, fn, fnp1, true, true, s);
+  if (rc != VLP4D_ERR_UNSUPPORTED) return rc;
+  if ((rc = fused_declined(ctx))) return rc;
   return launch_advect_pair_generic(ctx, true, fn, fnp1, &ctx->tab_vx, &ctx->tab_vy, s);
 }
 
@@ -314,11 +351,24 @@ int vlp4d_diags_compute(vlp4d_ctx *ctx, int iter, void *stream) {
   return launch_diags(ctx, iter, as_stream(stream));
 }
 
+int vlp4d_check(vlp4d_ctx *ctx) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  VLP4D_CUDA_TRY(cudaDeviceSynchronize());
+  int flag = 0;
+  VLP4D_CUDA_TRY(cudaMemcpy(&flag, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag) {
+    VLP4D_CUDA_TRY(cudaMemset(ctx->d_err, 0, sizeof(int)));
+    return fail(VLP4D_ERR_TIMEOUT, "an asynchronous copy did not complete within its time limit");
+  }
+  return VLP4D_OK;
+}
+
 int vlp4d_diags_read(vlp4d_ctx *ctx, double *nrj, double *mass, int count) {
   int rc = check_ctx(ctx);
   if (rc) return rc;
   if (count < 0 || count > ctx->hist_len) return fail(VLP4D_ERR_INVALID_ARG, "count outside [0, nbiter+1]");
-  VLP4D_CUDA_TRY(cudaDeviceSynchronize());
+  if ((rc = vlp4d_check(ctx))) return rc;
   if (nrj) VLP4D_CUDA_TRY(cudaMemcpy(nrj, ctx->nrj, sizeof(double) * count, cudaMemcpyDeviceToHost));
   if (mass) VLP4D_CUDA_TRY(cudaMemcpy(mass, ctx->mass, sizeof(double) * count, cudaMemcpyDeviceToHost));
   return VLP4D_OK;
@@ -390,6 +440,7 @@ int vlp4d_run(vlp4d_ctx *ctx, const void *f0_host, void *f_out_host, int nsteps,
   }
   if (f_out_host) VLP4D_CUDA_TRY(cudaMemcpyAsync(f_out_host, cur, bytes, cudaMemcpyDeviceToHost, s));
   VLP4D_CUDA_TRY(cudaStreamSynchronize(s));
+  if ((rc = vlp4d_check(ctx))) return rc;
   if (nrj) memcpy(nrj, ctx->h_diag, sizeof(double) * (nsteps + 1));
   if (mass) memcpy(mass, ctx->h_diag + ctx->hist_len, sizeof(double) * (nsteps + 1));
   // Leave the final state in fn, as the reference's loop does.

@@ -18,6 +18,10 @@ constexpr int kNumSMs = 148;  // B200; the launchers read the real count from th
 // Thread-local last error message (vlp4d_last_error).
 void set_error(const std::string &msg);
 
+// Process-wide count of this library's own kernel launches (cuFFT's are not
+// included), read by vlp4d_kernel_launches().
+void count_launch();
+
 #define VLP4D_CUDA_TRY(expr)                                                                   \
   do {                                                                                         \
     cudaError_t _e = (expr);                                                                   \
@@ -38,6 +42,7 @@ void set_error(const std::string &msg);
 
 #define VLP4D_LAUNCH_CHECK()                                                                   \
   do {                                                                                         \
+    ::vlp4d::count_launch();                                                                   \
     cudaError_t _e = cudaGetLastError();                                                       \
     if (_e != cudaSuccess) {                                                                   \
       ::vlp4d::set_error(std::string("kernel launch: ") + cudaGetErrorString(_e));             \
@@ -87,9 +92,23 @@ struct vlp4d_ctx {
   double *nrj = nullptr, *mass = nullptr;
   int hist_len = 0;
 
-  // Rho reduction partials: rho_groups x nxy FP64.
+  // Moment partials: rho_part_groups x nxy FP64.  The generic reduction
+  // uses rho_groups of them, the fused x/y pass up to rho_part_groups.
   double *rho_part = nullptr;
   int rho_groups = 0;
+  int rho_part_groups = 0;
+
+  // Kernel selection, read from VLP4D_KERNELS at context creation:
+  // unset = fused kernels where the shape allows, generic otherwise;
+  // "generic" = generic per-cell kernels only; "fused" = fused kernels only
+  // (an unsupported shape is an error instead of a silent fallback).
+  bool fused = true;
+  bool fused_only = false;
+  // Set to 1 by a kernel whose bounded wait for an asynchronous copy ran out.
+  int *d_err = nullptr;
+  // Per column chunk (min, max) signed vy offset for the fused v pass.
+  int2 *vspan = nullptr;
+  int vspan_cap = 0;
 
   // Stencil tables: x/y lines for the two dt values of a Strang step (built
   // on the host and uploaded once), v lines rebuilt from E on the device.
@@ -110,11 +129,12 @@ int launch_advect_generic(vlp4d_ctx *c, int dim, const void *fn, void *fnp1, con
                           cudaStream_t s);
 int launch_advect_pair_generic(vlp4d_ctx *c, bool v, const void *fn, void *fnp1, const StencilTable *ta,
                                const StencilTable *tb, cudaStream_t s);
+// advect_plane.cu / advect_vslab.cu: VLP4D_ERR_UNSUPPORTED (nothing
+// launched) when the shape or buffers do not fit; callers then use the
+// generic kernels.
 int launch_advect_xy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *tx,
                      const StencilTable *ty, bool do_x, bool do_y, bool with_rho, cudaStream_t s);
 int launch_advect_vxvy(vlp4d_ctx *c, const void *fn, void *fnp1, bool do_vx, bool do_vy, cudaStream_t s);
-bool xy_fused_supported(const vlp4d_ctx *c);
-bool vv_fused_supported(const vlp4d_ctx *c);
 
 // field.cu
 int launch_field_rho(vlp4d_ctx *c, const void *fn, cudaStream_t s);

@@ -20,7 +20,7 @@ from typing import Optional, Sequence
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libvlp4d_b200.so"
 
-OK, ERR_INVALID_ARG, ERR_CUDA, ERR_UNSUPPORTED, ERR_NO_DEVICE, ERR_IO = 0, 1, 2, 3, 4, 5
+OK, ERR_INVALID_ARG, ERR_CUDA, ERR_UNSUPPORTED, ERR_NO_DEVICE, ERR_IO, ERR_TIMEOUT = 0, 1, 2, 3, 4, 5, 6
 F64, F32 = 0, 1
 FIELD_RHO, FIELD_EX, FIELD_EY = 0, 1, 2
 IC_CYL02, IC_CYL05, IC_SLD10, IC_TSI20, IC_LANDAU_SUM, IC_TWO_STREAM = 2, 5, 10, 20, 110, 120
@@ -31,7 +31,7 @@ EXPORTS = (
     "vlp4d_field_ptr", "vlp4d_init_case", "vlp4d_advect_x", "vlp4d_advect_y", "vlp4d_advect_vx",
     "vlp4d_advect_vy", "vlp4d_advect_xy", "vlp4d_advect_vxvy", "vlp4d_field_rho", "vlp4d_field_poisson",
     "vlp4d_diags_compute", "vlp4d_diags_read", "vlp4d_diags_save", "vlp4d_step", "vlp4d_run",
-    "vlp4d_print_fxvx", "vlp4d_transpose",
+    "vlp4d_print_fxvx", "vlp4d_transpose", "vlp4d_check", "vlp4d_kernel_launches",
 )
 
 
@@ -90,11 +90,19 @@ def lib() -> C.CDLL:
         L.vlp4d_run.argtypes = [vp, vp, vp, i, dp, dp, vp, vp, vp]
         L.vlp4d_print_fxvx.argtypes = [vp, vp, C.c_char_p]
         L.vlp4d_transpose.argtypes = [vp, vp, i, i, i, vp]
+        L.vlp4d_check.argtypes = [vp]
+        L.vlp4d_kernel_launches.argtypes = []
         for n in EXPORTS:
-            if n != "vlp4d_last_error":
+            if n not in ("vlp4d_last_error", "vlp4d_kernel_launches"):
                 getattr(L, n).restype = C.c_int
+        L.vlp4d_kernel_launches.restype = C.c_ulonglong
         _lib = L
     return _lib
+
+
+def kernel_launches() -> int:
+    """This library's own kernel launches so far in the process."""
+    return int(lib().vlp4d_kernel_launches())
 
 
 def _check(rc: int) -> None:
@@ -287,6 +295,10 @@ class Context:
         _check(lib().vlp4d_run(self.h, C.c_void_p(f0_host.data_ptr()), out_ptr, nsteps, nrj, mass, self._f(fn),
                                self._f(fnp1), _stream_ptr(stream)))
         return np.array(nrj[:]), np.array(mass[:])
+
+    def check(self):
+        """Synchronise and raise if a kernel reported a lost asynchronous copy."""
+        _check(lib().vlp4d_check(self.h))
 
     def print_fxvx(self, fn, path):
         _check(lib().vlp4d_print_fxvx(self.h, self._f(fn), str(path).encode()))

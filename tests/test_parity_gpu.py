@@ -264,7 +264,8 @@ def test_diags_save_and_fxvx_formats(pkg, cuda, tmp_path):
     line = (tmp_path / "nrj.out").read_text().splitlines()[0]
     assert line == "%17.13e %17.13e %17.13e" % (0.0, rows[0, 1], rows[0, 2])
     csv = np.loadtxt(tmp_path / "fxvx.csv", delimiter=",")
-    assert np.array_equal(csv, f0[dom.nxmax[3] // 2, :, 0, :])
+    # "%20.13le" keeps 14 significant digits.
+    assert np.allclose(csv, f0[dom.nxmax[3] // 2, :, 0, :], rtol=1e-13, atol=0)
 
 
 def test_invalid_iter_rejected(pkg, cuda):
