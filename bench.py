@@ -45,6 +45,7 @@ def parse_args(argv=None):
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--n", type=int, default=N_GRID, help="cells per dimension (default 128)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end runs")
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip timing the reference CPU build")
     return ap.parse_args(argv)
 
 
@@ -416,7 +417,7 @@ def main(argv=None):
     ranks = Ranks(world)
     try:
         line = gpu_arm(args, ranks)
-        if rank == 0 and world == 1:
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
             _set_omp_env()
             line["cpu_baseline"] = reference_cpu(args.n, 3, 20.0) or {
                 "value": None, "unit": METRIC, "cores": 0, "kind": "reference", "sample": "oracle/_ref absent"}
