@@ -16,6 +16,8 @@ oracle/ref_driver.cpp) on small seeded inputs and stores what it computes:
   conditions on a small deck-like domain.
 * ``fft_kat.npz``: the reference's FFT round-trip case
   (tests/openmp/test_fft.cpp:7-71) through its Impl::FFT wrapper.
+* ``<deck>_nrj.out``: nrj.out written by the reference's own driver
+  (oracle/_ref/vlp4d_ref) on the small decks in decks/.
 
 Usage (needs the reference tree, which only the build container has):
     python tests/golden/make_golden.py
@@ -120,6 +122,43 @@ def fft_kat():
     print("fft_kat: round-trip err", float(np.abs(back - u3).max()))
 
 
+def write_deck(path, n, mins, maxs, case, dt, steps, freq, fxvx):
+    """An input deck in the reference's format (import(), init.cpp:12-82):
+    the value after each colon, in a fixed order."""
+    names = ["x", "y", "vx", "vy"]
+    lines = ["# vlp4d input deck; the parser reads the value after each colon, in this order"]
+    lines += [f"grid points along {nm} : {v}" for nm, v in zip(names, n)]
+    for nm, a, b in zip(names, mins, maxs):
+        lines += [f"lower bound of {nm} : {a}", f"upper bound of {nm} : {b}"]
+    lines += [f"test case (10 Landau, 20 two-beam) : {case}", f"time step : {dt}", f"number of steps : {steps}",
+              f"diagnostic frequency : {freq}", f"write fxvx slices : {fxvx}"]
+    Path(path).write_text("\n".join(lines) + "\n")
+
+
+def deck_runs():
+    """The reference's own driver (oracle/_ref/vlp4d_ref, main() of
+    miniapps/vlp4d/openmp/vlp4d.cpp) on two small decks; keeps its nrj.out."""
+    import shutil
+    import subprocess
+    import tempfile
+
+    from oracle.oracle import REFERENCE_EXE
+
+    decks = OUT / "decks"
+    write_deck(decks / "sld10_16.dat", [16] * 4, ["0.", "0.", "-9.", "-9."], ["12.56637112"] * 2 + ["9.", "9."],
+               10, 0.125, 20, 4, 0)
+    write_deck(decks / "tsi20_32x4.dat", [32, 4, 32, 4], ["0.", "0.", "-9.", "-9."],
+               ["25.13274122871834590"] * 2 + ["9.", "9."], 20, 0.125, 20, 4, 1)
+    for name in ("sld10_16", "tsi20_32x4"):
+        with tempfile.TemporaryDirectory() as d:
+            (Path(d) / "data" / "vlp4d").mkdir(parents=True)
+            shutil.copy(decks / f"{name}.dat", Path(d) / "deck.dat")
+            subprocess.run([str(REFERENCE_EXE), "deck.dat"], cwd=d, check=True, capture_output=True,
+                           env={"OMP_NUM_THREADS": "4", "PATH": "/usr/bin:/bin"})
+            shutil.copy(Path(d) / "nrj.out", OUT / f"{name}_nrj.out")
+        print("deck run:", name)
+
+
 def main():
     build(reference=True)
     if not Reference.available():
@@ -131,6 +170,7 @@ def main():
     landau32()
     initcases()
     fft_kat()
+    deck_runs()
 
 
 if __name__ == "__main__":
