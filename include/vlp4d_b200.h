@@ -163,6 +163,22 @@ int vlp4d_run(vlp4d_ctx *ctx, const void *f0_host, void *f_out_host, int nsteps,
  * ivy=nvy/2 as CSV into `path`.  Synchronous. */
 int vlp4d_print_fxvx(vlp4d_ctx *ctx, const void *fn, const char *path);
 
+/* field_rho for callers that cannot allocate device memory: callers whose
+ * device memory is owned by their own pool allocator, or whose time loop must
+ * not pay cudaMalloc/cudaFree (cudaFree synchronises the whole device), and so
+ * cannot create a vlp4d_ctx.  No counterpart in the reference.  Computes
+ * rho = dvx*dvy*sum_v f (FP64, nx*ny device array) from f (device, dtype
+ * VLP4D_F64/VLP4D_F32) without allocating: the reduction's partial sums use a
+ * fixed 4 MiB array built into the library (present on every GPU that loads
+ * it, until exit), so nx*ny may not exceed 524288 (larger grids return
+ * VLP4D_ERR_INVALID_ARG).  The first call on each device, with that device
+ * current, looks up the array's device address once; make that first call
+ * before any stream capture.  All calls share the array: calls whose kernels
+ * overlap on the GPU race, so issue them on one stream or otherwise in
+ * order. */
+int vlp4d_field_rho_noalloc(const void *fn, int dtype, int nx, int ny, int nvx, int nvy, double dvx, double dvy,
+                            double *rho, void *stream);
+
 /* Impl::Transpose::forward/backward (lib/Cuda_Transpose.hpp:38-46):
  * out-of-place transpose of a (rows x cols) column-major matrix of
  * elements of `elem_size` bytes (4, 8 or 16). */

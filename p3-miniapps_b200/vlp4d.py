@@ -32,6 +32,7 @@ EXPORTS = (
     "vlp4d_advect_vy", "vlp4d_advect_xy", "vlp4d_advect_vxvy", "vlp4d_field_rho", "vlp4d_field_poisson",
     "vlp4d_diags_compute", "vlp4d_diags_read", "vlp4d_diags_save", "vlp4d_step", "vlp4d_run",
     "vlp4d_print_fxvx", "vlp4d_transpose", "vlp4d_check", "vlp4d_kernel_launches",
+    "vlp4d_field_rho_noalloc",
 )
 
 
@@ -92,6 +93,7 @@ def lib() -> C.CDLL:
         L.vlp4d_transpose.argtypes = [vp, vp, i, i, i, vp]
         L.vlp4d_check.argtypes = [vp]
         L.vlp4d_kernel_launches.argtypes = []
+        L.vlp4d_field_rho_noalloc.argtypes = [vp, i, i, i, i, i, d, d, vp, vp]
         for n in EXPORTS:
             if n not in ("vlp4d_last_error", "vlp4d_kernel_launches"):
                 getattr(L, n).restype = C.c_int
@@ -302,6 +304,17 @@ class Context:
 
     def print_fxvx(self, fn, path):
         _check(lib().vlp4d_print_fxvx(self.h, self._f(fn), str(path).encode()))
+
+
+def field_rho_noalloc(f, rho, nxmax, dvx, dvy, stream=None):
+    """vlp4d_field_rho_noalloc: the velocity moment of f into rho (FP64, (ny, nx))
+    without a context and without allocating device memory."""
+    import torch
+
+    dtype = F64 if f.dtype == torch.float64 else F32
+    nx, ny, nvx, nvy = (int(v) for v in nxmax)
+    _check(lib().vlp4d_field_rho_noalloc(C.c_void_p(f.data_ptr()), dtype, nx, ny, nvx, nvy, float(dvx), float(dvy),
+                                         C.c_void_p(rho.data_ptr()), _stream_ptr(stream)))
 
 
 def transpose(a, out, stream=None):
