@@ -15,10 +15,15 @@ namespace vlp4d {
 
 namespace {
 
-// FP32 copy of a line's weights (used by the FP32-storage difference form,
-// stencil.cuh, which never reads the centre weight w[2]).
+// FP32 difference weights of a line for the adjacent-difference form of
+// stencil.cuh: v = (-w0, -(w0+w1), w3+w4+w5, w4+w5, w5), summed in FP64.
 __host__ __device__ inline void weights_to_f32(const double w[6], float wf[6]) {
-  for (int k = 0; k < 6; ++k) wf[k] = (float)w[k];
+  wf[0] = (float)(-w[0]);
+  wf[1] = (float)(-(w[0] + w[1]));
+  wf[2] = (float)(w[3] + w[4] + w[5]);
+  wf[3] = (float)(w[4] + w[5]);
+  wf[4] = (float)w[5];
+  wf[5] = 0.0f;
 }
 
 // One v-line per (ix, iy): displacement dt*E(ix, iy) (advection.hpp:243, 306).

@@ -40,72 +40,92 @@ struct PlaneArgs {
   int cpp;     // chunks per plane = ny / R
   int halo;    // 5 when the y sweep runs, else 0
   int stages;  // pipeline depth
-  int rt;      // output rows per thread task in phase Y (divides R)
   StencilTable tx, ty;
   double *rho_part;  // [G][nx*ny] partial moments, when the moment is fused
   int *err;
 };
 
-// Elements a0..a0+11 (mod nx) of a shared row, a0 a multiple of 4, nx a
-// multiple of 4: three aligned 4-vectors, so no access straddles the wrap.
-template <typename T>
-__device__ __forceinline__ void load12(const T *row, int a0, int nx, T (&v)[12]) {
-  T q[4];
-#pragma unroll
-  for (int b = 0; b < 3; ++b) {
-    load4(row + a0, q);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) v[4 * b + i] = q[i];
-    a0 += 4;
-    if (a0 >= nx) a0 -= nx;
-  }
+// Wraps a column index below 3*nx back into [0, nx) (two wraps happen only
+// for nx = 4, where o0 + 8 = 8).
+template <int NX>
+__device__ __forceinline__ int wrap_col(int c, int nx) {
+  if (NX && (NX & (NX - 1)) == 0) return c & (NX - 1);
+  c = c >= nx ? c - nx : c;
+  return c >= nx ? c - nx : c;
 }
 
-// Four x-swept outputs at columns c0..c0+3 of one staged row; r = (c0+mx)%4
-// is uniform over the CTA, so the switch does not diverge.
+// Four x-swept outputs from the twelve staged values t[0..11] starting at the
+// aligned column a0 = c0 + mx - r; output q uses t[r+q .. r+q+5].  r is the
+// same for the whole CTA (c0 is a multiple of 4), so the switch is uniform.
+template <int R_>
+__device__ __forceinline__ void x4_from(const double (&t)[12], const double (&w)[6], double (&o)[4]) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    o[q] = interp6(w, t[R_ + q], t[R_ + q + 1], t[R_ + q + 2], t[R_ + q + 3], t[R_ + q + 4], t[R_ + q + 5]);
+}
+template <int R_>
+__device__ __forceinline__ void x4_from(const float (&t)[12], const float (&v)[6], float (&o)[4]) {
+  float d[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) d[j] = t[R_ + j + 1] - t[R_ + j];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) o[q] = interp_diff(v, t[R_ + q + 2], d[q], d[q + 1], d[q + 2], d[q + 3], d[q + 4]);
+}
 template <typename T>
-__device__ __forceinline__ void sweep_x4(const T *row, int c0, int mx, int nx, const T (&w)[6], T (&o)[4]) {
-  int base = c0 + mx;
-  if (base >= nx) base -= nx;
-  const int r = base & 3;
-  T v[12];
-  load12(row, base - r, nx, v);
-#define VLP4D_SX(R_)                                                                                 \
-  _Pragma("unroll") for (int q = 0; q < 4; ++q) o[q] =                                              \
-      interp6(w, v[R_ + q], v[R_ + q + 1], v[R_ + q + 2], v[R_ + q + 3], v[R_ + q + 4], v[R_ + q + 5])
+__device__ __forceinline__ void sweep_x4(const T (&t)[12], int r, const T (&w)[6], T (&o)[4]) {
   switch (r) {
-    case 0: VLP4D_SX(0); break;
-    case 1: VLP4D_SX(1); break;
-    case 2: VLP4D_SX(2); break;
-    default: VLP4D_SX(3); break;
+    case 0: x4_from<0>(t, w, o); break;
+    case 1: x4_from<1>(t, w, o); break;
+    case 2: x4_from<2>(t, w, o); break;
+    default: x4_from<3>(t, w, o); break;
   }
-#undef VLP4D_SX
 }
 
-__device__ __forceinline__ void rho_add4(double *p, const float (&o)[4]) {
-  double2 a = reinterpret_cast<double2 *>(p)[0], b = reinterpret_cast<double2 *>(p)[1];
-  a.x += (double)o[0]; a.y += (double)o[1]; b.x += (double)o[2]; b.y += (double)o[3];
-  reinterpret_cast<double2 *>(p)[0] = a;
-  reinterpret_cast<double2 *>(p)[1] = b;
+// RT outputs of a column quad from rows y[0..RT+4] along y.
+template <int RT>
+__device__ __forceinline__ void sweep_y(const double (&y)[RT + 5][4], const double (&w)[6], double (&o)[RT][4]) {
+#pragma unroll
+  for (int i = 0; i < RT; ++i)
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      o[i][q] = interp6(w, y[i][q], y[i + 1][q], y[i + 2][q], y[i + 3][q], y[i + 4][q], y[i + 5][q]);
 }
-__device__ __forceinline__ void rho_add4(double *p, const double (&o)[4]) {
-  double2 a = reinterpret_cast<double2 *>(p)[0], b = reinterpret_cast<double2 *>(p)[1];
-  a.x += o[0]; a.y += o[1]; b.x += o[2]; b.y += o[3];
-  reinterpret_cast<double2 *>(p)[0] = a;
-  reinterpret_cast<double2 *>(p)[1] = b;
+template <int RT>
+__device__ __forceinline__ void sweep_y(const float (&y)[RT + 5][4], const float (&v)[6], float (&o)[RT][4]) {
+  float d[RT + 4][4];
+#pragma unroll
+  for (int j = 0; j < RT + 4; ++j)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) d[j][q] = y[j + 1][q] - y[j][q];
+#pragma unroll
+  for (int i = 0; i < RT; ++i)
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      o[i][q] = interp_diff(v, y[i + 2][q], d[i][q], d[i + 1][q], d[i + 2][q], d[i + 3][q], d[i + 4][q]);
 }
 
-template <typename T, bool DX, bool DY, bool RHO>
+// Template parameters: element type, row width (0 = runtime a.nx), output
+// rows per thread in the y phase, which sweeps run, moment epilogue.
+// Thread t owns column quad c0 = 4*(t % (nx/4)) and row group t / (nx/4)
+// for the whole kernel; blockDim = (nx/4) * (R/RT).
+template <typename T, int NX, int RT, bool DX, bool DY, bool RHO>
 __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
-  const int nx = a.nx, ny = a.ny, R = a.R, S = a.stages;
-  const int vrows = R + a.halo;
+  const int nx = NX ? NX : a.nx;
+  const int ny = a.ny, R = a.R, S = a.stages;
+  const int vrows = R + (DY ? 5 : 0);
+  const int ncg = nx >> 2;
   const size_t slot_elems = (size_t)vrows * nx;
   const uint32_t slot_bytes = (uint32_t)(slot_elems * sizeof(T));
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
   T *slots = reinterpret_cast<T *>(smem + kBarBytes);
   T *xs = slots + (size_t)S * slot_elems;  // x-swept rows (x and y both on)
-  double *rho_s = reinterpret_cast<double *>(xs + ((DX && DY) ? slot_elems : 0));
+
+  const int cg = threadIdx.x % ncg;
+  const int rg = threadIdx.x / ncg;
+  const int RG = blockDim.x / ncg;  // row groups; R == RG * RT
+  const int c0 = cg * 4;
+  const int r0 = rg * RT;
 
   const int chunk = blockIdx.x % a.cpp;
   const int G = gridDim.x / a.cpp;
@@ -118,11 +138,9 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
     mbar_fence_init();
   }
-  if (RHO)
-    for (int e = threadIdx.x; e < R * nx; e += blockDim.x) rho_s[e] = 0.0;
   __syncthreads();
 
-  // Thread 0: stage the R + halo input rows of item `it` into its slot.
+  // Thread 0: stage the input rows of item `it` into its slot.
   auto issue = [&](long long it) {
     const long long p = g + it * G;
     int phys = chunk * R;
@@ -148,7 +166,12 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
     for (long long it = 0; it < pre; ++it) issue(it);
   }
 
-  const int ncg = nx >> 2;
+  double racc[RHO ? RT : 1][4];
+#pragma unroll
+  for (int i = 0; i < (RHO ? RT : 1); ++i)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) racc[i][q] = 0.0;
+
   for (long long it = 0; it < n_items; ++it) {
     const int slot = (int)(it % S);
     const bool ok = mbar_wait_bounded(&bars[slot], (uint32_t)((it / S) & 1));
@@ -156,56 +179,53 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
     const int ivx = (int)(p % a.nvx), ivy = (int)(p / a.nvx);
     const T *in = slots + (size_t)slot * slot_elems;
     T *outp = static_cast<T *>(a.fout) + p * plane_elems + (long long)chunk * R * nx;
-    T wx[6], wy[6];
-    int mx = 0;
-    if (DX) {
-      mx = __ldg(a.tx.m + ivx);
-      load_weights(WeightsOf<T>::get(a.tx), ivx, wx);
-    }
-    if (DY) load_weights(WeightsOf<T>::get(a.ty), ivy, wy);
 
-    if (DX) {  // Phase X: every staged row, four columns per task.
-      const int tasks = vrows * ncg;
-      for (int t = threadIdx.x; t < tasks; t += blockDim.x) {
-        const int v = t / ncg, c0 = (t - v * ncg) * 4;
+    if (DX) {  // Phase X: staged rows rg, rg+RG, ...; this thread's column quad.
+      T wx[6];
+      load_weights(WeightsOf<T>::get(a.tx), ivx, wx);
+      int base = c0 + __ldg(a.tx.m + ivx);
+      base = wrap_col<NX>(base, nx);
+      const int rr = base & 3;
+      const int o0 = base - rr, o1 = wrap_col<NX>(o0 + 4, nx), o2 = wrap_col<NX>(o0 + 8, nx);
+      for (int v = rg; v < vrows; v += RG) {
+        const T *row = in + (size_t)v * nx;
+        T t[12], q4[4];
+        load4(row + o0, q4);
+        t[0] = q4[0]; t[1] = q4[1]; t[2] = q4[2]; t[3] = q4[3];
+        load4(row + o1, q4);
+        t[4] = q4[0]; t[5] = q4[1]; t[6] = q4[2]; t[7] = q4[3];
+        load4(row + o2, q4);
+        t[8] = q4[0]; t[9] = q4[1]; t[10] = q4[2]; t[11] = q4[3];
         T o[4];
-        sweep_x4(in + (size_t)v * nx, c0, mx, nx, wx, o);
+        sweep_x4(t, rr, wx, o);
         if (DY) {
           store4(xs + (size_t)v * nx + c0, o);
         } else {
           store4(outp + (size_t)v * nx + c0, o);
-          if (RHO) rho_add4(rho_s + (size_t)v * nx + c0, o);
         }
       }
     }
-    if (DY) {  // Phase Y: rt consecutive output rows x four columns per task.
+    if (DY) {  // Phase Y: rows r0 .. r0+RT-1 of this thread's column quad.
       if (DX) __syncthreads();
-      const T *src = DX ? xs : in;
-      const int rt = a.rt;
-      const int tasks = (R / rt) * ncg;
-      for (int t = threadIdx.x; t < tasks; t += blockDim.x) {
-        const int rg = t / ncg, c0 = (t - rg * ncg) * 4, r0 = rg * rt;
-        T w0[4], w1[4], w2[4], w3[4], w4[4], w5[4];
-        load4(src + (size_t)(r0 + 0) * nx + c0, w1);
-        load4(src + (size_t)(r0 + 1) * nx + c0, w2);
-        load4(src + (size_t)(r0 + 2) * nx + c0, w3);
-        load4(src + (size_t)(r0 + 3) * nx + c0, w4);
-        load4(src + (size_t)(r0 + 4) * nx + c0, w5);
-        for (int i = 0; i < rt; ++i) {
+      T wy[6];
+      load_weights(WeightsOf<T>::get(a.ty), ivy, wy);
+      const T *src = (DX ? xs : in) + (size_t)r0 * nx + c0;
+      T y[RT + 5][4];
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            w0[q] = w1[q]; w1[q] = w2[q]; w2[q] = w3[q]; w3[q] = w4[q]; w4[q] = w5[q];
-          }
-          load4(src + (size_t)(r0 + i + 5) * nx + c0, w5);
-          T o[4];
+      for (int j = 0; j < RT + 5; ++j) load4(src + (size_t)j * nx, y[j]);
+      T o[RT][4];
+      sweep_y<RT>(y, wy, o);
+      T *dst = outp + (size_t)r0 * nx + c0;
 #pragma unroll
-          for (int q = 0; q < 4; ++q) o[q] = interp6(wy, w0[q], w1[q], w2[q], w3[q], w4[q], w5[q]);
-          store4(outp + (size_t)(r0 + i) * nx + c0, o);
-          if (RHO) rho_add4(rho_s + (size_t)(r0 + i) * nx + c0, o);
+      for (int i = 0; i < RT; ++i) {
+        store4(dst + (size_t)i * nx, o[i]);
+        if (RHO) {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) racc[i][q] += (double)o[i][q];
         }
       }
     }
-    // Slot (and the x-swept buffer) are free once every thread is here.
+    // The slot (and the x-swept buffer) are free once every thread is here.
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) {
         atomicExch(a.err, 1);
@@ -218,8 +238,12 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
     if (threadIdx.x == 0 && it + S < n_items) issue(it + S);
   }
   if (RHO) {
-    double *dst = a.rho_part + (long long)g * plane_elems + (long long)chunk * R * nx;
-    for (int e = threadIdx.x; e < R * nx; e += blockDim.x) dst[e] = rho_s[e];
+    double *dst = a.rho_part + (long long)g * plane_elems + ((long long)chunk * R + r0) * nx + c0;
+#pragma unroll
+    for (int i = 0; i < RT; ++i) {
+      reinterpret_cast<double2 *>(dst + (size_t)i * nx)[0] = make_double2(racc[i][0], racc[i][1]);
+      reinterpret_cast<double2 *>(dst + (size_t)i * nx)[1] = make_double2(racc[i][2], racc[i][3]);
+    }
   }
 }
 
@@ -240,51 +264,55 @@ int env_int(const char *name, int dflt) {
   return v && *v ? atoi(v) : dflt;
 }
 
-size_t plane_smem(int R, int halo, int nx, size_t elem, int stages, bool dx, bool dy, bool rho) {
+size_t plane_smem(int R, int halo, int nx, size_t elem, int stages, bool dx, bool dy) {
   const size_t slot = (size_t)(R + halo) * nx * elem;
-  return kBarBytes + stages * slot + ((dx && dy) ? slot : 0) + (rho ? (size_t)R * nx * sizeof(double) : 0);
+  return kBarBytes + stages * slot + ((dx && dy) ? slot : 0);
 }
 
-// Chooses the chunk height R (a divisor of ny), the pipeline depth and the
-// block size.  Preference: the tallest chunk (least halo re-read) that still
-// lets two CTAs share an SM, else one CTA per SM.  VLP4D_PLANE_R and
-// VLP4D_PLANE_STAGES override the choice for tuning sweeps.
-bool plane_config(const vlp4d_ctx *c, bool dx, bool dy, bool rho, PlaneCfg &cfg) {
+// Chooses the chunk height R (a divisor of ny), rows per thread RT (4 when R
+// allows, else 1), the pipeline depth and the block size nx/4 * R/RT.
+// Preference: the tallest chunk (least halo re-read) whose CTA fits twice on
+// an SM, else once.  VLP4D_PLANE_R / _STAGES / _RT override for tuning.
+bool plane_config(const vlp4d_ctx *c, bool dx, bool dy, PlaneCfg &cfg) {
   const int nx = c->g.n[0], ny = c->g.n[1];
   const size_t elem = c->elem;
   if (nx % 4 != 0 || nx > 2048) return false;
   const int halo = dy ? 5 : 0;
-  cfg.stages = env_int("VLP4D_PLANE_STAGES", 3);
+  cfg.stages = env_int("VLP4D_PLANE_STAGES", 4);
   if (cfg.stages < 2 || cfg.stages > kMaxStages) return false;
-  const int forced = env_int("VLP4D_PLANE_R", 0);
+  const int forced_r = env_int("VLP4D_PLANE_R", 0);
+  const int forced_rt = env_int("VLP4D_PLANE_RT", 0);
+  const int ncg = nx / 4;
   const size_t two_per_sm = 110 * 1024, one_per_sm = 220 * 1024;
-  int best = 0;
+  int best = 0, best_rt = 1;
   for (const size_t budget : {two_per_sm, one_per_sm}) {
     for (int R = ny < 64 ? ny : 64; R >= 1 && !best; --R) {
       if (ny % R) continue;
-      if (forced && R != forced) continue;
-      if (plane_smem(R, halo, nx, elem, cfg.stages, dx, dy, rho) <= budget) best = R;
+      if (forced_r && R != forced_r) continue;
+      int rt = forced_rt ? forced_rt : (R % 4 == 0 ? 4 : 1);
+      if (rt != 1 && rt != 4) continue;
+      if (R % rt) continue;
+      const int threads = ncg * (R / rt);
+      if (threads > 512 || threads < 1) continue;
+      if (plane_smem(R, halo, nx, elem, cfg.stages, dx, dy) <= budget) {
+        best = R;
+        best_rt = rt;
+      }
     }
     if (best) break;
   }
   if (!best) return false;
   cfg.R = best;
-  cfg.rt = best % 4 == 0 ? 4 : (best % 2 == 0 ? 2 : 1);
+  cfg.rt = best_rt;
   cfg.cpp = ny / best;
-  const int ytasks = dy ? (best / cfg.rt) * (nx / 4) : 0;
-  const int xtasks = dx ? (best + halo) * (nx / 4) : 0;
-  int threads = ytasks > 0 ? ytasks : xtasks;
-  threads = ((threads + 31) / 32) * 32;
-  if (threads < 64) threads = 64;
-  if (threads > 512) threads = 512;
-  cfg.threads = threads;
-  cfg.smem = plane_smem(best, halo, nx, elem, cfg.stages, dx, dy, rho);
+  cfg.threads = ncg * (best / best_rt);
+  cfg.smem = plane_smem(best, halo, nx, elem, cfg.stages, dx, dy);
   return true;
 }
 
-template <typename T, bool DX, bool DY, bool RHO>
+template <typename T, int NX, int RT, bool DX, bool DY, bool RHO>
 int run_plane(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, cudaStream_t s) {
-  auto kern = k_plane<T, DX, DY, RHO>;
+  auto kern = k_plane<T, NX, RT, DX, DY, RHO>;
   VLP4D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
   int per_sm = 0;
   VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, cfg.threads, cfg.smem));
@@ -301,6 +329,25 @@ int run_plane(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, cudaStream_t s
   return VLP4D_OK;
 }
 
+// Row-width specialisations: the common power-of-two widths get a
+// compile-time nx (index math folds, wraps become masks), others run with
+// the width read at run time.
+template <typename T, int RT, bool DX, bool DY, bool RHO>
+int run_plane_nx(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, cudaStream_t s) {
+  switch (args.nx) {
+    case 64: return run_plane<T, 64, RT, DX, DY, RHO>(c, args, cfg, s);
+    case 128: return run_plane<T, 128, RT, DX, DY, RHO>(c, args, cfg, s);
+    case 256: return run_plane<T, 256, RT, DX, DY, RHO>(c, args, cfg, s);
+    default: return run_plane<T, 0, RT, DX, DY, RHO>(c, args, cfg, s);
+  }
+}
+
+template <typename T, bool DX, bool DY, bool RHO>
+int run_plane_rt(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, cudaStream_t s) {
+  if (cfg.rt == 4) return run_plane_nx<T, 4, DX, DY, RHO>(c, args, cfg, s);
+  return run_plane_nx<T, 1, DX, DY, RHO>(c, args, cfg, s);
+}
+
 }  // namespace
 
 // Returns VLP4D_ERR_UNSUPPORTED (without launching anything) when the shape
@@ -312,7 +359,7 @@ int launch_advect_xy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTabl
   if (((uintptr_t)fn & 15) || ((uintptr_t)fnp1 & 15)) return VLP4D_ERR_UNSUPPORTED;
   if (!do_x && !do_y) return VLP4D_ERR_UNSUPPORTED;
   PlaneCfg cfg;
-  if (!plane_config(c, do_x, do_y, with_rho, cfg)) return VLP4D_ERR_UNSUPPORTED;
+  if (!plane_config(c, do_x, do_y, cfg)) return VLP4D_ERR_UNSUPPORTED;
   PlaneArgs a;
   a.fin = fn;
   a.fout = fnp1;
@@ -324,13 +371,12 @@ int launch_advect_xy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTabl
   a.cpp = cfg.cpp;
   a.halo = do_y ? 5 : 0;
   a.stages = cfg.stages;
-  a.rt = cfg.rt;
   if (tx) a.tx = *tx;
   if (ty) a.ty = *ty;
   a.rho_part = c->rho_part;
   a.err = c->d_err;
   int rc;
-#define VLP4D_PLANE(T, DX, DY, RHO) rc = run_plane<T, DX, DY, RHO>(c, a, cfg, s)
+#define VLP4D_PLANE(T, DX, DY, RHO) rc = run_plane_rt<T, DX, DY, RHO>(c, a, cfg, s)
   if (c->dtype == VLP4D_F64) {
     if (do_x && do_y) { if (with_rho) VLP4D_PLANE(double, true, true, true); else VLP4D_PLANE(double, true, true, false); }
     else if (do_x) VLP4D_PLANE(double, true, false, false);

@@ -45,6 +45,22 @@ struct VslabArgs {
 // Signed form of a tap offset m in [0, n): the shift in cells, in (-n/2, n/2].
 __device__ __forceinline__ int signed_offset(int m, int n) { return m > n / 2 ? m - n : m; }
 
+// vx sweep of V outputs from V+5 taps (plain FP64 form / FP32 adjacent
+// differences shared between neighbouring outputs).
+template <int V>
+__device__ __forceinline__ void vx_sweep(const double (&t)[V + 5], const double (&w)[6], double (&o)[V]) {
+#pragma unroll
+  for (int i = 0; i < V; ++i) o[i] = interp6(w, t[i], t[i + 1], t[i + 2], t[i + 3], t[i + 4], t[i + 5]);
+}
+template <int V>
+__device__ __forceinline__ void vx_sweep(const float (&t)[V + 5], const float (&w)[6], float (&o)[V]) {
+  float d[V + 4];
+#pragma unroll
+  for (int j = 0; j < V + 4; ++j) d[j] = t[j + 1] - t[j];
+#pragma unroll
+  for (int i = 0; i < V; ++i) o[i] = interp_diff(w, t[i + 2], d[i], d[i + 1], d[i + 2], d[i + 3], d[i + 4]);
+}
+
 template <typename T, bool DVX, bool DVY, int V>
 __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorMap tin, VslabArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -100,79 +116,93 @@ __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorM
   if (threadIdx.x == 0)
     for (int s = 0; s < S; ++s) issue_next();
 
-  const long long vstride = a.nxy;                      // consecutive ivx
-  const long long ystride = (long long)a.nxy * nvx;     // consecutive ivy
-  long long k = 0;                                      // slabs consumed
+  const long long vstride = a.nxy;                   // consecutive ivx
+  const long long ystride = (long long)a.nxy * nvx;  // consecutive ivy
+  long long k = 0;                                   // slabs consumed
   for (long long item = blockIdx.x; item < a.nitems; item += gridDim.x) {
     int cnt, start, cc;
     item_range(item, cnt, start, cc);
     const int sg = (int)(item % a.nseg);
     const long long ixy = (long long)cc * C + col;
     T wvx[6], wvy[6];
-    int mvx = 0, lag0 = 0;
-    if (DVX) {
-      mvx = __ldg(a.tvx.m + ixy);
-      load_weights(WeightsOf<T>::get(a.tvx), ixy, wvx);
+    int lag0 = 0;
+    // Shared-memory offsets of this thread's V+5 vx taps ([ivx][c] layout),
+    // the same for every slab of the item.
+    int off[V + 5];
+    {
+      int j = vx0;
+      if (DVX) {
+        j += __ldg(a.tvx.m + ixy);
+        if (j >= nvx) j -= nvx;
+        load_weights(WeightsOf<T>::get(a.tvx), ixy, wvx);
+      }
+#pragma unroll
+      for (int q = 0; q < V + 5; ++q) {
+        off[q] = j * C + col;
+        if (++j == nvx) j = 0;
+      }
     }
     if (DVY) {
       lag0 = 5 + signed_offset(__ldg(a.tvy.m + ixy), nvy) - a.span[cc].x;
       load_weights(WeightsOf<T>::get(a.tvy), ixy, wvy);
     }
-    T *outc = static_cast<T *>(a.fout) + ixy + vstride * vx0 + ystride * (long long)sg * a.Q;
-    T win[6][V];
+    // Output pointer of the next row this thread writes.
+    T *orow = static_cast<T *>(a.fout) + ixy + vstride * vx0 + ystride * (long long)sg * a.Q;
+    T win[6][V];  // ring of vx-swept rows, slot = t % 6 (static after unrolling)
 #pragma unroll
     for (int j = 0; j < 6; ++j)
 #pragma unroll
       for (int i = 0; i < V; ++i) win[j][i] = T(0);
 
-    for (int t = 0; t < cnt; ++t, ++k) {
-      const int slot = (int)(k % S);
-      const bool ok = mbar_wait_bounded(&bars[slot], (uint32_t)((k / S) & 1));
-      const T *sl = slabs + (size_t)slot * slab_elems;  // [ivx][c]
-      T tmp[V];
-      if (DVX) {
-        int j = vx0 + mvx;
-        if (j >= nvx) j -= nvx;
-        T tap[V + 5];
+    for (int t0 = 0; t0 < cnt; t0 += 6) {
 #pragma unroll
-        for (int q = 0; q < V + 5; ++q) {
-          tap[q] = sl[(size_t)j * C + col];
-          if (++j == nvx) j = 0;
+      for (int u = 0; u < 6; ++u) {
+        const int t = t0 + u;
+        if (t >= cnt) break;  // uniform over the CTA
+        const int slot = (int)(k % S);
+        const bool ok = mbar_wait_bounded(&bars[slot], (uint32_t)((k / S) & 1));
+        const T *sl = slabs + (size_t)slot * slab_elems;
+        if (DVX) {
+          T tap[V + 5];
+#pragma unroll
+          for (int q = 0; q < V + 5; ++q) tap[q] = sl[off[q]];
+          vx_sweep<V>(tap, wvx, win[u]);
+        } else {
+#pragma unroll
+          for (int i = 0; i < V; ++i) win[u][i] = sl[off[i]];
         }
+        bool emit = true;
+        if (DVY) {
+          const int e = t - lag0;
+          emit = e >= 0 && e < a.Q;
+        }
+        if (emit) {
+          T *o = orow;
 #pragma unroll
-        for (int i = 0; i < V; ++i) tmp[i] = interp6(wvx, tap[i], tap[i + 1], tap[i + 2], tap[i + 3], tap[i + 4], tap[i + 5]);
-      } else {
-#pragma unroll
-        for (int i = 0; i < V; ++i) tmp[i] = sl[(size_t)(vx0 + i) * C + col];
+          for (int i = 0; i < V; ++i) {
+            T val;
+            if (DVY)  // rows t-5 .. t sit in slots u+1 .. u+6 (mod 6)
+              val = interp6(wvy, win[(u + 1) % 6][i], win[(u + 2) % 6][i], win[(u + 3) % 6][i],
+                            win[(u + 4) % 6][i], win[(u + 5) % 6][i], win[u][i]);
+            else
+              val = win[u][i];
+            *o = val;
+            o += vstride;
+          }
+          orow += ystride;
+        }
+        // The slot is free once every thread is here.
+        if (__syncthreads_or(!ok)) {
+          if (threadIdx.x == 0) {
+            atomicExch(a.err, 1);
+            for (long long q = k; q < p_k; ++q) mbar_wait_bounded(&bars[q % S], (uint32_t)((q / S) & 1));
+          }
+          __syncthreads();
+          return;
+        }
+        if (threadIdx.x == 0) issue_next();
+        ++k;
       }
-      if (DVY) {
-#pragma unroll
-        for (int i = 0; i < V; ++i) {
-          win[0][i] = win[1][i]; win[1][i] = win[2][i]; win[2][i] = win[3][i];
-          win[3][i] = win[4][i]; win[4][i] = win[5][i]; win[5][i] = tmp[i];
-        }
-        const int e = t - lag0;
-        if (e >= 0 && e < a.Q) {
-          T *o = outc + ystride * e;
-#pragma unroll
-          for (int i = 0; i < V; ++i)
-            o[vstride * i] = interp6(wvy, win[0][i], win[1][i], win[2][i], win[3][i], win[4][i], win[5][i]);
-        }
-      } else {
-        T *o = outc + ystride * t;
-#pragma unroll
-        for (int i = 0; i < V; ++i) o[vstride * i] = tmp[i];
-      }
-      // The slot is free once every thread is here.
-      if (__syncthreads_or(!ok)) {
-        if (threadIdx.x == 0) {
-          atomicExch(a.err, 1);
-          for (long long q = k; q < p_k; ++q) mbar_wait_bounded(&bars[q % S], (uint32_t)((q / S) & 1));
-        }
-        __syncthreads();
-        return;
-      }
-      if (threadIdx.x == 0) issue_next();
     }
   }
 }

@@ -60,7 +60,8 @@ struct Grid {
 };
 
 // Device-side line stencil tables, one entry per swept line.
-//   m[line] : tap offset, w[6*line + k] : weights (FP64 and an FP32 copy).
+//   m[line] : tap offset, w[6*line + k] : FP64 weights,
+//   wf[6*line + j] : FP32 difference weights (stencil.cuh), j < 5.
 struct StencilTable {
   int *m = nullptr;
   double *w = nullptr;

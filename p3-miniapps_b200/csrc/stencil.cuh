@@ -2,12 +2,15 @@
 // per-line weight loads shared by the advection kernels.
 //
 // FP64 (the reference's arithmetic, advection.hpp:128-135): out = sum_k w_k f_k.
-// FP32 storage: out = f_2 + sum_{k != 2} w_k (f_k - f_2).  The two are equal in
-// exact arithmetic because the weights sum to one.  In FP32 the difference
-// form makes every rounding term (weights, products, partial sums)
-// proportional to the local variation of f instead of to f itself; with the
-// plain form, the FP32-rounded weights of a line are re-applied identically
-// every step and their bias accumulates in the field energy.
+// FP32 storage, adjacent-difference form:
+//   out = f_2 + sum_{j=0..4} v_j (f_{j+1} - f_j),
+//   v = (-w0, -(w0+w1), w3+w4+w5, w4+w5, w5)   (from the FP64 weights),
+// equal to the plain form in exact arithmetic because the weights sum to one.
+// In FP32 it makes every rounding term (weights, products, partial sums)
+// proportional to the local variation of f instead of to f itself: with the
+// plain form the FP32-rounded weights of a line are re-applied identically
+// every step and their bias accumulates in the field energy.  Neighbouring
+// outputs share their differences, which the fused kernels exploit.
 #pragma once
 
 #include "internal.cuh"
@@ -25,14 +28,21 @@ __device__ __forceinline__ double interp6(const double (&w)[6], double f0, doubl
   return acc;
 }
 
-__device__ __forceinline__ float interp6(const float (&w)[6], float f0, float f1, float f2, float f3, float f4,
-                                         float f5) {
-  float acc = w[0] * (f0 - f2);
-  acc = fmaf(w[1], f1 - f2, acc);
-  acc = fmaf(w[3], f3 - f2, acc);
-  acc = fmaf(w[4], f4 - f2, acc);
-  acc = fmaf(w[5], f5 - f2, acc);
+// The adjacent-difference form on precomputed differences d_j = f_{j+1} - f_j.
+__device__ __forceinline__ float interp_diff(const float (&v)[6], float f2, float d0, float d1, float d2, float d3,
+                                             float d4) {
+  float acc = v[0] * d0;
+  acc = fmaf(v[1], d1, acc);
+  acc = fmaf(v[2], d2, acc);
+  acc = fmaf(v[3], d3, acc);
+  acc = fmaf(v[4], d4, acc);
   return f2 + acc;
+}
+
+// v holds the difference weights in slots 0..4.
+__device__ __forceinline__ float interp6(const float (&v)[6], float f0, float f1, float f2, float f3, float f4,
+                                         float f5) {
+  return interp_diff(v, f2, f1 - f0, f2 - f1, f3 - f2, f4 - f3, f5 - f4);
 }
 
 template <typename T>
