@@ -104,6 +104,17 @@ __device__ __forceinline__ void sweep_y(const float (&y)[RT + 5][4], const float
       o[i][q] = interp_diff(v, y[i + 2][q], d[i][q], d[i + 1][q], d[i + 2][q], d[i + 3][q], d[i + 4][q]);
 }
 
+// Error exit after a copy timed out: flag it, let the copies already issued
+// for items it .. it+S-1 land (bounded waits), then leave.
+__device__ __noinline__ void plane_abort(const PlaneArgs &a, uint64_t *bars, long long it, long long n_items, int S) {
+  if (threadIdx.x == 0) {
+    atomicExch(a.err, 1);
+    const long long last = n_items < it + S ? n_items : it + S;
+    for (long long k = it; k < last; ++k) mbar_wait_bounded(&bars[k % S], (uint32_t)((k / S) & 1));
+  }
+  __syncthreads();
+}
+
 // Template parameters: element type, row width (0 = runtime a.nx), output
 // rows per thread in the y phase, which sweeps run, moment epilogue.
 // Thread t owns column quad c0 = 4*(t % (nx/4)) and row group t / (nx/4)
@@ -119,7 +130,9 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
   const uint32_t slot_bytes = (uint32_t)(slot_elems * sizeof(T));
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
   T *slots = reinterpret_cast<T *>(smem + kBarBytes);
-  T *xs = slots + (size_t)S * slot_elems;  // x-swept rows (x and y both on)
+  // Two x-swept buffers (x and y both on): item it writes xs[it & 1], so the
+  // only barrier per item is the one between phase X and phase Y.
+  T *xs_base = slots + (size_t)S * slot_elems;
 
   const int cg = threadIdx.x % ncg;
   const int rg = threadIdx.x / ncg;
@@ -179,6 +192,7 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
     const int ivx = (int)(p % a.nvx), ivy = (int)(p / a.nvx);
     const T *in = slots + (size_t)slot * slot_elems;
     T *outp = static_cast<T *>(a.fout) + p * plane_elems + (long long)chunk * R * nx;
+    T *xs = xs_base + (size_t)(it & 1) * slot_elems;
 
     if (DX) {  // Phase X: staged rows rg, rg+RG, ...; this thread's column quad.
       T wx[6];
@@ -205,8 +219,15 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
         }
       }
     }
+    if (DX && DY) {
+      // xs is complete and the staged slot is no longer read: refill it.
+      if (__syncthreads_or(!ok)) {
+        plane_abort(a, bars, it, n_items, S);
+        return;
+      }
+      if (threadIdx.x == 0 && it + S < n_items) issue(it + S);
+    }
     if (DY) {  // Phase Y: rows r0 .. r0+RT-1 of this thread's column quad.
-      if (DX) __syncthreads();
       T wy[6];
       load_weights(WeightsOf<T>::get(a.ty), ivy, wy);
       const T *src = (DX ? xs : in) + (size_t)r0 * nx + c0;
@@ -225,14 +246,10 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
         }
       }
     }
-    // The slot (and the x-swept buffer) are free once every thread is here.
+    if (DX && DY) continue;
+    // One sweep only: the slot is free once every thread is here.
     if (__syncthreads_or(!ok)) {
-      if (threadIdx.x == 0) {
-        atomicExch(a.err, 1);
-        const long long last = n_items < it + S ? n_items : it + S;
-        for (long long k = it; k < last; ++k) mbar_wait_bounded(&bars[k % S], (uint32_t)((k / S) & 1));
-      }
-      __syncthreads();
+      plane_abort(a, bars, it, n_items, S);
       return;
     }
     if (threadIdx.x == 0 && it + S < n_items) issue(it + S);
@@ -266,7 +283,7 @@ int env_int(const char *name, int dflt) {
 
 size_t plane_smem(int R, int halo, int nx, size_t elem, int stages, bool dx, bool dy) {
   const size_t slot = (size_t)(R + halo) * nx * elem;
-  return kBarBytes + stages * slot + ((dx && dy) ? slot : 0);
+  return kBarBytes + stages * slot + ((dx && dy) ? 2 * slot : 0);
 }
 
 // Chooses the chunk height R (a divisor of ny), rows per thread RT (4 when R
@@ -278,12 +295,12 @@ bool plane_config(const vlp4d_ctx *c, bool dx, bool dy, PlaneCfg &cfg) {
   const size_t elem = c->elem;
   if (nx % 4 != 0 || nx > 2048) return false;
   const int halo = dy ? 5 : 0;
-  cfg.stages = env_int("VLP4D_PLANE_STAGES", 4);
+  cfg.stages = env_int("VLP4D_PLANE_STAGES", 3);
   if (cfg.stages < 2 || cfg.stages > kMaxStages) return false;
   const int forced_r = env_int("VLP4D_PLANE_R", 0);
   const int forced_rt = env_int("VLP4D_PLANE_RT", 0);
   const int ncg = nx / 4;
-  const size_t two_per_sm = 110 * 1024, one_per_sm = 220 * 1024;
+  const size_t two_per_sm = 112 * 1024, one_per_sm = 224 * 1024;
   int best = 0, best_rt = 1;
   for (const size_t budget : {two_per_sm, one_per_sm}) {
     for (int R = ny < 64 ? ny : 64; R >= 1 && !best; --R) {

@@ -26,8 +26,11 @@ namespace vlp4d {
 
 namespace {
 
-constexpr int kBarBytes = 128;
 constexpr int kMaxStages = 12;
+// Header ahead of the slabs: kMaxStages full barriers (8 B each), kMaxStages
+// release counters and the issued-slab counter (4 B each).
+constexpr int kBarBytes = 256;
+static_assert(8 * kMaxStages + 4 * kMaxStages + 4 <= kBarBytes, "slab header overflow");
 
 struct VslabArgs {
   void *fout;
@@ -45,6 +48,19 @@ struct VslabArgs {
 // Signed form of a tap offset m in [0, n): the shift in cells, in (-n/2, n/2].
 __device__ __forceinline__ int signed_offset(int m, int n) { return m > n / 2 ? m - n : m; }
 
+// Error exit of one warp after a copy timed out: flag it, let the copies
+// already issued for slabs k .. issued-1 land (bounded waits), then leave.
+// The other warps reach their own time limits on the slabs this warp no
+// longer releases and leave the same way.
+__device__ __noinline__ void vslab_abort(const VslabArgs &a, uint64_t *bars, const int *issued, long long k, int S) {
+  if ((threadIdx.x & 31) == 0) {
+    atomicExch(a.err, 1);
+    const long long n = *(volatile const int *)issued;
+    for (long long q = k; q < n; ++q) mbar_wait_bounded(&bars[q % S], (uint32_t)((q / S) & 1));
+  }
+  __syncwarp();
+}
+
 // vx sweep of V outputs from V+5 taps (plain FP64 form / FP32 adjacent
 // differences shared between neighbouring outputs).
 template <int V>
@@ -61,67 +77,102 @@ __device__ __forceinline__ void vx_sweep(const float (&t)[V + 5], const float (&
   for (int i = 0; i < V; ++i) o[i] = interp_diff(w, t[i + 2], d[i], d[i + 1], d[i + 2], d[i + 3], d[i + 4]);
 }
 
+// Position in the CTA's slab sequence: item, slab index within the item,
+// slab count and first vy row of the item, column chunk.  Every warp keeps
+// an identical cursor S slabs ahead of the slab it consumes, so whichever
+// warp releases a slot last can refill it without asking anyone.
+struct SlabCursor {
+  long long item;
+  int t, cnt, start, cc;
+};
+
+template <bool DVY>
+__device__ __forceinline__ void cursor_item(const VslabArgs &a, SlabCursor &c) {
+  if (c.item >= a.nitems) return;
+  c.cc = (int)(c.item / a.nseg);
+  const int sg = (int)(c.item % a.nseg);
+  if (DVY) {
+    const int2 sp = a.span[c.cc];
+    c.cnt = a.Q + (sp.y - sp.x) + 5;
+    c.start = sg * a.Q + sp.x;
+  } else {
+    c.cnt = a.Q;
+    c.start = sg * a.Q;
+  }
+}
+
+template <bool DVY>
+__device__ __forceinline__ void cursor_next(const VslabArgs &a, SlabCursor &c) {
+  if (c.item >= a.nitems) return;
+  if (++c.t == c.cnt) {
+    c.t = 0;
+    c.item += gridDim.x;
+    cursor_item<DVY>(a, c);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void issue_slab(const CUtensorMap *tin, const VslabArgs &a, const SlabCursor &c,
+                                           T *slabs, uint64_t *bars, int slot, size_t slab_elems,
+                                           uint32_t slab_bytes) {
+  int row = (c.start + c.t) % a.nvy;
+  if (row < 0) row += a.nvy;
+  mbar_arrive_expect_tx(&bars[slot], slab_bytes);
+  tensor_load_3d(slabs + (size_t)slot * slab_elems, tin, c.cc * a.C, 0, row, &bars[slot]);
+}
+
 template <typename T, bool DVX, bool DVY, int V>
 __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorMap tin, VslabArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // Tensor-copy destinations on a 128-byte boundary whatever the base
   // alignment of dynamic shared memory (the launch adds 128 bytes of slack).
   unsigned char *smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
-  const int C = a.C, nvx = a.nvx, nvy = a.nvy, S = a.stages;
+  const int C = a.C, nvx = a.nvx, S = a.stages;
   const size_t slab_elems = (size_t)C * nvx;
   const uint32_t slab_bytes = (uint32_t)(slab_elems * sizeof(T));
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem);          // S full barriers
+  int *released = reinterpret_cast<int *>(smem + 8 * kMaxStages);  // S release counters
+  int *issued = released + kMaxStages;                          // slabs issued so far
   T *slabs = reinterpret_cast<T *>(smem + kBarBytes);
   const int col = threadIdx.x % C;
   const int vx0 = (threadIdx.x / C) * V;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
 
-  // Slab count and first vy row of an item.
-  auto item_range = [&](long long item, int &cnt, int &start, int &cc) {
-    cc = (int)(item / a.nseg);
-    const int sg = (int)(item % a.nseg);
-    if (DVY) {
-      const int2 sp = a.span[cc];
-      cnt = a.Q + (sp.y - sp.x) + 5;
-      start = sg * a.Q + sp.x;
-    } else {
-      cnt = a.Q;
-      start = sg * a.Q;
-    }
-  };
-
-  // Producer cursor (meaningful in thread 0 only).
-  long long p_item = blockIdx.x, p_k = 0;
-  int p_t = 0, p_cnt = 0, p_start = 0, p_cc = 0;
   if (threadIdx.x == 0) {
-    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&bars[s], 1);
+      released[s] = 0;
+    }
     mbar_fence_init();
-    if (p_item < a.nitems) item_range(p_item, p_cnt, p_start, p_cc);
   }
   __syncthreads();
 
-  auto issue_next = [&]() {
-    if (p_item >= a.nitems) return;
-    int row = (p_start + p_t) % nvy;
-    if (row < 0) row += nvy;
-    const int slot = (int)(p_k % S);
-    mbar_arrive_expect_tx(&bars[slot], slab_bytes);
-    tensor_load_3d(slabs + (size_t)slot * slab_elems, &tin, p_cc * C, 0, row, &bars[slot]);
-    ++p_k;
-    if (++p_t == p_cnt) {
-      p_t = 0;
-      p_item += gridDim.x;
-      if (p_item < a.nitems) item_range(p_item, p_cnt, p_start, p_cc);
+  // Look-ahead cursor: slab S of the sequence (the first S are issued here).
+  SlabCursor ahead;
+  ahead.item = blockIdx.x;
+  ahead.t = 0;
+  cursor_item<DVY>(a, ahead);
+  if (threadIdx.x == 0) {
+    int n = 0;
+    for (; n < S && ahead.item < a.nitems; ++n) {
+      issue_slab(&tin, a, ahead, slabs, bars, n, slab_elems, slab_bytes);
+      cursor_next<DVY>(a, ahead);
     }
-  };
-  if (threadIdx.x == 0)
-    for (int s = 0; s < S; ++s) issue_next();
+    *issued = n;
+  } else {
+    for (int n = 0; n < S && ahead.item < a.nitems; ++n) cursor_next<DVY>(a, ahead);
+  }
 
-  const long long vstride = a.nxy;                   // consecutive ivx
-  const long long ystride = (long long)a.nxy * nvx;  // consecutive ivy
-  long long k = 0;                                   // slabs consumed
+  const long long vstride = a.nxy;                        // consecutive ivx
+  const long long ystride = (long long)a.nxy * nvx;       // consecutive ivy
+  long long k = 0;                                        // slabs consumed
   for (long long item = blockIdx.x; item < a.nitems; item += gridDim.x) {
-    int cnt, start, cc;
-    item_range(item, cnt, start, cc);
+    SlabCursor cur;
+    cur.item = item;
+    cur.t = 0;
+    cursor_item<DVY>(a, cur);
+    const int cnt = cur.cnt, cc = cur.cc;
     const int sg = (int)(item % a.nseg);
     const long long ixy = (long long)cc * C + col;
     T wvx[6], wvy[6];
@@ -143,7 +194,7 @@ __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorM
       }
     }
     if (DVY) {
-      lag0 = 5 + signed_offset(__ldg(a.tvy.m + ixy), nvy) - a.span[cc].x;
+      lag0 = 5 + signed_offset(__ldg(a.tvy.m + ixy), a.nvy) - a.span[cc].x;
       load_weights(WeightsOf<T>::get(a.tvy), ixy, wvy);
     }
     // Output pointer of the next row this thread writes.
@@ -160,7 +211,10 @@ __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorM
         const int t = t0 + u;
         if (t >= cnt) break;  // uniform over the CTA
         const int slot = (int)(k % S);
-        const bool ok = mbar_wait_bounded(&bars[slot], (uint32_t)((k / S) & 1));
+        if (!mbar_wait_bounded(&bars[slot], (uint32_t)((k / S) & 1))) {
+          vslab_abort(a, bars, issued, k, S);
+          return;
+        }
         const T *sl = slabs + (size_t)slot * slab_elems;
         if (DVX) {
           T tap[V + 5];
@@ -171,6 +225,21 @@ __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorM
 #pragma unroll
           for (int i = 0; i < V; ++i) win[u][i] = sl[off[i]];
         }
+        // This warp is done with the slot: count it; the last warp refills it.
+        __syncwarp();
+        if (lane == 0) {
+          __threadfence_block();
+          if (atomicAdd(&released[slot], 1) == nwarps - 1) {
+            released[slot] = 0;
+            __threadfence_block();
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            if (ahead.item < a.nitems) {
+              issue_slab(&tin, a, ahead, slabs, bars, slot, slab_elems, slab_bytes);
+              atomicAdd(issued, 1);
+            }
+          }
+        }
+        cursor_next<DVY>(a, ahead);
         bool emit = true;
         if (DVY) {
           const int e = t - lag0;
@@ -191,16 +260,6 @@ __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorM
           }
           orow += ystride;
         }
-        // The slot is free once every thread is here.
-        if (__syncthreads_or(!ok)) {
-          if (threadIdx.x == 0) {
-            atomicExch(a.err, 1);
-            for (long long q = k; q < p_k; ++q) mbar_wait_bounded(&bars[q % S], (uint32_t)((q / S) & 1));
-          }
-          __syncthreads();
-          return;
-        }
-        if (threadIdx.x == 0) issue_next();
         ++k;
       }
     }
