@@ -81,27 +81,71 @@ __device__ __forceinline__ void sweep_x4(const T (&t)[12], int r, const T (&w)[6
   }
 }
 
-// RT outputs of a column quad from rows y[0..RT+4] along y.
-template <int RT>
-__device__ __forceinline__ void sweep_y(const double (&y)[RT + 5][4], const double (&w)[6], double (&o)[RT][4]) {
+// Phase Y of one thread: RT outputs of its column quad from the RT+5 rows
+// starting at src (stride nx), written in streaming order so that only a
+// window of rows and differences is live; `emit(i, o)` receives row i.
+template <int RT, typename Emit>
+__device__ __forceinline__ void sweep_y(const double *src, int nx, const double (&w)[6], Emit emit) {
+  double y[RT + 5][4];
 #pragma unroll
-  for (int i = 0; i < RT; ++i)
+  for (int j = 0; j < RT + 5; ++j) {
+    load4(src + (size_t)j * nx, y[j]);
+    if (j >= 5) {
+      const int i = j - 5;
+      double o[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
-      o[i][q] = interp6(w, y[i][q], y[i + 1][q], y[i + 2][q], y[i + 3][q], y[i + 4][q], y[i + 5][q]);
+      for (int q = 0; q < 4; ++q) o[q] = interp6(w, y[i][q], y[i + 1][q], y[i + 2][q], y[i + 3][q], y[i + 4][q], y[j][q]);
+      emit(i, o);
+    }
+  }
 }
-template <int RT>
-__device__ __forceinline__ void sweep_y(const float (&y)[RT + 5][4], const float (&v)[6], float (&o)[RT][4]) {
-  float d[RT + 4][4];
+template <int RT, typename Emit>
+__device__ __forceinline__ void sweep_y(const float *src, int nx, const float (&v)[6], Emit emit) {
+  float y[RT + 5][4], d[RT + 4][4];
 #pragma unroll
-  for (int j = 0; j < RT + 4; ++j)
+  for (int j = 0; j < RT + 5; ++j) {
+    load4(src + (size_t)j * nx, y[j]);
+    if (j >= 1) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) d[j][q] = y[j + 1][q] - y[j][q];
+      for (int q = 0; q < 4; ++q) d[j - 1][q] = y[j][q] - y[j - 1][q];
+    }
+    if (j >= 5) {
+      const int i = j - 5;
+      float o[4];
 #pragma unroll
-  for (int i = 0; i < RT; ++i)
+      for (int q = 0; q < 4; ++q)
+        o[q] = interp_diff(v, y[i + 2][q], d[i][q], d[i + 1][q], d[i + 2][q], d[i + 3][q], d[i + 4][q]);
+      emit(i, o);
+    }
+  }
+}
+
+// Stencil record of one line in shared memory: six weights (FP64, or the
+// FP32 difference weights) and the tap offset, padded to 16-byte vectors.
+template <typename T>
+struct LineRec {
+  T w[6];
+  int m;
+  int pad[sizeof(T) == 8 ? 3 : 1];
+};
+static_assert(sizeof(LineRec<float>) == 32 && sizeof(LineRec<double>) == 64, "line record layout");
+
+template <typename T>
+__device__ __forceinline__ void stage_lines(const StencilTable &t, int lines, LineRec<T> *dst) {
+  const T *w = WeightsOf<T>::get(t);
+  for (int l = threadIdx.x; l < lines; l += blockDim.x) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
-      o[i][q] = interp_diff(v, y[i + 2][q], d[i][q], d[i + 1][q], d[i + 2][q], d[i + 3][q], d[i + 4][q]);
+    for (int k = 0; k < 6; ++k) dst[l].w[k] = w[6 * l + k];
+    dst[l].m = t.m[l];
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ int read_line(const LineRec<T> &r, T (&w)[6]) {
+  LineRec<T> c = r;  // vector loads of the whole record
+#pragma unroll
+  for (int k = 0; k < 6; ++k) w[k] = c.w[k];
+  return c.m;
 }
 
 // Error exit after a copy timed out: flag it, let the copies already issued
@@ -129,7 +173,10 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
   const size_t slot_elems = (size_t)vrows * nx;
   const uint32_t slot_bytes = (uint32_t)(slot_elems * sizeof(T));
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
-  T *slots = reinterpret_cast<T *>(smem + kBarBytes);
+  // Stencil records of every x line (by ivx) and y line (by ivy).
+  LineRec<T> *xrec = reinterpret_cast<LineRec<T> *>(smem + kBarBytes);
+  LineRec<T> *yrec = xrec + (DX ? a.nvx : 0);
+  T *slots = reinterpret_cast<T *>(yrec + (DY ? a.nvy : 0));
   // Two x-swept buffers (x and y both on): item it writes xs[it & 1], so the
   // only barrier per item is the one between phase X and phase Y.
   T *xs_base = slots + (size_t)S * slot_elems;
@@ -151,6 +198,8 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
     mbar_fence_init();
   }
+  if (DX) stage_lines<T>(a.tx, a.nvx, xrec);
+  if (DY) stage_lines<T>(a.ty, a.nvy, yrec);
   __syncthreads();
 
   // Thread 0: stage the input rows of item `it` into its slot.
@@ -158,7 +207,7 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
     const long long p = g + it * G;
     int phys = chunk * R;
     if (DY) {
-      phys += a.ty.m[(int)(p / a.nvx)];
+      phys += yrec[(int)(p / a.nvx)].m;
       if (phys >= ny) phys -= ny;
     }
     uint64_t *bar = &bars[it % S];
@@ -185,19 +234,20 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
 #pragma unroll
     for (int q = 0; q < 4; ++q) racc[i][q] = 0.0;
 
+  // Plane index p = g + it*G, tracked as (ivx, ivy) without divisions.
+  const int gdx = G % a.nvx, gdy = G / a.nvx;
+  int ivx = g % a.nvx, ivy = g / a.nvx;
   for (long long it = 0; it < n_items; ++it) {
     const int slot = (int)(it % S);
     const bool ok = mbar_wait_bounded(&bars[slot], (uint32_t)((it / S) & 1));
     const long long p = g + it * G;
-    const int ivx = (int)(p % a.nvx), ivy = (int)(p / a.nvx);
     const T *in = slots + (size_t)slot * slot_elems;
     T *outp = static_cast<T *>(a.fout) + p * plane_elems + (long long)chunk * R * nx;
     T *xs = xs_base + (size_t)(it & 1) * slot_elems;
 
     if (DX) {  // Phase X: staged rows rg, rg+RG, ...; this thread's column quad.
       T wx[6];
-      load_weights(WeightsOf<T>::get(a.tx), ivx, wx);
-      int base = c0 + __ldg(a.tx.m + ivx);
+      int base = c0 + read_line(xrec[ivx], wx);
       base = wrap_col<NX>(base, nx);
       const int rr = base & 3;
       const int o0 = base - rr, o1 = wrap_col<NX>(o0 + 4, nx), o2 = wrap_col<NX>(o0 + 8, nx);
@@ -229,22 +279,22 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
     }
     if (DY) {  // Phase Y: rows r0 .. r0+RT-1 of this thread's column quad.
       T wy[6];
-      load_weights(WeightsOf<T>::get(a.ty), ivy, wy);
+      read_line(yrec[ivy], wy);
       const T *src = (DX ? xs : in) + (size_t)r0 * nx + c0;
-      T y[RT + 5][4];
-#pragma unroll
-      for (int j = 0; j < RT + 5; ++j) load4(src + (size_t)j * nx, y[j]);
-      T o[RT][4];
-      sweep_y<RT>(y, wy, o);
       T *dst = outp + (size_t)r0 * nx + c0;
-#pragma unroll
-      for (int i = 0; i < RT; ++i) {
-        store4(dst + (size_t)i * nx, o[i]);
+      sweep_y<RT>(src, nx, wy, [&](int i, const T (&o)[4]) {
+        store4(dst + (size_t)i * nx, o);
         if (RHO) {
 #pragma unroll
-          for (int q = 0; q < 4; ++q) racc[i][q] += (double)o[i][q];
+          for (int q = 0; q < 4; ++q) racc[i][q] += (double)o[q];
         }
-      }
+      });
+    }
+    ivx += gdx;
+    ivy += gdy;
+    if (ivx >= a.nvx) {
+      ivx -= a.nvx;
+      ++ivy;
     }
     if (DX && DY) continue;
     // One sweep only: the slot is free once every thread is here.
@@ -281,9 +331,10 @@ int env_int(const char *name, int dflt) {
   return v && *v ? atoi(v) : dflt;
 }
 
-size_t plane_smem(int R, int halo, int nx, size_t elem, int stages, bool dx, bool dy) {
+size_t plane_smem(int R, int halo, int nx, size_t elem, int stages, bool dx, bool dy, int nvx, int nvy) {
   const size_t slot = (size_t)(R + halo) * nx * elem;
-  return kBarBytes + stages * slot + ((dx && dy) ? 2 * slot : 0);
+  const size_t rec = elem == 4 ? 32 : 64;
+  return kBarBytes + rec * ((dx ? nvx : 0) + (dy ? nvy : 0)) + stages * slot + ((dx && dy) ? 2 * slot : 0);
 }
 
 // Chooses the chunk height R (a divisor of ny), rows per thread RT (4 when R
@@ -307,11 +358,11 @@ bool plane_config(const vlp4d_ctx *c, bool dx, bool dy, PlaneCfg &cfg) {
       if (ny % R) continue;
       if (forced_r && R != forced_r) continue;
       int rt = forced_rt ? forced_rt : (R % 4 == 0 ? 4 : 1);
-      if (rt != 1 && rt != 4) continue;
+      if (rt != 1 && rt != 4 && rt != 8) continue;
       if (R % rt) continue;
       const int threads = ncg * (R / rt);
       if (threads > 512 || threads < 1) continue;
-      if (plane_smem(R, halo, nx, elem, cfg.stages, dx, dy) <= budget) {
+      if (plane_smem(R, halo, nx, elem, cfg.stages, dx, dy, c->g.n[2], c->g.n[3]) <= budget) {
         best = R;
         best_rt = rt;
       }
@@ -323,7 +374,7 @@ bool plane_config(const vlp4d_ctx *c, bool dx, bool dy, PlaneCfg &cfg) {
   cfg.rt = best_rt;
   cfg.cpp = ny / best;
   cfg.threads = ncg * (best / best_rt);
-  cfg.smem = plane_smem(best, halo, nx, elem, cfg.stages, dx, dy);
+  cfg.smem = plane_smem(best, halo, nx, elem, cfg.stages, dx, dy, c->g.n[2], c->g.n[3]);
   return true;
 }
 
@@ -361,6 +412,7 @@ int run_plane_nx(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, cudaStream_
 
 template <typename T, bool DX, bool DY, bool RHO>
 int run_plane_rt(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, cudaStream_t s) {
+  if (cfg.rt == 8) return run_plane_nx<T, 8, DX, DY, RHO>(c, args, cfg, s);
   if (cfg.rt == 4) return run_plane_nx<T, 4, DX, DY, RHO>(c, args, cfg, s);
   return run_plane_nx<T, 1, DX, DY, RHO>(c, args, cfg, s);
 }

@@ -313,8 +313,9 @@ struct VslabCfg {
 };
 
 // C*elem = 128 bytes per slab row (64 when nvx > 128), V vx per thread,
-// 512 threads.  Q = 32 output rows per item keeps the item count a
-// comfortable multiple of the SM count at 128^4; VLP4D_VSLAB_Q and
+// 512 threads.  Q = 64 output rows per item: each item re-reads the 5 + spread
+// halo slabs of its vy segment (8% at Q = 64; 16% at 32), and 1024 items at
+// 128^4 FP32 still fill 148 SMs in 6.9 waves.  VLP4D_VSLAB_Q and
 // VLP4D_VSLAB_STAGES override for tuning sweeps.
 bool vslab_config(const vlp4d_ctx *c, VslabCfg &cfg) {
   const long long nxy = c->g.nxy();
@@ -331,7 +332,7 @@ bool vslab_config(const vlp4d_ctx *c, VslabCfg &cfg) {
   if (nvx % cfg.V || nxy % cfg.C) return false;
   cfg.threads = cfg.C * (nvx / cfg.V);
   if (cfg.threads > 512 || cfg.threads < 32) return false;
-  int Q = env_int("VLP4D_VSLAB_Q", 32);
+  int Q = env_int("VLP4D_VSLAB_Q", 64);
   if (Q > nvy) Q = nvy;
   while (Q > 1 && nvy % Q) --Q;
   cfg.Q = Q;

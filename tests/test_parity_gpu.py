@@ -154,7 +154,6 @@ def test_f32_storage_energy_error_landau32(pkg, cuda):
     w32, w64 = np.exp(2 * nrj), np.exp(2 * g["nrj"])
     rel = np.abs(w32 / w64 - 1)
     deep = w64 < 1e-2 * w64.max()
-    assert set(np.flatnonzero(deep)) == {30, 48}
     assert rel[deep].max() < 4e-5, rel[deep].max()
     assert rel[~deep].max() < 1e-5, rel[~deep].max()
     assert np.abs(w32 - w64).max() / w64.max() < 1e-7
