@@ -237,9 +237,10 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
   // Plane index p = g + it*G, tracked as (ivx, ivy) without divisions.
   const int gdx = G % a.nvx, gdy = G / a.nvx;
   int ivx = g % a.nvx, ivy = g / a.nvx;
+  int slot = 0;          // it % S
+  uint32_t parity = 0;   // (it / S) & 1
   for (long long it = 0; it < n_items; ++it) {
-    const int slot = (int)(it % S);
-    const bool ok = mbar_wait_bounded(&bars[slot], (uint32_t)((it / S) & 1));
+    const bool ok = mbar_wait_bounded(&bars[slot], parity);
     const long long p = g + it * G;
     const T *in = slots + (size_t)slot * slot_elems;
     T *outp = static_cast<T *>(a.fout) + p * plane_elems + (long long)chunk * R * nx;
@@ -295,6 +296,10 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
     if (ivx >= a.nvx) {
       ivx -= a.nvx;
       ++ivy;
+    }
+    if (++slot == S) {
+      slot = 0;
+      parity ^= 1u;
     }
     if (DX && DY) continue;
     // One sweep only: the slot is free once every thread is here.

@@ -121,7 +121,9 @@ __device__ __forceinline__ void issue_slab(const CUtensorMap *tin, const VslabAr
   tensor_load_3d(slabs + (size_t)slot * slab_elems, tin, c.cc * a.C, 0, row, &bars[slot]);
 }
 
-template <typename T, bool DVX, bool DVY, int V>
+// NXY: compile-time nx*ny (0 = read a.nxy at run time); with it the V output
+// stores of a thread use immediate offsets.
+template <typename T, bool DVX, bool DVY, int V, int NXY>
 __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorMap tin, VslabArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // Tensor-copy destinations on a 128-byte boundary whatever the base
@@ -164,9 +166,11 @@ __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorM
     for (int n = 0; n < S && ahead.item < a.nitems; ++n) cursor_next<DVY>(a, ahead);
   }
 
-  const long long vstride = a.nxy;                        // consecutive ivx
-  const long long ystride = (long long)a.nxy * nvx;       // consecutive ivy
-  long long k = 0;                                        // slabs consumed
+  const long long vstride = NXY ? NXY : a.nxy;            // consecutive ivx
+  const long long ystride = vstride * nvx;                 // consecutive ivy
+  long long k = 0;                                         // slabs consumed
+  int slot = 0;                                            // k % S
+  uint32_t parity = 0;                                     // (k / S) & 1
   for (long long item = blockIdx.x; item < a.nitems; item += gridDim.x) {
     SlabCursor cur;
     cur.item = item;
@@ -210,8 +214,7 @@ __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorM
       for (int u = 0; u < 6; ++u) {
         const int t = t0 + u;
         if (t >= cnt) break;  // uniform over the CTA
-        const int slot = (int)(k % S);
-        if (!mbar_wait_bounded(&bars[slot], (uint32_t)((k / S) & 1))) {
+        if (!mbar_wait_bounded(&bars[slot], parity)) {
           vslab_abort(a, bars, issued, k, S);
           return;
         }
@@ -246,7 +249,6 @@ __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorM
           emit = e >= 0 && e < a.Q;
         }
         if (emit) {
-          T *o = orow;
 #pragma unroll
           for (int i = 0; i < V; ++i) {
             T val;
@@ -255,12 +257,15 @@ __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorM
                             win[(u + 4) % 6][i], win[(u + 5) % 6][i], win[u][i]);
             else
               val = win[u][i];
-            *o = val;
-            o += vstride;
+            orow[vstride * i] = val;
           }
           orow += ystride;
         }
         ++k;
+        if (++slot == S) {
+          slot = 0;
+          parity ^= 1u;
+        }
       }
     }
   }
@@ -313,10 +318,12 @@ struct VslabCfg {
 };
 
 // C*elem = 128 bytes per slab row (64 when nvx > 128), V vx per thread,
-// 512 threads.  Q = 64 output rows per item: each item re-reads the 5 + spread
-// halo slabs of its vy segment (8% at Q = 64; 16% at 32), and 1024 items at
-// 128^4 FP32 still fill 148 SMs in 6.9 waves.  VLP4D_VSLAB_Q and
-// VLP4D_VSLAB_STAGES override for tuning sweeps.
+// 512 threads.  Q output rows per item: each item re-reads the 5 + spread
+// halo slabs of its vy segment (4% at Q = 128, 8% at 64), so Q is the
+// tallest segment that still leaves six items per SM (at 128^4: 64 in FP32,
+// 128 in FP64, whose chunks are half as wide).  Stages as measured best at
+// 128^4 (4 FP32, 10 FP64).  VLP4D_VSLAB_Q and VLP4D_VSLAB_STAGES override
+// for tuning sweeps.
 bool vslab_config(const vlp4d_ctx *c, VslabCfg &cfg) {
   const long long nxy = c->g.nxy();
   const int nvx = c->g.n[2], nvy = c->g.n[3];
@@ -332,19 +339,30 @@ bool vslab_config(const vlp4d_ctx *c, VslabCfg &cfg) {
   if (nvx % cfg.V || nxy % cfg.C) return false;
   cfg.threads = cfg.C * (nvx / cfg.V);
   if (cfg.threads > 512 || cfg.threads < 32) return false;
-  int Q = env_int("VLP4D_VSLAB_Q", 64);
+  // Q: the tallest vy segment (fewest halo re-reads) that still leaves at
+  // least six items per SM.
+  const long long nchunks = nxy / cfg.C;
+  int Q = env_int("VLP4D_VSLAB_Q", 0);
+  if (Q <= 0) {
+    Q = 1;
+    for (int q = nvy < 128 ? nvy : 128; q >= 1; --q)
+      if (nvy % q == 0 && (nchunks * (nvy / q) >= 6LL * c->num_sms || q == 1)) {
+        Q = q;
+        break;
+      }
+  }
   if (Q > nvy) Q = nvy;
   while (Q > 1 && nvy % Q) --Q;
   cfg.Q = Q;
-  cfg.stages = env_int("VLP4D_VSLAB_STAGES", 6);
+  cfg.stages = env_int("VLP4D_VSLAB_STAGES", f32 ? 4 : 10);
   if (cfg.stages < 2 || cfg.stages > kMaxStages) return false;
   cfg.smem = 128 + kBarBytes + (size_t)cfg.stages * cfg.C * nvx * c->elem;
   return cfg.smem <= 200 * 1024;
 }
 
-template <typename T, bool DVX, bool DVY, int V>
+template <typename T, bool DVX, bool DVY, int V, int NXY>
 int run_vslab(vlp4d_ctx *c, const CUtensorMap &map, const VslabArgs &args, const VslabCfg &cfg, cudaStream_t s) {
-  auto kern = k_vslab<T, DVX, DVY, V>;
+  auto kern = k_vslab<T, DVX, DVY, V, NXY>;
   VLP4D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
   int per_sm = 0;
   VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, cfg.threads, cfg.smem));
@@ -401,7 +419,12 @@ int launch_advect_vxvy(vlp4d_ctx *c, const void *fn, void *fnp1, bool do_vx, boo
   if (do_vy) a.tvy = c->tab_vy;
   a.span = c->vspan;
   a.err = c->d_err;
-#define VLP4D_VS(T, DVX, DVY, V) return run_vslab<T, DVX, DVY, V>(c, map, a, cfg, s)
+#define VLP4D_VS(T, DVX, DVY, V)                                                  \
+  switch (a.nxy) {                                                                \
+    case 16384: return run_vslab<T, DVX, DVY, V, 16384>(c, map, a, cfg, s);      \
+    case 4096: return run_vslab<T, DVX, DVY, V, 4096>(c, map, a, cfg, s);        \
+    default: return run_vslab<T, DVX, DVY, V, 0>(c, map, a, cfg, s);             \
+  }
   if (c->dtype == VLP4D_F64) {
     if (do_vx && do_vy) VLP4D_VS(double, true, true, 4);
     if (do_vx) VLP4D_VS(double, true, false, 4);
