@@ -150,6 +150,16 @@ int vlp4d_diags_save(vlp4d_ctx *ctx, const char *path);
  * buffer.) */
 int vlp4d_step(vlp4d_ctx *ctx, void *f_state, void *f_next, int iter, void *stream);
 
+/* `nsteps` consecutive steps, iterations iter0 .. iter0+nsteps-1 (the time
+ * loop of miniapps/vlp4d/thrust/vlp4d.cpp:63-72): the same sweeps, field
+ * solves and diagnostics as nsteps calls of vlp4d_step, and bit-identical to
+ * them, but the last x/y half step of each step and the first x/y half step
+ * of the next (consecutive, with no field solve between them) run as one
+ * pass, so the intermediate state between steps is never written to memory:
+ * 2*nsteps + 1 passes over f instead of 3*nsteps.  Reads f_state, writes the
+ * final state into f_next; f_state is scratch. */
+int vlp4d_steps(vlp4d_ctx *ctx, void *f_state, void *f_next, int iter0, int nsteps, void *stream);
+
 /* The time loop of main() (miniapps/vlp4d/thrust/vlp4d.cpp:55-73) with host
  * buffers: copies f0 (host, nx*ny*nvx*nvy elements of the context's dtype)
  * into fn, runs the initial field solve + diagnostic 0 and `nsteps` steps,

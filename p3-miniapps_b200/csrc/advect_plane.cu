@@ -319,6 +319,157 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
   }
 }
 
+// Two consecutive x/y half steps in one pass: x, y, x, y with the same
+// stencils (the end of one Strang step and the start of the next, which no
+// field solve separates), plus the moment of the result.  Every sweep is the
+// one the two separate passes would apply, in the same order and precision,
+// so the result is bit-identical; only the intermediate state is kept in
+// shared memory instead of HBM.  Output row r of the chunk needs staged rows
+// r + 2*my .. r + 2*my + 10, so R + 10 rows are staged.  Phases per item:
+//   X1: staged rows -> xa (R+10 rows)   | barrier, refill the slot
+//   Y1: xa -> ya (R+5 rows)             | barrier
+//   X2: ya -> xb (R+5 rows)             | barrier
+//   Y2: xb -> output (R rows), moment
+// The next item's X1/Y1/X2 writes are ordered after this item's reads by
+// the next item's barriers, so no barrier follows Y2.
+template <typename T, int NX, int RT>
+__global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int nx = NX ? NX : a.nx;
+  const int ny = a.ny, R = a.R, S = a.stages;
+  const int ncg = nx >> 2;
+  const size_t slot_elems = (size_t)(R + 10) * nx;
+  const uint32_t slot_bytes = (uint32_t)(slot_elems * sizeof(T));
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+  LineRec<T> *xrec = reinterpret_cast<LineRec<T> *>(smem + kBarBytes);
+  LineRec<T> *yrec = xrec + a.nvx;
+  T *slots = reinterpret_cast<T *>(yrec + a.nvy);
+  T *xa = slots + (size_t)S * slot_elems;
+  T *ya = xa + slot_elems;
+  T *xb = ya + (size_t)(R + 5) * nx;
+
+  const int cg = threadIdx.x % ncg;
+  const int rg = threadIdx.x / ncg;
+  const int RG = blockDim.x / ncg;
+  const int c0 = cg * 4;
+  const int r0 = rg * RT;
+  const int chunk = blockIdx.x % a.cpp;
+  const int G = gridDim.x / a.cpp;
+  const int g = blockIdx.x / a.cpp;
+  const long long planes = (long long)a.nvx * a.nvy;
+  const long long n_items = g < planes ? (planes - g + G - 1) / G : 0;
+  const long long plane_elems = (long long)nx * ny;
+
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < S; ++st) mbar_init(&bars[st], 1);
+    mbar_fence_init();
+  }
+  stage_lines<T>(a.tx, a.nvx, xrec);
+  stage_lines<T>(a.ty, a.nvy, yrec);
+  __syncthreads();
+
+  auto issue = [&](long long it) {
+    const long long p = g + it * G;
+    int phys = (chunk * R + 2 * yrec[(int)(p / a.nvx)].m) % ny;
+    uint64_t *bar = &bars[it % S];
+    mbar_arrive_expect_tx(bar, slot_bytes);
+    const T *src = static_cast<const T *>(a.fin) + p * plane_elems;
+    T *dst = slots + (size_t)(it % S) * slot_elems;
+    int remaining = R + 10;
+    while (remaining > 0) {
+      const int len = remaining < ny - phys ? remaining : ny - phys;
+      bulk_load(dst, src + (long long)phys * nx, (uint32_t)((size_t)len * nx * sizeof(T)), bar);
+      dst += (size_t)len * nx;
+      remaining -= len;
+      phys = 0;
+    }
+  };
+  if (threadIdx.x == 0) {
+    const long long pre = n_items < S ? n_items : S;
+    for (long long it = 0; it < pre; ++it) issue(it);
+  }
+
+  double racc[RT][4];
+#pragma unroll
+  for (int i = 0; i < RT; ++i)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) racc[i][q] = 0.0;
+
+  // x sweep of rows [0, nrows) of src into dst (rows rg, rg+RG, ...).
+  auto sweep_rows_x = [&](const T *src, T *dst, int nrows, int o0, int o1, int o2, int rr, const T (&wx)[6]) {
+    for (int v = rg; v < nrows; v += RG) {
+      const T *row = src + (size_t)v * nx;
+      T t[12], q4[4];
+      load4(row + o0, q4);
+      t[0] = q4[0]; t[1] = q4[1]; t[2] = q4[2]; t[3] = q4[3];
+      load4(row + o1, q4);
+      t[4] = q4[0]; t[5] = q4[1]; t[6] = q4[2]; t[7] = q4[3];
+      load4(row + o2, q4);
+      t[8] = q4[0]; t[9] = q4[1]; t[10] = q4[2]; t[11] = q4[3];
+      T o[4];
+      sweep_x4(t, rr, wx, o);
+      store4(dst + (size_t)v * nx + c0, o);
+    }
+  };
+
+  const int gdx = G % a.nvx, gdy = G / a.nvx;
+  int ivx = g % a.nvx, ivy = g / a.nvx;
+  int slot = 0;
+  uint32_t parity = 0;
+  for (long long it = 0; it < n_items; ++it) {
+    const bool ok = mbar_wait_bounded(&bars[slot], parity);
+    const long long p = g + it * G;
+    const T *in = slots + (size_t)slot * slot_elems;
+    T *outp = static_cast<T *>(a.fout) + p * plane_elems + (long long)chunk * R * nx;
+    T wx[6], wy[6];
+    int base = c0 + read_line(xrec[ivx], wx);
+    read_line(yrec[ivy], wy);
+    base = wrap_col<NX>(base, nx);
+    const int rr = base & 3;
+    const int o0 = base - rr, o1 = wrap_col<NX>(o0 + 4, nx), o2 = wrap_col<NX>(o0 + 8, nx);
+
+    sweep_rows_x(in, xa, R + 10, o0, o1, o2, rr, wx);  // X1
+    if (__syncthreads_or(!ok)) {
+      plane_abort(a, bars, it, n_items, S);
+      return;
+    }
+    if (threadIdx.x == 0 && it + S < n_items) issue(it + S);
+    // Y1: rows [0, R) streamed per thread, rows [R, R+5) one at a time.
+    sweep_y<RT>(xa + (size_t)r0 * nx + c0, nx, wy,
+                [&](int i, const T (&o)[4]) { store4(ya + (size_t)(r0 + i) * nx + c0, o); });
+    for (int v = R + rg; v < R + 5; v += RG) {
+      sweep_y<1>(xa + (size_t)v * nx + c0, nx, wy,
+                 [&](int, const T (&o)[4]) { store4(ya + (size_t)v * nx + c0, o); });
+    }
+    __syncthreads();
+    sweep_rows_x(ya, xb, R + 5, o0, o1, o2, rr, wx);  // X2
+    __syncthreads();
+    // Y2 and the moment.
+    T *dst = outp + (size_t)r0 * nx + c0;
+    sweep_y<RT>(xb + (size_t)r0 * nx + c0, nx, wy, [&](int i, const T (&o)[4]) {
+      store4(dst + (size_t)i * nx, o);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) racc[i][q] += (double)o[q];
+    });
+    ivx += gdx;
+    ivy += gdy;
+    if (ivx >= a.nvx) {
+      ivx -= a.nvx;
+      ++ivy;
+    }
+    if (++slot == S) {
+      slot = 0;
+      parity ^= 1u;
+    }
+  }
+  double *rdst = a.rho_part + (long long)g * plane_elems + ((long long)chunk * R + r0) * nx + c0;
+#pragma unroll
+  for (int i = 0; i < RT; ++i) {
+    reinterpret_cast<double2 *>(rdst + (size_t)i * nx)[0] = make_double2(racc[i][0], racc[i][1]);
+    reinterpret_cast<double2 *>(rdst + (size_t)i * nx)[1] = make_double2(racc[i][2], racc[i][3]);
+  }
+}
+
 }  // namespace
 }  // namespace vlp4d
 
@@ -342,44 +493,51 @@ size_t plane_smem(int R, int halo, int nx, size_t elem, int stages, bool dx, boo
   return kBarBytes + rec * ((dx ? nvx : 0) + (dy ? nvy : 0)) + stages * slot + ((dx && dy) ? 2 * slot : 0);
 }
 
-// Chooses the chunk height R (a divisor of ny), rows per thread RT (4 when R
-// allows, else 1), the pipeline depth and the block size nx/4 * R/RT.
-// Preference: the tallest chunk (least halo re-read) whose CTA fits twice on
-// an SM, else once.  VLP4D_PLANE_R / _STAGES / _RT override for tuning.
+// Chooses the chunk height R, rows per thread RT, the pipeline depth and the
+// block size nx/4 * R/RT.  R is the tallest divisor of ny up to 32 (the
+// halo re-read is 5/R of the rows, served from L2; taller chunks were not
+// faster at 128^4); then the deepest pipeline (3, else 2 stages) that lets
+// two CTAs share an SM, else one CTA per SM with 3 stages.
+// VLP4D_PLANE_R / _STAGES / _RT override for tuning sweeps.
 bool plane_config(const vlp4d_ctx *c, bool dx, bool dy, PlaneCfg &cfg) {
   const int nx = c->g.n[0], ny = c->g.n[1];
   const size_t elem = c->elem;
   if (nx % 4 != 0 || nx > 2048) return false;
   const int halo = dy ? 5 : 0;
-  cfg.stages = env_int("VLP4D_PLANE_STAGES", 3);
-  if (cfg.stages < 2 || cfg.stages > kMaxStages) return false;
+  const int ncg = nx / 4;
   const int forced_r = env_int("VLP4D_PLANE_R", 0);
   const int forced_rt = env_int("VLP4D_PLANE_RT", 0);
-  const int ncg = nx / 4;
-  const size_t two_per_sm = 112 * 1024, one_per_sm = 224 * 1024;
-  int best = 0, best_rt = 1;
-  for (const size_t budget : {two_per_sm, one_per_sm}) {
-    for (int R = ny < 64 ? ny : 64; R >= 1 && !best; --R) {
-      if (ny % R) continue;
-      if (forced_r && R != forced_r) continue;
-      int rt = forced_rt ? forced_rt : (R % 4 == 0 ? 4 : 1);
-      if (rt != 1 && rt != 4 && rt != 8) continue;
-      if (R % rt) continue;
-      const int threads = ncg * (R / rt);
-      if (threads > 512 || threads < 1) continue;
-      if (plane_smem(R, halo, nx, elem, cfg.stages, dx, dy, c->g.n[2], c->g.n[3]) <= budget) {
-        best = R;
-        best_rt = rt;
-      }
-    }
-    if (best) break;
+  const int forced_s = env_int("VLP4D_PLANE_STAGES", 0);
+  int R = 0, rt = 1;
+  for (int r = ny < 32 ? ny : 32; r >= 1; --r) {
+    if (ny % r) continue;
+    if (forced_r && r != forced_r) continue;
+    const int t = forced_rt ? forced_rt : (r % 4 == 0 ? 4 : 1);
+    if (t != 1 && t != 4 && t != 8) continue;
+    if (r % t || ncg * (r / t) > 512) continue;
+    R = r;
+    rt = t;
+    break;
   }
-  if (!best) return false;
-  cfg.R = best;
-  cfg.rt = best_rt;
-  cfg.cpp = ny / best;
-  cfg.threads = ncg * (best / best_rt);
-  cfg.smem = plane_smem(best, halo, nx, elem, cfg.stages, dx, dy, c->g.n[2], c->g.n[3]);
+  if (!R) return false;
+  const size_t two_per_sm = 112 * 1024, one_per_sm = 224 * 1024;
+  int stages = 0;
+  if (forced_s) {
+    stages = forced_s;
+  } else {
+    for (int st = 3; st >= 2 && !stages; --st)
+      if (plane_smem(R, halo, nx, elem, st, dx, dy, c->g.n[2], c->g.n[3]) <= two_per_sm) stages = st;
+    if (!stages) stages = 3;
+  }
+  if (stages < 2 || stages > kMaxStages) return false;
+  const size_t smem = plane_smem(R, halo, nx, elem, stages, dx, dy, c->g.n[2], c->g.n[3]);
+  if (smem > one_per_sm) return false;
+  cfg.R = R;
+  cfg.rt = rt;
+  cfg.stages = stages;
+  cfg.cpp = ny / R;
+  cfg.threads = ncg * (R / rt);
+  cfg.smem = smem;
   return true;
 }
 
@@ -465,6 +623,93 @@ int launch_advect_xy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTabl
   if (with_rho && do_x && do_y) return launch_rho_finish(c, cfg.G, s);
   if (with_rho) return launch_field_rho(c, fnp1, s);
   return VLP4D_OK;
+}
+
+namespace {
+
+size_t xyxy_smem(int R, int nx, size_t elem, int stages, int nvx, int nvy) {
+  const size_t rec = elem == 4 ? 32 : 64;
+  return kBarBytes + rec * (nvx + nvy) + (size_t)stages * (R + 10) * nx * elem +
+         (size_t)(R + 10 + 2 * (R + 5)) * nx * elem;
+}
+
+template <typename T, int NX, int RT>
+int run_xyxy(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, cudaStream_t s) {
+  auto kern = k_plane_xyxy<T, NX, RT>;
+  VLP4D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
+  int per_sm = 0;
+  VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, cfg.threads, cfg.smem));
+  if (per_sm < 1) return VLP4D_ERR_UNSUPPORTED;
+  const long long planes = (long long)args.nvx * args.nvy;
+  long long G = ((long long)per_sm * c->num_sms) / cfg.cpp;
+  if (G < 1) G = 1;
+  if (G > planes) G = planes;
+  if (G > c->rho_part_groups) G = c->rho_part_groups;
+  cfg.G = (int)G;
+  cfg.grid = (int)G * cfg.cpp;
+  kern<<<cfg.grid, cfg.threads, cfg.smem, s>>>(args);
+  VLP4D_LAUNCH_CHECK();
+  return VLP4D_OK;
+}
+
+template <typename T, int RT>
+int run_xyxy_nx(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, cudaStream_t s) {
+  switch (args.nx) {
+    case 64: return run_xyxy<T, 64, RT>(c, args, cfg, s);
+    case 128: return run_xyxy<T, 128, RT>(c, args, cfg, s);
+    case 256: return run_xyxy<T, 256, RT>(c, args, cfg, s);
+    default: return run_xyxy<T, 0, RT>(c, args, cfg, s);
+  }
+}
+
+}  // namespace
+
+// Two x/y half steps and the moment of the result in one pass; returns
+// VLP4D_ERR_UNSUPPORTED (nothing launched) when the shape does not fit.
+int launch_advect_xyxy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *tx, const StencilTable *ty,
+                       cudaStream_t s) {
+  if (!c->fused) return VLP4D_ERR_UNSUPPORTED;
+  if (((uintptr_t)fn & 15) || ((uintptr_t)fnp1 & 15)) return VLP4D_ERR_UNSUPPORTED;
+  const int nx = c->g.n[0], ny = c->g.n[1];
+  if (nx % 4 != 0 || nx > 2048) return VLP4D_ERR_UNSUPPORTED;
+  PlaneCfg cfg;
+  const int ncg = nx / 4;
+  for (int r = ny < 32 ? ny : 32; r >= 1 && !cfg.R; --r) {
+    if (ny % r) continue;
+    const int t = r % 4 == 0 ? 4 : 1;
+    if (ncg * (r / t) > 512 || ncg * (r / t) < 1) continue;
+    cfg.R = r;
+    cfg.rt = t;
+  }
+  if (!cfg.R) return VLP4D_ERR_UNSUPPORTED;
+  cfg.stages = env_int("VLP4D_XYXY_STAGES", 2);
+  if (cfg.stages < 2 || cfg.stages > kMaxStages) return VLP4D_ERR_UNSUPPORTED;
+  cfg.cpp = ny / cfg.R;
+  cfg.threads = ncg * (cfg.R / cfg.rt);
+  cfg.smem = xyxy_smem(cfg.R, nx, c->elem, cfg.stages, c->g.n[2], c->g.n[3]);
+  if (cfg.smem > 224 * 1024) return VLP4D_ERR_UNSUPPORTED;
+  PlaneArgs a;
+  a.fin = fn;
+  a.fout = fnp1;
+  a.nx = nx;
+  a.ny = ny;
+  a.nvx = c->g.n[2];
+  a.nvy = c->g.n[3];
+  a.R = cfg.R;
+  a.cpp = cfg.cpp;
+  a.halo = 10;
+  a.stages = cfg.stages;
+  a.tx = *tx;
+  a.ty = *ty;
+  a.rho_part = c->rho_part;
+  a.err = c->d_err;
+  int rc;
+  if (c->dtype == VLP4D_F64)
+    rc = cfg.rt == 4 ? run_xyxy_nx<double, 4>(c, a, cfg, s) : run_xyxy_nx<double, 1>(c, a, cfg, s);
+  else
+    rc = cfg.rt == 4 ? run_xyxy_nx<float, 4>(c, a, cfg, s) : run_xyxy_nx<float, 1>(c, a, cfg, s);
+  if (rc) return rc;
+  return launch_rho_finish(c, cfg.G, s);
 }
 
 }  // namespace vlp4d

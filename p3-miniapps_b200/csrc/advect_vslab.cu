@@ -322,7 +322,7 @@ struct VslabCfg {
 // halo slabs of its vy segment (4% at Q = 128, 8% at 64), so Q is the
 // tallest segment that still leaves six items per SM (at 128^4: 64 in FP32,
 // 128 in FP64, whose chunks are half as wide).  Stages as measured best at
-// 128^4 (4 FP32, 10 FP64).  VLP4D_VSLAB_Q and VLP4D_VSLAB_STAGES override
+// 128^4 (8 FP32, 4 FP64).  VLP4D_VSLAB_Q and VLP4D_VSLAB_STAGES override
 // for tuning sweeps.
 bool vslab_config(const vlp4d_ctx *c, VslabCfg &cfg) {
   const long long nxy = c->g.nxy();
@@ -354,7 +354,7 @@ bool vslab_config(const vlp4d_ctx *c, VslabCfg &cfg) {
   if (Q > nvy) Q = nvy;
   while (Q > 1 && nvy % Q) --Q;
   cfg.Q = Q;
-  cfg.stages = env_int("VLP4D_VSLAB_STAGES", f32 ? 4 : 10);
+  cfg.stages = env_int("VLP4D_VSLAB_STAGES", f32 ? 8 : 4);
   if (cfg.stages < 2 || cfg.stages > kMaxStages) return false;
   cfg.smem = 128 + kBarBytes + (size_t)cfg.stages * cfg.C * nvx * c->elem;
   return cfg.smem <= 200 * 1024;

@@ -414,6 +414,51 @@ int vlp4d_step(vlp4d_ctx *ctx, void *f_state, void *f_next, int iter, void *stre
   return advect_xy_impl(ctx, f_state, f_next, 0.5 * dt, false, s);
 }
 
+// The reference's time loop (vlp4d.cpp:63-72, onetimestep per step) with
+// the last x/y half step of each step fused with the first of the next.
+int vlp4d_steps(vlp4d_ctx *ctx, void *f_state, void *f_next, int iter0, int nsteps, void *stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if ((rc = check_pair(f_state, f_next))) return rc;
+  if (nsteps < 1) return fail(VLP4D_ERR_INVALID_ARG, "nsteps must be at least 1");
+  if (iter0 < 0 || (long long)iter0 + nsteps - 1 >= ctx->hist_len)
+    return fail(VLP4D_ERR_INVALID_ARG, "iterations outside [0, nbiter]");
+  cudaStream_t s = as_stream(stream);
+  const double dt = ctx->dom.dt;
+  StencilTable *tx = nullptr, *ty = nullptr;
+  if ((rc = ensure_xy_table(ctx, 0, 0.5 * dt, &tx, s))) return rc;
+  if ((rc = ensure_xy_table(ctx, 1, 0.5 * dt, &ty, s))) return rc;
+  void *cur = f_state, *oth = f_next;
+  // timestep.hpp:17-28 of the first step: x/y half step and the moment.
+  if ((rc = advect_xy_impl(ctx, cur, oth, 0.5 * dt, true, s))) return rc;
+  std::swap(cur, oth);
+  for (int k = 0; k < nsteps; ++k) {
+    // timestep.hpp:30-48: field solve, diagnostic, vx/vy full step.
+    if ((rc = launch_field_poisson(ctx, s))) return rc;
+    if ((rc = launch_diags(ctx, iter0 + k, s))) return rc;
+    if ((rc = advect_vxvy_impl(ctx, cur, oth, dt, s))) return rc;
+    std::swap(cur, oth);
+    if (k + 1 == nsteps) break;
+    // timestep.hpp:50-58 of step k, then :17-28 of step k+1, in one pass.
+    rc = launch_advect_xyxy(ctx, cur, oth, tx, ty, s);
+    if (rc == VLP4D_ERR_UNSUPPORTED) {
+      if ((rc = fused_declined(ctx))) return rc;
+      if ((rc = advect_xy_impl(ctx, cur, oth, 0.5 * dt, false, s))) return rc;
+      std::swap(cur, oth);
+      if ((rc = advect_xy_impl(ctx, cur, oth, 0.5 * dt, true, s))) return rc;
+    } else if (rc) {
+      return rc;
+    }
+    std::swap(cur, oth);
+  }
+  // timestep.hpp:50-58 of the last step.
+  if ((rc = advect_xy_impl(ctx, cur, oth, 0.5 * dt, false, s))) return rc;
+  std::swap(cur, oth);
+  if (cur != f_next)
+    VLP4D_CUDA_TRY(cudaMemcpyAsync(f_next, cur, (size_t)ctx->g.cells() * ctx->elem, cudaMemcpyDeviceToDevice, s));
+  return VLP4D_OK;
+}
+
 int vlp4d_run(vlp4d_ctx *ctx, const void *f0_host, void *f_out_host, int nsteps, double *nrj, double *mass,
               void *fn, void *fnp1, void *stream) {
   int rc = check_ctx(ctx);
@@ -428,10 +473,10 @@ int vlp4d_run(vlp4d_ctx *ctx, const void *f0_host, void *f_out_host, int nsteps,
   if ((rc = launch_field_rho(ctx, fn, s))) return rc;
   if ((rc = launch_field_poisson(ctx, s))) return rc;
   if ((rc = launch_diags(ctx, 0, s))) return rc;
-  void *cur = fn, *nxt = fnp1;
-  for (int it = 1; it <= nsteps; ++it) {
-    if ((rc = vlp4d_step(ctx, cur, nxt, it, stream))) return rc;
-    std::swap(cur, nxt);
+  void *cur = fn;
+  if (nsteps > 0) {
+    if ((rc = vlp4d_steps(ctx, fn, fnp1, 1, nsteps, stream))) return rc;
+    cur = fnp1;
   }
   if (nrj || mass) {
     VLP4D_CUDA_TRY(cudaMemcpyAsync(ctx->h_diag, ctx->nrj, sizeof(double) * (nsteps + 1), cudaMemcpyDeviceToHost, s));

@@ -136,6 +136,8 @@ int launch_advect_pair_generic(vlp4d_ctx *c, bool v, const void *fn, void *fnp1,
 int launch_advect_xy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *tx,
                      const StencilTable *ty, bool do_x, bool do_y, bool with_rho, cudaStream_t s);
 int launch_advect_vxvy(vlp4d_ctx *c, const void *fn, void *fnp1, bool do_vx, bool do_vy, cudaStream_t s);
+int launch_advect_xyxy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *tx, const StencilTable *ty,
+                       cudaStream_t s);
 
 // field.cu
 int launch_field_rho(vlp4d_ctx *c, const void *fn, cudaStream_t s);

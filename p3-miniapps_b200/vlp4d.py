@@ -32,7 +32,7 @@ EXPORTS = (
     "vlp4d_advect_vy", "vlp4d_advect_xy", "vlp4d_advect_vxvy", "vlp4d_field_rho", "vlp4d_field_poisson",
     "vlp4d_diags_compute", "vlp4d_diags_read", "vlp4d_diags_save", "vlp4d_step", "vlp4d_run",
     "vlp4d_print_fxvx", "vlp4d_transpose", "vlp4d_check", "vlp4d_kernel_launches",
-    "vlp4d_field_rho_noalloc",
+    "vlp4d_field_rho_noalloc", "vlp4d_steps",
 )
 
 
@@ -88,6 +88,7 @@ def lib() -> C.CDLL:
         L.vlp4d_diags_read.argtypes = [vp, dp, dp, i]
         L.vlp4d_diags_save.argtypes = [vp, C.c_char_p]
         L.vlp4d_step.argtypes = [vp, vp, vp, i, vp]
+        L.vlp4d_steps.argtypes = [vp, vp, vp, i, i, vp]
         L.vlp4d_run.argtypes = [vp, vp, vp, i, dp, dp, vp, vp, vp]
         L.vlp4d_print_fxvx.argtypes = [vp, vp, C.c_char_p]
         L.vlp4d_transpose.argtypes = [vp, vp, i, i, i, vp]
@@ -284,6 +285,10 @@ class Context:
     def step(self, f_state, f_next, it, stream=None):
         """One fused Strang step: reads f_state, writes the new state into f_next (f_state becomes scratch)."""
         _check(lib().vlp4d_step(self.h, self._f(f_state), self._f(f_next), it, _stream_ptr(stream)))
+
+    def steps(self, f_state, f_next, iter0, nsteps, stream=None):
+        """nsteps fused Strang steps (diagnostics iter0 ..): final state in f_next, f_state is scratch."""
+        _check(lib().vlp4d_steps(self.h, self._f(f_state), self._f(f_next), iter0, nsteps, _stream_ptr(stream)))
 
     def run(self, f0_host, nsteps, fn, fnp1, f_out_host=None, stream=None):
         """vlp4d_run with host buffers (torch CPU tensors, ideally pinned). Returns (nrj, mass) numpy arrays."""

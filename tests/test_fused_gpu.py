@@ -139,3 +139,54 @@ def test_unaligned_buffers_fall_back_to_generic(pkg, cuda):
         ctx.advect_xy(f, out_u, 0.1)
         ctx.advect_xy(f.clone(), out_a, 0.1)
         assert _rel(out_u, out_a.reshape(-1)) < 2e-7
+
+
+@pytest.mark.parametrize("n", SHAPES)
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_steps_bit_identical_to_single_steps(pkg, cuda, n, dtype):
+    """vlp4d_steps runs the last x/y half step of each step and the first of
+    the next as one pass; every sweep is the same operation in the same
+    order and precision, so K fused steps equal K calls of vlp4d_step bit for
+    bit, diagnostics included."""
+    torch = cuda
+    K = 4
+    dom = pkg.Domain(list(n), [0.0, 0.0, -6.0, -6.0], [4 * np.pi, 4 * np.pi, 6.0, 6.0], 0.125, K + 1, 10)
+    with _ctx(pkg, dom, dtype, "fused") as ctx:
+        f0 = ctx.empty_f()
+        ctx.init_case(f0, IC_LANDAU_SUM, 0.05, 0.5)
+        a, b = f0.clone(), ctx.empty_f()
+        for it in range(1, K + 1):
+            ctx.step(a, b, it)
+            a, b = b, a
+        single = a.clone()
+        nrj1, mass1 = ctx.diags_read(K + 1)
+        c, d = f0.clone(), ctx.empty_f()
+        ctx.steps(c, d, 1, K)
+        nrj2, mass2 = ctx.diags_read(K + 1)
+        assert torch.equal(d, single)
+        assert np.array_equal(nrj1[1:], nrj2[1:]) and np.array_equal(mass1[1:], mass2[1:])
+
+
+@pytest.mark.parametrize("n", [(16, 4, 16, 4), (32, 32, 32, 32), (12, 10, 14, 10)])
+def test_steps_generic_and_oracle(pkg, cuda, n):
+    """The fused time loop against the generic kernels' separate passes and
+    against the FP64 CPU oracle (shapes include ones the fused passes decline)."""
+    torch = cuda
+    K = 3
+    dom = pkg.Domain(list(n), [0.0, 0.0, -6.0, -6.0], [4 * np.pi, 4 * np.pi, 6.0, 6.0], 0.125, K + 1, 10)
+    ora = Restatement(dom.nxmax, dom.min_phy, dom.max_phy, dom.dt, 10)
+    f0 = ora.init_case(IC_LANDAU_SUM, amp=0.05, k=0.5)
+    f_ref, nrj_ref, _, _, _ = ora.run(f0, K)
+    outs = {}
+    for kernels in ("", "generic"):
+        with _ctx(pkg, dom, "f64", kernels) as ctx:
+            a = torch.from_numpy(f0).cuda()
+            b = ctx.empty_f()
+            ctx.field_rho(a)
+            ctx.field_poisson()
+            ctx.diags_compute(0)
+            ctx.steps(a, b, 1, K)
+            outs[kernels] = (b.cpu().numpy(), ctx.diags_read(K + 1)[0])
+    for f, nrj in outs.values():
+        assert np.abs(f - f_ref).max() <= 1e-12 * np.abs(f_ref).max()
+        assert np.abs(nrj - nrj_ref).max() < 1e-10
