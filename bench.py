@@ -170,6 +170,22 @@ def time_calls(torch, stream, fn, reps):
     return e0.elapsed_time(e1) / 1e3 / reps
 
 
+def dram_traffic(n: int, kernel: str):
+    """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
+    summary of the n^4 FP32 workload (lines "<kernel> <bytes>"), or None."""
+    path = ROOT / "profiles" / f"dram_traffic_landau{n}_f32.txt"
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        parts = line.split()
+        if len(parts) == 2 and parts[0] == kernel and not line.startswith("#"):
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
 def gpu_arm(args, ranks):
     import torch
 
@@ -183,8 +199,6 @@ def gpu_arm(args, ranks):
     K, W = args.steps, max(args.warmup, 3)
     n = args.n
     dom = pkg.landau_domain(n, dt=DT, nbiter=W + K + 2, L=L_BOX, vmax=VMAX)
-    # Algorithmic f traffic of one step: 2 x/y passes + 1 v pass (read + write
-    # each) through vlp4d_steps, 3 such passes through vlp4d_step.
     cells = dom.cells
     sampler = ClockSampler(ranks.local_rank)
     try:
@@ -243,6 +257,7 @@ def gpu_arm(args, ranks):
             st["advec1D_vy"] = time_calls(torch, stream, lambda: ctx.advect_vy(cur, nxt, DT), reps)
             st["advect_xy"] = time_calls(torch, stream, lambda: ctx.advect_xy(cur, nxt, 0.5 * DT), reps)
             st["advect_vxvy"] = time_calls(torch, stream, lambda: ctx.advect_vxvy(cur, nxt, DT), reps)
+            st["advect_xyxy"] = time_calls(torch, stream, lambda: ctx.advect_xyxy(cur, nxt, 0.5 * DT), reps)
             st["field"] = time_calls(torch, stream, lambda: ctx.field_rho(cur), reps)
             st["Fourier"] = time_calls(torch, stream, lambda: ctx.field_poisson(), reps)
             st["diag"] = time_calls(torch, stream, lambda: ctx.diags_compute(1), reps)
@@ -259,26 +274,23 @@ def gpu_arm(args, ranks):
 
     clocks = sampler.stop()
 
-    # Roofline of the dominant kernel: the fused x/y plane pass (two of the
-    # three passes of a step).  Algorithmic bytes per launch: f read once +
-    # written once.
+    # Roofline of the dominant kernel of the time loop.  Each step between
+    # the first and the last runs one k_plane_xyxy pass (two x/y half steps)
+    # and one k_vslab pass (vx then vy); both read f once and write it once,
+    # so the algorithmic bytes per launch are 2 * cells * 4 (FP32).
     peak, peak_kind = measured_hbm_peak()
     f32 = per_dtype["f32"]
-    t_xy = f32["stages"]["advect_xy"]["ms"] / 1e3
+    t_xx = f32["stages"]["advect_xyxy"]["ms"] / 1e3
     t_vv = f32["stages"]["advect_vxvy"]["ms"] / 1e3
-    dominant = "advect_xy (k_plane, fused x+y half step)" if 2 * t_xy >= t_vv else "advect_vxvy (k_vslab)"
-    t_dom = t_xy if 2 * t_xy >= t_vv else t_vv
+    dominant = "advect_xyxy (k_plane_xyxy, two x/y half steps)" if t_xx >= t_vv else "advect_vxvy (k_vslab)"
+    t_dom = max(t_xx, t_vv)
     achieved = 2.0 * cells * 4 / t_dom / 1e9
-    traffic = None
-    tf = ROOT / "profiles" / "traffic.json"
-    if tf.exists():
-        try:
-            traffic = json.loads(tf.read_text()).get("plane_f32_128" if "xy" in dominant else "vslab_f32_128")
-        except ValueError:
-            traffic = None
+    traffic = dram_traffic(n, "k_plane_xyxy" if "xy" in dominant else "k_vslab")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "kernel": dominant, "peak_kind": peak_kind,
                 "bytes_per_launch": 2 * cells * 4,
+                # Whole-step fractions: f is read and written once per pass;
+                # vlp4d_steps runs 2 passes per step, vlp4d_step 3.
                 "step_frac_3pass": (6.0 * cells * 4 / (f32["per_step_api"]["ms_per_step"] / 1e3) / 1e9) / peak,
                 "step_frac_2pass": (4.0 * cells * 4 / (f32["ms_per_step"] / 1e3) / 1e9) / peak}
 

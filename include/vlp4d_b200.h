@@ -119,6 +119,17 @@ int vlp4d_advect_vy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void 
  * advect_1D_vy in one pass.  Equal to the 1D sequence up to FP rounding. */
 int vlp4d_advect_xy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream);
 int vlp4d_advect_vxvy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream);
+/* Two x/y shifts by dt in one pass followed by the moment of the result
+ * into the context's rho: the last x/y half step of one Strang step and the
+ * first of the next (timestep.hpp:50-58 then :17-28 with dt/2 each), the
+ * pass vlp4d_steps runs between steps.  f equals vlp4d_advect_xy applied
+ * twice, bit for bit; rho equals vlp4d_field_rho of it up to summation
+ * order.  Returns VLP4D_ERR_UNSUPPORTED, launching nothing, when the
+ * one-pass kernel does not fit the shape or the buffers (nx not a multiple
+ * of 4, not 16-byte aligned, shared memory) or VLP4D_KERNELS=generic: the
+ * caller then uses two vlp4d_advect_xy calls.  No reference counterpart as a
+ * single call. */
+int vlp4d_advect_xyxy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream);
 
 /* field_rho (miniapps/vlp4d/thrust/field.cpp:6-32): rho = dvx*dvy*sum_v f. */
 int vlp4d_field_rho(vlp4d_ctx *ctx, const void *fn, void *stream);

@@ -480,6 +480,9 @@ namespace {
 struct PlaneCfg {
   int R = 0, rt = 1, stages = 3, threads = 0, cpp = 1, grid = 0, G = 0;
   size_t smem = 0;
+  bool query = false;  // only fill per_sm (resident CTAs per SM), launch nothing
+  int per_sm = 0;
+  int fixed_G = 0;  // plane groups to launch (0: as many as fit one wave)
 };
 
 int env_int(const char *name, int dflt) {
@@ -548,8 +551,10 @@ int run_plane(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, cudaStream_t s
   int per_sm = 0;
   VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, cfg.threads, cfg.smem));
   if (per_sm < 1) return VLP4D_ERR_UNSUPPORTED;
+  cfg.per_sm = per_sm;
+  if (cfg.query) return VLP4D_OK;
   const long long planes = (long long)args.nvx * args.nvy;
-  long long G = ((long long)per_sm * c->num_sms) / cfg.cpp;
+  long long G = cfg.fixed_G > 0 ? cfg.fixed_G : ((long long)per_sm * c->num_sms) / cfg.cpp;
   if (G < 1) G = 1;
   if (G > planes) G = planes;
   if (RHO && G > c->rho_part_groups) G = c->rho_part_groups;
@@ -582,16 +587,9 @@ int run_plane_rt(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, cudaStream_
 
 }  // namespace
 
-// Returns VLP4D_ERR_UNSUPPORTED (without launching anything) when the shape
-// or the buffers do not meet the kernel's requirements; the caller then
-// uses the generic kernels.
-int launch_advect_xy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *tx, const StencilTable *ty,
-                     bool do_x, bool do_y, bool with_rho, cudaStream_t s) {
-  if (!c->fused) return VLP4D_ERR_UNSUPPORTED;
-  if (((uintptr_t)fn & 15) || ((uintptr_t)fnp1 & 15)) return VLP4D_ERR_UNSUPPORTED;
-  if (!do_x && !do_y) return VLP4D_ERR_UNSUPPORTED;
-  PlaneCfg cfg;
-  if (!plane_config(c, do_x, do_y, cfg)) return VLP4D_ERR_UNSUPPORTED;
+namespace {
+
+PlaneArgs plane_args(const vlp4d_ctx *c, const void *fn, void *fnp1, const PlaneCfg &cfg, int halo) {
   PlaneArgs a;
   a.fin = fn;
   a.fout = fnp1;
@@ -601,36 +599,41 @@ int launch_advect_xy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTabl
   a.nvy = c->g.n[3];
   a.R = cfg.R;
   a.cpp = cfg.cpp;
-  a.halo = do_y ? 5 : 0;
+  a.halo = halo;
   a.stages = cfg.stages;
-  if (tx) a.tx = *tx;
-  if (ty) a.ty = *ty;
   a.rho_part = c->rho_part;
   a.err = c->d_err;
-  int rc;
-#define VLP4D_PLANE(T, DX, DY, RHO) rc = run_plane_rt<T, DX, DY, RHO>(c, a, cfg, s)
-  if (c->dtype == VLP4D_F64) {
-    if (do_x && do_y) { if (with_rho) VLP4D_PLANE(double, true, true, true); else VLP4D_PLANE(double, true, true, false); }
-    else if (do_x) VLP4D_PLANE(double, true, false, false);
-    else VLP4D_PLANE(double, false, true, false);
-  } else {
-    if (do_x && do_y) { if (with_rho) VLP4D_PLANE(float, true, true, true); else VLP4D_PLANE(float, true, true, false); }
-    else if (do_x) VLP4D_PLANE(float, true, false, false);
-    else VLP4D_PLANE(float, false, true, false);
-  }
-#undef VLP4D_PLANE
-  if (rc) return rc;
-  if (with_rho && do_x && do_y) return launch_rho_finish(c, cfg.G, s);
-  if (with_rho) return launch_field_rho(c, fnp1, s);
-  return VLP4D_OK;
+  return a;
 }
-
-namespace {
 
 size_t xyxy_smem(int R, int nx, size_t elem, int stages, int nvx, int nvy) {
   const size_t rec = elem == 4 ? 32 : 64;
   return kBarBytes + rec * (nvx + nvy) + (size_t)stages * (R + 10) * nx * elem +
          (size_t)(R + 10 + 2 * (R + 5)) * nx * elem;
+}
+
+// Chunk height (the tallest divisor of ny up to 32 rows whose block and
+// shared memory fit), rows per thread and pipeline depth of k_plane_xyxy.
+bool xyxy_config(const vlp4d_ctx *c, PlaneCfg &cfg) {
+  const int nx = c->g.n[0], ny = c->g.n[1];
+  if (nx % 4 != 0 || nx > 2048) return false;
+  const int ncg = nx / 4;
+  cfg.stages = env_int("VLP4D_XYXY_STAGES", 2);
+  if (cfg.stages < 2 || cfg.stages > kMaxStages) return false;
+  cfg.R = 0;
+  for (int r = ny < 32 ? ny : 32; r >= 1 && !cfg.R; --r) {
+    if (ny % r) continue;
+    const int t = r % 4 == 0 ? 4 : 1;
+    if (ncg * (r / t) > 512 || ncg * (r / t) < 1) continue;
+    if (xyxy_smem(r, nx, c->elem, cfg.stages, c->g.n[2], c->g.n[3]) > 224 * 1024) continue;
+    cfg.R = r;
+    cfg.rt = t;
+  }
+  if (!cfg.R) return false;
+  cfg.cpp = ny / cfg.R;
+  cfg.threads = ncg * (cfg.R / cfg.rt);
+  cfg.smem = xyxy_smem(cfg.R, nx, c->elem, cfg.stages, c->g.n[2], c->g.n[3]);
+  return true;
 }
 
 template <typename T, int NX, int RT>
@@ -640,8 +643,10 @@ int run_xyxy(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, cudaStream_t s)
   int per_sm = 0;
   VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, cfg.threads, cfg.smem));
   if (per_sm < 1) return VLP4D_ERR_UNSUPPORTED;
+  cfg.per_sm = per_sm;
+  if (cfg.query) return VLP4D_OK;
   const long long planes = (long long)args.nvx * args.nvy;
-  long long G = ((long long)per_sm * c->num_sms) / cfg.cpp;
+  long long G = cfg.fixed_G > 0 ? cfg.fixed_G : ((long long)per_sm * c->num_sms) / cfg.cpp;
   if (G < 1) G = 1;
   if (G > planes) G = planes;
   if (G > c->rho_part_groups) G = c->rho_part_groups;
@@ -662,7 +667,88 @@ int run_xyxy_nx(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, cudaStream_t
   }
 }
 
+int run_xyxy_any(vlp4d_ctx *c, const PlaneArgs &a, PlaneCfg &cfg, cudaStream_t s) {
+  if (c->dtype == VLP4D_F64)
+    return cfg.rt == 4 ? run_xyxy_nx<double, 4>(c, a, cfg, s) : run_xyxy_nx<double, 1>(c, a, cfg, s);
+  return cfg.rt == 4 ? run_xyxy_nx<float, 4>(c, a, cfg, s) : run_xyxy_nx<float, 1>(c, a, cfg, s);
+}
+
+int run_plane_moment(vlp4d_ctx *c, const PlaneArgs &a, PlaneCfg &cfg, cudaStream_t s) {
+  if (c->dtype == VLP4D_F64) return run_plane_rt<double, true, true, true>(c, a, cfg, s);
+  return run_plane_rt<float, true, true, true>(c, a, cfg, s);
+}
+
+// The plane-group count of the fused moment: the smaller of the one-wave
+// group counts of k_plane (x+y with the moment) and k_plane_xyxy, so that
+// both use the same summation order; 0 when neither kernel fits the shape.
+int moment_groups(vlp4d_ctx *c) {
+  if (c->moment_G) return c->moment_G > 0 ? c->moment_G : 0;
+  const long long planes = (long long)c->g.n[2] * c->g.n[3];
+  long long G = 0;
+  PlaneCfg cp;
+  if (plane_config(c, true, true, cp)) {
+    cp.query = true;
+    PlaneArgs a = plane_args(c, nullptr, nullptr, cp, 5);
+    if (run_plane_moment(c, a, cp, 0) == VLP4D_OK && cp.per_sm > 0)
+      G = (long long)cp.per_sm * c->num_sms / cp.cpp;
+  }
+  PlaneCfg cx;
+  if (xyxy_config(c, cx)) {
+    cx.query = true;
+    PlaneArgs a = plane_args(c, nullptr, nullptr, cx, 10);
+    if (run_xyxy_any(c, a, cx, 0) == VLP4D_OK && cx.per_sm > 0) {
+      const long long gx = (long long)cx.per_sm * c->num_sms / cx.cpp;
+      G = G ? (gx < G ? gx : G) : gx;
+    }
+  }
+  cudaGetLastError();  // a failed query leaves nothing behind
+  if (G > planes) G = planes;
+  if (G > c->rho_part_groups) G = c->rho_part_groups;
+  if (G < 1) {
+    c->moment_G = -1;
+    return 0;
+  }
+  c->moment_G = (int)G;
+  return c->moment_G;
+}
+
 }  // namespace
+
+// Returns VLP4D_ERR_UNSUPPORTED (without launching anything) when the shape
+// or the buffers do not meet the kernel's requirements; the caller then
+// uses the generic kernels.
+int launch_advect_xy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *tx, const StencilTable *ty,
+                     bool do_x, bool do_y, bool with_rho, cudaStream_t s) {
+  if (!c->fused) return VLP4D_ERR_UNSUPPORTED;
+  if (((uintptr_t)fn & 15) || ((uintptr_t)fnp1 & 15)) return VLP4D_ERR_UNSUPPORTED;
+  if (!do_x && !do_y) return VLP4D_ERR_UNSUPPORTED;
+  PlaneCfg cfg;
+  if (!plane_config(c, do_x, do_y, cfg)) return VLP4D_ERR_UNSUPPORTED;
+  const bool moment = with_rho && do_x && do_y;
+  if (moment) {
+    cfg.fixed_G = moment_groups(c);
+    if (!cfg.fixed_G) return VLP4D_ERR_UNSUPPORTED;
+  }
+  PlaneArgs a = plane_args(c, fn, fnp1, cfg, do_y ? 5 : 0);
+  if (tx) a.tx = *tx;
+  if (ty) a.ty = *ty;
+  int rc;
+#define VLP4D_PLANE(T, DX, DY, RHO) rc = run_plane_rt<T, DX, DY, RHO>(c, a, cfg, s)
+  if (c->dtype == VLP4D_F64) {
+    if (do_x && do_y) { if (moment) VLP4D_PLANE(double, true, true, true); else VLP4D_PLANE(double, true, true, false); }
+    else if (do_x) VLP4D_PLANE(double, true, false, false);
+    else VLP4D_PLANE(double, false, true, false);
+  } else {
+    if (do_x && do_y) { if (moment) VLP4D_PLANE(float, true, true, true); else VLP4D_PLANE(float, true, true, false); }
+    else if (do_x) VLP4D_PLANE(float, true, false, false);
+    else VLP4D_PLANE(float, false, true, false);
+  }
+#undef VLP4D_PLANE
+  if (rc) return rc;
+  if (moment) return launch_rho_finish(c, cfg.G, s);
+  if (with_rho) return launch_field_rho(c, fnp1, s);
+  return VLP4D_OK;
+}
 
 // Two x/y half steps and the moment of the result in one pass; returns
 // VLP4D_ERR_UNSUPPORTED (nothing launched) when the shape does not fit.
@@ -670,44 +756,14 @@ int launch_advect_xyxy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTa
                        cudaStream_t s) {
   if (!c->fused) return VLP4D_ERR_UNSUPPORTED;
   if (((uintptr_t)fn & 15) || ((uintptr_t)fnp1 & 15)) return VLP4D_ERR_UNSUPPORTED;
-  const int nx = c->g.n[0], ny = c->g.n[1];
-  if (nx % 4 != 0 || nx > 2048) return VLP4D_ERR_UNSUPPORTED;
   PlaneCfg cfg;
-  const int ncg = nx / 4;
-  for (int r = ny < 32 ? ny : 32; r >= 1 && !cfg.R; --r) {
-    if (ny % r) continue;
-    const int t = r % 4 == 0 ? 4 : 1;
-    if (ncg * (r / t) > 512 || ncg * (r / t) < 1) continue;
-    cfg.R = r;
-    cfg.rt = t;
-  }
-  if (!cfg.R) return VLP4D_ERR_UNSUPPORTED;
-  cfg.stages = env_int("VLP4D_XYXY_STAGES", 2);
-  if (cfg.stages < 2 || cfg.stages > kMaxStages) return VLP4D_ERR_UNSUPPORTED;
-  cfg.cpp = ny / cfg.R;
-  cfg.threads = ncg * (cfg.R / cfg.rt);
-  cfg.smem = xyxy_smem(cfg.R, nx, c->elem, cfg.stages, c->g.n[2], c->g.n[3]);
-  if (cfg.smem > 224 * 1024) return VLP4D_ERR_UNSUPPORTED;
-  PlaneArgs a;
-  a.fin = fn;
-  a.fout = fnp1;
-  a.nx = nx;
-  a.ny = ny;
-  a.nvx = c->g.n[2];
-  a.nvy = c->g.n[3];
-  a.R = cfg.R;
-  a.cpp = cfg.cpp;
-  a.halo = 10;
-  a.stages = cfg.stages;
+  if (!xyxy_config(c, cfg)) return VLP4D_ERR_UNSUPPORTED;
+  cfg.fixed_G = moment_groups(c);
+  if (!cfg.fixed_G) return VLP4D_ERR_UNSUPPORTED;
+  PlaneArgs a = plane_args(c, fn, fnp1, cfg, 10);
   a.tx = *tx;
   a.ty = *ty;
-  a.rho_part = c->rho_part;
-  a.err = c->d_err;
-  int rc;
-  if (c->dtype == VLP4D_F64)
-    rc = cfg.rt == 4 ? run_xyxy_nx<double, 4>(c, a, cfg, s) : run_xyxy_nx<double, 1>(c, a, cfg, s);
-  else
-    rc = cfg.rt == 4 ? run_xyxy_nx<float, 4>(c, a, cfg, s) : run_xyxy_nx<float, 1>(c, a, cfg, s);
+  int rc = run_xyxy_any(c, a, cfg, s);
   if (rc) return rc;
   return launch_rho_finish(c, cfg.G, s);
 }

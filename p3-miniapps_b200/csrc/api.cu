@@ -202,6 +202,8 @@ int vlp4d_ctx_create(const vlp4d_domain *dom, int dtype, vlp4d_ctx **out) {
     const char *k = getenv("VLP4D_KERNELS");
     c->fused = !(k && strcmp(k, "generic") == 0);
     c->fused_only = k && strcmp(k, "fused") == 0;
+    const char *xx = getenv("VLP4D_XYXY");
+    if (xx && *xx) c->xyxy_mode = atoi(xx) ? 1 : 0;
   }
 #undef CTX_ALLOC
   if (cudaMemset(c->rho, 0, sizeof(double) * nxy) != cudaSuccess ||
@@ -322,6 +324,22 @@ int vlp4d_advect_xy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void 
   return advect_xy_impl(ctx, fn, fnp1, dt, false, as_stream(stream));
 }
 
+int vlp4d_advect_xyxy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if ((rc = check_pair(fn, fnp1))) return rc;
+  if (!std::isfinite(dt)) return fail(VLP4D_ERR_INVALID_ARG, "dt is not finite");
+  cudaStream_t s = as_stream(stream);
+  StencilTable *tx = nullptr, *ty = nullptr;
+  if ((rc = ensure_xy_table(ctx, 0, dt, &tx, s))) return rc;
+  if ((rc = ensure_xy_table(ctx, 1, dt, &ty, s))) return rc;
+  rc = launch_advect_xyxy(ctx, fn, fnp1, tx, ty, s);
+  if (rc == VLP4D_ERR_UNSUPPORTED)
+    return fail(rc, "advect_xyxy: the one-pass kernel does not fit this shape, these buffers or VLP4D_KERNELS; "
+                    "call vlp4d_advect_xy twice");
+  return rc;
+}
+
 int vlp4d_advect_vxvy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream) {
   int rc = check_ctx(ctx);
   if (rc) return rc;
@@ -416,6 +434,16 @@ int vlp4d_step(vlp4d_ctx *ctx, void *f_state, void *f_next, int iter, void *stre
 
 // The reference's time loop (vlp4d.cpp:63-72, onetimestep per step) with
 // the last x/y half step of each step fused with the first of the next.
+// Whether vlp4d_steps joins the x/y half steps of consecutive steps into one
+// k_plane_xyxy pass.  That pass does the arithmetic of two passes for the
+// HBM traffic of one: it pays off in FP32, while in FP64 its shared-memory
+// footprint leaves one CTA per SM and two k_plane passes are faster.
+// VLP4D_XYXY=0/1 at context creation overrides.
+static bool xyxy_preferred(const vlp4d_ctx *ctx) {
+  if (ctx->xyxy_mode >= 0) return ctx->xyxy_mode == 1;
+  return ctx->dtype == VLP4D_F32;
+}
+
 int vlp4d_steps(vlp4d_ctx *ctx, void *f_state, void *f_next, int iter0, int nsteps, void *stream) {
   int rc = check_ctx(ctx);
   if (rc) return rc;
@@ -439,9 +467,14 @@ int vlp4d_steps(vlp4d_ctx *ctx, void *f_state, void *f_next, int iter0, int nste
     if ((rc = advect_vxvy_impl(ctx, cur, oth, dt, s))) return rc;
     std::swap(cur, oth);
     if (k + 1 == nsteps) break;
-    // timestep.hpp:50-58 of step k, then :17-28 of step k+1, in one pass.
-    rc = launch_advect_xyxy(ctx, cur, oth, tx, ty, s);
-    if (rc == VLP4D_ERR_UNSUPPORTED) {
+    // timestep.hpp:50-58 of step k, then :17-28 of step k+1, in one pass
+    // where that pass is the faster choice.
+    rc = xyxy_preferred(ctx) ? launch_advect_xyxy(ctx, cur, oth, tx, ty, s) : VLP4D_ERR_UNSUPPORTED;
+    if (rc == VLP4D_ERR_UNSUPPORTED && !xyxy_preferred(ctx)) {
+      if ((rc = advect_xy_impl(ctx, cur, oth, 0.5 * dt, false, s))) return rc;
+      std::swap(cur, oth);
+      if ((rc = advect_xy_impl(ctx, cur, oth, 0.5 * dt, true, s))) return rc;
+    } else if (rc == VLP4D_ERR_UNSUPPORTED) {
       if ((rc = fused_declined(ctx))) return rc;
       if ((rc = advect_xy_impl(ctx, cur, oth, 0.5 * dt, false, s))) return rc;
       std::swap(cur, oth);

@@ -98,6 +98,14 @@ struct vlp4d_ctx {
   double *rho_part = nullptr;
   int rho_groups = 0;
   int rho_part_groups = 0;
+  // Plane groups of the moment fused into the x/y passes (k_plane with the
+  // moment, k_plane_xyxy): one value for both kernels, so that the moment's
+  // summation order, and with it every later bit, does not depend on which
+  // of the two produced it.  0 until first computed.
+  int moment_G = 0;
+  // VLP4D_XYXY at creation: -1 unset, 0 never join x/y half steps across
+  // steps, 1 always (when the kernel fits the shape).
+  int xyxy_mode = -1;
 
   // Kernel selection, read from VLP4D_KERNELS at context creation:
   // unset = fused kernels where the shape allows, generic otherwise;

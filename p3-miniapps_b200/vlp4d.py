@@ -32,7 +32,7 @@ EXPORTS = (
     "vlp4d_advect_vy", "vlp4d_advect_xy", "vlp4d_advect_vxvy", "vlp4d_field_rho", "vlp4d_field_poisson",
     "vlp4d_diags_compute", "vlp4d_diags_read", "vlp4d_diags_save", "vlp4d_step", "vlp4d_run",
     "vlp4d_print_fxvx", "vlp4d_transpose", "vlp4d_check", "vlp4d_kernel_launches",
-    "vlp4d_field_rho_noalloc", "vlp4d_steps",
+    "vlp4d_field_rho_noalloc", "vlp4d_steps", "vlp4d_advect_xyxy",
 )
 
 
@@ -80,7 +80,7 @@ def lib() -> C.CDLL:
         L.vlp4d_field_ptr.argtypes = [vp, i, C.POINTER(vp)]
         L.vlp4d_init_case.argtypes = [vp, vp, i, d, d, d, vp]
         for n in ("vlp4d_advect_x", "vlp4d_advect_y", "vlp4d_advect_vx", "vlp4d_advect_vy", "vlp4d_advect_xy",
-                  "vlp4d_advect_vxvy"):
+                  "vlp4d_advect_vxvy", "vlp4d_advect_xyxy"):
             getattr(L, n).argtypes = [vp, vp, vp, d, vp]
         L.vlp4d_field_rho.argtypes = [vp, vp, vp]
         L.vlp4d_field_poisson.argtypes = [vp, vp]
@@ -257,6 +257,10 @@ class Context:
 
     def advect_xy(self, fn, fnp1, dt, stream=None):
         _check(lib().vlp4d_advect_xy(self.h, self._f(fn), self._f(fnp1), dt, _stream_ptr(stream)))
+
+    def advect_xyxy(self, fn, fnp1, dt, stream=None):
+        """Two x/y shifts by dt in one pass, then the moment of fnp1 into rho."""
+        _check(lib().vlp4d_advect_xyxy(self.h, self._f(fn), self._f(fnp1), dt, _stream_ptr(stream)))
 
     def advect_vxvy(self, fn, fnp1, dt, stream=None):
         _check(lib().vlp4d_advect_vxvy(self.h, self._f(fn), self._f(fnp1), dt, _stream_ptr(stream)))

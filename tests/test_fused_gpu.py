@@ -19,16 +19,18 @@ pytestmark = pytest.mark.gpu
 SHAPES = [(8, 8, 8, 8), (16, 4, 16, 4), (32, 32, 32, 32), (64, 48, 16, 64), (128, 64, 32, 40)]
 
 
-def _ctx(pkg, dom, dtype, kernels):
-    old = os.environ.get("VLP4D_KERNELS")
+def _ctx(pkg, dom, dtype, kernels, xyxy=""):
+    saved = {k: os.environ.get(k) for k in ("VLP4D_KERNELS", "VLP4D_XYXY")}
     os.environ["VLP4D_KERNELS"] = kernels
+    os.environ["VLP4D_XYXY"] = xyxy
     try:
         return pkg.Context(dom, dtype)
     finally:
-        if old is None:
-            del os.environ["VLP4D_KERNELS"]
-        else:
-            os.environ["VLP4D_KERNELS"] = old
+        for k, v in saved.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
 
 
 def _dom(pkg, n, dt=0.2):
@@ -143,15 +145,16 @@ def test_unaligned_buffers_fall_back_to_generic(pkg, cuda):
 
 @pytest.mark.parametrize("n", SHAPES)
 @pytest.mark.parametrize("dtype", ["f64", "f32"])
-def test_steps_bit_identical_to_single_steps(pkg, cuda, n, dtype):
+@pytest.mark.parametrize("xyxy", ["0", "1"])
+def test_steps_bit_identical_to_single_steps(pkg, cuda, n, dtype, xyxy):
     """vlp4d_steps runs the last x/y half step of each step and the first of
-    the next as one pass; every sweep is the same operation in the same
-    order and precision, so K fused steps equal K calls of vlp4d_step bit for
-    bit, diagnostics included."""
+    the next as one pass (VLP4D_XYXY=1) or as two (=0); every sweep is the
+    same operation in the same order and precision, so K steps equal K calls
+    of vlp4d_step bit for bit, diagnostics included."""
     torch = cuda
     K = 4
     dom = pkg.Domain(list(n), [0.0, 0.0, -6.0, -6.0], [4 * np.pi, 4 * np.pi, 6.0, 6.0], 0.125, K + 1, 10)
-    with _ctx(pkg, dom, dtype, "fused") as ctx:
+    with _ctx(pkg, dom, dtype, "fused", xyxy) as ctx:
         f0 = ctx.empty_f()
         ctx.init_case(f0, IC_LANDAU_SUM, 0.05, 0.5)
         a, b = f0.clone(), ctx.empty_f()
@@ -190,3 +193,31 @@ def test_steps_generic_and_oracle(pkg, cuda, n):
     for f, nrj in outs.values():
         assert np.abs(f - f_ref).max() <= 1e-12 * np.abs(f_ref).max()
         assert np.abs(nrj - nrj_ref).max() < 1e-10
+
+
+@pytest.mark.parametrize("n", SHAPES + [(12, 10, 14, 10)])
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_advect_xyxy_matches_two_xy_passes(pkg, cuda, n, dtype):
+    """vlp4d_advect_xyxy (one pass) against vlp4d_advect_xy twice: bit-identical
+    f; the moment it leaves in rho against field_rho of the result."""
+    torch = cuda
+    dom = _dom(pkg, n)
+    for kernels in ("", "generic"):
+        with _ctx(pkg, dom, dtype, kernels) as ctx:
+            f0 = ctx.empty_f()
+            ctx.init_case(f0, IC_TWO_STREAM, 0.2, 0.5, 2.0)
+            a, b, c = ctx.empty_f(), ctx.empty_f(), ctx.empty_f()
+            ctx.advect_xy(f0, a, 0.15)
+            ctx.advect_xy(a, b, 0.15)
+            ctx.field_rho(b)
+            rho_sep = ctx.rho.clone()
+            if kernels == "generic":
+                with pytest.raises(pkg.vlp4d.Vlp4dError) as e:
+                    ctx.advect_xyxy(f0, c, 0.15)
+                assert e.value.code == pkg.vlp4d.ERR_UNSUPPORTED
+                continue
+            ctx.advect_xyxy(f0, c, 0.15)
+            rho_one = ctx.rho.clone()
+            assert torch.equal(b, c), kernels
+            assert float((rho_one - rho_sep).abs().max()) <= 1e-13 * float(rho_sep.abs().max())
+            ctx.check()
