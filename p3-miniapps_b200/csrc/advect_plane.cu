@@ -58,21 +58,30 @@ __device__ __forceinline__ int wrap_col(int c, int nx) {
 // aligned column a0 = c0 + mx - r; output q uses t[r+q .. r+q+5].  r is the
 // same for the whole CTA (c0 is a multiple of 4), so the switch is uniform.
 template <int R_>
-__device__ __forceinline__ void x4_from(const double (&t)[12], const double (&w)[6], double (&o)[4]) {
+__device__ __forceinline__ void x4_from(const double (&t)[12], const SweepW<double> &w, double (&o)[4]) {
 #pragma unroll
   for (int q = 0; q < 4; ++q)
-    o[q] = interp6(w, t[R_ + q], t[R_ + q + 1], t[R_ + q + 2], t[R_ + q + 3], t[R_ + q + 4], t[R_ + q + 5]);
+    o[q] = interp6(w.w, t[R_ + q], t[R_ + q + 1], t[R_ + q + 2], t[R_ + q + 3], t[R_ + q + 4], t[R_ + q + 5]);
 }
+// FP32: outputs (0,1) and (2,3) as packed pairs; pair j of differences is
+// (d_j, d_{j+1}) with d_j = t[r+j+1] - t[r+j].
 template <int R_>
-__device__ __forceinline__ void x4_from(const float (&t)[12], const float (&v)[6], float (&o)[4]) {
+__device__ __forceinline__ void x4_from(const float (&t)[12], const SweepW<float> &w, float (&o)[4]) {
   float d[8];
 #pragma unroll
   for (int j = 0; j < 8; ++j) d[j] = t[R_ + j + 1] - t[R_ + j];
+  float2 dp[7];
 #pragma unroll
-  for (int q = 0; q < 4; ++q) o[q] = interp_diff(v, t[R_ + q + 2], d[q], d[q + 1], d[q + 2], d[q + 3], d[q + 4]);
+  for (int j = 0; j < 7; ++j) dp[j] = make_float2(d[j], d[j + 1]);
+  const float2 lo = interp_diff2(w.v, make_float2(t[R_ + 2], t[R_ + 3]), dp[0], dp[1], dp[2], dp[3], dp[4]);
+  const float2 hi = interp_diff2(w.v, make_float2(t[R_ + 4], t[R_ + 5]), dp[2], dp[3], dp[4], dp[5], dp[6]);
+  o[0] = lo.x;
+  o[1] = lo.y;
+  o[2] = hi.x;
+  o[3] = hi.y;
 }
 template <typename T>
-__device__ __forceinline__ void sweep_x4(const T (&t)[12], int r, const T (&w)[6], T (&o)[4]) {
+__device__ __forceinline__ void sweep_x4(const T (&t)[12], int r, const SweepW<T> &w, T (&o)[4]) {
   switch (r) {
     case 0: x4_from<0>(t, w, o); break;
     case 1: x4_from<1>(t, w, o); break;
@@ -85,7 +94,7 @@ __device__ __forceinline__ void sweep_x4(const T (&t)[12], int r, const T (&w)[6
 // starting at src (stride nx), written in streaming order so that only a
 // window of rows and differences is live; `emit(i, o)` receives row i.
 template <int RT, typename Emit>
-__device__ __forceinline__ void sweep_y(const double *src, int nx, const double (&w)[6], Emit emit) {
+__device__ __forceinline__ void sweep_y(const double *src, int nx, const SweepW<double> &w, Emit emit) {
   double y[RT + 5][4];
 #pragma unroll
   for (int j = 0; j < RT + 5; ++j) {
@@ -94,27 +103,31 @@ __device__ __forceinline__ void sweep_y(const double *src, int nx, const double 
       const int i = j - 5;
       double o[4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) o[q] = interp6(w, y[i][q], y[i + 1][q], y[i + 2][q], y[i + 3][q], y[i + 4][q], y[j][q]);
+      for (int q = 0; q < 4; ++q)
+        o[q] = interp6(w.w, y[i][q], y[i + 1][q], y[i + 2][q], y[i + 3][q], y[i + 4][q], y[j][q]);
       emit(i, o);
     }
   }
 }
+// FP32: columns (0,1) and (2,3) of the quad as packed pairs.
 template <int RT, typename Emit>
-__device__ __forceinline__ void sweep_y(const float *src, int nx, const float (&v)[6], Emit emit) {
-  float y[RT + 5][4], d[RT + 4][4];
+__device__ __forceinline__ void sweep_y(const float *src, int nx, const SweepW<float> &w, Emit emit) {
+  float2 y[RT + 5][2], d[RT + 4][2];
 #pragma unroll
   for (int j = 0; j < RT + 5; ++j) {
-    load4(src + (size_t)j * nx, y[j]);
+    const float4 q4 = *reinterpret_cast<const float4 *>(src + (size_t)j * nx);
+    y[j][0] = make_float2(q4.x, q4.y);
+    y[j][1] = make_float2(q4.z, q4.w);
     if (j >= 1) {
 #pragma unroll
-      for (int q = 0; q < 4; ++q) d[j - 1][q] = y[j][q] - y[j - 1][q];
+      for (int h = 0; h < 2; ++h) d[j - 1][h] = sub2(y[j][h], y[j - 1][h]);
     }
     if (j >= 5) {
       const int i = j - 5;
-      float o[4];
+      float2 o2[2];
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
-        o[q] = interp_diff(v, y[i + 2][q], d[i][q], d[i + 1][q], d[i + 2][q], d[i + 3][q], d[i + 4][q]);
+      for (int h = 0; h < 2; ++h) o2[h] = interp_diff2(w.v, y[i + 2][h], d[i][h], d[i + 1][h], d[i + 2][h], d[i + 3][h], d[i + 4][h]);
+      const float o[4] = {o2[0].x, o2[0].y, o2[1].x, o2[1].y};
       emit(i, o);
     }
   }
@@ -247,8 +260,10 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
     T *xs = xs_base + (size_t)(it & 1) * slot_elems;
 
     if (DX) {  // Phase X: staged rows rg, rg+RG, ...; this thread's column quad.
-      T wx[6];
-      int base = c0 + read_line(xrec[ivx], wx);
+      T wl[6];
+      int base = c0 + read_line(xrec[ivx], wl);
+      SweepW<T> wx;
+      make_sweep_w(wl, wx);
       base = wrap_col<NX>(base, nx);
       const int rr = base & 3;
       const int o0 = base - rr, o1 = wrap_col<NX>(o0 + 4, nx), o2 = wrap_col<NX>(o0 + 8, nx);
@@ -279,8 +294,10 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
       if (threadIdx.x == 0 && it + S < n_items) issue(it + S);
     }
     if (DY) {  // Phase Y: rows r0 .. r0+RT-1 of this thread's column quad.
-      T wy[6];
-      read_line(yrec[ivy], wy);
+      T wl[6];
+      read_line(yrec[ivy], wl);
+      SweepW<T> wy;
+      make_sweep_w(wl, wy);
       const T *src = (DX ? xs : in) + (size_t)r0 * nx + c0;
       T *dst = outp + (size_t)r0 * nx + c0;
       sweep_y<RT>(src, nx, wy, [&](int i, const T (&o)[4]) {
@@ -396,7 +413,7 @@ __global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
     for (int q = 0; q < 4; ++q) racc[i][q] = 0.0;
 
   // x sweep of rows [0, nrows) of src into dst (rows rg, rg+RG, ...).
-  auto sweep_rows_x = [&](const T *src, T *dst, int nrows, int o0, int o1, int o2, int rr, const T (&wx)[6]) {
+  auto sweep_rows_x = [&](const T *src, T *dst, int nrows, int o0, int o1, int o2, int rr, const SweepW<T> &wx) {
     for (int v = rg; v < nrows; v += RG) {
       const T *row = src + (size_t)v * nx;
       T t[12], q4[4];
@@ -421,9 +438,12 @@ __global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
     const long long p = g + it * G;
     const T *in = slots + (size_t)slot * slot_elems;
     T *outp = static_cast<T *>(a.fout) + p * plane_elems + (long long)chunk * R * nx;
-    T wx[6], wy[6];
-    int base = c0 + read_line(xrec[ivx], wx);
-    read_line(yrec[ivy], wy);
+    T wlx[6], wly[6];
+    int base = c0 + read_line(xrec[ivx], wlx);
+    read_line(yrec[ivy], wly);
+    SweepW<T> wx, wy;
+    make_sweep_w(wlx, wx);
+    make_sweep_w(wly, wy);
     base = wrap_col<NX>(base, nx);
     const int rr = base & 3;
     const int o0 = base - rr, o1 = wrap_col<NX>(o0 + 4, nx), o2 = wrap_col<NX>(o0 + 8, nx);

@@ -15,7 +15,9 @@
 // depends only on the column, so per-column offsets never conflict), keeps
 // the last six vx-swept rows in registers and emits output row ivy once the
 // six rows ivy+o..ivy+o+5 of its own column's vy offset o are in the window.
-// Stores of a warp cover C consecutive columns: 128 contiguous bytes.
+// Stores of a warp cover C consecutive columns: 128 contiguous bytes.  In
+// FP32 a thread evaluates its vx rows i and i+V/2 as one packed pair (same
+// column, same weights), with the f32x2 instructions.
 #include <cudaTypedefs.h>
 
 #include "internal.cuh"
@@ -61,20 +63,11 @@ __device__ __noinline__ void vslab_abort(const VslabArgs &a, uint64_t *bars, con
   __syncwarp();
 }
 
-// vx sweep of V outputs from V+5 taps (plain FP64 form / FP32 adjacent
-// differences shared between neighbouring outputs).
+// FP64 vx sweep of V outputs from V+5 taps (the FP32 path is packed inline).
 template <int V>
 __device__ __forceinline__ void vx_sweep(const double (&t)[V + 5], const double (&w)[6], double (&o)[V]) {
 #pragma unroll
   for (int i = 0; i < V; ++i) o[i] = interp6(w, t[i], t[i + 1], t[i + 2], t[i + 3], t[i + 4], t[i + 5]);
-}
-template <int V>
-__device__ __forceinline__ void vx_sweep(const float (&t)[V + 5], const float (&w)[6], float (&o)[V]) {
-  float d[V + 4];
-#pragma unroll
-  for (int j = 0; j < V + 4; ++j) d[j] = t[j + 1] - t[j];
-#pragma unroll
-  for (int i = 0; i < V; ++i) o[i] = interp_diff(w, t[i + 2], d[i], d[i + 1], d[i + 2], d[i + 3], d[i + 4]);
 }
 
 // Position in the CTA's slab sequence: item, slab index within the item,
@@ -203,11 +196,25 @@ __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorM
     }
     // Output pointer of the next row this thread writes.
     T *orow = static_cast<T *>(a.fout) + ixy + vstride * vx0 + ystride * (long long)sg * a.Q;
-    T win[6][V];  // ring of vx-swept rows, slot = t % 6 (static after unrolling)
+    // Ring of vx-swept rows, slot = t % 6 (static after unrolling).  FP64:
+    // win[slot][i] is vx row vx0+i.  FP32: packed pairs, win2[slot][i] holds
+    // vx rows (vx0+i, vx0+i+V/2), which share the column's weights.
+    constexpr int H = V / 2;
+    constexpr bool kF32 = sizeof(T) == 4;
+    T win[6][kF32 ? 1 : V];
+    float2 win2[6][kF32 ? H : 1];
 #pragma unroll
-    for (int j = 0; j < 6; ++j)
+    for (int j = 0; j < 6; ++j) {
 #pragma unroll
-      for (int i = 0; i < V; ++i) win[j][i] = T(0);
+      for (int i = 0; i < (kF32 ? 1 : V); ++i) win[j][i] = T(0);
+#pragma unroll
+      for (int i = 0; i < (kF32 ? H : 1); ++i) win2[j][i] = make_float2(0.f, 0.f);
+    }
+    SweepW<float> svx, svy;
+    if constexpr (kF32) {
+      if (DVX) make_sweep_w(reinterpret_cast<const float(&)[6]>(wvx), svx);
+      if (DVY) make_sweep_w(reinterpret_cast<const float(&)[6]>(wvy), svy);
+    }
 
     for (int t0 = 0; t0 < cnt; t0 += 6) {
 #pragma unroll
@@ -219,14 +226,31 @@ __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorM
           return;
         }
         const T *sl = slabs + (size_t)slot * slab_elems;
-        if (DVX) {
-          T tap[V + 5];
+        if constexpr (kF32) {
+          const float *slf = reinterpret_cast<const float *>(sl);
+          if (DVX) {
+            // P[k] = (tap k, tap k+H); D[k] = (d_k, d_{k+H}), d_k = tap k+1 - tap k.
+            float2 P[H + 5], D[H + 4];
 #pragma unroll
-          for (int q = 0; q < V + 5; ++q) tap[q] = sl[off[q]];
-          vx_sweep<V>(tap, wvx, win[u]);
+            for (int q = 0; q < H + 5; ++q) P[q] = make_float2(slf[off[q]], slf[off[q + H]]);
+#pragma unroll
+            for (int q = 0; q < H + 4; ++q) D[q] = sub2(P[q + 1], P[q]);
+#pragma unroll
+            for (int i = 0; i < H; ++i) win2[u][i] = interp_diff2(svx.v, P[i + 2], D[i], D[i + 1], D[i + 2], D[i + 3], D[i + 4]);
+          } else {
+#pragma unroll
+            for (int i = 0; i < H; ++i) win2[u][i] = make_float2(slf[off[i]], slf[off[i + H]]);
+          }
         } else {
+          if (DVX) {
+            T tap[V + 5];
 #pragma unroll
-          for (int i = 0; i < V; ++i) win[u][i] = sl[off[i]];
+            for (int q = 0; q < V + 5; ++q) tap[q] = sl[off[q]];
+            vx_sweep<V>(tap, wvx, win[u]);
+          } else {
+#pragma unroll
+            for (int i = 0; i < V; ++i) win[u][i] = sl[off[i]];
+          }
         }
         // This warp is done with the slot: count it; the last warp refills it.
         __syncwarp();
@@ -249,15 +273,32 @@ __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorM
           emit = e >= 0 && e < a.Q;
         }
         if (emit) {
+          if constexpr (kF32) {
+            float *orowf = reinterpret_cast<float *>(orow);
 #pragma unroll
-          for (int i = 0; i < V; ++i) {
-            T val;
-            if (DVY)  // rows t-5 .. t sit in slots u+1 .. u+6 (mod 6)
-              val = interp6(wvy, win[(u + 1) % 6][i], win[(u + 2) % 6][i], win[(u + 3) % 6][i],
-                            win[(u + 4) % 6][i], win[(u + 5) % 6][i], win[u][i]);
-            else
-              val = win[u][i];
-            orow[vstride * i] = val;
+            for (int i = 0; i < H; ++i) {
+              float2 val;
+              if (DVY) {  // rows t-5 .. t sit in slots u+1 .. u+6 (mod 6)
+                const float2 f0 = win2[(u + 1) % 6][i], f1 = win2[(u + 2) % 6][i], f2 = win2[(u + 3) % 6][i],
+                             f3 = win2[(u + 4) % 6][i], f4 = win2[(u + 5) % 6][i], f5 = win2[u][i];
+                val = interp_diff2(svy.v, f2, sub2(f1, f0), sub2(f2, f1), sub2(f3, f2), sub2(f4, f3), sub2(f5, f4));
+              } else {
+                val = win2[u][i];
+              }
+              orowf[vstride * i] = val.x;
+              orowf[vstride * (i + H)] = val.y;
+            }
+          } else {
+#pragma unroll
+            for (int i = 0; i < V; ++i) {
+              T val;
+              if (DVY)  // rows t-5 .. t sit in slots u+1 .. u+6 (mod 6)
+                val = interp6(wvy, win[(u + 1) % 6][i], win[(u + 2) % 6][i], win[(u + 3) % 6][i],
+                              win[(u + 4) % 6][i], win[(u + 5) % 6][i], win[u][i]);
+              else
+                val = win[u][i];
+              orow[vstride * i] = val;
+            }
           }
           orow += ystride;
         }

@@ -45,6 +45,43 @@ __device__ __forceinline__ float interp6(const float (&v)[6], float f0, float f1
   return interp_diff(v, f2, f1 - f0, f2 - f1, f3 - f2, f4 - f3, f5 - f4);
 }
 
+// Packed FP32 pairs (the sm_100 f32x2 FMA/MUL/ADD instructions).  Each lane
+// rounds exactly as the scalar round-to-nearest operation does, so the
+// packed evaluation of the difference form gives the same bits as the
+// scalar one.  a - b is formed as fma(b, -1, a): -b is exact, so the single
+// rounding is that of the subtraction.
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+
+// interp_diff on two lanes that share their weights; v[j] = (v_j, v_j).
+__device__ __forceinline__ float2 interp_diff2(const float2 (&v)[5], float2 f2, float2 d0, float2 d1, float2 d2,
+                                               float2 d3, float2 d4) {
+  float2 acc = __fmul2_rn(v[0], d0);
+  acc = __ffma2_rn(v[1], d1, acc);
+  acc = __ffma2_rn(v[2], d2, acc);
+  acc = __ffma2_rn(v[3], d3, acc);
+  acc = __ffma2_rn(v[4], d4, acc);
+  return __fadd2_rn(f2, acc);
+}
+
+// Weights as the sweeps consume them: the six FP64 weights, or the five FP32
+// difference weights duplicated into both lanes of a pair.
+template <typename T>
+struct SweepW {
+  T w[6];
+};
+template <>
+struct SweepW<float> {
+  float2 v[5];
+};
+__device__ __forceinline__ void make_sweep_w(const double (&w)[6], SweepW<double> &s) {
+#pragma unroll
+  for (int k = 0; k < 6; ++k) s.w[k] = w[k];
+}
+__device__ __forceinline__ void make_sweep_w(const float (&w)[6], SweepW<float> &s) {
+#pragma unroll
+  for (int k = 0; k < 5; ++k) s.v[k] = make_float2(w[k], w[k]);
+}
+
 template <typename T>
 struct WeightsOf;
 template <>
