@@ -342,6 +342,8 @@ def gpu_arm(args, ranks):
         del finals
         torch.cuda.empty_cache()
 
+    adjoint = None if args.only_f32 else adjoint_arm(pkg, torch, stream)
+
     rec = per_dtype["f32"]
     line = {
         "metric": METRIC, "value": rec["value"], "unit": METRIC, "n_gpus": ranks.world, "steps": K, "warmup": W,
@@ -359,8 +361,47 @@ def gpu_arm(args, ranks):
                  "published_a100_stdpar_f64": 7.19,
                  "stages": per_dtype["f64"]["stages"]} if "f64" in per_dtype else None),
         "stages": rec["stages"], "error_f32_vs_f64": err,
+        "adjoint": adjoint,
     }
     return line
+
+
+def adjoint_arm(pkg, torch, stream, n=64, nsteps=200, every=8):
+    """Reverse mode on the adjoint configuration: Landau 64^4, dt 0.1, T = 20
+    (200 steps), FP32 f / FP64 fields, a checkpoint every 8 steps.  Times the
+    forward run with checkpoints, the reverse run (segment recomputation
+    included) and, as the forward reference, the same steps through
+    vlp4d_steps; device time with CUDA events."""
+    v = pkg.vlp4d
+    dom = pkg.landau_domain(n, dt=0.1, nbiter=nsteps + 1, idcase=110)
+    out = {"config": {"grid": [n] * 4, "dt": 0.1, "steps": nsteps, "checkpoint_every": every,
+                      "storage": "f32 f, f64 fields", "objective": "dx dy sum |E(T)|^2"}}
+    with pkg.Context(dom, "f32") as ctx, v.Adjoint(ctx, nsteps, every) as adj:
+        f0 = ctx.empty_f()
+        ctx.init_case(f0, v.IC_LANDAU_SUM, 0.05, 0.5)
+        a, b = f0.clone(), ctx.empty_f()
+        ctx.field_rho(a)
+        ctx.field_poisson()
+        ctx.diags_compute(0)
+        grad = ctx.empty_f()
+        adj.forward(f0)  # warm-up (allocations, tables)
+        adj.backward(grad)
+        fwd_steps = time_calls(torch, stream, lambda: ctx.steps(a.clone(), b, 1, nsteps), 3)
+        t_fwd = time_calls(torch, stream, lambda: adj.forward(f0), 3)
+        t_bwd = time_calls(torch, stream, lambda: adj.backward(grad), 3)
+        J = adj.forward(f0)
+        out.update({
+            "J": J,
+            "forward_steps_ms_per_step": fwd_steps * 1e3 / nsteps,
+            "forward_with_checkpoints_ms_per_step": t_fwd * 1e3 / nsteps,
+            "backward_ms_per_step": t_bwd * 1e3 / nsteps,
+            "ratio_backward_to_forward_steps": t_bwd / fwd_steps,
+            "ratio_backward_to_forward_checkpointed": t_bwd / t_fwd,
+            "grad_finite": bool(torch.isfinite(grad).all().item()),
+        })
+        del a, b, grad, f0
+    torch.cuda.empty_cache()
+    return out
 
 
 # ---------------------------------------------------------------- CPU reference

@@ -4,8 +4,8 @@
  * Every entry point replaces one function of the reference's single-process
  * CUDA variant (miniapps/vlp4d/thrust); the citation in each comment is the
  * reference interface it stands in for.  The C++ layer in
- * p3-miniapps_b200/cpp/vlp4d_api.hpp re-exports these under the reference's
- * own C++ signatures (Advection::advect_1D_x(Config*, const RealView4D&, ...)).
+ * p3-miniapps_b200/cpp/refshim/ re-exports these under the reference's own
+ * C++ signatures (Advection::advect_1D_x(Config*, const RealView4D&, ...)).
  *
  * Conventions
  * - The distribution function f is a caller-owned DEVICE buffer of
@@ -19,7 +19,8 @@
  *   context, index ix + nx*iy (miniapps/vlp4d/thrust/efield.hpp:13-16).
  * - `stream` is a cudaStream_t passed as void* (NULL = legacy default
  *   stream).  All calls are stream-ordered and asynchronous unless stated;
- *   none allocates device memory after vlp4d_ctx_create.
+ *   none allocates device memory after vlp4d_ctx_create except
+ *   vlp4d_adjoint_create, which allocates the reverse-mode state.
  * - Every function returns VLP4D_OK (0) or an error code; none exits the
  *   process (the reference's SafeCudaCall exits, lib/Cuda_Helper.hpp:8-16).
  *   vlp4d_last_error() gives a message for the calling thread.
@@ -204,6 +205,42 @@ int vlp4d_field_rho_noalloc(const void *fn, int dtype, int nx, int ny, int nvx, 
  * out-of-place transpose of a (rows x cols) column-major matrix of
  * elements of `elem_size` bytes (4, 8 or 16). */
 int vlp4d_transpose(const void *in, void *out, int rows, int cols, int elem_size, void *stream);
+
+/* ---- Reverse mode (discrete adjoint).  No reference counterpart: the
+ * reference has no derivative code.  The adjoint is that of vlp4d_step as
+ * computed here: transposed interpolation for the x/y shifts, transposed
+ * interpolation plus the derivative of the Lagrange weights with respect to
+ * E for the vx/vy shifts, back through field_poisson (the transpose of the
+ * spectral solve, from its impulse responses) and field_rho.  f, lambda and
+ * gradients have the context's element type and layout.
+ *
+ * The run-level objective is J(f_N) = dx*dy * sum_{x,y} (Ex^2 + Ey^2): the
+ * electric energy of the field solved from the state after nsteps steps. */
+typedef struct vlp4d_adjoint vlp4d_adjoint;
+
+/* Allocates the reverse-mode state for runs of nsteps steps of ctx with a
+ * checkpoint of f every `every` steps: ceil(nsteps/every) checkpoints, every-1
+ * recompute buffers and six work buffers, each one f.  The recomputation of
+ * a segment therefore holds `every` states at a time.  Runs one field solve
+ * on a unit impulse (the context's rho/Ex/Ey are restored). */
+int vlp4d_adjoint_create(vlp4d_ctx *ctx, int nsteps, int every, vlp4d_adjoint **out);
+int vlp4d_adjoint_destroy(vlp4d_adjoint *adj);
+
+/* nsteps steps from f0 (device, not modified), keeping the checkpoints;
+ * the final state is copied to f_out when f_out is not NULL and J receives
+ * the objective (host pointer, may be NULL).  Synchronises the stream. */
+int vlp4d_adjoint_forward(vlp4d_adjoint *adj, const void *f0, void *f_out, double *J, void *stream);
+/* grad = dJ/df0 for the last vlp4d_adjoint_forward; recomputes each segment
+ * from its checkpoint, then runs the reverse steps.  Synchronises. */
+int vlp4d_adjoint_backward(vlp4d_adjoint *adj, void *grad, void *stream);
+
+/* One reverse step: lam_out = (d step/d f)^T lam_next, the step taken at
+ * the state f_state (vlp4d_step's map f_state -> f_next).  lam_out must not
+ * alias the inputs.  Overwrites the context's rho/Ex/Ey and v tables. */
+int vlp4d_step_adjoint(vlp4d_adjoint *adj, const void *f_state, const void *lam_next, void *lam_out, void *stream);
+/* J(f) and lam = dJ/df; J is a host pointer (may be NULL; when given, the
+ * call synchronises the stream). */
+int vlp4d_energy_grad(vlp4d_adjoint *adj, const void *f, double *J, void *lam, void *stream);
 
 #ifdef __cplusplus
 }

@@ -78,6 +78,16 @@ class Restatement:
             lib.orc_step.argtypes = [P, _dp, _dp, _dp, _dp, _dp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
             lib.orc_run.argtypes = [P, _dp, _dp, _dp, _dp, _dp, C.c_int, _dp, _dp]
             lib.orc_init_case.argtypes = [P, _dp, C.c_int, C.c_double, C.c_double, C.c_double]
+            # FP64 discrete adjoint (vlp4d_adjoint.c).
+            lib.orc_lag_basis5_deriv.argtypes = [C.c_double, _dp]
+            for name in ("orc_advect_x_T", "orc_advect_y_T"):
+                getattr(lib, name).argtypes = [P, _dp, _dp, C.c_double]
+            for name in ("orc_advect_vx_T", "orc_advect_vy_T"):
+                getattr(lib, name).argtypes = [P, _dp, _dp, _dp, C.c_double, _dp, _dp]
+            lib.orc_field_poisson_T.argtypes = [P, _dp, _dp, _dp]
+            lib.orc_energy_grad.argtypes = [P, _dp, C.POINTER(C.c_double), _dp]
+            lib.orc_step_adjoint.argtypes = [P, _dp, _dp, _dp]
+            lib.orc_adjoint_run.argtypes = [P, _dp, C.c_int, C.POINTER(C.c_double), _dp]
             cls._lib = lib
         return cls._lib
 
@@ -160,6 +170,73 @@ class Restatement:
         out = np.zeros((ny, nx))
         self.L.orc_irfft2(nx, ny, buf, out)
         return out
+
+    # ---- FP64 discrete adjoint (oracle/vlp4d_adjoint.c) ----
+
+    def lag_basis_deriv(self, px):
+        c = np.zeros(6)
+        self.L.orc_lag_basis5_deriv(px, c)
+        return c
+
+    def advect_x_T(self, lam, dt):
+        out = self.empty4()
+        self.L.orc_advect_x_T(C.byref(self.d), np.ascontiguousarray(lam), out, dt)
+        return out
+
+    def advect_y_T(self, lam, dt):
+        out = self.empty4()
+        self.L.orc_advect_y_T(C.byref(self.d), np.ascontiguousarray(lam), out, dt)
+        return out
+
+    def advect_vx_T(self, lam, f_in, ex, dt):
+        """Returns (A^T lam, dJ/dEx) for the vx stage evaluated at its input f_in."""
+        out, g = self.empty4(), self.empty2()
+        self.L.orc_advect_vx_T(C.byref(self.d), np.ascontiguousarray(lam), np.ascontiguousarray(f_in),
+                               np.ascontiguousarray(ex), dt, out, g)
+        return out, g
+
+    def advect_vy_T(self, lam, f_in, ey, dt):
+        out, g = self.empty4(), self.empty2()
+        self.L.orc_advect_vy_T(C.byref(self.d), np.ascontiguousarray(lam), np.ascontiguousarray(f_in),
+                               np.ascontiguousarray(ey), dt, out, g)
+        return out, g
+
+    def field_poisson_T(self, gex, gey):
+        out = self.empty2()
+        self.L.orc_field_poisson_T(C.byref(self.d), np.ascontiguousarray(gex), np.ascontiguousarray(gey), out)
+        return out
+
+    def energy_grad(self, f):
+        """J = dx dy sum |E|^2 of the field solved from f, and dJ/df."""
+        J = C.c_double()
+        lam = self.empty4()
+        self.L.orc_energy_grad(C.byref(self.d), np.ascontiguousarray(f), C.byref(J), lam)
+        return J.value, lam
+
+    def step_adjoint(self, f_state, lam_next):
+        out = self.empty4()
+        self.L.orc_step_adjoint(C.byref(self.d), np.ascontiguousarray(f_state), np.ascontiguousarray(lam_next), out)
+        return out
+
+    def adjoint_run(self, f0, nsteps):
+        """J(f after nsteps steps) and dJ/df0."""
+        J = C.c_double()
+        grad = self.empty4()
+        self.L.orc_adjoint_run(C.byref(self.d), np.ascontiguousarray(f0, dtype=np.float64), nsteps, C.byref(J), grad)
+        return J.value, grad
+
+    def step(self, f):
+        """One Strang step of f (diagnostics discarded)."""
+        fn = np.array(f, dtype=np.float64, copy=True)
+        fnp1 = self.empty4()
+        rho, ex, ey = self.empty2(), self.empty2(), self.empty2()
+        nrj, mass = C.c_double(), C.c_double()
+        self.L.orc_step(C.byref(self.d), fn, fnp1, rho, ex, ey, C.byref(nrj), C.byref(mass))
+        return fn
+
+    def energy(self, f):
+        _, ex, ey = self.field_poisson(self.field_rho(f))
+        return float((ex * ex + ey * ey).sum() * self.dx[0] * self.dx[1])
 
     def run(self, f0, nsteps):
         """Initial solve + nsteps Strang steps; returns (f, nrj[nsteps+1], mass[nsteps+1], ex, ey)."""

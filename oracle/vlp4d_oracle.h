@@ -68,6 +68,20 @@ void orc_run(const orc_domain *d, double *fn, double *fnp1, double *rho, double 
 
 void orc_init_case(const orc_domain *d, double *f, int ic, double amp, double k, double u);
 
+/* FP64 discrete adjoint of the restated step (vlp4d_adjoint.c).  The
+ * objective is J(f) = dx*dy * sum (Ex^2 + Ey^2), E solved from f. */
+void orc_lag_basis5_deriv(double px, double dcoef[6]);
+void orc_advect_x_T(const orc_domain *d, const double *lam_out, double *lam_in, double dt);
+void orc_advect_y_T(const orc_domain *d, const double *lam_out, double *lam_in, double dt);
+void orc_advect_vx_T(const orc_domain *d, const double *lam_out, const double *f_in, const double *ex,
+                     double dt, double *lam_in, double *gex);
+void orc_advect_vy_T(const orc_domain *d, const double *lam_out, const double *f_in, const double *ey,
+                     double dt, double *lam_in, double *gey);
+void orc_field_poisson_T(const orc_domain *d, const double *gex, const double *gey, double *lam_rho);
+void orc_energy_grad(const orc_domain *d, const double *f, double *J, double *lam);
+void orc_step_adjoint(const orc_domain *d, const double *f_state, const double *lam_next, double *lam_out);
+void orc_adjoint_run(const orc_domain *d, const double *f0, int nsteps, double *J, double *grad);
+
 #ifdef __cplusplus
 }
 #endif

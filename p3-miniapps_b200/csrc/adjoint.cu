@@ -1,0 +1,584 @@
+// Reverse mode of the vlp4d step: the discrete adjoint of what vlp4d_step
+// computes, with step checkpointing for runs.
+//
+// Forward step n (timestep.hpp:14-67, as step_impl runs it):
+//   a = XY f                       x then y shifts by dt/2 (linear, fixed tables)
+//   rho = dvx*dvy * sum_v a ;  E = D rho     (D: the FP64 spectral field solve)
+//   b = VXVY(a; E)                 vx then vy shifts by dt*E(x, y)
+//   f' = XY b
+// Reverse step, given lambda' = dJ/df':
+//   lb = XY^T lambda'
+//   gE = dJ/dE: gEx = <lb, (dVX/dEx (x) VY) a>, gEy = <lb, (VX (x) dVY/dEy) a>
+//        per (x, y), summed over the velocity plane
+//   la = VXVY^T lb + dvx*dvy * broadcast(D^T gE)
+//   lambda = XY^T la
+// Facts used:
+// * a line's gather out[i] = sum_k w_k in[(i+m+k) mod n] has as transpose the
+//   gather with offset (-m-5) mod n and reversed weights, so XY^T and
+//   VXVY^T are the forward kernels (k_plane, k_vslab or the generic ones)
+//   run with transposed line tables; x and y sweeps commute exactly (their
+//   weights depend on different indices), and so do vx and vy, so the
+//   forward kernels' sweep order also serves the transposes;
+// * a shift's weights depend on E through the foot position d only:
+//   dd/dE = -dt/dh inside a cell, so dw_k/dE = lag_basis5'(d)_k * (-dt/dh);
+// * D is linear and translation-invariant (the rho -= 1 of cases 10/20 only
+//   touches the zeroed mode), so D^T is the correlation with D's impulse
+//   responses hx, hy: (D^T g)^ = conj(hx^) gx^ + conj(hy^) gy^.  The
+//   impulse responses are computed once by running the forward field solve
+//   on a unit impulse, so the transpose is exact for whatever the forward
+//   FFT path does (including its treatment of the Nyquist modes).
+//
+// Objective of the run-level API: J(f_N) = dx*dy * sum (Ex^2 + Ey^2), the
+// electric energy of the field solved from the final state.
+#include <cmath>
+#include <vector>
+
+#include "internal.cuh"
+#include "stencil.cuh"
+
+using vlp4d::StencilTable;
+
+struct vlp4d_adjoint {
+  vlp4d_ctx *ctx = nullptr;
+  int nsteps = 0, every = 0;
+  size_t fbytes = 0;
+  std::vector<void *> ckpt;  // f at steps 0, every, 2*every, ...
+  std::vector<void *> seg;   // recomputed states of one segment (every - 1)
+  void *P[2] = {nullptr, nullptr};  // forward ping-pong
+  void *W[2] = {nullptr, nullptr};  // step-adjoint work / forward scratch
+  void *L[2] = {nullptr, nullptr};  // adjoint states
+  // FP64 2D work: dJ/dEx, dJ/dEy, dJ/drho, the objective, saved fields.
+  double *gex = nullptr, *gey = nullptr, *lam_rho = nullptr, *d_J = nullptr, *save = nullptr;
+  double *gpart = nullptr;  // per-segment partial sums of gE
+  int gsegs = 0;
+  cufftDoubleComplex *hx_hat = nullptr, *hy_hat = nullptr;  // spectra of the impulse responses
+  bool field_linear = true;  // false for the analytic-field cases 2 and 6
+  StencilTable tab_x_adj, tab_y_adj, tab_vx_adj, tab_vy_adj;
+  double *dw_vx = nullptr, *dw_vy = nullptr;  // dw/dE per v line (6 each, FP64)
+  bool have_forward = false;
+  double J = 0.0;
+};
+
+namespace vlp4d {
+namespace {
+
+// Transposed v tables and the weight derivatives of one direction, from E.
+__global__ void k_build_vtable_adj(const double *__restrict__ e, int lines, double dt, double hmin, double hmax,
+                                   int n, int *__restrict__ m, double *__restrict__ w, float *__restrict__ wf,
+                                   double *__restrict__ dw) {
+  const int line = blockIdx.x * blockDim.x + threadIdx.x;
+  if (line >= lines) return;
+  const LineStencil s = line_stencil(__dmul_rn(dt, e[line]), hmin, hmax, n);
+  const LineStencil t = adjoint_stencil(s, n);
+  m[line] = t.m;
+  float f[6];
+  weights_to_f32(t.w, f);
+  double dc[6];
+  lag_basis5_deriv(s.d, dc);
+  const double scale = -dt / ((hmax - hmin) / (double)n);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    w[6 * line + k] = t.w[k];
+    wf[6 * line + k] = f[k];
+    dw[6 * line + k] = dc[k] * scale;
+  }
+}
+
+// gE partial sums.  Block (32 columns) x (GY vx groups); grid (column
+// chunks, vy segments).  A thread owns one column ixy and the output vx rows
+// ty, ty+GY, ...; for each it streams the input vy rows of its segment (the
+// Q outputs plus the five-row halo, starting at the column's vy offset),
+// keeping the last six vx-swept rows (value A and vx-derivative B) in a
+// ring, and accumulates lb * (sum_l wy_l B_l) and lb * (sum_l dwy_l A_l).
+// The ring slot of row r is r mod 6, static after unrolling by six.
+template <typename T>
+__global__ void __launch_bounds__(256) k_vgrad(const T *__restrict__ a, const T *__restrict__ lb, int nxy, int nvx,
+                                               int nvy, int Q, StencilTable tvx, StencilTable tvy,
+                                               const double *__restrict__ dwx, const double *__restrict__ dwy,
+                                               double *__restrict__ part) {
+  const int tx = threadIdx.x, ty = threadIdx.y, GY = blockDim.y;
+  const int ixy = blockIdx.x * 32 + tx;
+  const int seg = blockIdx.y;
+  const int ivy0 = seg * Q;
+  const int q = min(Q, nvy - ivy0);
+  double gx = 0., gy = 0.;
+  if (ixy < nxy && q > 0) {
+    const long long vstride = nxy, ystride = (long long)nxy * nvx;
+    double wx[6], dx[6], wy[6], dy[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      wx[k] = tvx.w[6 * (long long)ixy + k];
+      dx[k] = dwx[6 * (long long)ixy + k];
+      wy[k] = tvy.w[6 * (long long)ixy + k];
+      dy[k] = dwy[6 * (long long)ixy + k];
+    }
+    const int mx = tvx.m[ixy], my = tvy.m[ixy];
+    for (int ivx = ty; ivx < nvx; ivx += GY) {
+      long long toff[6];
+      int j = ivx + mx;
+      if (j >= nvx) j -= nvx;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        toff[k] = (long long)j * vstride + ixy;
+        if (++j == nvx) j = 0;
+      }
+      double A[6], B[6];
+      int row = (ivy0 + my) % nvy;
+      const int nrows = q + 5;
+      for (int r0 = 0; r0 < nrows; r0 += 6) {
+#pragma unroll
+        for (int u = 0; u < 6; ++u) {
+          const int r = r0 + u;
+          if (r >= nrows) break;
+          const T *p = a + (long long)row * ystride;
+          double s = 0., sd = 0.;
+#pragma unroll
+          for (int k = 0; k < 6; ++k) {
+            const double v = (double)__ldg(p + toff[k]);
+            s = fma(wx[k], v, s);
+            sd = fma(dx[k], v, sd);
+          }
+          A[u] = s;
+          B[u] = sd;
+          if (++row == nvy) row = 0;
+          if (r >= 5) {
+            const int ivy = ivy0 + r - 5;
+            const double l = (double)__ldg(lb + (long long)ivy * ystride + (long long)ivx * vstride + ixy);
+            double sx = 0., sy = 0.;
+#pragma unroll
+            for (int t = 0; t < 6; ++t) {
+              sx = fma(wy[t], B[(u + 1 + t) % 6], sx);
+              sy = fma(dy[t], A[(u + 1 + t) % 6], sy);
+            }
+            gx = fma(l, sx, gx);
+            gy = fma(l, sy, gy);
+          }
+        }
+      }
+    }
+  }
+  // Sum the vx groups in a fixed order.
+  __shared__ double sx[8][32], sy[8][32];
+  sx[ty][tx] = gx;
+  sy[ty][tx] = gy;
+  __syncthreads();
+  if (ty == 0 && ixy < nxy) {
+    double ax = 0., ay = 0.;
+    for (int g = 0; g < GY; ++g) {
+      ax += sx[g][tx];
+      ay += sy[g][tx];
+    }
+    part[(2LL * seg) * nxy + ixy] = ax;
+    part[(2LL * seg + 1) * nxy + ixy] = ay;
+  }
+}
+
+__global__ void k_vgrad_finish(const double *__restrict__ part, int nseg, int nxy, double *__restrict__ gex,
+                               double *__restrict__ gey) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nxy) return;
+  double ax = 0., ay = 0.;
+  for (int s = 0; s < nseg; ++s) {
+    ax += part[(2LL * s) * nxy + i];
+    ay += part[(2LL * s + 1) * nxy + i];
+  }
+  gex[i] = ax;
+  gey[i] = ay;
+}
+
+// lam_hat = (conj(hx_hat) gx_hat + conj(hy_hat) gy_hat) / (nx*ny).
+__global__ void k_field_transpose(const cufftDoubleComplex *__restrict__ gx, const cufftDoubleComplex *__restrict__ gy,
+                                  const cufftDoubleComplex *__restrict__ hx, const cufftDoubleComplex *__restrict__ hy,
+                                  cufftDoubleComplex *__restrict__ out, int nh, double norm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nh) return;
+  const cufftDoubleComplex a = gx[i], b = gy[i], p = hx[i], q = hy[i];
+  cufftDoubleComplex r;
+  r.x = (p.x * a.x + p.y * a.y + q.x * b.x + q.y * b.y) * norm;
+  r.y = (p.x * a.y - p.y * a.x + q.x * b.y - q.y * b.x) * norm;
+  out[i] = r;
+}
+
+// f[v*nxy + ixy] (+)= scale * col[ixy] for every velocity cell v.
+template <typename T, bool ADD>
+__global__ void k_columns(T *__restrict__ f, const double *__restrict__ col, double scale, long long nxy,
+                          long long total) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double c = scale * col[i % nxy];
+    f[i] = ADD ? (T)((double)f[i] + c) : (T)c;
+  }
+}
+
+// J = dxdy * sum (ex^2 + ey^2) (Kahan, one block, fixed order) and
+// gex = 2 dxdy ex, gey = 2 dxdy ey.
+__global__ void k_energy(const double *__restrict__ ex, const double *__restrict__ ey, long long n, double dxdy,
+                         double *__restrict__ J, double *__restrict__ gex, double *__restrict__ gey) {
+  double s = 0., c = 0.;
+  for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+    const double a = ex[i], b = ey[i];
+    const double y = (a * a + b * b) - c;
+    const double t = s + y;
+    c = (t - s) - y;
+    s = t;
+    gex[i] = 2. * dxdy * a;
+    gey[i] = 2. * dxdy * b;
+  }
+  s -= c;
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  __shared__ double ws[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) ws[warp] = s;
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    s = lane < nw ? ws[lane] : 0.;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) *J = s * dxdy;
+  }
+}
+
+int grid_cap(long long total, int threads, int sms) {
+  long long b = (total + threads - 1) / threads;
+  const long long cap = (long long)sms * 16;
+  return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
+}
+
+}  // namespace
+}  // namespace vlp4d
+
+namespace vlp4d {
+namespace {
+
+// Transposed x (dim 0) and y (dim 1) tables for shifts by dt*v, built on the
+// host like ensure_xy_table's and uploaded.
+int build_xy_adj(vlp4d_ctx *c, int dim, double dt, StencilTable &t, cudaStream_t s) {
+  const int vdim = dim == 0 ? 2 : 3;
+  const int lines = c->g.n[vdim];
+  int rc = alloc_table(t, lines);
+  if (rc) return rc;
+  std::vector<int> hm(lines);
+  std::vector<double> hw(6 * (size_t)lines);
+  std::vector<float> hwf(6 * (size_t)lines);
+  for (int l = 0; l < lines; ++l) {
+    const double v = c->g.minp[vdim] + l * c->g.dx[vdim];
+    const LineStencil st = adjoint_stencil(line_stencil(dt * v, c->g.minp[dim], c->g.maxp[dim], c->g.n[dim]), c->g.n[dim]);
+    hm[l] = st.m;
+    float f[6];
+    weights_to_f32(st.w, f);
+    for (int k = 0; k < 6; ++k) {
+      hw[6 * l + k] = st.w[k];
+      hwf[6 * l + k] = f[k];
+    }
+  }
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(t.m, hm.data(), sizeof(int) * lines, cudaMemcpyHostToDevice, s));
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(t.w, hw.data(), sizeof(double) * 6 * lines, cudaMemcpyHostToDevice, s));
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(t.wf, hwf.data(), sizeof(float) * 6 * lines, cudaMemcpyHostToDevice, s));
+  VLP4D_CUDA_TRY(cudaStreamSynchronize(s));
+  t.dt = dt;
+  t.valid = true;
+  return VLP4D_OK;
+}
+
+// Spectra of the field solve's impulse responses (section comment above).
+// The context's rho/Ex/Ey are saved and restored around the probe solve.
+int field_transpose_setup(vlp4d_adjoint *A, cudaStream_t s) {
+  vlp4d_ctx *c = A->ctx;
+  const long long n2 = c->g.nxy();
+  if (c->dom.idcase == 2 || c->dom.idcase == 6) {
+    A->field_linear = false;
+    return VLP4D_OK;
+  }
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(A->save, c->rho, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(A->save + n2, c->ex, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(A->save + 2 * n2, c->ey, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
+  static const double one = 1.0;
+  VLP4D_CUDA_TRY(cudaMemsetAsync(c->rho, 0, sizeof(double) * n2, s));
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(c->rho, &one, sizeof(double), cudaMemcpyHostToDevice, s));
+  int rc = launch_field_poisson(c, s);
+  if (rc) return rc;
+  VLP4D_CUFFT_TRY(cufftSetStream(c->plan_fwd, s));
+  VLP4D_CUFFT_TRY(cufftExecD2Z(c->plan_fwd, c->ex, A->hx_hat));
+  VLP4D_CUFFT_TRY(cufftExecD2Z(c->plan_fwd, c->ey, A->hy_hat));
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(c->rho, A->save, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(c->ex, A->save + n2, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(c->ey, A->save + 2 * n2, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
+  VLP4D_CUDA_TRY(cudaStreamSynchronize(s));
+  return VLP4D_OK;
+}
+
+// lam_rho = D^T (gex, gey).
+int field_transpose(vlp4d_adjoint *A, cudaStream_t s) {
+  vlp4d_ctx *c = A->ctx;
+  const int nx = c->g.n[0], ny = c->g.n[1];
+  if (!A->field_linear) {
+    VLP4D_CUDA_TRY(cudaMemsetAsync(A->lam_rho, 0, sizeof(double) * c->g.nxy(), s));
+    return VLP4D_OK;
+  }
+  VLP4D_CUFFT_TRY(cufftSetStream(c->plan_fwd, s));
+  VLP4D_CUFFT_TRY(cufftSetStream(c->plan_bwd, s));
+  VLP4D_CUFFT_TRY(cufftExecD2Z(c->plan_fwd, A->gex, c->ex_hat));
+  VLP4D_CUFFT_TRY(cufftExecD2Z(c->plan_fwd, A->gey, c->ey_hat));
+  const int nh = (nx / 2 + 1) * ny;
+  k_field_transpose<<<(nh + 255) / 256, 256, 0, s>>>(c->ex_hat, c->ey_hat, A->hx_hat, A->hy_hat, c->rho_hat, nh,
+                                                     1.0 / ((double)nx * ny));
+  VLP4D_LAUNCH_CHECK();
+  VLP4D_CUFFT_TRY(cufftExecZ2D(c->plan_bwd, c->rho_hat, A->lam_rho));
+  return VLP4D_OK;
+}
+
+// gE from the stage input a (of the vx/vy pass) and lb (the adjoint after it).
+int launch_vgrad(vlp4d_adjoint *A, const void *a, const void *lb, cudaStream_t s) {
+  vlp4d_ctx *c = A->ctx;
+  const int nxy = (int)c->g.nxy(), nvx = c->g.n[2], nvy = c->g.n[3];
+  const int bx = (nxy + 31) / 32;
+  int nseg = (2 * c->num_sms + bx - 1) / bx;
+  if (nseg < 1) nseg = 1;
+  if (nseg > nvy) nseg = nvy;
+  if (nseg > A->gsegs) nseg = A->gsegs;
+  const int Q = (nvy + nseg - 1) / nseg;
+  nseg = (nvy + Q - 1) / Q;
+  dim3 grid(bx, nseg), block(32, 8);
+  if (c->dtype == VLP4D_F64)
+    k_vgrad<double><<<grid, block, 0, s>>>((const double *)a, (const double *)lb, nxy, nvx, nvy, Q, c->tab_vx,
+                                           c->tab_vy, A->dw_vx, A->dw_vy, A->gpart);
+  else
+    k_vgrad<float><<<grid, block, 0, s>>>((const float *)a, (const float *)lb, nxy, nvx, nvy, Q, c->tab_vx,
+                                          c->tab_vy, A->dw_vx, A->dw_vy, A->gpart);
+  VLP4D_LAUNCH_CHECK();
+  k_vgrad_finish<<<(nxy + 255) / 256, 256, 0, s>>>(A->gpart, nseg, nxy, A->gex, A->gey);
+  VLP4D_LAUNCH_CHECK();
+  return VLP4D_OK;
+}
+
+int launch_columns(vlp4d_adjoint *A, void *f, bool add, double scale, cudaStream_t s) {
+  vlp4d_ctx *c = A->ctx;
+  const long long nxy = c->g.nxy(), total = c->g.cells();
+  const int threads = 256, blocks = grid_cap(total, threads, c->num_sms);
+  if (c->dtype == VLP4D_F64) {
+    if (add) k_columns<double, true><<<blocks, threads, 0, s>>>((double *)f, A->lam_rho, scale, nxy, total);
+    else k_columns<double, false><<<blocks, threads, 0, s>>>((double *)f, A->lam_rho, scale, nxy, total);
+  } else {
+    if (add) k_columns<float, true><<<blocks, threads, 0, s>>>((float *)f, A->lam_rho, scale, nxy, total);
+    else k_columns<float, false><<<blocks, threads, 0, s>>>((float *)f, A->lam_rho, scale, nxy, total);
+  }
+  VLP4D_LAUNCH_CHECK();
+  return VLP4D_OK;
+}
+
+// J of the field solved from f into A->d_J, lam = dJ/df.
+int energy_grad(vlp4d_adjoint *A, const void *f, void *lam, cudaStream_t s) {
+  vlp4d_ctx *c = A->ctx;
+  int rc;
+  if ((rc = launch_field_rho(c, f, s))) return rc;
+  if ((rc = launch_field_poisson(c, s))) return rc;
+  k_energy<<<1, 1024, 0, s>>>(c->ex, c->ey, c->g.nxy(), c->g.dx[0] * c->g.dx[1], A->d_J, A->gex, A->gey);
+  VLP4D_LAUNCH_CHECK();
+  if ((rc = field_transpose(A, s))) return rc;
+  return launch_columns(A, lam, false, c->g.dx[2] * c->g.dx[3], s);
+}
+
+// lam_out = (d step / d f)^T lam_next at the state f_state.
+int step_adjoint(vlp4d_adjoint *A, const void *f_state, const void *lam_next, void *lam_out, cudaStream_t s) {
+  vlp4d_ctx *c = A->ctx;
+  const double dt = c->dom.dt;
+  const int lines = (int)c->g.nxy();
+  int rc;
+  // Recompute the vx/vy stage input a = XY f and its field.
+  if ((rc = advect_xy_moment(c, f_state, A->W[0], 0.5 * dt, s))) return rc;
+  if ((rc = launch_field_poisson(c, s))) return rc;
+  if ((rc = build_v_tables(c, dt, true, true, s))) return rc;
+  if ((rc = alloc_table(A->tab_vx_adj, lines))) return rc;
+  if ((rc = alloc_table(A->tab_vy_adj, lines))) return rc;
+  const int threads = 256, blocks = (lines + threads - 1) / threads;
+  k_build_vtable_adj<<<blocks, threads, 0, s>>>(c->ex, lines, dt, c->g.minp[2], c->g.maxp[2], c->g.n[2],
+                                                A->tab_vx_adj.m, A->tab_vx_adj.w, A->tab_vx_adj.wf, A->dw_vx);
+  VLP4D_LAUNCH_CHECK();
+  k_build_vtable_adj<<<blocks, threads, 0, s>>>(c->ey, lines, dt, c->g.minp[3], c->g.maxp[3], c->g.n[3],
+                                                A->tab_vy_adj.m, A->tab_vy_adj.w, A->tab_vy_adj.wf, A->dw_vy);
+  VLP4D_LAUNCH_CHECK();
+  A->tab_vx_adj.valid = A->tab_vy_adj.valid = true;
+  // lb = XY^T lam_next.
+  if ((rc = advect_xy_any(c, lam_next, A->W[1], &A->tab_x_adj, &A->tab_y_adj, s))) return rc;
+  // dJ/dE, then dJ/drho.
+  if ((rc = launch_vgrad(A, A->W[0], A->W[1], s))) return rc;
+  if ((rc = field_transpose(A, s))) return rc;
+  // la = VXVY^T lb + dvx dvy broadcast(dJ/drho); lambda = XY^T la.
+  if ((rc = advect_vxvy_any(c, A->W[1], A->W[0], &A->tab_vx_adj, &A->tab_vy_adj, s))) return rc;
+  if ((rc = launch_columns(A, A->W[0], true, c->g.dx[2] * c->g.dx[3], s))) return rc;
+  return advect_xy_any(c, A->W[0], lam_out, &A->tab_x_adj, &A->tab_y_adj, s);
+}
+
+void destroy(vlp4d_adjoint *A) {
+  if (!A) return;
+  for (void *p : A->ckpt) cudaFree(p);
+  for (void *p : A->seg) cudaFree(p);
+  for (int i = 0; i < 2; ++i) {
+    cudaFree(A->P[i]);
+    cudaFree(A->W[i]);
+    cudaFree(A->L[i]);
+  }
+  cudaFree(A->gex);
+  cudaFree(A->gpart);
+  cudaFree(A->hx_hat);
+  cudaFree(A->hy_hat);
+  cudaFree(A->dw_vx);
+  free_table(A->tab_x_adj);
+  free_table(A->tab_y_adj);
+  free_table(A->tab_vx_adj);
+  free_table(A->tab_vy_adj);
+  delete A;
+}
+
+}  // namespace
+}  // namespace vlp4d
+
+using namespace vlp4d;
+
+extern "C" {
+
+int vlp4d_adjoint_create(vlp4d_ctx *ctx, int nsteps, int every, vlp4d_adjoint **out) {
+  if (!out) return fail_msg(VLP4D_ERR_INVALID_ARG, "out is NULL");
+  *out = nullptr;
+  if (!ctx) return fail_msg(VLP4D_ERR_INVALID_ARG, "ctx is NULL");
+  if (nsteps < 1) return fail_msg(VLP4D_ERR_INVALID_ARG, "nsteps must be at least 1");
+  if (every < 1) return fail_msg(VLP4D_ERR_INVALID_ARG, "the checkpoint interval must be at least 1");
+  if (every > nsteps) every = nsteps;
+  VLP4D_CUDA_TRY(cudaSetDevice(ctx->device));
+  vlp4d_adjoint *A = new vlp4d_adjoint();
+  A->ctx = ctx;
+  A->nsteps = nsteps;
+  A->every = every;
+  A->fbytes = (size_t)ctx->g.cells() * ctx->elem;
+  const long long n2 = ctx->g.nxy();
+  const int nh = (ctx->g.n[0] / 2 + 1) * ctx->g.n[1];
+  auto bail = [&](int rc) {
+    destroy(A);
+    return rc;
+  };
+#define ADJ_ALLOC(ptr, bytes)                                                                      \
+  do {                                                                                             \
+    if (cudaMalloc((void **)&(ptr), (bytes)) != cudaSuccess) {                                     \
+      cudaGetLastError();                                                                          \
+      return bail(fail_msg(VLP4D_ERR_CUDA, "cudaMalloc failed in vlp4d_adjoint_create (" #ptr ")")); \
+    }                                                                                              \
+  } while (0)
+  const int nck = (nsteps + every - 1) / every;
+  A->ckpt.assign(nck, nullptr);
+  for (auto &p : A->ckpt) ADJ_ALLOC(p, A->fbytes);
+  A->seg.assign(every - 1, nullptr);
+  for (auto &p : A->seg) ADJ_ALLOC(p, A->fbytes);
+  for (int i = 0; i < 2; ++i) {
+    ADJ_ALLOC(A->P[i], A->fbytes);
+    ADJ_ALLOC(A->W[i], A->fbytes);
+    ADJ_ALLOC(A->L[i], A->fbytes);
+  }
+  ADJ_ALLOC(A->gex, sizeof(double) * (6 * n2 + 1));
+  A->gey = A->gex + n2;
+  A->lam_rho = A->gey + n2;
+  A->save = A->lam_rho + n2;  // 3 * n2
+  A->d_J = A->save + 3 * n2;
+  A->gsegs = ctx->g.n[3] < 64 ? ctx->g.n[3] : 64;
+  ADJ_ALLOC(A->gpart, sizeof(double) * 2 * n2 * (size_t)A->gsegs);
+  ADJ_ALLOC(A->hx_hat, sizeof(cufftDoubleComplex) * nh);
+  ADJ_ALLOC(A->hy_hat, sizeof(cufftDoubleComplex) * nh);
+  ADJ_ALLOC(A->dw_vx, sizeof(double) * 12 * n2);
+  A->dw_vy = A->dw_vx + 6 * n2;
+#undef ADJ_ALLOC
+  int rc;
+  cudaStream_t s = 0;
+  if ((rc = build_xy_adj(ctx, 0, 0.5 * ctx->dom.dt, A->tab_x_adj, s))) return bail(rc);
+  if ((rc = build_xy_adj(ctx, 1, 0.5 * ctx->dom.dt, A->tab_y_adj, s))) return bail(rc);
+  if ((rc = alloc_table(A->tab_vx_adj, (int)n2))) return bail(rc);
+  if ((rc = alloc_table(A->tab_vy_adj, (int)n2))) return bail(rc);
+  if ((rc = field_transpose_setup(A, s))) return bail(rc);
+  *out = A;
+  return VLP4D_OK;
+}
+
+int vlp4d_adjoint_destroy(vlp4d_adjoint *adj) {
+  if (!adj) return VLP4D_OK;
+  cudaSetDevice(adj->ctx->device);
+  cudaDeviceSynchronize();
+  destroy(adj);
+  return VLP4D_OK;
+}
+
+int vlp4d_step_adjoint(vlp4d_adjoint *adj, const void *f_state, const void *lam_next, void *lam_out, void *stream) {
+  if (!adj) return fail_msg(VLP4D_ERR_INVALID_ARG, "adj is NULL");
+  if (!f_state || !lam_next || !lam_out) return fail_msg(VLP4D_ERR_INVALID_ARG, "NULL buffer");
+  if (lam_out == lam_next || lam_out == f_state) return fail_msg(VLP4D_ERR_INVALID_ARG, "lam_out must be a separate buffer");
+  return step_adjoint(adj, f_state, lam_next, lam_out, (cudaStream_t)stream);
+}
+
+int vlp4d_energy_grad(vlp4d_adjoint *adj, const void *f, double *J, void *lam, void *stream) {
+  if (!adj) return fail_msg(VLP4D_ERR_INVALID_ARG, "adj is NULL");
+  if (!f || !lam) return fail_msg(VLP4D_ERR_INVALID_ARG, "NULL buffer");
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = energy_grad(adj, f, lam, s);
+  if (rc) return rc;
+  if (J) {
+    VLP4D_CUDA_TRY(cudaMemcpyAsync(J, adj->d_J, sizeof(double), cudaMemcpyDeviceToHost, s));
+    VLP4D_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  return VLP4D_OK;
+}
+
+int vlp4d_adjoint_forward(vlp4d_adjoint *adj, const void *f0, void *f_out, double *J, void *stream) {
+  if (!adj) return fail_msg(VLP4D_ERR_INVALID_ARG, "adj is NULL");
+  if (!f0) return fail_msg(VLP4D_ERR_INVALID_ARG, "f0 is NULL");
+  vlp4d_adjoint *A = adj;
+  vlp4d_ctx *c = A->ctx;
+  cudaStream_t s = (cudaStream_t)stream;
+  A->have_forward = false;
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(A->ckpt[0], f0, A->fbytes, cudaMemcpyDeviceToDevice, s));
+  const void *in = A->ckpt[0];
+  int rc;
+  for (int n = 0; n < A->nsteps; ++n) {
+    const int next = n + 1;
+    void *out = (next % A->every == 0 && next < A->nsteps) ? A->ckpt[next / A->every] : A->P[n & 1];
+    if ((rc = step_impl(c, in, out, A->W[0], -1, s))) return rc;
+    in = out;
+  }
+  // J of the final state and dJ/df_N (kept for the reverse sweep).
+  if ((rc = energy_grad(A, in, A->L[0], s))) return rc;
+  if (f_out) VLP4D_CUDA_TRY(cudaMemcpyAsync(f_out, in, A->fbytes, cudaMemcpyDeviceToDevice, s));
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(&A->J, A->d_J, sizeof(double), cudaMemcpyDeviceToHost, s));
+  VLP4D_CUDA_TRY(cudaStreamSynchronize(s));
+  if ((rc = vlp4d_check(c))) return rc;
+  if (J) *J = A->J;
+  A->have_forward = true;
+  return VLP4D_OK;
+}
+
+int vlp4d_adjoint_backward(vlp4d_adjoint *adj, void *grad, void *stream) {
+  if (!adj) return fail_msg(VLP4D_ERR_INVALID_ARG, "adj is NULL");
+  if (!grad) return fail_msg(VLP4D_ERR_INVALID_ARG, "grad is NULL");
+  vlp4d_adjoint *A = adj;
+  if (!A->have_forward) return fail_msg(VLP4D_ERR_INVALID_ARG, "vlp4d_adjoint_backward needs a vlp4d_adjoint_forward first");
+  vlp4d_ctx *c = A->ctx;
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc;
+  int cur = 0;
+  const int nseg = (A->nsteps + A->every - 1) / A->every;
+  std::vector<const void *> states(A->every);
+  for (int sg = nseg - 1; sg >= 0; --sg) {
+    const int c0 = sg * A->every;
+    const int len = A->nsteps - c0 < A->every ? A->nsteps - c0 : A->every;
+    // Recompute the segment's step inputs from its checkpoint.
+    states[0] = A->ckpt[sg];
+    for (int j = 1; j < len; ++j) {
+      if ((rc = step_impl(c, states[j - 1], A->seg[j - 1], A->W[0], -1, s))) return rc;
+      states[j] = A->seg[j - 1];
+    }
+    for (int j = len - 1; j >= 0; --j) {
+      void *dst = (sg == 0 && j == 0) ? grad : A->L[cur ^ 1];
+      if ((rc = step_adjoint(A, states[j], A->L[cur], dst, s))) return rc;
+      cur ^= 1;
+    }
+  }
+  VLP4D_CUDA_TRY(cudaStreamSynchronize(s));
+  return vlp4d_check(c);
+}
+
+}  // extern "C"

@@ -15,17 +15,6 @@ namespace vlp4d {
 
 namespace {
 
-// FP32 difference weights of a line for the adjacent-difference form of
-// stencil.cuh: v = (-w0, -(w0+w1), w3+w4+w5, w4+w5, w5), summed in FP64.
-__host__ __device__ inline void weights_to_f32(const double w[6], float wf[6]) {
-  wf[0] = (float)(-w[0]);
-  wf[1] = (float)(-(w[0] + w[1]));
-  wf[2] = (float)(w[3] + w[4] + w[5]);
-  wf[3] = (float)(w[4] + w[5]);
-  wf[4] = (float)w[5];
-  wf[5] = 0.0f;
-}
-
 // One v-line per (ix, iy): displacement dt*E(ix, iy) (advection.hpp:243, 306).
 __global__ void k_build_vtable(const double *__restrict__ e, int lines, double dt, double hmin, double hmax,
                                int n, int *__restrict__ m, double *__restrict__ w, float *__restrict__ wf) {
@@ -124,6 +113,19 @@ __global__ void k_advect_pair_generic(const T *__restrict__ fn, T *__restrict__ 
   }
 }
 
+}  // namespace
+
+void free_table(StencilTable &t) {
+  cudaFree(t.m);
+  cudaFree(t.w);
+  cudaFree(t.wf);
+  t.m = nullptr;
+  t.w = nullptr;
+  t.wf = nullptr;
+  t.lines = 0;
+  t.valid = false;
+}
+
 int alloc_table(StencilTable &t, int lines) {
   if (t.m && t.lines >= lines) return VLP4D_OK;
   cudaFree(t.m);
@@ -137,6 +139,8 @@ int alloc_table(StencilTable &t, int lines) {
   t.valid = false;
   return VLP4D_OK;
 }
+
+namespace {
 
 int grid_for(long long total, int threads, int sms) {
   long long blocks = (total + threads - 1) / threads;

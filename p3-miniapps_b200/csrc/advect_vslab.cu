@@ -418,6 +418,12 @@ int run_vslab(vlp4d_ctx *c, const CUtensorMap &map, const VslabArgs &args, const
 }  // namespace
 
 int launch_advect_vxvy(vlp4d_ctx *c, const void *fn, void *fnp1, bool do_vx, bool do_vy, cudaStream_t s) {
+  return launch_advect_vxvy_tables(c, fn, fnp1, do_vx ? &c->tab_vx : nullptr, do_vy ? &c->tab_vy : nullptr, s);
+}
+
+int launch_advect_vxvy_tables(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *tvx,
+                              const StencilTable *tvy, cudaStream_t s) {
+  const bool do_vx = tvx != nullptr, do_vy = tvy != nullptr;
   if (!c->fused) return VLP4D_ERR_UNSUPPORTED;
   if (((uintptr_t)fn & 15) || ((uintptr_t)fnp1 & 15)) return VLP4D_ERR_UNSUPPORTED;
   if (!do_vx && !do_vy) return VLP4D_ERR_UNSUPPORTED;
@@ -443,7 +449,7 @@ int launch_advect_vxvy(vlp4d_ctx *c, const void *fn, void *fnp1, bool do_vx, boo
   if (r != CUDA_SUCCESS) return VLP4D_ERR_UNSUPPORTED;
 
   if (do_vy) {
-    k_vspan<<<(nchunks + 127) / 128, 128, 0, s>>>(c->tab_vy.m, nchunks, cfg.C, nvy, c->vspan);
+    k_vspan<<<(nchunks + 127) / 128, 128, 0, s>>>(tvy->m, nchunks, cfg.C, nvy, c->vspan);
     VLP4D_LAUNCH_CHECK();
   }
   VslabArgs a;
@@ -456,8 +462,8 @@ int launch_advect_vxvy(vlp4d_ctx *c, const void *fn, void *fnp1, bool do_vx, boo
   a.nseg = nvy / cfg.Q;
   a.nitems = (long long)nchunks * a.nseg;
   a.stages = cfg.stages;
-  if (do_vx) a.tvx = c->tab_vx;
-  if (do_vy) a.tvy = c->tab_vy;
+  if (do_vx) a.tvx = *tvx;
+  if (do_vy) a.tvy = *tvy;
   a.span = c->vspan;
   a.err = c->d_err;
 #define VLP4D_VS(T, DVX, DVY, V)                                                  \

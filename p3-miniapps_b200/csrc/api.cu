@@ -414,22 +414,59 @@ int vlp4d_diags_save(vlp4d_ctx *ctx, const char *path) {
   return VLP4D_OK;
 }
 
+}  // extern "C"
+
+namespace vlp4d {
+
+// One Strang step f_in -> f_out through `scratch` (f_in is left unchanged
+// when scratch != f_in); the mid-step diagnostic goes to history slot
+// `iter`, or nowhere when iter < 0.
+int step_impl(vlp4d_ctx *ctx, const void *f_in, void *f_out, void *scratch, int iter, cudaStream_t s) {
+  const double dt = ctx->dom.dt;
+  int rc;
+  // timestep.hpp:17-28: x(dt/2), y(dt/2) and the moment of the result.
+  if ((rc = advect_xy_impl(ctx, f_in, f_out, 0.5 * dt, true, s))) return rc;
+  // timestep.hpp:30-38: field solve and the mid-step diagnostic.
+  if ((rc = launch_field_poisson(ctx, s))) return rc;
+  if (iter >= 0 && (rc = launch_diags(ctx, iter, s))) return rc;
+  // timestep.hpp:40-48: vx(dt), vy(dt).
+  if ((rc = advect_vxvy_impl(ctx, f_out, scratch, dt, s))) return rc;
+  // timestep.hpp:50-58: x(dt/2), y(dt/2).
+  return advect_xy_impl(ctx, scratch, f_out, 0.5 * dt, false, s);
+}
+
+int advect_xy_moment(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, cudaStream_t s) {
+  return advect_xy_impl(ctx, fn, fnp1, dt, true, s);
+}
+
+int advect_xy_any(vlp4d_ctx *ctx, const void *fn, void *fnp1, const StencilTable *tx, const StencilTable *ty,
+                  cudaStream_t s) {
+  int rc = launch_advect_xy(ctx, fn, fnp1, tx, ty, true, true, false, s);
+  if (rc != VLP4D_ERR_UNSUPPORTED) return rc;
+  if ((rc = fused_declined(ctx))) return rc;
+  return launch_advect_pair_generic(ctx, false, fn, fnp1, tx, ty, s);
+}
+
+int advect_vxvy_any(vlp4d_ctx *ctx, const void *fn, void *fnp1, const StencilTable *tvx, const StencilTable *tvy,
+                    cudaStream_t s) {
+  int rc = launch_advect_vxvy_tables(ctx, fn, fnp1, tvx, tvy, s);
+  if (rc != VLP4D_ERR_UNSUPPORTED) return rc;
+  if ((rc = fused_declined(ctx))) return rc;
+  return launch_advect_pair_generic(ctx, true, fn, fnp1, tvx, tvy, s);
+}
+
+int fail_msg(int code, const std::string &msg) { return fail(code, msg); }
+
+}  // namespace vlp4d
+
+extern "C" {
+
 int vlp4d_step(vlp4d_ctx *ctx, void *f_state, void *f_next, int iter, void *stream) {
   int rc = check_ctx(ctx);
   if (rc) return rc;
   if ((rc = check_pair(f_state, f_next))) return rc;
   if (iter < 0 || iter >= ctx->hist_len) return fail(VLP4D_ERR_INVALID_ARG, "iter outside [0, nbiter]");
-  cudaStream_t s = as_stream(stream);
-  const double dt = ctx->dom.dt;
-  // timestep.hpp:17-28: x(dt/2), y(dt/2) and the moment of the result.
-  if ((rc = advect_xy_impl(ctx, f_state, f_next, 0.5 * dt, true, s))) return rc;
-  // timestep.hpp:30-38: field solve and the mid-step diagnostic.
-  if ((rc = launch_field_poisson(ctx, s))) return rc;
-  if ((rc = launch_diags(ctx, iter, s))) return rc;
-  // timestep.hpp:40-48: vx(dt), vy(dt).
-  if ((rc = advect_vxvy_impl(ctx, f_next, f_state, dt, s))) return rc;
-  // timestep.hpp:50-58: x(dt/2), y(dt/2).
-  return advect_xy_impl(ctx, f_state, f_next, 0.5 * dt, false, s);
+  return step_impl(ctx, f_state, f_next, f_state, iter, as_stream(stream));
 }
 
 // The reference's time loop (vlp4d.cpp:63-72, onetimestep per step) with

@@ -132,6 +132,8 @@ struct vlp4d_ctx {
 namespace vlp4d {
 
 // advect.cu
+int alloc_table(StencilTable &t, int lines);
+void free_table(StencilTable &t);
 int ensure_xy_table(vlp4d_ctx *c, int dim, double dt, StencilTable **out, cudaStream_t s);
 int build_v_tables(vlp4d_ctx *c, double dt, bool vx, bool vy, cudaStream_t s);
 int launch_advect_generic(vlp4d_ctx *c, int dim, const void *fn, void *fnp1, const StencilTable *t,
@@ -144,8 +146,23 @@ int launch_advect_pair_generic(vlp4d_ctx *c, bool v, const void *fn, void *fnp1,
 int launch_advect_xy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *tx,
                      const StencilTable *ty, bool do_x, bool do_y, bool with_rho, cudaStream_t s);
 int launch_advect_vxvy(vlp4d_ctx *c, const void *fn, void *fnp1, bool do_vx, bool do_vy, cudaStream_t s);
+// The same pass with explicit v tables (the reverse mode passes transposed ones).
+int launch_advect_vxvy_tables(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *tvx,
+                              const StencilTable *tvy, cudaStream_t s);
 int launch_advect_xyxy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *tx, const StencilTable *ty,
                        cudaStream_t s);
+
+// api.cu: one Strang step f_in -> f_out through scratch (diagnostic slot
+// `iter`, none when negative); x/y and vx/vy passes with explicit tables,
+// fused kernels first, generic ones when the fused kernels decline.
+int step_impl(vlp4d_ctx *ctx, const void *f_in, void *f_out, void *scratch, int iter, cudaStream_t s);
+int advect_xy_moment(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, cudaStream_t s);
+int advect_xy_any(vlp4d_ctx *ctx, const void *fn, void *fnp1, const StencilTable *tx, const StencilTable *ty,
+                  cudaStream_t s);
+int advect_vxvy_any(vlp4d_ctx *ctx, const void *fn, void *fnp1, const StencilTable *tvx, const StencilTable *tvy,
+                    cudaStream_t s);
+// Records msg as the calling thread's last error and returns code.
+int fail_msg(int code, const std::string &msg);
 
 // field.cu
 int launch_field_rho(vlp4d_ctx *c, const void *fn, cudaStream_t s);

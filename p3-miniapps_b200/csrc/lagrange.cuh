@@ -59,11 +59,58 @@ __host__ __device__ inline void lag_basis5(double px, double coef[6]) {
   coef[5] = VL_MUL(VL_MUL(VL_MUL(VL_MUL(loc5, p01), pxm2), VL_ADD(pxm2, 1.)), VL_SUB(pxm2, 2.));
 }
 
+// d/dpx of lag_basis5, for the reverse mode.  With x = px - 2 the weights
+// are products of linear factors and one quadratic,
+//   w0 = -1/24 x (x-1)^2 (x+1) (x-2)      w1 = 1/24 x (x-1) (x-2) (5x^2+x-8)
+//   w2 = -1/12 (x-1) (x-2) (x+1) (5x^2-3x-6)
+//   w3 =  1/12 x (x+1) (x-2) (5x^2-7x-4)  w4 = -1/24 x (x-1) (x+1) (5x^2-11x-2)
+//   w5 =  1/24 x^2 (x-1) (x+1) (x-2),
+// differentiated here with the product rule.
+__host__ __device__ inline double prod_rule4(double a, double b, double c, double d, double da, double db, double dc,
+                                             double dd) {
+  return da * b * c * d + a * db * c * d + a * b * dc * d + a * b * c * dd;
+}
+__host__ __device__ inline void lag_basis5_deriv(double px, double dcoef[6]) {
+  const double x = px - 2.;
+  const double xm1 = x - 1., xp1 = x + 1., xm2 = x - 2.;
+  // w0: x (x-1) (x+1) (x-2) * (x-1) ; w5: x (x-1) (x+1) (x-2) * x.
+  const double p4 = x * xm1 * xp1 * xm2;
+  const double dp4 = prod_rule4(x, xm1, xp1, xm2, 1., 1., 1., 1.);
+  dcoef[0] = -1. / 24 * (dp4 * xm1 + p4);
+  dcoef[1] = 1. / 24 * prod_rule4(x, xm1, xm2, 5 * x * x + x - 8., 1., 1., 1., 10 * x + 1.);
+  dcoef[2] = -1. / 12 * prod_rule4(xm1, xm2, xp1, 5 * x * x - 3 * x - 6., 1., 1., 1., 10 * x - 3.);
+  dcoef[3] = 1. / 12 * prod_rule4(x, xp1, xm2, 5 * x * x - 7 * x - 4., 1., 1., 1., 10 * x - 7.);
+  dcoef[4] = -1. / 24 * prod_rule4(x, xm1, xp1, 5 * x * x - 11 * x - 2., 1., 1., 1., 10 * x - 11.);
+  dcoef[5] = 1. / 24 * (dp4 * x + p4);
+}
+
+// FP32 difference weights of a line for the adjacent-difference form of
+// stencil.cuh: v = (-w0, -(w0+w1), w3+w4+w5, w4+w5, w5), summed in FP64.
+__host__ __device__ inline void weights_to_f32(const double w[6], float wf[6]) {
+  wf[0] = (float)(-w[0]);
+  wf[1] = (float)(-(w[0] + w[1]));
+  wf[2] = (float)(w[3] + w[4] + w[5]);
+  wf[3] = (float)(w[4] + w[5]);
+  wf[4] = (float)w[5];
+  wf[5] = 0.0f;
+}
+
 // The stencil of one swept line: cell i reads f[(i + m + k) mod n] * w[k].
 struct LineStencil {
   int m;        // in [0, n)
   double w[6];
+  double d;     // fractional foot position in [2, 3) the weights are evaluated at
 };
+
+// The transpose of a line's gather: cell j receives sum_k w[k] * l[(j - m - k) mod n],
+// which is again a gather, with offset (-m - 5) mod n and the weights reversed.
+__host__ __device__ inline LineStencil adjoint_stencil(const LineStencil &s, int n) {
+  LineStencil a;
+  a.m = (n - (s.m + 5) % n) % n;
+  for (int k = 0; k < 6; ++k) a.w[k] = s.w[5 - k];
+  a.d = s.d;
+  return a;
+}
 
 // disp: physical displacement of the line (dt*v or dt*E); hmin/hmax: the
 // swept dimension's minPhy/maxPhy; n: its number of points.
@@ -78,6 +125,7 @@ __host__ __device__ inline LineStencil line_stencil(double disp, double hmin, do
   const double d = VL_ADD(2., VL_MUL(idh, VL_SUB(hstar, VL_ADD(hmin, VL_MUL((double)ip, dh)))));
   LineStencil s;
   lag_basis5(d, s.w);
+  s.d = d;
   int m = (ip - 2) % n;
   if (m < 0) m += n;
   s.m = m;

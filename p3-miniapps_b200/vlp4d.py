@@ -33,6 +33,8 @@ EXPORTS = (
     "vlp4d_diags_compute", "vlp4d_diags_read", "vlp4d_diags_save", "vlp4d_step", "vlp4d_run",
     "vlp4d_print_fxvx", "vlp4d_transpose", "vlp4d_check", "vlp4d_kernel_launches",
     "vlp4d_field_rho_noalloc", "vlp4d_steps", "vlp4d_advect_xyxy",
+    "vlp4d_adjoint_create", "vlp4d_adjoint_destroy", "vlp4d_adjoint_forward", "vlp4d_adjoint_backward",
+    "vlp4d_step_adjoint", "vlp4d_energy_grad",
 )
 
 
@@ -95,6 +97,12 @@ def lib() -> C.CDLL:
         L.vlp4d_check.argtypes = [vp]
         L.vlp4d_kernel_launches.argtypes = []
         L.vlp4d_field_rho_noalloc.argtypes = [vp, i, i, i, i, i, d, d, vp, vp]
+        L.vlp4d_adjoint_create.argtypes = [vp, i, i, C.POINTER(vp)]
+        L.vlp4d_adjoint_destroy.argtypes = [vp]
+        L.vlp4d_adjoint_forward.argtypes = [vp, vp, vp, C.POINTER(d), vp]
+        L.vlp4d_adjoint_backward.argtypes = [vp, vp, vp]
+        L.vlp4d_step_adjoint.argtypes = [vp, vp, vp, vp, vp]
+        L.vlp4d_energy_grad.argtypes = [vp, vp, C.POINTER(d), vp, vp]
         for n in EXPORTS:
             if n not in ("vlp4d_last_error", "vlp4d_kernel_launches"):
                 getattr(L, n).restype = C.c_int
@@ -331,3 +339,72 @@ def transpose(a, out, stream=None):
     cols, rows = a.shape
     _check(lib().vlp4d_transpose(C.c_void_p(a.data_ptr()), C.c_void_p(out.data_ptr()), rows, cols,
                                  a.element_size(), _stream_ptr(stream)))
+
+
+class Adjoint:
+    """Reverse mode of a Context (vlp4d_adjoint_*): checkpointed runs of
+    `nsteps` steps with the objective J = dx dy sum |E(f_N)|^2."""
+
+    def __init__(self, ctx: Context, nsteps: int, every: int = 8):
+        self.ctx = ctx
+        self.nsteps = int(nsteps)
+        self.h = C.c_void_p()
+        _check(lib().vlp4d_adjoint_create(ctx.h, self.nsteps, int(every), C.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            lib().vlp4d_adjoint_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+        return False
+
+    def forward(self, f0, f_out=None, stream=None) -> float:
+        J = C.c_double()
+        out = self.ctx._f(f_out) if f_out is not None else None
+        _check(lib().vlp4d_adjoint_forward(self.h, self.ctx._f(f0), out, C.byref(J), _stream_ptr(stream)))
+        return J.value
+
+    def backward(self, grad=None, stream=None):
+        if grad is None:
+            grad = self.ctx.empty_f()
+        _check(lib().vlp4d_adjoint_backward(self.h, self.ctx._f(grad), _stream_ptr(stream)))
+        return grad
+
+    def step_adjoint(self, f_state, lam_next, lam_out, stream=None):
+        _check(lib().vlp4d_step_adjoint(self.h, self.ctx._f(f_state), self.ctx._f(lam_next), self.ctx._f(lam_out),
+                                        _stream_ptr(stream)))
+
+    def energy_grad(self, f, lam, stream=None) -> float:
+        J = C.c_double()
+        _check(lib().vlp4d_energy_grad(self.h, self.ctx._f(f), C.byref(J), self.ctx._f(lam), _stream_ptr(stream)))
+        return J.value
+
+
+def energy_after_steps(f0, adjoint: Adjoint):
+    """torch.autograd binding for tests: J(f0) = electric energy after the
+    adjoint's nsteps steps, differentiable in f0 through vlp4d_adjoint_backward."""
+    import torch
+
+    class _EnergyAfterSteps(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx_, f):
+            f = f.detach().contiguous()
+            return torch.tensor(adjoint.forward(f), dtype=torch.float64, device=f.device)
+
+        @staticmethod
+        def backward(ctx_, gJ):
+            g = adjoint.backward()
+            return g * gJ.to(g.dtype)
+
+    return _EnergyAfterSteps.apply(f0)
