@@ -43,10 +43,17 @@ struct vlp4d_adjoint {
   int nsteps = 0, every = 0;
   size_t fbytes = 0;
   std::vector<void *> ckpt;  // f at steps 0, every, 2*every, ...
-  std::vector<void *> seg;   // recomputed states of one segment (every - 1)
-  void *P[2] = {nullptr, nullptr};  // forward ping-pong
-  void *W[2] = {nullptr, nullptr};  // step-adjoint work / forward scratch
+  std::vector<void *> seg;   // a = XY f of each step of a segment (every)
+  double *seg_e = nullptr;   // Ex, Ey of each step of a segment (every x 2 x nx*ny)
+  void *P[2] = {nullptr, nullptr};  // forward work / final state
+  void *W[2] = {nullptr, nullptr};  // reverse-step work
   void *L[2] = {nullptr, nullptr};  // adjoint states
+  cudaStream_t own = nullptr;       // used when the caller passes the legacy stream
+  // CUDA graphs of the forward and reverse sweeps, keyed by the caller's
+  // buffers; use_graphs is cleared if a capture fails (eager from then on).
+  bool use_graphs = true;
+  cudaGraphExec_t g_fwd = nullptr, g_bwd = nullptr;
+  const void *k_fwd[2] = {nullptr, nullptr}, *k_bwd = nullptr;
   // FP64 2D work: dJ/dEx, dJ/dEy, dJ/drho, the objective, saved fields.
   double *gex = nullptr, *gey = nullptr, *lam_rho = nullptr, *d_J = nullptr, *save = nullptr;
   double *gpart = nullptr;  // per-segment partial sums of gE
@@ -167,6 +174,107 @@ __global__ void __launch_bounds__(256) k_vgrad(const T *__restrict__ a, const T 
     for (int g = 0; g < GY; ++g) {
       ax += sx[g][tx];
       ay += sy[g][tx];
+    }
+    part[(2LL * seg) * nxy + ixy] = ax;
+    part[(2LL * seg + 1) * nxy + ixy] = ay;
+  }
+}
+
+// The same sums with the vx taps shared: thread (cw, g) of a block owns
+// column ixy = blockIdx.x*CW + cw and the V consecutive output vx rows
+// g*V .. g*V+V-1 (blockDim = CW x nvx/V), so one input row costs V+5 loads
+// for V outputs.  The stencil sums run in the element type, the products
+// with lb and the accumulation in FP64.  Ring slot of row r: r mod 6,
+// static after unrolling by six.
+template <typename T, int V>
+__global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const T *__restrict__ lb, int nxy,
+                                                 int nvx, int nvy, int Q, StencilTable tvx, StencilTable tvy,
+                                                 const double *__restrict__ dwx, const double *__restrict__ dwy,
+                                                 double *__restrict__ part) {
+  const int CW = blockDim.x;
+  const int cw = threadIdx.x, g = threadIdx.y;
+  const int ixy = blockIdx.x * CW + cw;
+  const int seg = blockIdx.y;
+  const int ivy0 = seg * Q;
+  const int q = min(Q, nvy - ivy0);
+  const int vx0 = g * V;
+  double gx = 0., gy = 0.;
+  if (ixy < nxy && q > 0) {
+    const long long vstride = nxy, ystride = (long long)nxy * nvx;
+    T wx[6], dx[6];
+    double wy[6], dy[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      wx[k] = (T)tvx.w[6 * (long long)ixy + k];
+      dx[k] = (T)dwx[6 * (long long)ixy + k];
+      wy[k] = tvy.w[6 * (long long)ixy + k];
+      dy[k] = dwy[6 * (long long)ixy + k];
+    }
+    int toff[V + 5];  // vx tap rows of this thread, times nothing yet
+    {
+      int j = vx0 + tvx.m[ixy];
+      if (j >= nvx) j -= nvx;
+#pragma unroll
+      for (int k = 0; k < V + 5; ++k) {
+        toff[k] = j;
+        if (++j == nvx) j = 0;
+      }
+    }
+    const int my = tvy.m[ixy];
+    const T *lcol = lb + (long long)vx0 * vstride + ixy;
+    T A[6][V], B[6][V];
+    int row = (ivy0 + my) % nvy;
+    const int nrows = q + 5;
+    for (int r0 = 0; r0 < nrows; r0 += 6) {
+#pragma unroll
+      for (int u = 0; u < 6; ++u) {
+        const int r = r0 + u;
+        if (r >= nrows) break;
+        const T *p = a + (long long)row * ystride + ixy;
+        T t[V + 5];
+#pragma unroll
+        for (int k = 0; k < V + 5; ++k) t[k] = __ldg(p + (long long)toff[k] * vstride);
+#pragma unroll
+        for (int i = 0; i < V; ++i) {
+          T sa = wx[0] * t[i], sb = dx[0] * t[i];
+#pragma unroll
+          for (int k = 1; k < 6; ++k) {
+            sa = fma(wx[k], t[i + k], sa);
+            sb = fma(dx[k], t[i + k], sb);
+          }
+          A[u][i] = sa;
+          B[u][i] = sb;
+        }
+        if (++row == nvy) row = 0;
+        if (r >= 5) {
+          const T *lp = lcol + (long long)(ivy0 + r - 5) * ystride;
+#pragma unroll
+          for (int i = 0; i < V; ++i) {
+            const double l = (double)__ldg(lp + (long long)i * vstride);
+            double sx = 0., sy = 0.;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+              sx = fma(wy[k], (double)B[(u + 1 + k) % 6][i], sx);
+              sy = fma(dy[k], (double)A[(u + 1 + k) % 6][i], sy);
+            }
+            gx = fma(l, sx, gx);
+            gy = fma(l, sy, gy);
+          }
+        }
+      }
+    }
+  }
+  // Sum the vx groups of each column in a fixed order.
+  extern __shared__ double red[];  // [2][blockDim.y][CW]
+  const int G = blockDim.y;
+  red[g * CW + cw] = gx;
+  red[(G + g) * CW + cw] = gy;
+  __syncthreads();
+  if (g == 0 && ixy < nxy) {
+    double ax = 0., ay = 0.;
+    for (int k = 0; k < G; ++k) {
+      ax += red[k * CW + cw];
+      ay += red[(G + k) * CW + cw];
     }
     part[(2LL * seg) * nxy + ixy] = ax;
     part[(2LL * seg + 1) * nxy + ixy] = ay;
@@ -338,6 +446,33 @@ int launch_vgrad(vlp4d_adjoint *A, const void *a, const void *lb, cudaStream_t s
   if (nseg > A->gsegs) nseg = A->gsegs;
   const int Q = (nvy + nseg - 1) / nseg;
   nseg = (nvy + Q - 1) / Q;
+  // Shared-tap kernel: V vx rows per thread (4 in FP32, 2 in FP64), nvx/V
+  // threads per column, as many columns per block as fit 512 threads.
+  const int V = c->dtype == VLP4D_F32 ? 4 : 2;
+  if (nvx % V == 0 && nvx / V <= 512) {
+    const int gy = nvx / V;
+    int cw = 512 / gy;
+    if (cw > 32) cw = 32;
+    const int bxv = (nxy + cw - 1) / cw;
+    int ns = (2 * c->num_sms + bxv - 1) / bxv;
+    if (ns < 1) ns = 1;
+    if (ns > nvy) ns = nvy;
+    if (ns > A->gsegs) ns = A->gsegs;
+    const int Qv = (nvy + ns - 1) / ns;
+    ns = (nvy + Qv - 1) / Qv;
+    dim3 gridv(bxv, ns), blockv(cw, gy);
+    const size_t sm = sizeof(double) * 2 * gy * cw;
+    if (c->dtype == VLP4D_F64)
+      k_vgrad_v<double, 2><<<gridv, blockv, sm, s>>>((const double *)a, (const double *)lb, nxy, nvx, nvy, Qv,
+                                                     c->tab_vx, c->tab_vy, A->dw_vx, A->dw_vy, A->gpart);
+    else
+      k_vgrad_v<float, 4><<<gridv, blockv, sm, s>>>((const float *)a, (const float *)lb, nxy, nvx, nvy, Qv,
+                                                    c->tab_vx, c->tab_vy, A->dw_vx, A->dw_vy, A->gpart);
+    VLP4D_LAUNCH_CHECK();
+    k_vgrad_finish<<<(nxy + 255) / 256, 256, 0, s>>>(A->gpart, ns, nxy, A->gex, A->gey);
+    VLP4D_LAUNCH_CHECK();
+    return VLP4D_OK;
+  }
   dim3 grid(bx, nseg), block(32, 8);
   if (c->dtype == VLP4D_F64)
     k_vgrad<double><<<grid, block, 0, s>>>((const double *)a, (const double *)lb, nxy, nvx, nvy, Q, c->tab_vx,
@@ -379,17 +514,20 @@ int energy_grad(vlp4d_adjoint *A, const void *f, void *lam, cudaStream_t s) {
 }
 
 // lam_out = (d step / d f)^T lam_next at the state f_state.
-int step_adjoint(vlp4d_adjoint *A, const void *f_state, const void *lam_next, void *lam_out, cudaStream_t s) {
+// The reverse step from the stored stage input a (= XY f) and its field E:
+// lam_out = (d step/d f)^T lam_next.
+int step_adjoint_stored(vlp4d_adjoint *A, const void *a, const double *e, const void *lam_next, void *lam_out,
+                        cudaStream_t s) {
   vlp4d_ctx *c = A->ctx;
   const double dt = c->dom.dt;
-  const int lines = (int)c->g.nxy();
+  const long long n2 = c->g.nxy();
+  const int lines = (int)n2;
   int rc;
-  // Recompute the vx/vy stage input a = XY f and its field.
-  if ((rc = advect_xy_moment(c, f_state, A->W[0], 0.5 * dt, s))) return rc;
-  if ((rc = launch_field_poisson(c, s))) return rc;
+  if (e) {
+    VLP4D_CUDA_TRY(cudaMemcpyAsync(c->ex, e, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
+    VLP4D_CUDA_TRY(cudaMemcpyAsync(c->ey, e + n2, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
+  }
   if ((rc = build_v_tables(c, dt, true, true, s))) return rc;
-  if ((rc = alloc_table(A->tab_vx_adj, lines))) return rc;
-  if ((rc = alloc_table(A->tab_vy_adj, lines))) return rc;
   const int threads = 256, blocks = (lines + threads - 1) / threads;
   k_build_vtable_adj<<<blocks, threads, 0, s>>>(c->ex, lines, dt, c->g.minp[2], c->g.maxp[2], c->g.n[2],
                                                 A->tab_vx_adj.m, A->tab_vx_adj.w, A->tab_vx_adj.wf, A->dw_vx);
@@ -397,20 +535,157 @@ int step_adjoint(vlp4d_adjoint *A, const void *f_state, const void *lam_next, vo
   k_build_vtable_adj<<<blocks, threads, 0, s>>>(c->ey, lines, dt, c->g.minp[3], c->g.maxp[3], c->g.n[3],
                                                 A->tab_vy_adj.m, A->tab_vy_adj.w, A->tab_vy_adj.wf, A->dw_vy);
   VLP4D_LAUNCH_CHECK();
-  A->tab_vx_adj.valid = A->tab_vy_adj.valid = true;
   // lb = XY^T lam_next.
   if ((rc = advect_xy_any(c, lam_next, A->W[1], &A->tab_x_adj, &A->tab_y_adj, s))) return rc;
   // dJ/dE, then dJ/drho.
-  if ((rc = launch_vgrad(A, A->W[0], A->W[1], s))) return rc;
+  if ((rc = launch_vgrad(A, a, A->W[1], s))) return rc;
   if ((rc = field_transpose(A, s))) return rc;
-  // la = VXVY^T lb + dvx dvy broadcast(dJ/drho); lambda = XY^T la.
-  if ((rc = advect_vxvy_any(c, A->W[1], A->W[0], &A->tab_vx_adj, &A->tab_vy_adj, s))) return rc;
-  if ((rc = launch_columns(A, A->W[0], true, c->g.dx[2] * c->g.dx[3], s))) return rc;
+  // la = VXVY^T lb + dvx dvy broadcast(dJ/drho), the broadcast folded into
+  // the v-slab pass where it runs; lambda = XY^T la.
+  const double scale = c->g.dx[2] * c->g.dx[3];
+  rc = launch_advect_vxvy_tables(c, A->W[1], A->W[0], &A->tab_vx_adj, &A->tab_vy_adj, s, A->lam_rho, scale);
+  if (rc == VLP4D_ERR_UNSUPPORTED) {
+    if ((rc = advect_vxvy_any(c, A->W[1], A->W[0], &A->tab_vx_adj, &A->tab_vy_adj, s))) return rc;
+    if ((rc = launch_columns(A, A->W[0], true, scale, s))) return rc;
+  } else if (rc) {
+    return rc;
+  }
   return advect_xy_any(c, A->W[0], lam_out, &A->tab_x_adj, &A->tab_y_adj, s);
+}
+
+// The reverse step at the state f_state: recompute a = XY f and its field.
+int step_adjoint(vlp4d_adjoint *A, const void *f_state, const void *lam_next, void *lam_out, cudaStream_t s) {
+  vlp4d_ctx *c = A->ctx;
+  int rc;
+  if ((rc = advect_xy_moment(c, f_state, A->P[0], 0.5 * c->dom.dt, s))) return rc;
+  if ((rc = launch_field_poisson(c, s))) return rc;
+  return step_adjoint_stored(A, A->P[0], nullptr, lam_next, lam_out, s);
+}
+
+void save_field(vlp4d_adjoint *A, int j, cudaStream_t s) {
+  vlp4d_ctx *c = A->ctx;
+  const long long n2 = c->g.nxy();
+  double *e = A->seg_e + 2 * n2 * (long long)j;
+  cudaMemcpyAsync(e, c->ex, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s);
+  cudaMemcpyAsync(e + n2, c->ey, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s);
+}
+
+// The closing x/y half step of one step and the opening one (with the
+// moment) of the next: one k_plane_xyxy pass where it is the faster kernel,
+// else two x/y passes through `tmp`.
+int xy_xy_moment(vlp4d_ctx *c, const void *in, void *out, void *tmp, cudaStream_t s) {
+  StencilTable *tx = nullptr, *ty = nullptr;
+  int rc;
+  if ((rc = ensure_xy_table(c, 0, 0.5 * c->dom.dt, &tx, s))) return rc;
+  if ((rc = ensure_xy_table(c, 1, 0.5 * c->dom.dt, &ty, s))) return rc;
+  if (xyxy_join(c)) {
+    rc = launch_advect_xyxy(c, in, out, tx, ty, s);
+    if (rc != VLP4D_ERR_UNSUPPORTED) return rc;
+  }
+  if ((rc = advect_xy_any(c, in, tmp, tx, ty, s))) return rc;
+  return advect_xy_moment(c, tmp, out, 0.5 * c->dom.dt, s);
+}
+
+// Forward sweep: nsteps steps from f0, each segment's final state written to
+// the next checkpoint (the last one to P[1]); J and dJ/df_N into d_J, L[0].
+int forward_body(vlp4d_adjoint *A, const void *f0, void *f_out, cudaStream_t s) {
+  vlp4d_ctx *c = A->ctx;
+  const double dt = c->dom.dt;
+  int rc;
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(A->ckpt[0], f0, A->fbytes, cudaMemcpyDeviceToDevice, s));
+  const int nseg = (int)A->ckpt.size();
+  for (int sg = 0; sg < nseg; ++sg) {
+    const int len = A->nsteps - sg * A->every < A->every ? A->nsteps - sg * A->every : A->every;
+    void *out = sg + 1 < nseg ? A->ckpt[sg + 1] : A->P[1];
+    // Steps ckpt[sg] -> out through W[0] / W[1] (ckpt[sg] is only read).
+    void *cur = A->W[0], *oth = A->W[1];
+    if ((rc = advect_xy_moment(c, A->ckpt[sg], cur, 0.5 * dt, s))) return rc;
+    for (int k = 0; k < len; ++k) {
+      if ((rc = launch_field_poisson(c, s))) return rc;
+      if ((rc = build_v_tables(c, dt, true, true, s))) return rc;
+      if ((rc = advect_vxvy_any(c, cur, oth, &c->tab_vx, &c->tab_vy, s))) return rc;
+      std::swap(cur, oth);
+      if (k + 1 < len) {
+        if ((rc = xy_xy_moment(c, cur, oth, out, s))) return rc;
+        std::swap(cur, oth);
+      }
+    }
+    StencilTable *tx = nullptr, *ty = nullptr;
+    if ((rc = ensure_xy_table(c, 0, 0.5 * dt, &tx, s))) return rc;
+    if ((rc = ensure_xy_table(c, 1, 0.5 * dt, &ty, s))) return rc;
+    if ((rc = advect_xy_any(c, cur, out, tx, ty, s))) return rc;
+  }
+  if ((rc = energy_grad(A, A->P[1], A->L[0], s))) return rc;
+  if (f_out) VLP4D_CUDA_TRY(cudaMemcpyAsync(f_out, A->P[1], A->fbytes, cudaMemcpyDeviceToDevice, s));
+  return VLP4D_OK;
+}
+
+// Reverse sweep: per segment (last first) recompute the stage inputs a and
+// fields E of its steps from the checkpoint, then run its reverse steps.
+int backward_body(vlp4d_adjoint *A, void *grad, cudaStream_t s) {
+  vlp4d_ctx *c = A->ctx;
+  const double dt = c->dom.dt;
+  const long long n2 = c->g.nxy();
+  int rc;
+  int cur = 0;
+  const int nseg = (int)A->ckpt.size();
+  for (int sg = nseg - 1; sg >= 0; --sg) {
+    const int len = A->nsteps - sg * A->every < A->every ? A->nsteps - sg * A->every : A->every;
+    if ((rc = advect_xy_moment(c, A->ckpt[sg], A->seg[0], 0.5 * dt, s))) return rc;
+    if ((rc = launch_field_poisson(c, s))) return rc;
+    save_field(A, 0, s);
+    for (int j = 1; j < len; ++j) {
+      if ((rc = build_v_tables(c, dt, true, true, s))) return rc;
+      if ((rc = advect_vxvy_any(c, A->seg[j - 1], A->W[0], &c->tab_vx, &c->tab_vy, s))) return rc;
+      if ((rc = xy_xy_moment(c, A->W[0], A->seg[j], A->W[1], s))) return rc;
+      if ((rc = launch_field_poisson(c, s))) return rc;
+      save_field(A, j, s);
+    }
+    for (int j = len - 1; j >= 0; --j) {
+      void *dst = (sg == 0 && j == 0) ? grad : A->L[cur ^ 1];
+      if ((rc = step_adjoint_stored(A, A->seg[j], A->seg_e + 2 * n2 * j, A->L[cur], dst, s))) return rc;
+      cur ^= 1;
+    }
+  }
+  return VLP4D_OK;
+}
+
+// Runs body(s) through a cached CUDA graph keyed by `key` (captured on the
+// first call with that key); eager when graphs are off or a capture fails.
+template <typename Body>
+int run_graph(vlp4d_adjoint *A, cudaGraphExec_t &exec, const void **cached, const void *const *key, int nkey,
+              cudaStream_t s, Body body) {
+  if (!A->use_graphs) return body(s);
+  bool hit = exec != nullptr;
+  for (int i = 0; i < nkey && hit; ++i) hit = cached[i] == key[i];
+  if (!hit) {
+    if (exec) {
+      cudaGraphExecDestroy(exec);
+      exec = nullptr;
+    }
+    VLP4D_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+    const int rc = body(s);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s, &g);
+    cudaError_t ie = cudaErrorUnknown;
+    if (rc == VLP4D_OK && e == cudaSuccess && g) ie = cudaGraphInstantiate(&exec, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (rc != VLP4D_OK || e != cudaSuccess || ie != cudaSuccess) {
+      cudaGetLastError();
+      exec = nullptr;
+      A->use_graphs = false;
+      return body(s);
+    }
+    for (int i = 0; i < nkey; ++i) cached[i] = key[i];
+  }
+  VLP4D_CUDA_TRY(cudaGraphLaunch(exec, s));
+  return VLP4D_OK;
 }
 
 void destroy(vlp4d_adjoint *A) {
   if (!A) return;
+  if (A->g_fwd) cudaGraphExecDestroy(A->g_fwd);
+  if (A->g_bwd) cudaGraphExecDestroy(A->g_bwd);
   for (void *p : A->ckpt) cudaFree(p);
   for (void *p : A->seg) cudaFree(p);
   for (int i = 0; i < 2; ++i) {
@@ -418,6 +693,7 @@ void destroy(vlp4d_adjoint *A) {
     cudaFree(A->W[i]);
     cudaFree(A->L[i]);
   }
+  cudaFree(A->seg_e);
   cudaFree(A->gex);
   cudaFree(A->gpart);
   cudaFree(A->hx_hat);
@@ -427,7 +703,12 @@ void destroy(vlp4d_adjoint *A) {
   free_table(A->tab_y_adj);
   free_table(A->tab_vx_adj);
   free_table(A->tab_vy_adj);
+  if (A->own) cudaStreamDestroy(A->own);
   delete A;
+}
+
+cudaStream_t pick_stream(vlp4d_adjoint *A, void *stream) {
+  return stream ? (cudaStream_t)stream : A->own;
 }
 
 }  // namespace
@@ -450,6 +731,8 @@ int vlp4d_adjoint_create(vlp4d_ctx *ctx, int nsteps, int every, vlp4d_adjoint **
   A->nsteps = nsteps;
   A->every = every;
   A->fbytes = (size_t)ctx->g.cells() * ctx->elem;
+  const char *g = getenv("VLP4D_ADJOINT_GRAPHS");
+  if (g && *g == '0') A->use_graphs = false;
   const long long n2 = ctx->g.nxy();
   const int nh = (ctx->g.n[0] / 2 + 1) * ctx->g.n[1];
   auto bail = [&](int rc) {
@@ -466,13 +749,14 @@ int vlp4d_adjoint_create(vlp4d_ctx *ctx, int nsteps, int every, vlp4d_adjoint **
   const int nck = (nsteps + every - 1) / every;
   A->ckpt.assign(nck, nullptr);
   for (auto &p : A->ckpt) ADJ_ALLOC(p, A->fbytes);
-  A->seg.assign(every - 1, nullptr);
+  A->seg.assign(every, nullptr);
   for (auto &p : A->seg) ADJ_ALLOC(p, A->fbytes);
   for (int i = 0; i < 2; ++i) {
     ADJ_ALLOC(A->P[i], A->fbytes);
     ADJ_ALLOC(A->W[i], A->fbytes);
     ADJ_ALLOC(A->L[i], A->fbytes);
   }
+  ADJ_ALLOC(A->seg_e, sizeof(double) * 2 * n2 * (size_t)every);
   ADJ_ALLOC(A->gex, sizeof(double) * (6 * n2 + 1));
   A->gey = A->gex + n2;
   A->lam_rho = A->gey + n2;
@@ -485,12 +769,24 @@ int vlp4d_adjoint_create(vlp4d_ctx *ctx, int nsteps, int every, vlp4d_adjoint **
   ADJ_ALLOC(A->dw_vx, sizeof(double) * 12 * n2);
   A->dw_vy = A->dw_vx + 6 * n2;
 #undef ADJ_ALLOC
+  if (cudaStreamCreate(&A->own) != cudaSuccess) {
+    cudaGetLastError();
+    return bail(fail_msg(VLP4D_ERR_CUDA, "cudaStreamCreate failed"));
+  }
   int rc;
-  cudaStream_t s = 0;
+  cudaStream_t s = A->own;
   if ((rc = build_xy_adj(ctx, 0, 0.5 * ctx->dom.dt, A->tab_x_adj, s))) return bail(rc);
   if ((rc = build_xy_adj(ctx, 1, 0.5 * ctx->dom.dt, A->tab_y_adj, s))) return bail(rc);
   if ((rc = alloc_table(A->tab_vx_adj, (int)n2))) return bail(rc);
   if ((rc = alloc_table(A->tab_vy_adj, (int)n2))) return bail(rc);
+  A->tab_vx_adj.valid = A->tab_vy_adj.valid = true;
+  if ((rc = alloc_table(ctx->tab_vx, (int)n2))) return bail(rc);
+  if ((rc = alloc_table(ctx->tab_vy, (int)n2))) return bail(rc);
+  // The forward x/y tables (host-built; their upload synchronises, which a
+  // graph capture must not meet).
+  StencilTable *t = nullptr;
+  if ((rc = ensure_xy_table(ctx, 0, 0.5 * ctx->dom.dt, &t, s))) return bail(rc);
+  if ((rc = ensure_xy_table(ctx, 1, 0.5 * ctx->dom.dt, &t, s))) return bail(rc);
   if ((rc = field_transpose_setup(A, s))) return bail(rc);
   *out = A;
   return VLP4D_OK;
@@ -528,24 +824,15 @@ int vlp4d_adjoint_forward(vlp4d_adjoint *adj, const void *f0, void *f_out, doubl
   if (!adj) return fail_msg(VLP4D_ERR_INVALID_ARG, "adj is NULL");
   if (!f0) return fail_msg(VLP4D_ERR_INVALID_ARG, "f0 is NULL");
   vlp4d_adjoint *A = adj;
-  vlp4d_ctx *c = A->ctx;
-  cudaStream_t s = (cudaStream_t)stream;
+  cudaStream_t s = pick_stream(A, stream);
   A->have_forward = false;
-  VLP4D_CUDA_TRY(cudaMemcpyAsync(A->ckpt[0], f0, A->fbytes, cudaMemcpyDeviceToDevice, s));
-  const void *in = A->ckpt[0];
-  int rc;
-  for (int n = 0; n < A->nsteps; ++n) {
-    const int next = n + 1;
-    void *out = (next % A->every == 0 && next < A->nsteps) ? A->ckpt[next / A->every] : A->P[n & 1];
-    if ((rc = step_impl(c, in, out, A->W[0], -1, s))) return rc;
-    in = out;
-  }
-  // J of the final state and dJ/df_N (kept for the reverse sweep).
-  if ((rc = energy_grad(A, in, A->L[0], s))) return rc;
-  if (f_out) VLP4D_CUDA_TRY(cudaMemcpyAsync(f_out, in, A->fbytes, cudaMemcpyDeviceToDevice, s));
+  const void *key[2] = {f0, f_out};
+  int rc = run_graph(A, A->g_fwd, A->k_fwd, key, 2, s,
+                     [&](cudaStream_t st) { return forward_body(A, f0, f_out, st); });
+  if (rc) return rc;
   VLP4D_CUDA_TRY(cudaMemcpyAsync(&A->J, A->d_J, sizeof(double), cudaMemcpyDeviceToHost, s));
   VLP4D_CUDA_TRY(cudaStreamSynchronize(s));
-  if ((rc = vlp4d_check(c))) return rc;
+  if ((rc = vlp4d_check(A->ctx))) return rc;
   if (J) *J = A->J;
   A->have_forward = true;
   return VLP4D_OK;
@@ -556,29 +843,12 @@ int vlp4d_adjoint_backward(vlp4d_adjoint *adj, void *grad, void *stream) {
   if (!grad) return fail_msg(VLP4D_ERR_INVALID_ARG, "grad is NULL");
   vlp4d_adjoint *A = adj;
   if (!A->have_forward) return fail_msg(VLP4D_ERR_INVALID_ARG, "vlp4d_adjoint_backward needs a vlp4d_adjoint_forward first");
-  vlp4d_ctx *c = A->ctx;
-  cudaStream_t s = (cudaStream_t)stream;
-  int rc;
-  int cur = 0;
-  const int nseg = (A->nsteps + A->every - 1) / A->every;
-  std::vector<const void *> states(A->every);
-  for (int sg = nseg - 1; sg >= 0; --sg) {
-    const int c0 = sg * A->every;
-    const int len = A->nsteps - c0 < A->every ? A->nsteps - c0 : A->every;
-    // Recompute the segment's step inputs from its checkpoint.
-    states[0] = A->ckpt[sg];
-    for (int j = 1; j < len; ++j) {
-      if ((rc = step_impl(c, states[j - 1], A->seg[j - 1], A->W[0], -1, s))) return rc;
-      states[j] = A->seg[j - 1];
-    }
-    for (int j = len - 1; j >= 0; --j) {
-      void *dst = (sg == 0 && j == 0) ? grad : A->L[cur ^ 1];
-      if ((rc = step_adjoint(A, states[j], A->L[cur], dst, s))) return rc;
-      cur ^= 1;
-    }
-  }
+  cudaStream_t s = pick_stream(A, stream);
+  const void *key[1] = {grad};
+  int rc = run_graph(A, A->g_bwd, &A->k_bwd, key, 1, s, [&](cudaStream_t st) { return backward_body(A, grad, st); });
+  if (rc) return rc;
   VLP4D_CUDA_TRY(cudaStreamSynchronize(s));
-  return vlp4d_check(c);
+  return vlp4d_check(A->ctx);
 }
 
 }  // extern "C"

@@ -45,6 +45,10 @@ struct VslabArgs {
   StencilTable tvx, tvy;
   const int2 *span;  // per chunk: (min, max) signed vy offset of its columns
   int *err;
+  // Optional per-column term added to every output of the column:
+  // out += bias_scale * bias[ixy] (the reverse mode's field term); NULL = none.
+  const double *bias;
+  double bias_scale;
 };
 
 // Signed form of a tap offset m in [0, n): the shift in cells, in (-n/2, n/2].
@@ -194,6 +198,8 @@ __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorM
       lag0 = 5 + signed_offset(__ldg(a.tvy.m + ixy), a.nvy) - a.span[cc].x;
       load_weights(WeightsOf<T>::get(a.tvy), ixy, wvy);
     }
+    const bool has_bias = a.bias != nullptr;
+    const double bias = has_bias ? a.bias_scale * __ldg(a.bias + ixy) : 0.0;
     // Output pointer of the next row this thread writes.
     T *orow = static_cast<T *>(a.fout) + ixy + vstride * vx0 + ystride * (long long)sg * a.Q;
     // Ring of vx-swept rows, slot = t % 6 (static after unrolling).  FP64:
@@ -285,6 +291,10 @@ __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorM
               } else {
                 val = win2[u][i];
               }
+              if (has_bias) {
+                val.x = (float)((double)val.x + bias);
+                val.y = (float)((double)val.y + bias);
+              }
               orowf[vstride * i] = val.x;
               orowf[vstride * (i + H)] = val.y;
             }
@@ -297,6 +307,7 @@ __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorM
                               win[(u + 4) % 6][i], win[(u + 5) % 6][i], win[u][i]);
               else
                 val = win[u][i];
+              if (has_bias) val = (T)((double)val + bias);
               orow[vstride * i] = val;
             }
           }
@@ -422,7 +433,7 @@ int launch_advect_vxvy(vlp4d_ctx *c, const void *fn, void *fnp1, bool do_vx, boo
 }
 
 int launch_advect_vxvy_tables(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *tvx,
-                              const StencilTable *tvy, cudaStream_t s) {
+                              const StencilTable *tvy, cudaStream_t s, const double *bias, double bias_scale) {
   const bool do_vx = tvx != nullptr, do_vy = tvy != nullptr;
   if (!c->fused) return VLP4D_ERR_UNSUPPORTED;
   if (((uintptr_t)fn & 15) || ((uintptr_t)fnp1 & 15)) return VLP4D_ERR_UNSUPPORTED;
@@ -466,6 +477,8 @@ int launch_advect_vxvy_tables(vlp4d_ctx *c, const void *fn, void *fnp1, const St
   if (do_vy) a.tvy = *tvy;
   a.span = c->vspan;
   a.err = c->d_err;
+  a.bias = bias;
+  a.bias_scale = bias_scale;
 #define VLP4D_VS(T, DVX, DVY, V)                                                  \
   switch (a.nxy) {                                                                \
     case 16384: return run_vslab<T, DVX, DVY, V, 16384>(c, map, a, cfg, s);      \

@@ -457,6 +457,16 @@ int advect_vxvy_any(vlp4d_ctx *ctx, const void *fn, void *fnp1, const StencilTab
 
 int fail_msg(int code, const std::string &msg) { return fail(code, msg); }
 
+// Whether the x/y half steps of consecutive steps run as one k_plane_xyxy
+// pass.  That pass does the arithmetic of two passes for the HBM traffic of
+// one: it pays off in FP32, while in FP64 its shared-memory footprint leaves
+// one CTA per SM and two k_plane passes are faster.  VLP4D_XYXY=0/1 at
+// context creation overrides.
+bool xyxy_join(const vlp4d_ctx *ctx) {
+  if (ctx->xyxy_mode >= 0) return ctx->xyxy_mode == 1;
+  return ctx->dtype == VLP4D_F32;
+}
+
 }  // namespace vlp4d
 
 extern "C" {
@@ -471,16 +481,6 @@ int vlp4d_step(vlp4d_ctx *ctx, void *f_state, void *f_next, int iter, void *stre
 
 // The reference's time loop (vlp4d.cpp:63-72, onetimestep per step) with
 // the last x/y half step of each step fused with the first of the next.
-// Whether vlp4d_steps joins the x/y half steps of consecutive steps into one
-// k_plane_xyxy pass.  That pass does the arithmetic of two passes for the
-// HBM traffic of one: it pays off in FP32, while in FP64 its shared-memory
-// footprint leaves one CTA per SM and two k_plane passes are faster.
-// VLP4D_XYXY=0/1 at context creation overrides.
-static bool xyxy_preferred(const vlp4d_ctx *ctx) {
-  if (ctx->xyxy_mode >= 0) return ctx->xyxy_mode == 1;
-  return ctx->dtype == VLP4D_F32;
-}
-
 int vlp4d_steps(vlp4d_ctx *ctx, void *f_state, void *f_next, int iter0, int nsteps, void *stream) {
   int rc = check_ctx(ctx);
   if (rc) return rc;
@@ -506,8 +506,8 @@ int vlp4d_steps(vlp4d_ctx *ctx, void *f_state, void *f_next, int iter0, int nste
     if (k + 1 == nsteps) break;
     // timestep.hpp:50-58 of step k, then :17-28 of step k+1, in one pass
     // where that pass is the faster choice.
-    rc = xyxy_preferred(ctx) ? launch_advect_xyxy(ctx, cur, oth, tx, ty, s) : VLP4D_ERR_UNSUPPORTED;
-    if (rc == VLP4D_ERR_UNSUPPORTED && !xyxy_preferred(ctx)) {
+    rc = xyxy_join(ctx) ? launch_advect_xyxy(ctx, cur, oth, tx, ty, s) : VLP4D_ERR_UNSUPPORTED;
+    if (rc == VLP4D_ERR_UNSUPPORTED && !xyxy_join(ctx)) {
       if ((rc = advect_xy_impl(ctx, cur, oth, 0.5 * dt, false, s))) return rc;
       std::swap(cur, oth);
       if ((rc = advect_xy_impl(ctx, cur, oth, 0.5 * dt, true, s))) return rc;

@@ -146,9 +146,11 @@ int launch_advect_pair_generic(vlp4d_ctx *c, bool v, const void *fn, void *fnp1,
 int launch_advect_xy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *tx,
                      const StencilTable *ty, bool do_x, bool do_y, bool with_rho, cudaStream_t s);
 int launch_advect_vxvy(vlp4d_ctx *c, const void *fn, void *fnp1, bool do_vx, bool do_vy, cudaStream_t s);
-// The same pass with explicit v tables (the reverse mode passes transposed ones).
+// The same pass with explicit v tables (the reverse mode passes transposed
+// ones) and an optional per-column term: out += bias_scale * bias[ix + nx*iy].
 int launch_advect_vxvy_tables(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *tvx,
-                              const StencilTable *tvy, cudaStream_t s);
+                              const StencilTable *tvy, cudaStream_t s, const double *bias = nullptr,
+                              double bias_scale = 0.0);
 int launch_advect_xyxy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *tx, const StencilTable *ty,
                        cudaStream_t s);
 
@@ -163,6 +165,9 @@ int advect_vxvy_any(vlp4d_ctx *ctx, const void *fn, void *fnp1, const StencilTab
                     cudaStream_t s);
 // Records msg as the calling thread's last error and returns code.
 int fail_msg(int code, const std::string &msg);
+// Whether time loops join the x/y half steps of consecutive steps into one
+// k_plane_xyxy pass (FP32 by default; VLP4D_XYXY overrides).
+bool xyxy_join(const vlp4d_ctx *ctx);
 
 // field.cu
 int launch_field_rho(vlp4d_ctx *c, const void *fn, cudaStream_t s);

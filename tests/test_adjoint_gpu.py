@@ -125,3 +125,28 @@ def test_energy_gradient_wrt_perturbation_field_fd_and_fp32(pkg, cuda):
                     assert abs(g - fd) <= 1e-5 * abs(fd) + 1e-12 * abs(J.item()), (idx, g, fd)
     g64, g32 = grads["f64"], grads["f32"]
     assert np.linalg.norm(g32 - g64) <= 1e-3 * np.linalg.norm(g64)
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_graph_and_eager_reverse_sweeps_agree(pkg, cuda, dtype):
+    """The forward and reverse sweeps run as captured CUDA graphs by default;
+    VLP4D_ADJOINT_GRAPHS=0 runs them eagerly.  Same kernels, same order: the
+    results are bit-identical, also on a second call through the cached graphs."""
+    torch = cuda
+    n, nsteps = (32, 16, 32, 24), 10
+    dom = _dom(pkg, n, nbiter=nsteps)
+    res = []
+    for graphs in ("1", "0"):
+        os.environ["VLP4D_ADJOINT_GRAPHS"] = graphs
+        try:
+            with pkg.Context(dom, dtype) as ctx, pkg.Adjoint(ctx, nsteps, 4) as adj:
+                f0 = ctx.empty_f()
+                ctx.init_case(f0, IC_LANDAU_SUM, 0.05, 0.5)
+                for _ in range(2):
+                    J = adj.forward(f0)
+                    g = adj.backward()
+                res.append((J, g.cpu()))
+        finally:
+            del os.environ["VLP4D_ADJOINT_GRAPHS"]
+    assert res[0][0] == res[1][0]
+    assert torch.equal(res[0][1], res[1][1])
