@@ -343,6 +343,7 @@ def gpu_arm(args, ranks):
         torch.cuda.empty_cache()
 
     adjoint = None if args.only_f32 else adjoint_arm(pkg, torch, stream)
+    ensemble = None if args.only_f32 else ensemble_arm(pkg, torch, stream, peak)
 
     rec = per_dtype["f32"]
     line = {
@@ -362,8 +363,33 @@ def gpu_arm(args, ranks):
                  "stages": per_dtype["f64"]["stages"]} if "f64" in per_dtype else None),
         "stages": rec["stages"], "error_f32_vs_f64": err,
         "adjoint": adjoint,
+        "ensemble": ensemble,
     }
     return line
+
+
+def ensemble_arm(pkg, torch, stream, peak, nruns=256, nsteps=50):
+    """The batched-ensemble configuration: 256 Landau members, N per dimension
+    drawn from {16, 24, 32, 48}, amp ~ U[0.01, 0.1], k in {0.3, 0.5}, 50 steps
+    of dt 0.1, FP32 f, in one persistent launch replayed from a CUDA graph.
+    Tiles from the autotuner (3 steps per configuration).  Algorithmic bytes:
+    f read and written by each of the three passes of a step."""
+    v = pkg.vlp4d
+    members = v.landau_ensemble_members(nruns)
+    with v.Ensemble(members, nsteps) as ens:
+        tiles = ens.autotune(3)
+        ens.run()  # capture
+        ens.check()
+        t = time_calls(torch, stream, lambda: ens.run(stream), 3)
+        ens.check()
+        cells = ens.cells
+        gbs = 3 * 2 * 4.0 * cells * nsteps / t / 1e9
+        return {"config": {"members": nruns, "sizes": [16, 24, 32, 48], "steps": nsteps, "dt": 0.1,
+                           "amp": [0.01, 0.1], "k": [0.3, 0.5], "storage": "f32 f, f64 fields"},
+                "cells": cells, "ms": t * 1e3, "value": cells * nsteps / t / 1e9, "unit": METRIC,
+                "tiles": {"threads": tiles[0], "cols_per_tile": tiles[1], "ctas_per_sm": tiles[2]},
+                "hbm": {"achieved_gbs": gbs, "frac": gbs / peak, "bytes_per_step": 3 * 2 * 4 * cells},
+                "launches_per_run": 3}
 
 
 def adjoint_arm(pkg, torch, stream, n=64, nsteps=200, every=8):

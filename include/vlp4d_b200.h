@@ -242,6 +242,43 @@ int vlp4d_step_adjoint(vlp4d_adjoint *adj, const void *f_state, const void *lam_
  * call synchronises the stream). */
 int vlp4d_energy_grad(vlp4d_adjoint *adj, const void *f, double *J, void *lam, void *stream);
 
+/* ---- Batched ensemble.  No reference counterpart (the reference runs one
+ * domain per process).  Many independent runs of uneven grids, each the
+ * vlp4d step of timestep.hpp:14-67 with FP32 f and FP64 fields from the
+ * Landau initial condition f0 = M(vx) M(vy) (1 + amp (cos k x + cos k y)),
+ * advance in ONE persistent kernel launch that a CUDA graph replays (with
+ * the initial condition and the scheduler reset).  Members need
+ * nx, ny, nvx <= 64.  The energy history of each member (nsteps + 1 values,
+ * log of the electric-energy norm as Diags::compute) is kept on the device. */
+typedef struct {
+  int n[4];            /* nx, ny, nvx, nvy */
+  double min_phy[4];
+  double max_phy[4];
+  double dt;
+  double amp, k;       /* initial perturbation amplitude and wave number */
+} vlp4d_ens_member;
+typedef struct vlp4d_ensemble vlp4d_ensemble;
+
+int vlp4d_ensemble_create(const vlp4d_ens_member *members, int nruns, int nsteps, vlp4d_ensemble **out);
+int vlp4d_ensemble_destroy(vlp4d_ensemble *ens);
+/* Initial condition + nsteps steps of every member (graph replay; the first
+ * call captures).  Asynchronous; vlp4d_ensemble_check synchronises and
+ * reports VLP4D_ERR_TIMEOUT if a CTA gave up waiting for work. */
+int vlp4d_ensemble_run(vlp4d_ensemble *ens, void *stream);
+int vlp4d_ensemble_check(vlp4d_ensemble *ens);
+/* Final f of member `run` (device copy, FP32, its own layout_left extents)
+ * and its energy history (host, nsteps + 1 values); either may be NULL. */
+int vlp4d_ensemble_read(vlp4d_ensemble *ens, int run, void *f_out, double *nrj, void *stream);
+long long vlp4d_ensemble_cells(const vlp4d_ensemble *ens);
+/* Tile configuration: threads per CTA, columns per vx/vy tile, CTAs per SM
+ * (0 = as many as fit).  The autotuner scans threads {128, 256, 512},
+ * columns {8, 16, 32, 64} and CTAs per SM {1..4}, timing `steps` steps per
+ * configuration; it writes one CSV line per configuration to csv_path
+ * (NULL: none) and keeps the fastest. */
+int vlp4d_ensemble_set_tiles(vlp4d_ensemble *ens, int threads, int cols_per_tile, int ctas_per_sm);
+int vlp4d_ensemble_get_tiles(const vlp4d_ensemble *ens, int *threads, int *cols_per_tile, int *ctas_per_sm);
+int vlp4d_ensemble_autotune(vlp4d_ensemble *ens, int steps, const char *csv_path, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

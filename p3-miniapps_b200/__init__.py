@@ -8,4 +8,5 @@ The directory name contains a hyphen, so it is loaded by path:
 ``__graft_entry__.load_package()`` registers it as ``p3_miniapps_b200``.
 """
 from . import vlp4d  # noqa: F401
-from .vlp4d import Adjoint, Context, Domain, build, energy_after_steps, landau_domain, lib  # noqa: F401
+from .vlp4d import (Adjoint, Context, Domain, Ensemble, EnsembleMember, build, energy_after_steps,  # noqa: F401
+                    landau_domain, landau_ensemble_members, lib)

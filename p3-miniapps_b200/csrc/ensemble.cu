@@ -1,0 +1,782 @@
+// Batched ensemble: many independent vlp4d runs of uneven grids advanced in
+// ONE persistent kernel launch (captured in a CUDA graph together with the
+// initial condition and the scheduler reset).
+//
+// No reference counterpart: the reference runs one domain per process.  Each
+// member is the single-process step of timestep.hpp:14-67 on its own grid,
+// FP32 f with FP64 fields, with the Landau sum initial condition
+// f0 = M(vx) M(vy) (1 + amp (cos kx + cos ky)).
+//
+// Work decomposition.  Member r's run is a sequence of stages
+//   0: moment of f0                     tiles: nvy  (one vy row of planes each)
+//   1: field solve, diagnostic 0        tiles: 1
+//   per step t (stage 2 + 4t + sub):
+//   sub 0: x, y (dt/2) + moment         tiles: nvy
+//   sub 1: field solve, diagnostic t+1  tiles: 1
+//   sub 2: vx, vy (dt)                  tiles: ceil(nx*ny / cc)   (cc columns each)
+//   sub 3: x, y (dt/2)                  tiles: nvy
+// A stage's tiles may start only when the member's previous stage is
+// complete; different members are independent.  Scheduling is dynamic and
+// wait-free: a CTA picks a member, atomically takes the next tile of the
+// member's current stage (one 64-bit word per member holds (stage, next
+// tile)), runs it and counts it done; the CTA that completes a stage's last
+// tile advances the member's word to the next stage.  A CTA that finds no
+// tile moves on to another member, so no CTA ever waits for a specific
+// other CTA: progress does not depend on which CTAs are resident.  A CTA
+// leaves when every member has finished, or (error flag set) when it has
+// found no tile for about two seconds.
+//
+// Data written inside the kernel and read by other CTAs (f between stages,
+// moment partials, fields) is read with L2-only loads (ld.global.cg): the
+// SM-local L1 is not coherent across CTAs.  Visibility follows the counter
+// chain: writers fence then count their tile done; the CTA that sees the
+// stage complete fences before publishing the next stage; a CTA that takes
+// a tile of the new stage fences before reading.
+//
+// The field solve of a member (nx, ny <= 64) is a 2D DFT in FP64 shared
+// memory (direct sums with tabulated twiddles: a few hundred thousand
+// multiply-adds), the spectral solve of efield.cpp:43-105 (kx0 = 2*pi/xmax,
+// mode 0 zeroed), and the inverse DFT keeping the real part.
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "internal.cuh"
+#include "stencil.cuh"
+
+namespace vlp4d {
+namespace {
+
+constexpr int kEnsMaxN = 64;  // largest nx, ny of a member (field solve in shared memory)
+
+struct EnsRun {
+  int n[4];
+  double minp[4], maxp[4], dx[4];
+  double dt, amp, k;
+  long long f_off;  // element offset of f in the arenas (multiple of 64)
+  long long p_off;  // moment partials: nvy * nx*ny doubles
+  long long e_off;  // fields: ex, ey (2 * nx*ny doubles)
+  long long d_off;  // diagnostic history: nsteps + 1 doubles
+};
+
+struct EnsArgs {
+  const EnsRun *runs;
+  int nruns, nsteps;
+  float *F0, *F1;
+  double *part, *fld, *nrj;
+  unsigned long long *word;
+  unsigned int *done;
+  int *remaining;
+  int *err;
+  int cc;      // columns per vx/vy tile
+  int maxnxy;  // largest nx*ny of a member (shared-memory layout)
+  long long idle_limit;
+};
+
+__device__ __forceinline__ int stage_tiles(const EnsRun &R, int S, int cc) {
+  if (S == 0) return R.n[3];
+  if (S == 1) return 1;
+  const int sub = (S - 2) & 3;
+  if (sub == 1) return 1;
+  if (sub == 2) return (R.n[0] * R.n[1] + cc - 1) / cc;
+  return R.n[3];
+}
+
+// Stencil record of one line: FP32 difference weights and the tap offset.
+struct EnsLine {
+  float v[6];
+  int m;
+};
+
+__device__ __forceinline__ EnsLine ens_line(double disp, double hmin, double hmax, int n) {
+  const LineStencil s = line_stencil(disp, hmin, hmax, n);
+  EnsLine l;
+  weights_to_f32(s.w, l.v);
+  l.m = s.m;
+  return l;
+}
+
+// Moment of f0 (stage 0) or x/y half step (+ moment) of the vy row `ivy`.
+// Shared memory: two plane buffers (floats), x lines (nvx), the moment (FP64).
+template <bool SWEEP, bool MOMENT>
+__device__ void ens_planes(const EnsArgs &a, const EnsRun &R, const float *fin, float *fout, int ivy,
+                           unsigned char *smem) {
+  const int nx = R.n[0], ny = R.n[1], nvx = R.n[2];
+  const int nxy = nx * ny;
+  // Layout: acc (maxnxy doubles) | b0, b1 (maxnxy floats each) | x lines.
+  double *acc = reinterpret_cast<double *>(smem);
+  float *b0 = reinterpret_cast<float *>(acc + a.maxnxy);
+  float *b1 = b0 + a.maxnxy;
+  EnsLine *xl = reinterpret_cast<EnsLine *>(b1 + a.maxnxy);
+  __shared__ EnsLine yl;
+  const double hdt = 0.5 * R.dt;
+  if (SWEEP) {
+    for (int l = threadIdx.x; l < nvx; l += blockDim.x)
+      xl[l] = ens_line(hdt * (R.minp[2] + l * R.dx[2]), R.minp[0], R.maxp[0], nx);
+    if (threadIdx.x == 0) yl = ens_line(hdt * (R.minp[3] + ivy * R.dx[3]), R.minp[1], R.maxp[1], ny);
+  }
+  if (MOMENT)
+    for (int c = threadIdx.x; c < nxy; c += blockDim.x) acc[c] = 0.;
+  __syncthreads();
+  for (int ivx = 0; ivx < nvx; ++ivx) {
+    const long long base = R.f_off + ((long long)ivy * nvx + ivx) * nxy;
+    if (!SWEEP) {
+      for (int c = threadIdx.x; c < nxy; c += blockDim.x) acc[c] += (double)__ldcg(fin + base + c);
+      continue;
+    }
+    for (int c = threadIdx.x; c < nxy; c += blockDim.x) b0[c] = __ldcg(fin + base + c);
+    __syncthreads();
+    const EnsLine lx = xl[ivx];
+    for (int c = threadIdx.x; c < nxy; c += blockDim.x) {
+      const int ix = c % nx, row = c - ix;
+      int j = ix + lx.m;
+      j = j >= nx ? j - nx : j;
+      float t[6];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        t[k] = b0[row + j];
+        if (++j == nx) j = 0;
+      }
+      b1[c] = interp6(lx.v, t[0], t[1], t[2], t[3], t[4], t[5]);
+    }
+    __syncthreads();
+    const EnsLine ly = yl;
+    for (int c = threadIdx.x; c < nxy; c += blockDim.x) {
+      const int ix = c % nx, iy = c / nx;
+      int j = iy + ly.m;
+      j = j >= ny ? j - ny : j;
+      float t[6];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        t[k] = b1[j * nx + ix];
+        if (++j == ny) j = 0;
+      }
+      const float o = interp6(ly.v, t[0], t[1], t[2], t[3], t[4], t[5]);
+      fout[base + c] = o;
+      if (MOMENT) acc[c] += (double)o;
+    }
+    __syncthreads();
+  }
+  if (MOMENT) {
+    __syncthreads();
+    double *p = a.part + R.p_off + (long long)ivy * nxy;
+    for (int c = threadIdx.x; c < nxy; c += blockDim.x) p[c] = acc[c];
+  }
+}
+
+// vx then vy (dt) of the columns [tile*cc, tile*cc + cc).  Thread (col, g)
+// handles output vx rows g, g+G, ...; for each it streams the vy rows from
+// the column's vy offset, keeping six vx-swept values in a ring.
+__device__ void ens_vxvy(const EnsArgs &a, const EnsRun &R, const float *fin, float *fout, int tile) {
+  const int nx = R.n[0], ny = R.n[1], nvx = R.n[2], nvy = R.n[3];
+  const int nxy = nx * ny;
+  const int cc = a.cc;
+  const int G = blockDim.x / cc;
+  const int lc = threadIdx.x % cc, g = threadIdx.x / cc;
+  const int col = tile * cc + lc;
+  if (g >= G || col >= nxy) return;
+  const double *ex = a.fld + R.e_off, *ey = ex + nxy;
+  const EnsLine lx = ens_line(R.dt * __ldcg(ex + col), R.minp[2], R.maxp[2], nvx);
+  const EnsLine ly = ens_line(R.dt * __ldcg(ey + col), R.minp[3], R.maxp[3], nvy);
+  const long long vstride = nxy, ystride = (long long)nxy * nvx;
+  const float *src = fin + R.f_off + col;
+  float *dst = fout + R.f_off + col;
+  for (int ivx = g; ivx < nvx; ivx += G) {
+    int toff[6];
+    int j = ivx + lx.m;
+    j = j >= nvx ? j - nvx : j;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      toff[k] = j;
+      if (++j == nvx) j = 0;
+    }
+    float ring[6];
+    int row = ly.m;
+    const int nrows = nvy + 5;
+    for (int r0 = 0; r0 < nrows; r0 += 6) {
+#pragma unroll
+      for (int u = 0; u < 6; ++u) {
+        const int r = r0 + u;
+        if (r >= nrows) break;
+        const float *p = src + (long long)row * ystride;
+        float t[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) t[k] = __ldcg(p + (long long)toff[k] * vstride);
+        ring[u] = interp6(lx.v, t[0], t[1], t[2], t[3], t[4], t[5]);
+        if (++row == nvy) row = 0;
+        if (r >= 5) {
+          const int ivy = r - 5;
+          dst[(long long)ivy * ystride + (long long)ivx * vstride] =
+              interp6(ly.v, ring[(u + 1) % 6], ring[(u + 2) % 6], ring[(u + 3) % 6], ring[(u + 4) % 6],
+                      ring[(u + 5) % 6], ring[u]);
+        }
+      }
+    }
+  }
+}
+
+// One 1D DFT pass over a (rows x len) complex array in shared memory:
+// out[r][k] = sum_j in[r][j] * w^(sign k j), w = exp(2 pi i / len); strides
+// select rows/columns.  tw[m] = (cos(2 pi m/len), sin(2 pi m/len)).
+__device__ void ens_dft(const double2 *in, double2 *out, int rows, int len, int rstride, int estride,
+                        const double2 *tw, double sign) {
+  for (int o = threadIdx.x; o < rows * len; o += blockDim.x) {
+    const int r = o / len, k = o % len;
+    double sr = 0., si = 0.;
+    int m = 0;
+    for (int j = 0; j < len; ++j) {
+      const double2 v = in[r * rstride + j * estride];
+      const double2 w = tw[m];
+      const double wi = sign * w.y;
+      sr = fma(v.x, w.x, fma(-v.y, wi, sr));
+      si = fma(v.x, wi, fma(v.y, w.x, si));
+      m += k;
+      if (m >= len) m -= len;
+    }
+    out[r * rstride + k * estride] = make_double2(sr, si);
+  }
+}
+
+// Field solve of member R from its moment partials, diagnostic slot `iter`.
+// Shared memory: two complex (maxnxy) arrays and the twiddles.
+__device__ void ens_field(const EnsArgs &a, const EnsRun &R, int iter, unsigned char *smem) {
+  const int nx = R.n[0], ny = R.n[1], nvy = R.n[3];
+  const int nxy = nx * ny;
+  double2 *H1 = reinterpret_cast<double2 *>(smem);
+  double2 *H2 = H1 + a.maxnxy;
+  double2 *twx = H2 + a.maxnxy;
+  double2 *twy = twx + kEnsMaxN;
+  for (int m = threadIdx.x; m < nx; m += blockDim.x) {
+    double sn, cs;
+    sincospi(2.0 * m / nx, &sn, &cs);
+    twx[m] = make_double2(cs, sn);
+  }
+  for (int m = threadIdx.x; m < ny; m += blockDim.x) {
+    double sn, cs;
+    sincospi(2.0 * m / ny, &sn, &cs);
+    twy[m] = make_double2(cs, sn);
+  }
+  // rho = dvx dvy * (sum of the vy rows' partials, fixed order), as complex.
+  const double dvv = R.dx[2] * R.dx[3];
+  const double *p = a.part + R.p_off;
+  for (int c = threadIdx.x; c < nxy; c += blockDim.x) {
+    double sum = 0.;
+    for (int v = 0; v < nvy; ++v) sum += __ldcg(p + (long long)v * nxy + c);
+    H1[c] = make_double2(sum * dvv, 0.);
+  }
+  __syncthreads();
+  ens_dft(H1, H2, ny, nx, nx, 1, twx, -1.);  // along x, every row
+  __syncthreads();
+  ens_dft(H2, H1, nx, ny, 1, nx, twy, -1.);  // along y, every column: H1 = rho_hat
+  __syncthreads();
+  const double kx0 = 2 * M_PI / R.maxp[0], ky0 = 2 * M_PI / R.maxp[1];
+  const double norm = 1.0 / ((double)nx * ny);
+  for (int comp = 0; comp < 2; ++comp) {
+    // H2 = inverse DFT along y of (-i k_comp / |k|^2 / (nx ny)) * rho_hat
+    // (mode 0 zeroed), column by column.
+    for (int o = threadIdx.x; o < nxy; o += blockDim.x) {
+      const int ix = o % nx, y = o / nx;
+      const double kx = (ix <= nx / 2 ? ix : ix - nx) * kx0;
+      double sr = 0., si = 0.;
+      int m = 0;
+      for (int iy = 0; iy < ny; ++iy) {
+        const double ky = (iy <= ny / 2 ? iy : iy - ny) * ky0;
+        const double k2 = kx * kx + ky * ky;
+        const double q = (ix == 0 && iy == 0) ? 0. : (comp == 0 ? kx : ky) / k2 * norm;
+        const double2 h = H1[iy * nx + ix];
+        const double vr = q * h.y, vi = -q * h.x;
+        const double2 w = twy[m];
+        sr = fma(vr, w.x, fma(-vi, w.y, sr));
+        si = fma(vr, w.y, fma(vi, w.x, si));
+        m += y;
+        if (m >= ny) m -= ny;
+      }
+      H2[o] = make_double2(sr, si);
+    }
+    __syncthreads();
+    // Real part of the inverse DFT along x, to the field arena.
+    double *e = a.fld + R.e_off + (long long)comp * nxy;
+    for (int o = threadIdx.x; o < nxy; o += blockDim.x) {
+      const int x = o % nx, y = o / nx;
+      double sr = 0.;
+      int m = 0;
+      for (int ix = 0; ix < nx; ++ix) {
+        const double2 v = H2[y * nx + ix];
+        const double2 w = twx[m];
+        sr = fma(v.x, w.x, fma(-v.y, w.y, sr));
+        m += x;
+        if (m >= nx) m -= nx;
+      }
+      e[o] = sr;
+    }
+    __syncthreads();
+  }
+  // Energy: a fixed reduction order whatever the block size (lane l sums
+  // cells l, l+32, ...; then a fixed shuffle tree), so the history does not
+  // depend on the tile configuration.
+  if (threadIdx.x < 32) {
+    const double *ex = a.fld + R.e_off, *ey = ex + nxy;
+    double e2 = 0.;
+    for (int c = threadIdx.x; c < nxy; c += 32) e2 += ex[c] * ex[c] + ey[c] * ey[c];
+    for (int o = 16; o > 0; o >>= 1) e2 += __shfl_down_sync(0xffffffffu, e2, o);
+    if (threadIdx.x == 0) {
+      const double en = sqrt(e2 * R.dx[0] * R.dx[1]);
+      a.nrj[R.d_off + iter] = en > 1.e-30 ? log(en) : -1.e9;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(512) k_ensemble(EnsArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_run, s_stage, s_tile;
+  const int total_stages = 2 + 4 * a.nsteps;
+  // Scheduler state, kept by thread 0 only.
+  int r = (int)((blockIdx.x * 7919LL) % a.nruns);
+  long long idle_start = clock64();
+  int misses = 0;
+  while (true) {
+    if (threadIdx.x == 0) {
+      // -1: leave (all members done, or no work for idle_limit cycles);
+      // -2: nothing taken this round; >= 0: a tile of member s_run.
+      int got_run = -2;
+      if (*(volatile int *)a.remaining <= 0) {
+        got_run = -1;
+      } else {
+        const EnsRun &R = a.runs[r];
+        const unsigned long long w = *(volatile unsigned long long *)(a.word + r);
+        const int stage = (int)(w >> 32);
+        if (stage < total_stages && (int)(w & 0xffffffffu) < stage_tiles(R, stage, a.cc)) {
+          const unsigned long long got = atomicAdd(a.word + r, 1ULL);
+          const int st = (int)(got >> 32), tl = (int)(got & 0xffffffffu);
+          if (st < total_stages && tl < stage_tiles(R, st, a.cc)) {
+            got_run = r;
+            s_stage = st;
+            s_tile = tl;
+            __threadfence();
+          }
+        }
+        if (got_run >= 0) {
+          idle_start = clock64();
+          misses = 0;
+        } else {
+          r = r + 1 == a.nruns ? 0 : r + 1;
+          if (++misses >= a.nruns) {
+            misses = 0;
+            __nanosleep(512);
+            if (clock64() - idle_start > a.idle_limit) {
+              atomicExch(a.err, 1);
+              got_run = -1;
+            }
+          }
+        }
+      }
+      s_run = got_run;
+    }
+    __syncthreads();
+    const int run = s_run;
+    if (run == -1) break;
+    if (run >= 0) {
+      const EnsRun &R = a.runs[run];
+      const int S = s_stage, tile = s_tile;
+      if (S == 0) {
+        ens_planes<false, true>(a, R, a.F0, nullptr, tile, smem);
+      } else if (S == 1) {
+        ens_field(a, R, 0, smem);
+      } else {
+        const int t = (S - 2) >> 2, sub = (S - 2) & 3;
+        float *fa = (t & 1) ? a.F1 : a.F0, *fb = (t & 1) ? a.F0 : a.F1;
+        if (sub == 0) ens_planes<true, true>(a, R, fa, fb, tile, smem);
+        else if (sub == 1) ens_field(a, R, t + 1, smem);
+        else if (sub == 2) ens_vxvy(a, R, fb, fa, tile);
+        else ens_planes<true, false>(a, R, fa, fb, tile, smem);
+      }
+      // Every thread's writes, then the tile count.
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        const unsigned int n = (unsigned int)stage_tiles(R, S, a.cc);
+        if (atomicAdd(a.done + run, 1u) + 1u == n) {
+          a.done[run] = 0u;
+          __threadfence();
+          if (S + 1 == total_stages) atomicSub(a.remaining, 1);
+          atomicExch(a.word + run, (unsigned long long)(S + 1) << 32);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_ens_init(EnsArgs a) {
+  const EnsRun &R = a.runs[blockIdx.y];
+  const long long total = (long long)R.n[0] * R.n[1] * R.n[2] * R.n[3];
+  const double PI = 3.14159265358979323846;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(idx % R.n[0]);
+    long long q = idx / R.n[0];
+    const int iy = (int)(q % R.n[1]);
+    q /= R.n[1];
+    const int ivx = (int)(q % R.n[2]);
+    const int ivy = (int)(q / R.n[2]);
+    const double x = R.minp[0] + ix * R.dx[0];
+    const double y = R.minp[1] + iy * R.dx[1];
+    const double vx = R.minp[2] + ivx * R.dx[2];
+    const double vy = R.minp[3] + ivy * R.dx[3];
+    const double val = (1. + R.amp * cos(R.k * x) + R.amp * cos(R.k * y)) * (exp(-0.5 * (vx * vx + vy * vy)) / (2 * PI));
+    a.F0[R.f_off + idx] = (float)val;
+  }
+}
+
+__global__ void k_ens_reset(EnsArgs a) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < a.nruns) {
+    a.word[r] = 0ull;
+    a.done[r] = 0u;
+  }
+  if (r == 0) {
+    *a.remaining = a.nruns;
+    *a.err = 0;
+  }
+}
+
+}  // namespace
+}  // namespace vlp4d
+
+struct vlp4d_ensemble {
+  int device = 0, num_sms = 0;
+  int nruns = 0, nsteps = 0;
+  std::vector<vlp4d::EnsRun> host_runs;
+  vlp4d::EnsRun *runs = nullptr;
+  float *F[2] = {nullptr, nullptr};
+  double *part = nullptr, *fld = nullptr, *nrj = nullptr;
+  unsigned long long *word = nullptr;
+  unsigned int *done = nullptr;
+  int *remaining = nullptr, *err = nullptr;
+  long long total_cells = 0, max_cells = 0;
+  int maxnxy = 0;
+  // Tile configuration (vlp4d_ensemble_set_tiles / _autotune).
+  int threads = 256, cc = 32, ctas_per_sm = 0;  // 0: as many as fit
+  size_t smem = 0;
+  cudaGraphExec_t graph = nullptr;
+};
+
+namespace vlp4d {
+namespace {
+
+size_t ens_smem(int maxnxy) {
+  const size_t planes = sizeof(double) * maxnxy + 2 * sizeof(float) * maxnxy + sizeof(EnsLine) * kEnsMaxN;
+  const size_t field = 2 * sizeof(double2) * maxnxy + 2 * sizeof(double2) * kEnsMaxN;
+  return ((planes > field ? planes : field) + 255) / 256 * 256;
+}
+
+EnsArgs ens_args(vlp4d_ensemble *E, int nsteps) {
+  EnsArgs a;
+  a.runs = E->runs;
+  a.nruns = E->nruns;
+  a.nsteps = nsteps;
+  a.F0 = E->F[0];
+  a.F1 = E->F[1];
+  a.part = E->part;
+  a.fld = E->fld;
+  a.nrj = E->nrj;
+  a.word = E->word;
+  a.done = E->done;
+  a.remaining = E->remaining;
+  a.err = E->err;
+  a.cc = E->cc;
+  a.maxnxy = E->maxnxy;
+  a.idle_limit = 4000000000LL;  // about two seconds at 1.9 GHz
+  return a;
+}
+
+// Initial condition, scheduler reset and the persistent launch.
+int ens_launch(vlp4d_ensemble *E, int nsteps, cudaStream_t s) {
+  const EnsArgs a = ens_args(E, nsteps);
+  dim3 ig((unsigned)((E->max_cells + 255) / 256 < 4096 ? (E->max_cells + 255) / 256 : 4096), (unsigned)E->nruns);
+  k_ens_init<<<ig, 256, 0, s>>>(a);
+  VLP4D_LAUNCH_CHECK();
+  k_ens_reset<<<(E->nruns + 255) / 256, 256, 0, s>>>(a);
+  VLP4D_LAUNCH_CHECK();
+  int per_sm = 0;
+  VLP4D_CUDA_TRY(cudaFuncSetAttribute(k_ensemble, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)E->smem));
+  VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ensemble, E->threads, E->smem));
+  if (per_sm < 1) return fail_msg(VLP4D_ERR_UNSUPPORTED, "ensemble: tile configuration does not fit an SM");
+  if (E->ctas_per_sm > 0 && E->ctas_per_sm < per_sm) per_sm = E->ctas_per_sm;
+  k_ensemble<<<per_sm * E->num_sms, E->threads, E->smem, s>>>(a);
+  VLP4D_LAUNCH_CHECK();
+  return VLP4D_OK;
+}
+
+void ens_free(vlp4d_ensemble *E) {
+  if (!E) return;
+  if (E->graph) cudaGraphExecDestroy(E->graph);
+  cudaFree(E->runs);
+  cudaFree(E->F[0]);
+  cudaFree(E->F[1]);
+  cudaFree(E->part);
+  cudaFree(E->fld);
+  cudaFree(E->nrj);
+  cudaFree(E->word);
+  cudaFree(E->done);
+  cudaFree(E->remaining);
+  delete E;
+}
+
+int ens_check(vlp4d_ensemble *E) {
+  int h = 0;
+  VLP4D_CUDA_TRY(cudaMemcpy(&h, E->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) return fail_msg(VLP4D_ERR_TIMEOUT, "ensemble: a CTA found no work for its whole time limit");
+  return VLP4D_OK;
+}
+
+}  // namespace
+}  // namespace vlp4d
+
+using namespace vlp4d;
+
+extern "C" {
+
+int vlp4d_ensemble_create(const vlp4d_ens_member *members, int nruns, int nsteps, vlp4d_ensemble **out) {
+  if (!out) return fail_msg(VLP4D_ERR_INVALID_ARG, "out is NULL");
+  *out = nullptr;
+  if (!members || nruns < 1) return fail_msg(VLP4D_ERR_INVALID_ARG, "no members");
+  if (nsteps < 0 || nsteps > (1 << 28)) return fail_msg(VLP4D_ERR_INVALID_ARG, "nsteps out of range");
+  int dev = 0, nd = 0;
+  if (cudaGetDeviceCount(&nd) != cudaSuccess || nd < 1) {
+    cudaGetLastError();
+    return fail_msg(VLP4D_ERR_NO_DEVICE, "no CUDA device");
+  }
+  VLP4D_CUDA_TRY(cudaGetDevice(&dev));
+  vlp4d_ensemble *E = new vlp4d_ensemble();
+  E->device = dev;
+  VLP4D_CUDA_TRY(cudaDeviceGetAttribute(&E->num_sms, cudaDevAttrMultiProcessorCount, dev));
+  E->nruns = nruns;
+  E->nsteps = nsteps;
+  long long foff = 0, poff = 0, eoff = 0, doff = 0;
+  for (int r = 0; r < nruns; ++r) {
+    const vlp4d_ens_member &m = members[r];
+    EnsRun R;
+    for (int i = 0; i < 4; ++i) {
+      if (m.n[i] < 1 || !(m.max_phy[i] > m.min_phy[i])) {
+        ens_free(E);
+        return fail_msg(VLP4D_ERR_INVALID_ARG, "ensemble member " + std::to_string(r) + ": bad extent or box");
+      }
+      R.n[i] = m.n[i];
+      R.minp[i] = m.min_phy[i];
+      R.maxp[i] = m.max_phy[i];
+      R.dx[i] = (m.max_phy[i] - m.min_phy[i]) / m.n[i];
+    }
+    if (R.n[0] > kEnsMaxN || R.n[1] > kEnsMaxN || R.n[2] > kEnsMaxN) {
+      ens_free(E);
+      return fail_msg(VLP4D_ERR_UNSUPPORTED, "ensemble member " + std::to_string(r) + ": nx, ny, nvx must be at most 64");
+    }
+    if (!std::isfinite(m.dt)) {
+      ens_free(E);
+      return fail_msg(VLP4D_ERR_INVALID_ARG, "ensemble member " + std::to_string(r) + ": dt is not finite");
+    }
+    R.dt = m.dt;
+    R.amp = m.amp;
+    R.k = m.k;
+    const long long nxy = (long long)R.n[0] * R.n[1];
+    const long long cells = nxy * R.n[2] * R.n[3];
+    R.f_off = foff;
+    foff += (cells + 63) / 64 * 64;
+    R.p_off = poff;
+    poff += nxy * R.n[3];
+    R.e_off = eoff;
+    eoff += 2 * nxy;
+    R.d_off = doff;
+    doff += nsteps + 1;
+    E->total_cells += cells;
+    if (cells > E->max_cells) E->max_cells = cells;
+    if (nxy > E->maxnxy) E->maxnxy = (int)nxy;
+    E->host_runs.push_back(R);
+  }
+  E->smem = ens_smem(E->maxnxy);
+  bool ok = cudaMalloc(&E->runs, sizeof(EnsRun) * nruns) == cudaSuccess &&
+            cudaMalloc(&E->F[0], sizeof(float) * foff) == cudaSuccess &&
+            cudaMalloc(&E->F[1], sizeof(float) * foff) == cudaSuccess &&
+            cudaMalloc(&E->part, sizeof(double) * poff) == cudaSuccess &&
+            cudaMalloc(&E->fld, sizeof(double) * eoff) == cudaSuccess &&
+            cudaMalloc(&E->nrj, sizeof(double) * doff) == cudaSuccess &&
+            cudaMalloc(&E->word, sizeof(unsigned long long) * nruns) == cudaSuccess &&
+            cudaMalloc(&E->done, sizeof(unsigned int) * nruns) == cudaSuccess &&
+            cudaMalloc(&E->remaining, sizeof(int) * 2) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    ens_free(E);
+    return fail_msg(VLP4D_ERR_CUDA, "cudaMalloc failed in vlp4d_ensemble_create");
+  }
+  E->err = E->remaining + 1;
+  if (cudaMemcpy(E->runs, E->host_runs.data(), sizeof(EnsRun) * nruns, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemset(E->F[1], 0, sizeof(float) * foff) != cudaSuccess ||
+      cudaMemset(E->remaining, 0, sizeof(int) * 2) != cudaSuccess) {
+    cudaGetLastError();
+    ens_free(E);
+    return fail_msg(VLP4D_ERR_CUDA, "ensemble upload failed");
+  }
+  *out = E;
+  return VLP4D_OK;
+}
+
+int vlp4d_ensemble_destroy(vlp4d_ensemble *ens) {
+  if (!ens) return VLP4D_OK;
+  cudaSetDevice(ens->device);
+  cudaDeviceSynchronize();
+  ens_free(ens);
+  return VLP4D_OK;
+}
+
+int vlp4d_ensemble_set_tiles(vlp4d_ensemble *ens, int threads, int cols_per_tile, int ctas_per_sm) {
+  if (!ens) return fail_msg(VLP4D_ERR_INVALID_ARG, "ens is NULL");
+  if (threads < 32 || threads > 512 || threads % 32) return fail_msg(VLP4D_ERR_INVALID_ARG, "threads: a multiple of 32 in [32, 512]");
+  if (cols_per_tile < 1 || cols_per_tile > threads) return fail_msg(VLP4D_ERR_INVALID_ARG, "cols_per_tile: in [1, threads]");
+  if (ctas_per_sm < 0 || ctas_per_sm > 32) return fail_msg(VLP4D_ERR_INVALID_ARG, "ctas_per_sm: in [0, 32]");
+  ens->threads = threads;
+  ens->cc = cols_per_tile;
+  ens->ctas_per_sm = ctas_per_sm;
+  if (ens->graph) {
+    cudaGraphExecDestroy(ens->graph);
+    ens->graph = nullptr;
+  }
+  return VLP4D_OK;
+}
+
+int vlp4d_ensemble_get_tiles(const vlp4d_ensemble *ens, int *threads, int *cols_per_tile, int *ctas_per_sm) {
+  if (!ens) return fail_msg(VLP4D_ERR_INVALID_ARG, "ens is NULL");
+  if (threads) *threads = ens->threads;
+  if (cols_per_tile) *cols_per_tile = ens->cc;
+  if (ctas_per_sm) *ctas_per_sm = ens->ctas_per_sm;
+  return VLP4D_OK;
+}
+
+int vlp4d_ensemble_run(vlp4d_ensemble *ens, void *stream) {
+  if (!ens) return fail_msg(VLP4D_ERR_INVALID_ARG, "ens is NULL");
+  vlp4d_ensemble *E = ens;
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc;
+  if (!E->graph) {
+    // Capture on a private stream (the legacy stream cannot be captured).
+    cudaStream_t cs;
+    VLP4D_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+      cudaGetLastError();
+      cudaStreamDestroy(cs);
+      return fail_msg(VLP4D_ERR_CUDA, "ensemble: stream capture failed");
+    }
+    rc = ens_launch(E, E->nsteps, cs);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(cs, &g);
+    cudaStreamDestroy(cs);
+    if (rc || e != cudaSuccess || !g) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      return rc ? rc : fail_msg(VLP4D_ERR_CUDA, "ensemble: stream capture failed");
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&E->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+      cudaGetLastError();
+      E->graph = nullptr;
+      return fail_msg(VLP4D_ERR_CUDA, std::string("ensemble: cudaGraphInstantiate: ") + cudaGetErrorString(ie));
+    }
+  }
+  VLP4D_CUDA_TRY(cudaGraphLaunch(E->graph, s));
+  return VLP4D_OK;
+}
+
+int vlp4d_ensemble_check(vlp4d_ensemble *ens) {
+  if (!ens) return fail_msg(VLP4D_ERR_INVALID_ARG, "ens is NULL");
+  VLP4D_CUDA_TRY(cudaDeviceSynchronize());
+  return ens_check(ens);
+}
+
+int vlp4d_ensemble_read(vlp4d_ensemble *ens, int run, void *f_out, double *nrj, void *stream) {
+  if (!ens) return fail_msg(VLP4D_ERR_INVALID_ARG, "ens is NULL");
+  if (run < 0 || run >= ens->nruns) return fail_msg(VLP4D_ERR_INVALID_ARG, "run index out of range");
+  const EnsRun &R = ens->host_runs[run];
+  cudaStream_t s = (cudaStream_t)stream;
+  const long long cells = (long long)R.n[0] * R.n[1] * R.n[2] * R.n[3];
+  if (f_out)
+    VLP4D_CUDA_TRY(cudaMemcpyAsync(f_out, ens->F[ens->nsteps & 1] + R.f_off, sizeof(float) * cells,
+                                   cudaMemcpyDeviceToDevice, s));
+  if (nrj) {
+    VLP4D_CUDA_TRY(cudaMemcpyAsync(nrj, ens->nrj + R.d_off, sizeof(double) * (ens->nsteps + 1),
+                                   cudaMemcpyDeviceToHost, s));
+    VLP4D_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  return VLP4D_OK;
+}
+
+long long vlp4d_ensemble_cells(const vlp4d_ensemble *ens) { return ens ? ens->total_cells : 0; }
+
+// Scans thread counts {128, 256, 512}, columns per v tile {8, 16, 32, 64}
+// and CTAs per SM {1, 2, 3, 4} (those that fit), timing `steps` steps of
+// the ensemble for each (CUDA events, best of two), appends one CSV line per
+// configuration to csv_path (when not NULL) and keeps the fastest.
+int vlp4d_ensemble_autotune(vlp4d_ensemble *ens, int steps, const char *csv_path, void *stream) {
+  if (!ens) return fail_msg(VLP4D_ERR_INVALID_ARG, "ens is NULL");
+  if (steps < 1 || steps > ens->nsteps) steps = ens->nsteps > 0 ? ens->nsteps : 1;
+  vlp4d_ensemble *E = ens;
+  cudaStream_t s = (cudaStream_t)stream;
+  FILE *csv = csv_path ? fopen(csv_path, "w") : nullptr;
+  if (csv_path && !csv) return fail_msg(VLP4D_ERR_IO, std::string("cannot write ") + csv_path);
+  if (csv) fprintf(csv, "threads,cols_per_tile,ctas_per_sm,steps,ms\n");
+  cudaEvent_t e0, e1;
+  VLP4D_CUDA_TRY(cudaEventCreate(&e0));
+  VLP4D_CUDA_TRY(cudaEventCreate(&e1));
+  const int th_list[3] = {128, 256, 512}, cc_list[4] = {8, 16, 32, 64}, cps_list[4] = {1, 2, 3, 4};
+  float best = 1e30f;
+  int bt = E->threads, bc = E->cc, bp = E->ctas_per_sm;
+  int rc = VLP4D_OK;
+  VLP4D_CUDA_TRY(cudaFuncSetAttribute(k_ensemble, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)E->smem));
+  for (int th : th_list)
+    for (int cc : cc_list) {
+      if (cc > th) continue;
+      for (int cps : cps_list) {
+        int fit = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k_ensemble, th, E->smem) != cudaSuccess) {
+          cudaGetLastError();
+          continue;
+        }
+        if (cps > fit) continue;
+        E->threads = th;
+        E->cc = cc;
+        E->ctas_per_sm = cps;
+        float ms = 1e30f;
+        for (int rep = 0; rep < 2 && rc == VLP4D_OK; ++rep) {
+          cudaEventRecord(e0, s);
+          rc = ens_launch(E, steps, s);
+          cudaEventRecord(e1, s);
+          if (cudaEventSynchronize(e1) != cudaSuccess) rc = fail_msg(VLP4D_ERR_CUDA, "ensemble autotune: launch failed");
+          float t = 0.f;
+          cudaEventElapsedTime(&t, e0, e1);
+          if (t < ms) ms = t;
+        }
+        if (rc == VLP4D_OK) rc = ens_check(E);
+        if (rc) break;
+        if (csv) fprintf(csv, "%d,%d,%d,%d,%.4f\n", th, cc, cps, steps, ms);
+        if (ms < best) {
+          best = ms;
+          bt = th;
+          bc = cc;
+          bp = cps;
+        }
+      }
+      if (rc) break;
+    }
+  if (csv) fclose(csv);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  E->threads = bt;
+  E->cc = bc;
+  E->ctas_per_sm = bp;
+  if (E->graph) {
+    cudaGraphExecDestroy(E->graph);
+    E->graph = nullptr;
+  }
+  return rc;
+}
+
+}  // extern "C"

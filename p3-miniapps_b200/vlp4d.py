@@ -35,6 +35,9 @@ EXPORTS = (
     "vlp4d_field_rho_noalloc", "vlp4d_steps", "vlp4d_advect_xyxy",
     "vlp4d_adjoint_create", "vlp4d_adjoint_destroy", "vlp4d_adjoint_forward", "vlp4d_adjoint_backward",
     "vlp4d_step_adjoint", "vlp4d_energy_grad",
+    "vlp4d_ensemble_create", "vlp4d_ensemble_destroy", "vlp4d_ensemble_run", "vlp4d_ensemble_check",
+    "vlp4d_ensemble_read", "vlp4d_ensemble_cells", "vlp4d_ensemble_set_tiles", "vlp4d_ensemble_get_tiles",
+    "vlp4d_ensemble_autotune",
 )
 
 
@@ -54,6 +57,17 @@ class CDomain(C.Structure):
         ("ifreq", C.c_int32),
         ("idcase", C.c_int32),
         ("fxvx", C.c_int32),
+    ]
+
+
+class CEnsMember(C.Structure):
+    _fields_ = [
+        ("n", C.c_int32 * 4),
+        ("min_phy", C.c_double * 4),
+        ("max_phy", C.c_double * 4),
+        ("dt", C.c_double),
+        ("amp", C.c_double),
+        ("k", C.c_double),
     ]
 
 
@@ -103,9 +117,19 @@ def lib() -> C.CDLL:
         L.vlp4d_adjoint_backward.argtypes = [vp, vp, vp]
         L.vlp4d_step_adjoint.argtypes = [vp, vp, vp, vp, vp]
         L.vlp4d_energy_grad.argtypes = [vp, vp, C.POINTER(d), vp, vp]
+        L.vlp4d_ensemble_create.argtypes = [C.POINTER(CEnsMember), i, i, C.POINTER(vp)]
+        L.vlp4d_ensemble_destroy.argtypes = [vp]
+        L.vlp4d_ensemble_run.argtypes = [vp, vp]
+        L.vlp4d_ensemble_check.argtypes = [vp]
+        L.vlp4d_ensemble_read.argtypes = [vp, i, vp, dp, vp]
+        L.vlp4d_ensemble_cells.argtypes = [vp]
+        L.vlp4d_ensemble_set_tiles.argtypes = [vp, i, i, i]
+        L.vlp4d_ensemble_get_tiles.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
+        L.vlp4d_ensemble_autotune.argtypes = [vp, i, C.c_char_p, vp]
         for n in EXPORTS:
-            if n not in ("vlp4d_last_error", "vlp4d_kernel_launches"):
+            if n not in ("vlp4d_last_error", "vlp4d_kernel_launches", "vlp4d_ensemble_cells"):
                 getattr(L, n).restype = C.c_int
+        L.vlp4d_ensemble_cells.restype = C.c_longlong
         L.vlp4d_kernel_launches.restype = C.c_ulonglong
         _lib = L
     return _lib
@@ -408,3 +432,107 @@ def energy_after_steps(f0, adjoint: Adjoint):
             return g * gJ.to(g.dtype)
 
     return _EnergyAfterSteps.apply(f0)
+
+
+@dataclass
+class EnsembleMember:
+    """One member of a batched ensemble: grid, box, dt and the Landau initial
+    condition f0 = M(vx) M(vy) (1 + amp (cos k x + cos k y))."""
+
+    n: Sequence[int]
+    min_phy: Sequence[float]
+    max_phy: Sequence[float]
+    dt: float
+    amp: float
+    k: float
+
+    def domain(self, nbiter: int, idcase: int = 110) -> Domain:
+        return Domain(list(self.n), list(self.min_phy), list(self.max_phy), self.dt, nbiter, idcase)
+
+
+class Ensemble:
+    """vlp4d_ensemble_*: members advanced together in one persistent launch."""
+
+    def __init__(self, members: Sequence[EnsembleMember], nsteps: int):
+        self.members = list(members)
+        self.nsteps = int(nsteps)
+        arr = (CEnsMember * len(self.members))()
+        for i, m in enumerate(self.members):
+            for k in range(4):
+                arr[i].n[k] = int(m.n[k])
+                arr[i].min_phy[k] = float(m.min_phy[k])
+                arr[i].max_phy[k] = float(m.max_phy[k])
+            arr[i].dt, arr[i].amp, arr[i].k = float(m.dt), float(m.amp), float(m.k)
+        self.h = C.c_void_p()
+        _check(lib().vlp4d_ensemble_create(arr, len(self.members), self.nsteps, C.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            lib().vlp4d_ensemble_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+        return False
+
+    @property
+    def cells(self) -> int:
+        return int(lib().vlp4d_ensemble_cells(self.h))
+
+    def run(self, stream=None):
+        _check(lib().vlp4d_ensemble_run(self.h, _stream_ptr(stream)))
+
+    def check(self):
+        _check(lib().vlp4d_ensemble_check(self.h))
+
+    def read(self, i: int, stream=None):
+        """(final f of member i as a float32 CUDA tensor (nvy, nvx, ny, nx), energy history)."""
+        import numpy as np
+        import torch
+
+        m = self.members[i]
+        f = torch.empty((m.n[3], m.n[2], m.n[1], m.n[0]), dtype=torch.float32, device="cuda")
+        nrj = np.zeros(self.nsteps + 1)
+        _check(lib().vlp4d_ensemble_read(self.h, int(i), C.c_void_p(f.data_ptr()),
+                                         nrj.ctypes.data_as(C.POINTER(C.c_double)), _stream_ptr(stream)))
+        return f, nrj
+
+    def set_tiles(self, threads: int, cols_per_tile: int, ctas_per_sm: int = 0):
+        _check(lib().vlp4d_ensemble_set_tiles(self.h, threads, cols_per_tile, ctas_per_sm))
+
+    def tiles(self):
+        t, c, p = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().vlp4d_ensemble_get_tiles(self.h, C.byref(t), C.byref(c), C.byref(p)))
+        return t.value, c.value, p.value
+
+    def autotune(self, steps: int, csv_path: Optional[str] = None, stream=None):
+        _check(lib().vlp4d_ensemble_autotune(self.h, int(steps), csv_path.encode() if csv_path else None,
+                                             _stream_ptr(stream)))
+        return self.tiles()
+
+
+def landau_ensemble_members(nruns=256, sizes=(16, 24, 32, 48), seed=20261203, dt=0.1, vmax=6.0,
+                            ks=(0.3, 0.5), amp_range=(0.01, 0.1)):
+    """The batched-ensemble configuration: per member, N per dimension drawn
+    independently from `sizes`, amp ~ U(amp_range), k from `ks`, box
+    x, y in [0, 2 pi / k), v in [-vmax, vmax) (seeded)."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(nruns):
+        n = [int(v) for v in rng.choice(sizes, size=4)]
+        k = float(rng.choice(ks))
+        amp = float(rng.uniform(*amp_range))
+        L = 2 * math.pi / k
+        out.append(EnsembleMember(n, [0.0, 0.0, -vmax, -vmax], [L, L, vmax, vmax], dt, amp, k))
+    return out

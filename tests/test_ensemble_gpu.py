@@ -1,0 +1,106 @@
+"""Batched ensemble (vlp4d_ensemble_*): members of uneven grids advanced in
+one persistent launch, against the single-run path member by member;
+replays of the captured graph; the autotuner; the batched-ensemble
+configuration (256 members, N per dimension from {16, 24, 32, 48}, 50 steps)."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _single_run(pkg, torch, m, nsteps):
+    """The same member through a Context (FP32 f) and vlp4d_steps."""
+    v = pkg.vlp4d
+    dom = m.domain(nsteps + 1)
+    with pkg.Context(dom, "f32") as ctx:
+        a, b = ctx.empty_f(), ctx.empty_f()
+        ctx.init_case(a, v.IC_LANDAU_SUM, m.amp, m.k)
+        ctx.field_rho(a)
+        ctx.field_poisson()
+        ctx.diags_compute(0)
+        if nsteps:
+            ctx.steps(a, b, 1, nsteps)
+        else:
+            b.copy_(a)
+        nrj, _ = ctx.diags_read(nsteps + 1)
+        return b.clone(), nrj
+
+
+def _members(pkg, dims, nsteps_dt=0.1):
+    out = []
+    for i, n in enumerate(dims):
+        k = 0.5 if i % 2 == 0 else 0.3
+        L = 2 * math.pi / k
+        out.append(pkg.EnsembleMember(list(n), [0, 0, -6, -6], [L, L, 6, 6], nsteps_dt, 0.02 + 0.01 * i, k))
+    return out
+
+
+DIMS = [(16, 24, 32, 16), (24, 16, 16, 32), (32, 32, 24, 24), (16, 16, 16, 16), (48, 24, 16, 24),
+        (24, 48, 48, 16), (8, 12, 20, 10), (40, 16, 24, 36)]
+
+
+def test_members_match_single_runs(pkg, cuda):
+    torch = cuda
+    nsteps = 6
+    members = _members(pkg, DIMS)
+    with pkg.Ensemble(members, nsteps) as ens:
+        ens.run()
+        ens.check()
+        for i, m in enumerate(members):
+            f, nrj = ens.read(i)
+            f_ref, nrj_ref = _single_run(pkg, torch, m, nsteps)
+            scale = float(f_ref.abs().max())
+            assert float((f - f_ref).abs().max()) <= 2e-6 * scale, i
+            assert np.abs(nrj - nrj_ref).max() < 1e-6, (i, nrj, nrj_ref)
+
+
+def test_graph_replays_are_bit_identical(pkg, cuda):
+    torch = cuda
+    members = _members(pkg, DIMS[:5])
+    with pkg.Ensemble(members, 4) as ens:
+        ens.run()
+        ens.check()
+        first = [ens.read(i) for i in range(len(members))]
+        ens.set_tiles(128, 16, 1)  # another schedule: a different tile order
+        ens.run()
+        ens.run()
+        ens.check()
+        for i in range(len(members)):
+            f, nrj = ens.read(i)
+            assert torch.equal(f, first[i][0])
+            assert np.array_equal(nrj, first[i][1])
+
+
+def test_autotuner_writes_csv_and_keeps_best(pkg, cuda, tmp_path):
+    members = _members(pkg, DIMS)
+    csv = tmp_path / "tiles.csv"
+    with pkg.Ensemble(members, 3) as ens:
+        best = ens.autotune(2, str(csv))
+        rows = [line.split(",") for line in csv.read_text().splitlines()[1:]]
+        assert len(rows) >= 12
+        times = {(int(r[0]), int(r[1]), int(r[2])): float(r[4]) for r in rows}
+        assert best in times and times[best] == min(times.values())
+        ens.run()
+        ens.check()
+
+
+def test_batched_ensemble_configuration(pkg, cuda):
+    """256 members, N per dimension from {16, 24, 32, 48}, amp ~ U[0.01, 0.1],
+    k in {0.3, 0.5}, 50 steps of dt 0.1, FP32 f, one persistent launch."""
+    torch = cuda
+    nsteps = 50
+    members = pkg.landau_ensemble_members(256)
+    with pkg.Ensemble(members, nsteps) as ens:
+        ens.run()
+        ens.check()
+        rng = np.random.default_rng(3)
+        for i in rng.choice(len(members), 3, replace=False):
+            f, nrj = ens.read(int(i))
+            assert bool(torch.isfinite(f).all())
+            f_ref, nrj_ref = _single_run(pkg, torch, members[int(i)], nsteps)
+            assert float((f - f_ref).abs().max()) <= 1e-5 * float(f_ref.abs().max())
+            assert np.abs(nrj - nrj_ref).max() < 1e-5
