@@ -43,6 +43,7 @@
 
 #include "internal.cuh"
 #include "stencil.cuh"
+#include "tma.cuh"
 
 namespace vlp4d {
 namespace {
@@ -96,39 +97,85 @@ __device__ __forceinline__ EnsLine ens_line(double disp, double hmin, double hma
   return l;
 }
 
+// 16-byte asynchronous global-to-shared copies (L2 only), in commit groups.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 // Moment of f0 (stage 0) or x/y half step (+ moment) of the vy row `ivy`.
-// Shared memory: two plane buffers (floats), x lines (nvx), the moment (FP64).
+// The row's nvx planes are contiguous; they are processed in groups of P
+// planes (P * nx*ny <= maxnxy cells) so that small planes share the loads
+// and barriers.  Shared memory: the moment (FP64, one per cell), the loaded
+// group, its x-swept copy, the x lines of the row.  The thread that owns
+// cell q of a plane owns it in every plane of the row, so the moment adds
+// the planes in ivx order whatever the block size.
 template <bool SWEEP, bool MOMENT>
 __device__ void ens_planes(const EnsArgs &a, const EnsRun &R, const float *fin, float *fout, int ivy,
                            unsigned char *smem) {
   const int nx = R.n[0], ny = R.n[1], nvx = R.n[2];
   const int nxy = nx * ny;
-  // Layout: acc (maxnxy doubles) | b0, b1 (maxnxy floats each) | x lines.
+  // Layout: acc (maxnxy doubles) | two load buffers | x-swept buffer | x lines.
   double *acc = reinterpret_cast<double *>(smem);
-  float *b0 = reinterpret_cast<float *>(acc + a.maxnxy);
-  float *b1 = b0 + a.maxnxy;
+  float *bin[2] = {reinterpret_cast<float *>(acc + a.maxnxy), reinterpret_cast<float *>(acc + a.maxnxy) + a.maxnxy};
+  float *b1 = bin[1] + a.maxnxy;
   EnsLine *xl = reinterpret_cast<EnsLine *>(b1 + a.maxnxy);
   __shared__ EnsLine yl;
   const double hdt = 0.5 * R.dt;
+  int P = a.maxnxy / nxy;
+  P = P < 1 ? 1 : (P > nvx ? nvx : P);
   if (SWEEP) {
     for (int l = threadIdx.x; l < nvx; l += blockDim.x)
       xl[l] = ens_line(hdt * (R.minp[2] + l * R.dx[2]), R.minp[0], R.maxp[0], nx);
     if (threadIdx.x == 0) yl = ens_line(hdt * (R.minp[3] + ivy * R.dx[3]), R.minp[1], R.maxp[1], ny);
   }
   if (MOMENT)
-    for (int c = threadIdx.x; c < nxy; c += blockDim.x) acc[c] = 0.;
+    for (int q = threadIdx.x; q < nxy; q += blockDim.x) acc[q] = 0.;
   __syncthreads();
-  for (int ivx = 0; ivx < nvx; ++ivx) {
-    const long long base = R.f_off + ((long long)ivy * nvx + ivx) * nxy;
+  const long long row0 = R.f_off + (long long)ivy * nvx * nxy;
+  const bool vec = (nxy & 3) == 0;  // f_off is a multiple of 64 elements
+  // Group p0's copies into bin[buf]: asynchronous (vec) or plain loads.
+  auto load_group = [&](int p0, int buf) {
+    const int np = nvx - p0 < P ? nvx - p0 : P;
+    const long long gbase = row0 + (long long)p0 * nxy;
+    if (vec) {
+      const float4 *src = reinterpret_cast<const float4 *>(fin + gbase);
+      float4 *dst = reinterpret_cast<float4 *>(bin[buf]);
+      for (int c = threadIdx.x; c < np * nxy / 4; c += blockDim.x) cp_async16(dst + c, src + c);
+    } else {
+      for (int c = threadIdx.x; c < np * nxy; c += blockDim.x) bin[buf][c] = __ldcg(fin + gbase + c);
+    }
+    cp_async_commit();
+  };
+  if (SWEEP) load_group(0, 0);
+  int buf = 0;
+  for (int p0 = 0; p0 < nvx; p0 += P, buf ^= 1) {
+    const int np = nvx - p0 < P ? nvx - p0 : P;
+    const int cells = np * nxy;
+    const long long gbase = row0 + (long long)p0 * nxy;
     if (!SWEEP) {
-      for (int c = threadIdx.x; c < nxy; c += blockDim.x) acc[c] += (double)__ldcg(fin + base + c);
+      for (int q = threadIdx.x; q < nxy; q += blockDim.x) {
+        double s = acc[q];
+        for (int p = 0; p < np; ++p) s += (double)__ldcg(fin + gbase + (long long)p * nxy + q);
+        acc[q] = s;
+      }
       continue;
     }
-    for (int c = threadIdx.x; c < nxy; c += blockDim.x) b0[c] = __ldcg(fin + base + c);
+    // Next group in flight while this one is swept.
+    if (p0 + P < nvx) {
+      load_group(p0 + P, buf ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
     __syncthreads();
-    const EnsLine lx = xl[ivx];
-    for (int c = threadIdx.x; c < nxy; c += blockDim.x) {
-      const int ix = c % nx, row = c - ix;
+    const float *b0 = bin[buf];
+    for (int c = threadIdx.x; c < cells; c += blockDim.x) {
+      const int p = c / nxy, qc = c - p * nxy;
+      const int ix = qc % nx, row = c - ix;
+      const EnsLine &lx = xl[p0 + p];
       int j = ix + lx.m;
       j = j >= nx ? j - nx : j;
       float t[6];
@@ -141,33 +188,41 @@ __device__ void ens_planes(const EnsArgs &a, const EnsRun &R, const float *fin, 
     }
     __syncthreads();
     const EnsLine ly = yl;
-    for (int c = threadIdx.x; c < nxy; c += blockDim.x) {
-      const int ix = c % nx, iy = c / nx;
-      int j = iy + ly.m;
-      j = j >= ny ? j - ny : j;
-      float t[6];
+    for (int q = threadIdx.x; q < nxy; q += blockDim.x) {
+      const int ix = q % nx, iy = q / nx;
+      int j0 = iy + ly.m;
+      j0 = j0 >= ny ? j0 - ny : j0;
+      double s = MOMENT ? acc[q] : 0.;
+      for (int p = 0; p < np; ++p) {
+        const float *pl = b1 + p * nxy + ix;
+        int j = j0;
+        float t[6];
 #pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        t[k] = b1[j * nx + ix];
-        if (++j == ny) j = 0;
+        for (int k = 0; k < 6; ++k) {
+          t[k] = pl[j * nx];
+          if (++j == ny) j = 0;
+        }
+        const float o = interp6(ly.v, t[0], t[1], t[2], t[3], t[4], t[5]);
+        fout[gbase + (long long)p * nxy + q] = o;
+        if (MOMENT) s += (double)o;
       }
-      const float o = interp6(ly.v, t[0], t[1], t[2], t[3], t[4], t[5]);
-      fout[base + c] = o;
-      if (MOMENT) acc[c] += (double)o;
+      if (MOMENT) acc[q] = s;
     }
     __syncthreads();
   }
   if (MOMENT) {
     __syncthreads();
-    double *p = a.part + R.p_off + (long long)ivy * nxy;
-    for (int c = threadIdx.x; c < nxy; c += blockDim.x) p[c] = acc[c];
+    double *pp = a.part + R.p_off + (long long)ivy * nxy;
+    for (int q = threadIdx.x; q < nxy; q += blockDim.x) pp[q] = acc[q];
   }
 }
 
 // vx then vy (dt) of the columns [tile*cc, tile*cc + cc).  Thread (col, g)
-// handles output vx rows g, g+G, ...; for each it streams the vy rows from
-// the column's vy offset, keeping six vx-swept values in a ring.
+// handles the groups of V consecutive output vx rows g, g+G, ...; for each
+// group it streams the vy rows from the column's vy offset (V+5 vx taps per
+// row, shared by the V outputs), keeping six vx-swept rows in a ring.
 __device__ void ens_vxvy(const EnsArgs &a, const EnsRun &R, const float *fin, float *fout, int tile) {
+  constexpr int V = 4;
   const int nx = R.n[0], ny = R.n[1], nvx = R.n[2], nvy = R.n[3];
   const int nxy = nx * ny;
   const int cc = a.cc;
@@ -181,34 +236,48 @@ __device__ void ens_vxvy(const EnsArgs &a, const EnsRun &R, const float *fin, fl
   const long long vstride = nxy, ystride = (long long)nxy * nvx;
   const float *src = fin + R.f_off + col;
   float *dst = fout + R.f_off + col;
-  for (int ivx = g; ivx < nvx; ivx += G) {
-    int toff[6];
-    int j = ivx + lx.m;
-    j = j >= nvx ? j - nvx : j;
+  for (int v0 = g * V; v0 < nvx; v0 += G * V) {
+    long long toff[V + 5];
+    int j = v0 + lx.m;
+    while (j >= nvx) j -= nvx;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      toff[k] = j;
+    for (int k = 0; k < V + 5; ++k) {
+      toff[k] = (long long)j * vstride;
       if (++j == nvx) j = 0;
     }
-    float ring[6];
+    float ring[6][V];
     int row = ly.m;
     const int nrows = nvy + 5;
+    // Row r's taps are loaded one row ahead (tn) so their latency overlaps
+    // the arithmetic of the row before.
+    float t[V + 5];
+#pragma unroll
+    for (int k = 0; k < V + 5; ++k) t[k] = __ldcg(src + (long long)row * ystride + toff[k]);
     for (int r0 = 0; r0 < nrows; r0 += 6) {
 #pragma unroll
       for (int u = 0; u < 6; ++u) {
         const int r = r0 + u;
         if (r >= nrows) break;
-        const float *p = src + (long long)row * ystride;
-        float t[6];
-#pragma unroll
-        for (int k = 0; k < 6; ++k) t[k] = __ldcg(p + (long long)toff[k] * vstride);
-        ring[u] = interp6(lx.v, t[0], t[1], t[2], t[3], t[4], t[5]);
         if (++row == nvy) row = 0;
+        float tn[V + 5];
+        if (r + 1 < nrows) {
+          const float *pn = src + (long long)row * ystride;
+#pragma unroll
+          for (int k = 0; k < V + 5; ++k) tn[k] = __ldcg(pn + toff[k]);
+        }
+#pragma unroll
+        for (int i = 0; i < V; ++i) ring[u][i] = interp6(lx.v, t[i], t[i + 1], t[i + 2], t[i + 3], t[i + 4], t[i + 5]);
+#pragma unroll
+        for (int k = 0; k < V + 5; ++k) t[k] = tn[k];
         if (r >= 5) {
-          const int ivy = r - 5;
-          dst[(long long)ivy * ystride + (long long)ivx * vstride] =
-              interp6(ly.v, ring[(u + 1) % 6], ring[(u + 2) % 6], ring[(u + 3) % 6], ring[(u + 4) % 6],
-                      ring[(u + 5) % 6], ring[u]);
+          float *orow = dst + (long long)(r - 5) * ystride;
+#pragma unroll
+          for (int i = 0; i < V; ++i) {
+            if (v0 + i < nvx)
+              orow[(long long)(v0 + i) * vstride] =
+                  interp6(ly.v, ring[(u + 1) % 6][i], ring[(u + 2) % 6][i], ring[(u + 3) % 6][i],
+                          ring[(u + 4) % 6][i], ring[(u + 5) % 6][i], ring[u][i]);
+          }
         }
       }
     }
@@ -330,47 +399,69 @@ __global__ void __launch_bounds__(512) k_ensemble(EnsArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_run, s_stage, s_tile;
   const int total_stages = 2 + 4 * a.nsteps;
-  // Scheduler state, kept by thread 0 only.
+  // Scheduler state, kept (identically) by the lanes of warp 0.
   int r = (int)((blockIdx.x * 7919LL) % a.nruns);
   long long idle_start = clock64();
-  int misses = 0;
+  const int lane = threadIdx.x & 31;
   while (true) {
-    if (threadIdx.x == 0) {
-      // -1: leave (all members done, or no work for idle_limit cycles);
-      // -2: nothing taken this round; >= 0: a tile of member s_run.
-      int got_run = -2;
-      if (*(volatile int *)a.remaining <= 0) {
+    if (threadIdx.x < 32) {
+      // Warp 0 looks for a tile: 32 members per round, starting at r (the
+      // member last worked on), one sweep over all members at most.
+      // got_run: -1 leave (all members done, or no work for idle_limit
+      // cycles); -2 nothing taken; >= 0 a tile of that member.
+      int got_run = -2, got_stage = 0, got_tile = 0;
+      const int rem = __shfl_sync(0xffffffffu, lane == 0 ? *(volatile int *)a.remaining : 0, 0);
+      if (rem <= 0) {
         got_run = -1;
       } else {
-        const EnsRun &R = a.runs[r];
-        const unsigned long long w = *(volatile unsigned long long *)(a.word + r);
-        const int stage = (int)(w >> 32);
-        if (stage < total_stages && (int)(w & 0xffffffffu) < stage_tiles(R, stage, a.cc)) {
-          const unsigned long long got = atomicAdd(a.word + r, 1ULL);
-          const int st = (int)(got >> 32), tl = (int)(got & 0xffffffffu);
-          if (st < total_stages && tl < stage_tiles(R, st, a.cc)) {
-            got_run = r;
-            s_stage = st;
-            s_tile = tl;
-            __threadfence();
+        const int rounds = (a.nruns + 31) / 32;
+        for (int rd = 0; rd < rounds && got_run == -2; ++rd) {
+          const int idx = rd * 32 + lane;
+          const int cand = (int)(((long long)r + idx) % a.nruns);
+          bool avail = false;
+          if (idx < a.nruns) {
+            const unsigned long long w = *(volatile unsigned long long *)(a.word + cand);
+            const int stage = (int)(w >> 32);
+            avail = stage < total_stages && (int)(w & 0xffffffffu) < stage_tiles(a.runs[cand], stage, a.cc);
+          }
+          unsigned ballot = __ballot_sync(0xffffffffu, avail);
+          while (ballot) {
+            const int leader = __ffs(ballot) - 1;
+            int ok = 0, st = 0, tl = 0;
+            if (lane == leader) {
+              const unsigned long long got = atomicAdd(a.word + cand, 1ULL);
+              st = (int)(got >> 32);
+              tl = (int)(got & 0xffffffffu);
+              ok = st < total_stages && tl < stage_tiles(a.runs[cand], st, a.cc);
+              if (ok) __threadfence();
+            }
+            ok = __shfl_sync(0xffffffffu, ok, leader);
+            if (ok) {
+              got_run = __shfl_sync(0xffffffffu, cand, leader);
+              got_stage = __shfl_sync(0xffffffffu, st, leader);
+              got_tile = __shfl_sync(0xffffffffu, tl, leader);
+              break;
+            }
+            ballot &= ballot - 1;
           }
         }
         if (got_run >= 0) {
+          r = got_run;
           idle_start = clock64();
-          misses = 0;
         } else {
-          r = r + 1 == a.nruns ? 0 : r + 1;
-          if (++misses >= a.nruns) {
-            misses = 0;
-            __nanosleep(512);
-            if (clock64() - idle_start > a.idle_limit) {
-              atomicExch(a.err, 1);
-              got_run = -1;
-            }
+          __nanosleep(256);
+          if (clock64() - idle_start > a.idle_limit) {
+            if (lane == 0) atomicExch(a.err, 1);
+            got_run = -1;
           }
+          got_run = __shfl_sync(0xffffffffu, got_run, 0);
         }
       }
-      s_run = got_run;
+      if (lane == 0) {
+        s_run = got_run;
+        s_stage = got_stage;
+        s_tile = got_tile;
+      }
     }
     __syncthreads();
     const int run = s_run;
@@ -465,7 +556,7 @@ namespace vlp4d {
 namespace {
 
 size_t ens_smem(int maxnxy) {
-  const size_t planes = sizeof(double) * maxnxy + 2 * sizeof(float) * maxnxy + sizeof(EnsLine) * kEnsMaxN;
+  const size_t planes = sizeof(double) * maxnxy + 3 * sizeof(float) * maxnxy + sizeof(EnsLine) * kEnsMaxN;
   const size_t field = 2 * sizeof(double2) * maxnxy + 2 * sizeof(double2) * kEnsMaxN;
   return ((planes > field ? planes : field) + 255) / 256 * 256;
 }
@@ -593,6 +684,7 @@ int vlp4d_ensemble_create(const vlp4d_ens_member *members, int nruns, int nsteps
     if (nxy > E->maxnxy) E->maxnxy = (int)nxy;
     E->host_runs.push_back(R);
   }
+  E->maxnxy = (E->maxnxy + 3) / 4 * 4;  // 16-byte aligned shared-memory buffers
   E->smem = ens_smem(E->maxnxy);
   bool ok = cudaMalloc(&E->runs, sizeof(EnsRun) * nruns) == cudaSuccess &&
             cudaMalloc(&E->F[0], sizeof(float) * foff) == cudaSuccess &&
