@@ -206,6 +206,17 @@ int vlp4d_field_rho_noalloc(const void *fn, int dtype, int nx, int ny, int nvx, 
  * elements of `elem_size` bytes (4, 8 or 16). */
 int vlp4d_transpose(const void *in, void *out, int rows, int cols, int elem_size, void *stream);
 
+/* Self-test of the bounded device waits (no reference counterpart).  The
+ * fused kernels wait for their asynchronous copies with a time limit and,
+ * when it runs out, record a timeout in the context's error word and
+ * return, so a lost copy becomes VLP4D_ERR_TIMEOUT from vlp4d_check instead
+ * of a hung GPU.  This launches one thread that waits, with the same
+ * primitive, on a barrier phase that nothing completes, for limit_cycles
+ * clock cycles (at most the fused kernels' own limit of 4e9); vlp4d_check
+ * then returns VLP4D_ERR_TIMEOUT and clears the word; the context stays
+ * usable. */
+int vlp4d_selftest_wait_timeout(vlp4d_ctx *ctx, long long limit_cycles, void *stream);
+
 /* ---- Reverse mode (discrete adjoint).  No reference counterpart: the
  * reference has no derivative code.  The adjoint is that of vlp4d_step as
  * computed here: transposed interpolation for the x/y shifts, transposed

@@ -8,6 +8,7 @@
 #include <atomic>
 
 #include "internal.cuh"
+#include "tma.cuh"
 
 namespace vlp4d {
 
@@ -593,6 +594,14 @@ int vlp4d_print_fxvx(vlp4d_ctx *ctx, const void *fn, const char *path) {
   fclose(f);
   free(h);
   return VLP4D_OK;
+}
+
+int vlp4d_selftest_wait_timeout(vlp4d_ctx *ctx, long long limit_cycles, void *stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (limit_cycles < 0 || limit_cycles > kWaitCycles)
+    return fail(VLP4D_ERR_INVALID_ARG, "limit_cycles outside [0, the fused kernels' own limit]");
+  return launch_wait_selftest(ctx, limit_cycles, as_stream(stream));
 }
 
 int vlp4d_transpose(const void *in, void *out, int rows, int cols, int elem_size, void *stream) {

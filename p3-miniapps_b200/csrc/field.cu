@@ -7,6 +7,7 @@
 // Diags::compute (diags.cpp:13-55), initcase (init.cpp:118-285),
 // Impl::Transpose (lib/Cuda_Transpose.hpp:18-136).
 #include "internal.cuh"
+#include "tma.cuh"
 
 namespace vlp4d {
 
@@ -284,6 +285,25 @@ int launch_transpose(const void *in, void *out, int rows, int cols, int elem, cu
   if (elem == 4) k_transpose<float><<<grid, block, 0, s>>>((const float *)in, (float *)out, rows, cols);
   else if (elem == 8) k_transpose<double><<<grid, block, 0, s>>>((const double *)in, (double *)out, rows, cols);
   else k_transpose<double2><<<grid, block, 0, s>>>((const double2 *)in, (double2 *)out, rows, cols);
+  VLP4D_LAUNCH_CHECK();
+  return VLP4D_OK;
+}
+
+// Self-test of the bounded waits: one thread waits on a barrier phase that
+// nothing completes (no arrival, no copy), gives up after `limit` cycles and
+// records the timeout in the context's error word, exactly as the fused
+// kernels do when a copy does not land.
+__global__ void k_wait_selftest(int *err, long long limit) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_fence_init();
+    if (!mbar_wait_limit(&bar, 0, limit)) atomicExch(err, 1);
+  }
+}
+
+int launch_wait_selftest(vlp4d_ctx *c, long long limit, cudaStream_t s) {
+  k_wait_selftest<<<1, 32, 0, s>>>(c->d_err, limit);
   VLP4D_LAUNCH_CHECK();
   return VLP4D_OK;
 }

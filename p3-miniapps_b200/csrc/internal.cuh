@@ -176,5 +176,6 @@ int launch_field_poisson(vlp4d_ctx *c, cudaStream_t s);
 int launch_diags(vlp4d_ctx *c, int iter, cudaStream_t s);
 int launch_init_case(vlp4d_ctx *c, void *f, int ic, double amp, double k, double u, cudaStream_t s);
 int launch_transpose(const void *in, void *out, int rows, int cols, int elem, cudaStream_t s);
+int launch_wait_selftest(vlp4d_ctx *c, long long limit, cudaStream_t s);
 
 }  // namespace vlp4d

@@ -45,14 +45,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
 }
 
 // Waits for the phase with the given parity to complete; false after
-// kWaitCycles without completion.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+// `limit` clock cycles without completion.
+__device__ __forceinline__ bool mbar_wait_limit(uint64_t *bar, uint32_t parity, long long limit) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity)) {
-    if (clock64() - t0 > kWaitCycles) return false;
+    if (clock64() - t0 > limit) return false;
   }
   return true;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+  return mbar_wait_limit(bar, parity, kWaitCycles);
 }
 
 // Contiguous global -> shared copy; both addresses 16-byte aligned, bytes a

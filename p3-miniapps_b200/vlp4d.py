@@ -37,7 +37,7 @@ EXPORTS = (
     "vlp4d_step_adjoint", "vlp4d_energy_grad",
     "vlp4d_ensemble_create", "vlp4d_ensemble_destroy", "vlp4d_ensemble_run", "vlp4d_ensemble_check",
     "vlp4d_ensemble_read", "vlp4d_ensemble_cells", "vlp4d_ensemble_set_tiles", "vlp4d_ensemble_get_tiles",
-    "vlp4d_ensemble_autotune",
+    "vlp4d_ensemble_autotune", "vlp4d_selftest_wait_timeout",
 )
 
 
@@ -126,6 +126,7 @@ def lib() -> C.CDLL:
         L.vlp4d_ensemble_set_tiles.argtypes = [vp, i, i, i]
         L.vlp4d_ensemble_get_tiles.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
         L.vlp4d_ensemble_autotune.argtypes = [vp, i, C.c_char_p, vp]
+        L.vlp4d_selftest_wait_timeout.argtypes = [vp, C.c_longlong, vp]
         for n in EXPORTS:
             if n not in ("vlp4d_last_error", "vlp4d_kernel_launches", "vlp4d_ensemble_cells"):
                 getattr(L, n).restype = C.c_int
@@ -342,6 +343,10 @@ class Context:
     def check(self):
         """Synchronise and raise if a kernel reported a lost asynchronous copy."""
         _check(lib().vlp4d_check(self.h))
+
+    def selftest_wait_timeout(self, limit_cycles: int, stream=None):
+        """Launch a bounded wait that nothing completes (see the C header)."""
+        _check(lib().vlp4d_selftest_wait_timeout(self.h, int(limit_cycles), _stream_ptr(stream)))
 
     def print_fxvx(self, fn, path):
         _check(lib().vlp4d_print_fxvx(self.h, self._f(fn), str(path).encode()))
