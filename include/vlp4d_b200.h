@@ -123,9 +123,11 @@ int vlp4d_advect_vxvy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, voi
 /* Two x/y shifts by dt in one pass followed by the moment of the result
  * into the context's rho: the last x/y half step of one Strang step and the
  * first of the next (timestep.hpp:50-58 then :17-28 with dt/2 each), the
- * pass vlp4d_steps runs between steps.  f equals vlp4d_advect_xy applied
- * twice, bit for bit; rho equals vlp4d_field_rho of it up to summation
- * order.  Returns VLP4D_ERR_UNSUPPORTED, launching nothing, when the
+ * pass vlp4d_steps runs between steps.  The two x shifts are applied as
+ * one 11-tap stencil (offset 2m, weights w*w) and likewise the y shifts, y
+ * before x (the x and y shifts commute): equal to vlp4d_advect_xy applied
+ * twice in exact arithmetic, and to rounding in floating point; rho equals
+ * vlp4d_field_rho of the result up to summation order.  Returns VLP4D_ERR_UNSUPPORTED, launching nothing, when the
  * one-pass kernel does not fit the shape or the buffers (nx not a multiple
  * of 4, not 16-byte aligned, shared memory) or VLP4D_KERNELS=generic: the
  * caller then uses two vlp4d_advect_xy calls.  No reference counterpart as a
@@ -163,13 +165,15 @@ int vlp4d_diags_save(vlp4d_ctx *ctx, const char *path);
 int vlp4d_step(vlp4d_ctx *ctx, void *f_state, void *f_next, int iter, void *stream);
 
 /* `nsteps` consecutive steps, iterations iter0 .. iter0+nsteps-1 (the time
- * loop of miniapps/vlp4d/thrust/vlp4d.cpp:63-72): the same sweeps, field
- * solves and diagnostics as nsteps calls of vlp4d_step, and bit-identical to
- * them, but the last x/y half step of each step and the first x/y half step
- * of the next (consecutive, with no field solve between them) run as one
- * pass, so the intermediate state between steps is never written to memory:
- * 2*nsteps + 1 passes over f instead of 3*nsteps.  Reads f_state, writes the
- * final state into f_next; f_state is scratch. */
+ * loop of miniapps/vlp4d/thrust/vlp4d.cpp:63-72): the same steps, field
+ * solves and diagnostics as nsteps calls of vlp4d_step.  In FP32 contexts
+ * (VLP4D_XYXY=1/0 at context creation forces it on/off) the last x/y half
+ * step of each step and the first of the next (consecutive, with no field
+ * solve between them) run as one pass (vlp4d_advect_xyxy's), so the state
+ * between steps is never written to memory: 2*nsteps + 1 passes over f
+ * instead of 3*nsteps, equal to nsteps vlp4d_step calls to rounding.  With
+ * the joining off the result is bit-identical to them.  Reads f_state,
+ * writes the final state into f_next; f_state is scratch. */
 int vlp4d_steps(vlp4d_ctx *ctx, void *f_state, void *f_next, int iter0, int nsteps, void *stream);
 
 /* The time loop of main() (miniapps/vlp4d/thrust/vlp4d.cpp:55-73) with host

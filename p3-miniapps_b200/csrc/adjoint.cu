@@ -787,6 +787,10 @@ int vlp4d_adjoint_create(vlp4d_ctx *ctx, int nsteps, int every, vlp4d_adjoint **
   StencilTable *t = nullptr;
   if ((rc = ensure_xy_table(ctx, 0, 0.5 * ctx->dom.dt, &t, s))) return bail(rc);
   if ((rc = ensure_xy_table(ctx, 1, 0.5 * ctx->dom.dt, &t, s))) return bail(rc);
+  if (xyxy_join(ctx)) {
+    if ((rc = ensure_xy11_table(ctx, 0, 0.5 * ctx->dom.dt, &t, s))) return bail(rc);
+    if ((rc = ensure_xy11_table(ctx, 1, 0.5 * ctx->dom.dt, &t, s))) return bail(rc);
+  }
   if ((rc = field_transpose_setup(A, s))) return bail(rc);
   *out = A;
   return VLP4D_OK;

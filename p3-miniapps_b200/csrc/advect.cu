@@ -126,15 +126,15 @@ void free_table(StencilTable &t) {
   t.valid = false;
 }
 
-int alloc_table(StencilTable &t, int lines) {
+int alloc_table(StencilTable &t, int lines, int taps) {
   if (t.m && t.lines >= lines) return VLP4D_OK;
   cudaFree(t.m);
   cudaFree(t.w);
   cudaFree(t.wf);
   t.m = nullptr; t.w = nullptr; t.wf = nullptr;
   VLP4D_CUDA_TRY(cudaMalloc(&t.m, sizeof(int) * lines));
-  VLP4D_CUDA_TRY(cudaMalloc(&t.w, sizeof(double) * 6 * lines));
-  VLP4D_CUDA_TRY(cudaMalloc(&t.wf, sizeof(float) * 6 * lines));
+  VLP4D_CUDA_TRY(cudaMalloc(&t.w, sizeof(double) * taps * lines));
+  VLP4D_CUDA_TRY(cudaMalloc(&t.wf, sizeof(float) * taps * lines));
   t.lines = lines;
   t.valid = false;
   return VLP4D_OK;
@@ -193,6 +193,57 @@ int ensure_xy_table(vlp4d_ctx *c, int dim, double dt, StencilTable **out, cudaSt
   t->dt = dt;
   t->valid = true;
   t->stamp = ++c->table_clock;
+  *out = t;
+  return VLP4D_OK;
+}
+
+int ensure_xy11_table(vlp4d_ctx *c, int dim, double dt, StencilTable **out, cudaStream_t s) {
+  StencilTable *t = dim == 0 ? &c->tab_x11 : &c->tab_y11;
+  if (t->valid && t->dt == dt) {
+    *out = t;
+    return VLP4D_OK;
+  }
+  t->valid = false;
+  const int vdim = dim == 0 ? 2 : 3;
+  const int lines = c->g.n[vdim], n = c->g.n[dim];
+  int rc = alloc_table(*t, lines, 11);
+  if (rc) return rc;
+  std::vector<int> hm(lines);
+  std::vector<double> hw(11 * (size_t)lines);
+  std::vector<float> hwf(11 * (size_t)lines);
+  for (int l = 0; l < lines; ++l) {
+    const double v = c->g.minp[vdim] + l * c->g.dx[vdim];
+    const LineStencil st = line_stencil(dt * v, c->g.minp[dim], c->g.maxp[dim], n);
+    // out[i] = sum_k w_k sum_j w_j f[i + m + k + m + j] = sum_q W_q f[i + 2m + q].
+    double W[11] = {0.};
+    for (int k = 0; k < 6; ++k)
+      for (int j = 0; j < 6; ++j) W[k + j] += st.w[k] * st.w[j];
+    hm[l] = (int)((2LL * st.m) % n);
+    // FP32 difference form about tap 5 (the weights sum to one):
+    // out = f5 + sum_j u_j (f_{j+1} - f_j), u_j = -(W_0+..+W_j) for j < 5,
+    // u_j = W_{j+1}+..+W_10 for j >= 5.
+    double u[10];
+    double acc = 0.;
+    for (int j = 0; j < 5; ++j) {
+      acc += W[j];
+      u[j] = -acc;
+    }
+    acc = 0.;
+    for (int j = 9; j >= 5; --j) {
+      acc += W[j + 1];
+      u[j] = acc;
+    }
+    for (int k = 0; k < 11; ++k) {
+      hw[11 * l + k] = W[k];
+      hwf[11 * l + k] = k < 10 ? (float)u[k] : 0.f;
+    }
+  }
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(t->m, hm.data(), sizeof(int) * lines, cudaMemcpyHostToDevice, s));
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(t->w, hw.data(), sizeof(double) * 11 * lines, cudaMemcpyHostToDevice, s));
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(t->wf, hwf.data(), sizeof(float) * 11 * lines, cudaMemcpyHostToDevice, s));
+  VLP4D_CUDA_TRY(cudaStreamSynchronize(s));
+  t->dt = dt;
+  t->valid = true;
   *out = t;
   return VLP4D_OK;
 }

@@ -336,19 +336,158 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
   }
 }
 
-// Two consecutive x/y half steps in one pass: x, y, x, y with the same
-// stencils (the end of one Strang step and the start of the next, which no
-// field solve separates), plus the moment of the result.  Every sweep is the
-// one the two separate passes would apply, in the same order and precision,
-// so the result is bit-identical; only the intermediate state is kept in
-// shared memory instead of HBM.  Output row r of the chunk needs staged rows
-// r + 2*my .. r + 2*my + 10, so R + 10 rows are staged.  Phases per item:
-//   X1: staged rows -> xa (R+10 rows)   | barrier, refill the slot
-//   Y1: xa -> ya (R+5 rows)             | barrier
-//   X2: ya -> xb (R+5 rows)             | barrier
-//   Y2: xb -> output (R rows), moment
-// The next item's X1/Y1/X2 writes are ordered after this item's reads by
-// the next item's barriers, so no barrier follows Y2.
+// Two consecutive x/y half steps in one pass: the closing x, y half step of
+// one Strang step and the opening one of the next, which no field solve
+// separates.  Two x shifts by the same dt are one 11-tap x stencil (offset
+// 2m mod nx, weights w * w), likewise in y, and the x and y shifts commute
+// exactly (their weights depend on different indices), so
+//   y x y x = (y y)(x x):   Y11 on the staged rows, then X11,
+// which equals the four sweeps in exact arithmetic and in floating point up
+// to rounding.  Per item: stage the R + 10 input rows the chunk needs,
+// Y11 (thread: RT output rows of its column quad) into a double-buffered
+// shared tile, one barrier, X11 of the thread's rows to the output, with the
+// moment of the result in FP64 registers as in k_plane.
+template <typename T>
+struct LineRec11;
+template <>
+struct LineRec11<float> {
+  float w[11];  // difference weights u[0..9] (u[10] unused)
+  int m;
+};
+template <>
+struct LineRec11<double> {
+  double w[11];
+  int m;
+  int pad;
+};
+static_assert(sizeof(LineRec11<float>) == 48 && sizeof(LineRec11<double>) == 96, "11-tap record layout");
+
+template <typename T>
+__device__ __forceinline__ void stage_lines11(const StencilTable &t, int lines, LineRec11<T> *dst) {
+  for (int l = threadIdx.x; l < lines; l += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < 11; ++k) dst[l].w[k] = sizeof(T) == 4 ? (T)t.wf[11 * l + k] : (T)t.w[11 * l + k];
+    dst[l].m = t.m[l];
+  }
+}
+
+// FP32: weights as packed pairs (u_j, u_j); FP64: the 11 weights.
+template <typename T>
+struct W11 {
+  T w[11];
+};
+template <>
+struct W11<float> {
+  float2 u[10];
+};
+__device__ __forceinline__ int read_line11(const LineRec11<float> &r, W11<float> &w) {
+  LineRec11<float> c = r;
+#pragma unroll
+  for (int k = 0; k < 10; ++k) w.u[k] = make_float2(c.w[k], c.w[k]);
+  return c.m;
+}
+__device__ __forceinline__ int read_line11(const LineRec11<double> &r, W11<double> &w) {
+  LineRec11<double> c = r;
+#pragma unroll
+  for (int k = 0; k < 11; ++k) w.w[k] = c.w[k];
+  return c.m;
+}
+
+// out = f_5 + sum_j u_j d_j on packed pairs (d_j = f_{j+1} - f_j).
+__device__ __forceinline__ float2 interp11_2(const float2 (&u)[10], float2 f5, const float2 *d) {
+  float2 acc = __fmul2_rn(u[0], d[0]);
+#pragma unroll
+  for (int j = 1; j < 10; ++j) acc = __ffma2_rn(u[j], d[j], acc);
+  return __fadd2_rn(f5, acc);
+}
+
+// Y11 of one thread: RT output rows of its column quad from the RT + 10
+// rows starting at src (stride nx), streamed; emit(i, o) receives row i.
+template <int RT, typename Emit>
+__device__ __forceinline__ void sweep_y11(const float *src, int nx, const W11<float> &w, Emit emit) {
+  float2 y[RT + 10][2], d[RT + 9][2];
+#pragma unroll
+  for (int j = 0; j < RT + 10; ++j) {
+    const float4 q4 = *reinterpret_cast<const float4 *>(src + (size_t)j * nx);
+    y[j][0] = make_float2(q4.x, q4.y);
+    y[j][1] = make_float2(q4.z, q4.w);
+    if (j >= 1) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) d[j - 1][h] = sub2(y[j][h], y[j - 1][h]);
+    }
+    if (j >= 10) {
+      const int i = j - 10;
+      float2 o2[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        float2 dd[10];
+#pragma unroll
+        for (int k = 0; k < 10; ++k) dd[k] = d[i + k][h];
+        o2[h] = interp11_2(w.u, y[i + 5][h], dd);
+      }
+      const float o[4] = {o2[0].x, o2[0].y, o2[1].x, o2[1].y};
+      emit(i, o);
+    }
+  }
+}
+template <int RT, typename Emit>
+__device__ __forceinline__ void sweep_y11(const double *src, int nx, const W11<double> &w, Emit emit) {
+  double y[RT + 10][4];
+#pragma unroll
+  for (int j = 0; j < RT + 10; ++j) {
+    load4(src + (size_t)j * nx, y[j]);
+    if (j >= 10) {
+      const int i = j - 10;
+      double o[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        double acc = w.w[0] * y[i][q];
+#pragma unroll
+        for (int k = 1; k < 11; ++k) acc = fma(w.w[k], y[i + k][q], acc);
+        o[q] = acc;
+      }
+      emit(i, o);
+    }
+  }
+}
+
+// X11 of four outputs from the twenty values t[0..19] starting at the
+// aligned column a0 = c0 + mx - r (output q uses t[r+q .. r+q+10]).
+template <int R_>
+__device__ __forceinline__ void x11_from(const float (&t)[20], const W11<float> &w, float (&o)[4]) {
+  float d[13];
+#pragma unroll
+  for (int j = 0; j < 13; ++j) d[j] = t[R_ + j + 1] - t[R_ + j];
+  float2 dp[12];
+#pragma unroll
+  for (int j = 0; j < 12; ++j) dp[j] = make_float2(d[j], d[j + 1]);
+  const float2 lo = interp11_2(w.u, make_float2(t[R_ + 5], t[R_ + 6]), dp);
+  const float2 hi = interp11_2(w.u, make_float2(t[R_ + 7], t[R_ + 8]), dp + 2);
+  o[0] = lo.x;
+  o[1] = lo.y;
+  o[2] = hi.x;
+  o[3] = hi.y;
+}
+template <int R_>
+__device__ __forceinline__ void x11_from(const double (&t)[20], const W11<double> &w, double (&o)[4]) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    double acc = w.w[0] * t[R_ + q];
+#pragma unroll
+    for (int k = 1; k < 11; ++k) acc = fma(w.w[k], t[R_ + q + k], acc);
+    o[q] = acc;
+  }
+}
+template <typename T>
+__device__ __forceinline__ void sweep_x11(const T (&t)[20], int r, const W11<T> &w, T (&o)[4]) {
+  switch (r) {
+    case 0: x11_from<0>(t, w, o); break;
+    case 1: x11_from<1>(t, w, o); break;
+    case 2: x11_from<2>(t, w, o); break;
+    default: x11_from<3>(t, w, o); break;
+  }
+}
+
 template <typename T, int NX, int RT>
 __global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -358,16 +497,13 @@ __global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
   const size_t slot_elems = (size_t)(R + 10) * nx;
   const uint32_t slot_bytes = (uint32_t)(slot_elems * sizeof(T));
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
-  LineRec<T> *xrec = reinterpret_cast<LineRec<T> *>(smem + kBarBytes);
-  LineRec<T> *yrec = xrec + a.nvx;
+  LineRec11<T> *xrec = reinterpret_cast<LineRec11<T> *>(smem + kBarBytes);
+  LineRec11<T> *yrec = xrec + a.nvx;
   T *slots = reinterpret_cast<T *>(yrec + a.nvy);
-  T *xa = slots + (size_t)S * slot_elems;
-  T *ya = xa + slot_elems;
-  T *xb = ya + (size_t)(R + 5) * nx;
+  T *ys_base = slots + (size_t)S * slot_elems;  // two R-row tiles
 
   const int cg = threadIdx.x % ncg;
   const int rg = threadIdx.x / ncg;
-  const int RG = blockDim.x / ncg;
   const int c0 = cg * 4;
   const int r0 = rg * RT;
   const int chunk = blockIdx.x % a.cpp;
@@ -381,13 +517,13 @@ __global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
     for (int st = 0; st < S; ++st) mbar_init(&bars[st], 1);
     mbar_fence_init();
   }
-  stage_lines<T>(a.tx, a.nvx, xrec);
-  stage_lines<T>(a.ty, a.nvy, yrec);
+  stage_lines11<T>(a.tx, a.nvx, xrec);
+  stage_lines11<T>(a.ty, a.nvy, yrec);
   __syncthreads();
 
   auto issue = [&](long long it) {
     const long long p = g + it * G;
-    int phys = (chunk * R + 2 * yrec[(int)(p / a.nvx)].m) % ny;
+    int phys = (chunk * R + yrec[(int)(p / a.nvx)].m) % ny;
     uint64_t *bar = &bars[it % S];
     mbar_arrive_expect_tx(bar, slot_bytes);
     const T *src = static_cast<const T *>(a.fin) + p * plane_elems;
@@ -412,23 +548,6 @@ __global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
 #pragma unroll
     for (int q = 0; q < 4; ++q) racc[i][q] = 0.0;
 
-  // x sweep of rows [0, nrows) of src into dst (rows rg, rg+RG, ...).
-  auto sweep_rows_x = [&](const T *src, T *dst, int nrows, int o0, int o1, int o2, int rr, const SweepW<T> &wx) {
-    for (int v = rg; v < nrows; v += RG) {
-      const T *row = src + (size_t)v * nx;
-      T t[12], q4[4];
-      load4(row + o0, q4);
-      t[0] = q4[0]; t[1] = q4[1]; t[2] = q4[2]; t[3] = q4[3];
-      load4(row + o1, q4);
-      t[4] = q4[0]; t[5] = q4[1]; t[6] = q4[2]; t[7] = q4[3];
-      load4(row + o2, q4);
-      t[8] = q4[0]; t[9] = q4[1]; t[10] = q4[2]; t[11] = q4[3];
-      T o[4];
-      sweep_x4(t, rr, wx, o);
-      store4(dst + (size_t)v * nx + c0, o);
-    }
-  };
-
   const int gdx = G % a.nvx, gdy = G / a.nvx;
   int ivx = g % a.nvx, ivy = g / a.nvx;
   int slot = 0;
@@ -437,40 +556,51 @@ __global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
     const bool ok = mbar_wait_bounded(&bars[slot], parity);
     const long long p = g + it * G;
     const T *in = slots + (size_t)slot * slot_elems;
+    T *ys = ys_base + (size_t)(it & 1) * R * nx;
     T *outp = static_cast<T *>(a.fout) + p * plane_elems + (long long)chunk * R * nx;
-    T wlx[6], wly[6];
-    int base = c0 + read_line(xrec[ivx], wlx);
-    read_line(yrec[ivy], wly);
-    SweepW<T> wx, wy;
-    make_sweep_w(wlx, wx);
-    make_sweep_w(wly, wy);
-    base = wrap_col<NX>(base, nx);
-    const int rr = base & 3;
-    const int o0 = base - rr, o1 = wrap_col<NX>(o0 + 4, nx), o2 = wrap_col<NX>(o0 + 8, nx);
-
-    sweep_rows_x(in, xa, R + 10, o0, o1, o2, rr, wx);  // X1
+    {  // Y11: rows r0 .. r0+RT-1 of this thread's column quad.
+      W11<T> wy;
+      read_line11(yrec[ivy], wy);
+      sweep_y11<RT>(in + (size_t)r0 * nx + c0, nx, wy,
+                    [&](int i, const T (&o)[4]) { store4(ys + (size_t)(r0 + i) * nx + c0, o); });
+    }
+    // ys is complete and the staged slot is no longer read: refill it.
     if (__syncthreads_or(!ok)) {
       plane_abort(a, bars, it, n_items, S);
       return;
     }
     if (threadIdx.x == 0 && it + S < n_items) issue(it + S);
-    // Y1: rows [0, R) streamed per thread, rows [R, R+5) one at a time.
-    sweep_y<RT>(xa + (size_t)r0 * nx + c0, nx, wy,
-                [&](int i, const T (&o)[4]) { store4(ya + (size_t)(r0 + i) * nx + c0, o); });
-    for (int v = R + rg; v < R + 5; v += RG) {
-      sweep_y<1>(xa + (size_t)v * nx + c0, nx, wy,
-                 [&](int, const T (&o)[4]) { store4(ya + (size_t)v * nx + c0, o); });
-    }
-    __syncthreads();
-    sweep_rows_x(ya, xb, R + 5, o0, o1, o2, rr, wx);  // X2
-    __syncthreads();
-    // Y2 and the moment.
-    T *dst = outp + (size_t)r0 * nx + c0;
-    sweep_y<RT>(xb + (size_t)r0 * nx + c0, nx, wy, [&](int i, const T (&o)[4]) {
-      store4(dst + (size_t)i * nx, o);
+    {  // X11 of the thread's rows, the moment.
+      W11<T> wx;
+      int base = c0 + read_line11(xrec[ivx], wx);
+      base = base % nx;
+      const int rr = base & 3;
+      int o[5];
+      o[0] = base - rr;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) racc[i][q] += (double)o[q];
-    });
+      for (int k = 1; k < 5; ++k) {
+        o[k] = o[k - 1] + 4;
+        if (o[k] >= nx) o[k] -= nx;
+      }
+#pragma unroll
+      for (int i = 0; i < RT; ++i) {
+        const T *row = ys + (size_t)(r0 + i) * nx;
+        T t[20], q4[4];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+          load4(row + o[k], q4);
+          t[4 * k] = q4[0];
+          t[4 * k + 1] = q4[1];
+          t[4 * k + 2] = q4[2];
+          t[4 * k + 3] = q4[3];
+        }
+        T out[4];
+        sweep_x11(t, rr, wx, out);
+        store4(outp + (size_t)(r0 + i) * nx + c0, out);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) racc[i][q] += (double)out[q];
+      }
+    }
     ivx += gdx;
     ivy += gdy;
     if (ivx >= a.nvx) {
@@ -500,9 +630,7 @@ namespace {
 struct PlaneCfg {
   int R = 0, rt = 1, stages = 3, threads = 0, cpp = 1, grid = 0, G = 0;
   size_t smem = 0;
-  bool query = false;  // only fill per_sm (resident CTAs per SM), launch nothing
   int per_sm = 0;
-  int fixed_G = 0;  // plane groups to launch (0: as many as fit one wave)
 };
 
 int env_int(const char *name, int dflt) {
@@ -572,9 +700,8 @@ int run_plane(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, cudaStream_t s
   VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, cfg.threads, cfg.smem));
   if (per_sm < 1) return VLP4D_ERR_UNSUPPORTED;
   cfg.per_sm = per_sm;
-  if (cfg.query) return VLP4D_OK;
   const long long planes = (long long)args.nvx * args.nvy;
-  long long G = cfg.fixed_G > 0 ? cfg.fixed_G : ((long long)per_sm * c->num_sms) / cfg.cpp;
+  long long G = ((long long)per_sm * c->num_sms) / cfg.cpp;
   if (G < 1) G = 1;
   if (G > planes) G = planes;
   if (RHO && G > c->rho_part_groups) G = c->rho_part_groups;
@@ -627,27 +754,33 @@ PlaneArgs plane_args(const vlp4d_ctx *c, const void *fn, void *fnp1, const Plane
 }
 
 size_t xyxy_smem(int R, int nx, size_t elem, int stages, int nvx, int nvy) {
-  const size_t rec = elem == 4 ? 32 : 64;
-  return kBarBytes + rec * (nvx + nvy) + (size_t)stages * (R + 10) * nx * elem +
-         (size_t)(R + 10 + 2 * (R + 5)) * nx * elem;
+  const size_t rec = elem == 4 ? 48 : 96;
+  return kBarBytes + rec * (nvx + nvy) + (size_t)stages * (R + 10) * nx * elem + 2 * (size_t)R * nx * elem;
 }
 
 // Chunk height (the tallest divisor of ny up to 32 rows whose block and
-// shared memory fit), rows per thread and pipeline depth of k_plane_xyxy.
+// shared memory fit), rows per thread (4 in FP32 when R allows, 1 in FP64)
+// and pipeline depth (3 stages if two CTAs then share an SM, else 2) of
+// k_plane_xyxy.  VLP4D_XYXY_STAGES overrides the depth.
 bool xyxy_config(const vlp4d_ctx *c, PlaneCfg &cfg) {
   const int nx = c->g.n[0], ny = c->g.n[1];
   if (nx % 4 != 0 || nx > 2048) return false;
   const int ncg = nx / 4;
-  cfg.stages = env_int("VLP4D_XYXY_STAGES", 2);
-  if (cfg.stages < 2 || cfg.stages > kMaxStages) return false;
+  const int forced = env_int("VLP4D_XYXY_STAGES", 0);
+  if (forced && (forced < 2 || forced > kMaxStages)) return false;
   cfg.R = 0;
   for (int r = ny < 32 ? ny : 32; r >= 1 && !cfg.R; --r) {
     if (ny % r) continue;
-    const int t = r % 4 == 0 ? 4 : 1;
+    const int t = (c->elem == 4 && r % 4 == 0) ? 4 : 1;
     if (ncg * (r / t) > 512 || ncg * (r / t) < 1) continue;
-    if (xyxy_smem(r, nx, c->elem, cfg.stages, c->g.n[2], c->g.n[3]) > 224 * 1024) continue;
+    int st = forced;
+    if (!st) {
+      st = xyxy_smem(r, nx, c->elem, 3, c->g.n[2], c->g.n[3]) <= 112 * 1024 ? 3 : 2;
+    }
+    if (xyxy_smem(r, nx, c->elem, st, c->g.n[2], c->g.n[3]) > 224 * 1024) continue;
     cfg.R = r;
     cfg.rt = t;
+    cfg.stages = st;
   }
   if (!cfg.R) return false;
   cfg.cpp = ny / cfg.R;
@@ -664,9 +797,8 @@ int run_xyxy(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, cudaStream_t s)
   VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, cfg.threads, cfg.smem));
   if (per_sm < 1) return VLP4D_ERR_UNSUPPORTED;
   cfg.per_sm = per_sm;
-  if (cfg.query) return VLP4D_OK;
   const long long planes = (long long)args.nvx * args.nvy;
-  long long G = cfg.fixed_G > 0 ? cfg.fixed_G : ((long long)per_sm * c->num_sms) / cfg.cpp;
+  long long G = ((long long)per_sm * c->num_sms) / cfg.cpp;
   if (G < 1) G = 1;
   if (G > planes) G = planes;
   if (G > c->rho_part_groups) G = c->rho_part_groups;
@@ -693,44 +825,6 @@ int run_xyxy_any(vlp4d_ctx *c, const PlaneArgs &a, PlaneCfg &cfg, cudaStream_t s
   return cfg.rt == 4 ? run_xyxy_nx<float, 4>(c, a, cfg, s) : run_xyxy_nx<float, 1>(c, a, cfg, s);
 }
 
-int run_plane_moment(vlp4d_ctx *c, const PlaneArgs &a, PlaneCfg &cfg, cudaStream_t s) {
-  if (c->dtype == VLP4D_F64) return run_plane_rt<double, true, true, true>(c, a, cfg, s);
-  return run_plane_rt<float, true, true, true>(c, a, cfg, s);
-}
-
-// The plane-group count of the fused moment: the smaller of the one-wave
-// group counts of k_plane (x+y with the moment) and k_plane_xyxy, so that
-// both use the same summation order; 0 when neither kernel fits the shape.
-int moment_groups(vlp4d_ctx *c) {
-  if (c->moment_G) return c->moment_G > 0 ? c->moment_G : 0;
-  const long long planes = (long long)c->g.n[2] * c->g.n[3];
-  long long G = 0;
-  PlaneCfg cp;
-  if (plane_config(c, true, true, cp)) {
-    cp.query = true;
-    PlaneArgs a = plane_args(c, nullptr, nullptr, cp, 5);
-    if (run_plane_moment(c, a, cp, 0) == VLP4D_OK && cp.per_sm > 0)
-      G = (long long)cp.per_sm * c->num_sms / cp.cpp;
-  }
-  PlaneCfg cx;
-  if (xyxy_config(c, cx)) {
-    cx.query = true;
-    PlaneArgs a = plane_args(c, nullptr, nullptr, cx, 10);
-    if (run_xyxy_any(c, a, cx, 0) == VLP4D_OK && cx.per_sm > 0) {
-      const long long gx = (long long)cx.per_sm * c->num_sms / cx.cpp;
-      G = G ? (gx < G ? gx : G) : gx;
-    }
-  }
-  cudaGetLastError();  // a failed query leaves nothing behind
-  if (G > planes) G = planes;
-  if (G > c->rho_part_groups) G = c->rho_part_groups;
-  if (G < 1) {
-    c->moment_G = -1;
-    return 0;
-  }
-  c->moment_G = (int)G;
-  return c->moment_G;
-}
 
 }  // namespace
 
@@ -745,10 +839,6 @@ int launch_advect_xy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTabl
   PlaneCfg cfg;
   if (!plane_config(c, do_x, do_y, cfg)) return VLP4D_ERR_UNSUPPORTED;
   const bool moment = with_rho && do_x && do_y;
-  if (moment) {
-    cfg.fixed_G = moment_groups(c);
-    if (!cfg.fixed_G) return VLP4D_ERR_UNSUPPORTED;
-  }
   PlaneArgs a = plane_args(c, fn, fnp1, cfg, do_y ? 5 : 0);
   if (tx) a.tx = *tx;
   if (ty) a.ty = *ty;
@@ -770,19 +860,22 @@ int launch_advect_xy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTabl
   return VLP4D_OK;
 }
 
-// Two x/y half steps and the moment of the result in one pass; returns
-// VLP4D_ERR_UNSUPPORTED (nothing launched) when the shape does not fit.
+// Two x/y half steps (the composed 11-tap stencils of tx, ty) and the
+// moment of the result in one pass; returns VLP4D_ERR_UNSUPPORTED (nothing
+// launched) when the shape does not fit.
 int launch_advect_xyxy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *tx, const StencilTable *ty,
                        cudaStream_t s) {
   if (!c->fused) return VLP4D_ERR_UNSUPPORTED;
   if (((uintptr_t)fn & 15) || ((uintptr_t)fnp1 & 15)) return VLP4D_ERR_UNSUPPORTED;
   PlaneCfg cfg;
   if (!xyxy_config(c, cfg)) return VLP4D_ERR_UNSUPPORTED;
-  cfg.fixed_G = moment_groups(c);
-  if (!cfg.fixed_G) return VLP4D_ERR_UNSUPPORTED;
+  StencilTable *x11 = nullptr, *y11 = nullptr;
+  int rc0;
+  if ((rc0 = ensure_xy11_table(c, 0, tx->dt, &x11, s))) return rc0;
+  if ((rc0 = ensure_xy11_table(c, 1, ty->dt, &y11, s))) return rc0;
   PlaneArgs a = plane_args(c, fn, fnp1, cfg, 10);
-  a.tx = *tx;
-  a.ty = *ty;
+  a.tx = *x11;
+  a.ty = *y11;
   int rc = run_xyxy_any(c, a, cfg, s);
   if (rc) return rc;
   return launch_rho_finish(c, cfg.G, s);

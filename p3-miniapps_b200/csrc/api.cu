@@ -82,7 +82,8 @@ void free_ctx(vlp4d_ctx *c) {
   cudaFree(c->rho_part);
   cudaFree(c->d_err);
   cudaFree(c->vspan);
-  for (StencilTable *t : {&c->tab_x[0], &c->tab_x[1], &c->tab_y[0], &c->tab_y[1], &c->tab_vx, &c->tab_vy}) {
+  for (StencilTable *t : {&c->tab_x[0], &c->tab_x[1], &c->tab_y[0], &c->tab_y[1], &c->tab_vx, &c->tab_vy,
+                          &c->tab_x11, &c->tab_y11}) {
     cudaFree(t->m);
     cudaFree(t->w);
     cudaFree(t->wf);

@@ -98,11 +98,6 @@ struct vlp4d_ctx {
   double *rho_part = nullptr;
   int rho_groups = 0;
   int rho_part_groups = 0;
-  // Plane groups of the moment fused into the x/y passes (k_plane with the
-  // moment, k_plane_xyxy): one value for both kernels, so that the moment's
-  // summation order, and with it every later bit, does not depend on which
-  // of the two produced it.  0 until first computed.
-  int moment_G = 0;
   // VLP4D_XYXY at creation: -1 unset, 0 never join x/y half steps across
   // steps, 1 always (when the kernel fits the shape).
   int xyxy_mode = -1;
@@ -123,6 +118,9 @@ struct vlp4d_ctx {
   // on the host and uploaded once), v lines rebuilt from E on the device.
   vlp4d::StencilTable tab_x[2], tab_y[2];
   vlp4d::StencilTable tab_vx, tab_vy;
+  // Two x (y) shifts by the same dt composed into one 11-tap stencil, for
+  // the x/y/x/y pass: m = 2*m1 mod n, w = w1 * w1 (convolution).
+  vlp4d::StencilTable tab_x11, tab_y11;
   unsigned long long table_clock = 0;
 
   // Pinned host staging for vlp4d_run's per-step diagnostic read-back.
@@ -132,9 +130,12 @@ struct vlp4d_ctx {
 namespace vlp4d {
 
 // advect.cu
-int alloc_table(StencilTable &t, int lines);
+int alloc_table(StencilTable &t, int lines, int taps = 6);
 void free_table(StencilTable &t);
 int ensure_xy_table(vlp4d_ctx *c, int dim, double dt, StencilTable **out, cudaStream_t s);
+// The composed 11-tap table of two x (dim 0) or y (dim 1) shifts by dt:
+// per line m and 11 FP64 weights; for FP32, 10 difference weights about tap 5.
+int ensure_xy11_table(vlp4d_ctx *c, int dim, double dt, StencilTable **out, cudaStream_t s);
 int build_v_tables(vlp4d_ctx *c, double dt, bool vx, bool vy, cudaStream_t s);
 int launch_advect_generic(vlp4d_ctx *c, int dim, const void *fn, void *fnp1, const StencilTable *t,
                           cudaStream_t s);

@@ -148,9 +148,11 @@ def test_unaligned_buffers_fall_back_to_generic(pkg, cuda):
 @pytest.mark.parametrize("xyxy", ["0", "1"])
 def test_steps_bit_identical_to_single_steps(pkg, cuda, n, dtype, xyxy):
     """vlp4d_steps runs the last x/y half step of each step and the first of
-    the next as one pass (VLP4D_XYXY=1) or as two (=0); every sweep is the
-    same operation in the same order and precision, so K steps equal K calls
-    of vlp4d_step bit for bit, diagnostics included."""
+    the next as two passes (VLP4D_XYXY=0), every sweep the same operation in
+    the same order and precision as vlp4d_step: K steps equal K calls of
+    vlp4d_step bit for bit, diagnostics included.  With VLP4D_XYXY=1 the two
+    half steps are one pass of the composed 11-tap stencils, equal in exact
+    arithmetic: the results agree to rounding."""
     torch = cuda
     K = 4
     dom = pkg.Domain(list(n), [0.0, 0.0, -6.0, -6.0], [4 * np.pi, 4 * np.pi, 6.0, 6.0], 0.125, K + 1, 10)
@@ -166,8 +168,13 @@ def test_steps_bit_identical_to_single_steps(pkg, cuda, n, dtype, xyxy):
         c, d = f0.clone(), ctx.empty_f()
         ctx.steps(c, d, 1, K)
         nrj2, mass2 = ctx.diags_read(K + 1)
-        assert torch.equal(d, single)
-        assert np.array_equal(nrj1[1:], nrj2[1:]) and np.array_equal(mass1[1:], mass2[1:])
+        if xyxy == "0":
+            assert torch.equal(d, single)
+            assert np.array_equal(nrj1[1:], nrj2[1:]) and np.array_equal(mass1[1:], mass2[1:])
+        else:
+            tol = 1e-13 if dtype == "f64" else 2e-6
+            assert _rel(d, single) < tol
+            assert np.abs(nrj1[1:] - nrj2[1:]).max() < (1e-11 if dtype == "f64" else 1e-6)
 
 
 @pytest.mark.parametrize("n", [(16, 4, 16, 4), (32, 32, 32, 32), (12, 10, 14, 10)])
@@ -198,8 +205,9 @@ def test_steps_generic_and_oracle(pkg, cuda, n):
 @pytest.mark.parametrize("n", SHAPES + [(12, 10, 14, 10)])
 @pytest.mark.parametrize("dtype", ["f64", "f32"])
 def test_advect_xyxy_matches_two_xy_passes(pkg, cuda, n, dtype):
-    """vlp4d_advect_xyxy (one pass) against vlp4d_advect_xy twice: bit-identical
-    f; the moment it leaves in rho against field_rho of the result."""
+    """vlp4d_advect_xyxy (one pass of the composed 11-tap stencils) against
+    vlp4d_advect_xy twice, to rounding; the moment it leaves in rho against
+    field_rho of the result."""
     torch = cuda
     dom = _dom(pkg, n)
     for kernels in ("", "generic"):
@@ -218,6 +226,7 @@ def test_advect_xyxy_matches_two_xy_passes(pkg, cuda, n, dtype):
                 continue
             ctx.advect_xyxy(f0, c, 0.15)
             rho_one = ctx.rho.clone()
-            assert torch.equal(b, c), kernels
-            assert float((rho_one - rho_sep).abs().max()) <= 1e-13 * float(rho_sep.abs().max())
+            assert _rel(c, b) < (1e-13 if dtype == "f64" else 2e-6), kernels
+            assert float((rho_one - rho_sep).abs().max()) <= (1e-13 if dtype == "f64" else 1e-6) * float(
+                rho_sep.abs().max())
             ctx.check()
