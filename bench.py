@@ -47,6 +47,10 @@ def parse_args(argv=None):
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end runs")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip timing the reference CPU build")
     ap.add_argument("--only-f32", action="store_true", help="FP32 storage only (no FP64 run, no e2e): profiling")
+    ap.add_argument("--case", choices=["main", "adjoint", "ensemble"], default="main",
+                    help="profiling cases: the reverse-mode or the ensemble arm alone (--steps steps, "
+                         "--members members, default tiles), one JSON line")
+    ap.add_argument("--members", type=int, default=256, help="ensemble members for --case ensemble")
     return ap.parse_args(argv)
 
 
@@ -368,7 +372,7 @@ def gpu_arm(args, ranks):
     return line
 
 
-def ensemble_arm(pkg, torch, stream, peak, nruns=256, nsteps=50):
+def ensemble_arm(pkg, torch, stream, peak, nruns=256, nsteps=50, autotune=True):
     """The batched-ensemble configuration: 256 Landau members, N per dimension
     drawn from {16, 24, 32, 48}, amp ~ U[0.01, 0.1], k in {0.3, 0.5}, 50 steps
     of dt 0.1, FP32 f, in one persistent launch replayed from a CUDA graph.
@@ -377,7 +381,7 @@ def ensemble_arm(pkg, torch, stream, peak, nruns=256, nsteps=50):
     v = pkg.vlp4d
     members = v.landau_ensemble_members(nruns)
     with v.Ensemble(members, nsteps) as ens:
-        tiles = ens.autotune(3)
+        tiles = ens.autotune(3) if autotune else ens.tiles()
         ens.run()  # capture
         ens.check()
         t = time_calls(torch, stream, lambda: ens.run(stream), 3)
@@ -508,6 +512,20 @@ def main(argv=None):
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(reference_arm(args)), flush=True)
+        return 0
+    if args.case != "main":
+        import torch
+
+        import __graft_entry__ as ge
+
+        pkg = ge.load_package()
+        stream = torch.cuda.current_stream()
+        peak, _ = measured_hbm_peak()
+        if args.case == "adjoint":
+            out = adjoint_arm(pkg, torch, stream, nsteps=args.steps)
+        else:
+            out = ensemble_arm(pkg, torch, stream, peak, nruns=args.members, nsteps=args.steps, autotune=False)
+        print(json.dumps({"case": args.case, **out}), flush=True)
         return 0
     ranks = Ranks(world)
     try:

@@ -45,8 +45,8 @@ struct VslabArgs {
   StencilTable tvx, tvy;
   const int2 *span;  // per chunk: (min, max) signed vy offset of its columns
   int *err;
-  // Optional per-column term added to every output of the column:
-  // out += bias_scale * bias[ixy] (the reverse mode's field term); NULL = none.
+  // Per-column term added to every output of the column (kernels with
+  // BIAS only): out += bias_scale * bias[ixy], the reverse mode's field term.
   const double *bias;
   double bias_scale;
 };
@@ -120,7 +120,7 @@ __device__ __forceinline__ void issue_slab(const CUtensorMap *tin, const VslabAr
 
 // NXY: compile-time nx*ny (0 = read a.nxy at run time); with it the V output
 // stores of a thread use immediate offsets.
-template <typename T, bool DVX, bool DVY, int V, int NXY>
+template <typename T, bool DVX, bool DVY, int V, int NXY, bool BIAS = false>
 __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorMap tin, VslabArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // Tensor-copy destinations on a 128-byte boundary whatever the base
@@ -198,8 +198,8 @@ __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorM
       lag0 = 5 + signed_offset(__ldg(a.tvy.m + ixy), a.nvy) - a.span[cc].x;
       load_weights(WeightsOf<T>::get(a.tvy), ixy, wvy);
     }
-    const bool has_bias = a.bias != nullptr;
-    const double bias = has_bias ? a.bias_scale * __ldg(a.bias + ixy) : 0.0;
+    constexpr bool has_bias = BIAS;
+    const double bias = BIAS ? a.bias_scale * __ldg(a.bias + ixy) : 0.0;
     // Output pointer of the next row this thread writes.
     T *orow = static_cast<T *>(a.fout) + ixy + vstride * vx0 + ystride * (long long)sg * a.Q;
     // Ring of vx-swept rows, slot = t % 6 (static after unrolling).  FP64:
@@ -291,7 +291,7 @@ __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorM
               } else {
                 val = win2[u][i];
               }
-              if (has_bias) {
+              if constexpr (has_bias) {
                 val.x = (float)((double)val.x + bias);
                 val.y = (float)((double)val.y + bias);
               }
@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorM
                               win[(u + 4) % 6][i], win[(u + 5) % 6][i], win[u][i]);
               else
                 val = win[u][i];
-              if (has_bias) val = (T)((double)val + bias);
+              if constexpr (has_bias) val = (T)((double)val + bias);
               orow[vstride * i] = val;
             }
           }
@@ -412,9 +412,9 @@ bool vslab_config(const vlp4d_ctx *c, VslabCfg &cfg) {
   return cfg.smem <= 200 * 1024;
 }
 
-template <typename T, bool DVX, bool DVY, int V, int NXY>
+template <typename T, bool DVX, bool DVY, int V, int NXY, bool BIAS = false>
 int run_vslab(vlp4d_ctx *c, const CUtensorMap &map, const VslabArgs &args, const VslabCfg &cfg, cudaStream_t s) {
-  auto kern = k_vslab<T, DVX, DVY, V, NXY>;
+  auto kern = k_vslab<T, DVX, DVY, V, NXY, BIAS>;
   VLP4D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
   int per_sm = 0;
   VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, cfg.threads, cfg.smem));
@@ -484,6 +484,11 @@ int launch_advect_vxvy_tables(vlp4d_ctx *c, const void *fn, void *fnp1, const St
     case 16384: return run_vslab<T, DVX, DVY, V, 16384>(c, map, a, cfg, s);      \
     case 4096: return run_vslab<T, DVX, DVY, V, 4096>(c, map, a, cfg, s);        \
     default: return run_vslab<T, DVX, DVY, V, 0>(c, map, a, cfg, s);             \
+  }
+  if (bias) {  // the reverse mode's vx+vy pass with the per-column term
+    if (!(do_vx && do_vy)) return VLP4D_ERR_UNSUPPORTED;
+    if (c->dtype == VLP4D_F64) return run_vslab<double, true, true, 4, 0, true>(c, map, a, cfg, s);
+    return run_vslab<float, true, true, 8, 0, true>(c, map, a, cfg, s);
   }
   if (c->dtype == VLP4D_F64) {
     if (do_vx && do_vy) VLP4D_VS(double, true, true, 4);
