@@ -54,42 +54,6 @@ __device__ __forceinline__ int wrap_col(int c, int nx) {
   return c >= nx ? c - nx : c;
 }
 
-// Four x-swept outputs from the twelve staged values t[0..11] starting at the
-// aligned column a0 = c0 + mx - r; output q uses t[r+q .. r+q+5].  r is the
-// same for the whole CTA (c0 is a multiple of 4), so the switch is uniform.
-template <int R_>
-__device__ __forceinline__ void x4_from(const double (&t)[12], const SweepW<double> &w, double (&o)[4]) {
-#pragma unroll
-  for (int q = 0; q < 4; ++q)
-    o[q] = interp6(w.w, t[R_ + q], t[R_ + q + 1], t[R_ + q + 2], t[R_ + q + 3], t[R_ + q + 4], t[R_ + q + 5]);
-}
-// FP32: outputs (0,1) and (2,3) as packed pairs; pair j of differences is
-// (d_j, d_{j+1}) with d_j = t[r+j+1] - t[r+j].
-template <int R_>
-__device__ __forceinline__ void x4_from(const float (&t)[12], const SweepW<float> &w, float (&o)[4]) {
-  float d[8];
-#pragma unroll
-  for (int j = 0; j < 8; ++j) d[j] = t[R_ + j + 1] - t[R_ + j];
-  float2 dp[7];
-#pragma unroll
-  for (int j = 0; j < 7; ++j) dp[j] = make_float2(d[j], d[j + 1]);
-  const float2 lo = interp_diff2(w.v, make_float2(t[R_ + 2], t[R_ + 3]), dp[0], dp[1], dp[2], dp[3], dp[4]);
-  const float2 hi = interp_diff2(w.v, make_float2(t[R_ + 4], t[R_ + 5]), dp[2], dp[3], dp[4], dp[5], dp[6]);
-  o[0] = lo.x;
-  o[1] = lo.y;
-  o[2] = hi.x;
-  o[3] = hi.y;
-}
-template <typename T>
-__device__ __forceinline__ void sweep_x4(const T (&t)[12], int r, const SweepW<T> &w, T (&o)[4]) {
-  switch (r) {
-    case 0: x4_from<0>(t, w, o); break;
-    case 1: x4_from<1>(t, w, o); break;
-    case 2: x4_from<2>(t, w, o); break;
-    default: x4_from<3>(t, w, o); break;
-  }
-}
-
 // Phase Y of one thread: RT outputs of its column quad from the RT+5 rows
 // starting at src (stride nx), written in streaming order so that only a
 // window of rows and differences is live; `emit(i, o)` receives row i.

@@ -172,6 +172,86 @@ __device__ void ens_planes(const EnsArgs &a, const EnsRun &R, const float *fin, 
     }
     __syncthreads();
     const float *b0 = bin[buf];
+    if (vec && (nx & 3) == 0) {
+      // Column quads (the planes' rows are multiples of four floats): three
+      // 16-byte taps per quad in x and six rows of quads in y, packed f32x2
+      // arithmetic, as the single-run plane pass does.
+      const int nq = nx >> 2;
+      for (int qd = threadIdx.x; qd < (cells >> 2); qd += blockDim.x) {
+        const int c = qd << 2;
+        const int p = c / nxy, qc = c - p * nxy;
+        const int ix0 = qc % nx, row = c - ix0;
+        const EnsLine &lx = xl[p0 + p];
+        int base = ix0 + lx.m;
+        base = base >= nx ? base - nx : base;
+        const int rr = base & 3;
+        int o[3];
+        o[0] = base - rr;
+        o[1] = o[0] + 4 >= nx ? o[0] + 4 - nx : o[0] + 4;
+        o[2] = o[1] + 4 >= nx ? o[1] + 4 - nx : o[1] + 4;
+        float t[12];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const float4 v = *reinterpret_cast<const float4 *>(b0 + row + o[k]);
+          t[4 * k] = v.x;
+          t[4 * k + 1] = v.y;
+          t[4 * k + 2] = v.z;
+          t[4 * k + 3] = v.w;
+        }
+        SweepW<float> w;
+        make_sweep_w(lx.v, w);
+        float out[4];
+        sweep_x4(t, rr, w, out);
+        *reinterpret_cast<float4 *>(b1 + c) = make_float4(out[0], out[1], out[2], out[3]);
+      }
+      __syncthreads();
+      SweepW<float> wy;
+      make_sweep_w(yl.v, wy);
+      const int my = yl.m;
+      for (int qi = threadIdx.x; qi < (nxy >> 2); qi += blockDim.x) {
+        const int iy = qi / nq, ix0 = (qi - iy * nq) << 2;
+        int rows[6];
+        int j = iy + my;
+        j = j >= ny ? j - ny : j;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          rows[k] = j * nx + ix0;
+          if (++j == ny) j = 0;
+        }
+        double s4[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) s4[q] = MOMENT ? acc[(qi << 2) + q] : 0.;
+        for (int p = 0; p < np; ++p) {
+          const float *pl = b1 + p * nxy;
+          float2 y[6][2];
+#pragma unroll
+          for (int k = 0; k < 6; ++k) {
+            const float4 v = *reinterpret_cast<const float4 *>(pl + rows[k]);
+            y[k][0] = make_float2(v.x, v.y);
+            y[k][1] = make_float2(v.z, v.w);
+          }
+          float2 o2[2];
+#pragma unroll
+          for (int h = 0; h < 2; ++h)
+            o2[h] = interp_diff2(wy.v, y[2][h], sub2(y[1][h], y[0][h]), sub2(y[2][h], y[1][h]), sub2(y[3][h], y[2][h]),
+                                 sub2(y[4][h], y[3][h]), sub2(y[5][h], y[4][h]));
+          *reinterpret_cast<float4 *>(fout + gbase + (long long)p * nxy + (qi << 2)) =
+              make_float4(o2[0].x, o2[0].y, o2[1].x, o2[1].y);
+          if (MOMENT) {
+            s4[0] += (double)o2[0].x;
+            s4[1] += (double)o2[0].y;
+            s4[2] += (double)o2[1].x;
+            s4[3] += (double)o2[1].y;
+          }
+        }
+        if (MOMENT) {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[(qi << 2) + q] = s4[q];
+        }
+      }
+      __syncthreads();
+      continue;
+    }
     for (int c = threadIdx.x; c < cells; c += blockDim.x) {
       const int p = c / nxy, qc = c - p * nxy;
       const int ix = qc % nx, row = c - ix;
