@@ -201,16 +201,18 @@ __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const 
   double gx = 0., gy = 0.;
   if (ixy < nxy && q > 0) {
     const long long vstride = nxy, ystride = (long long)nxy * nvx;
-    T wx[6], dx[6];
-    double wy[6], dy[6];
+    // Stencil sums in the element type (FP32 sums of FP32 data are
+    // accurate to ~1e-7 for a gradient); products with lb and the
+    // accumulation in FP64.
+    T wx[6], dx[6], wy[6], dy[6];
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
       wx[k] = (T)tvx.w[6 * (long long)ixy + k];
       dx[k] = (T)dwx[6 * (long long)ixy + k];
-      wy[k] = tvy.w[6 * (long long)ixy + k];
-      dy[k] = dwy[6 * (long long)ixy + k];
+      wy[k] = (T)tvy.w[6 * (long long)ixy + k];
+      dy[k] = (T)dwy[6 * (long long)ixy + k];
     }
-    int toff[V + 5];  // vx tap rows of this thread, times nothing yet
+    int toff[V + 5];  // vx tap rows of this thread
     {
       int j = vx0 + tvx.m[ixy];
       if (j >= nvx) j -= nvx;
@@ -225,15 +227,31 @@ __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const 
     T A[6][V], B[6][V];
     int row = (ivy0 + my) % nvy;
     const int nrows = q + 5;
+    // Loads run one row ahead: the taps of row r+1 and the adjoint values
+    // of the output row r+1-5 are in flight while row r is computed.
+    T t[V + 5], l[V];
+    {
+      const T *p = a + (long long)row * ystride + ixy;
+#pragma unroll
+      for (int k = 0; k < V + 5; ++k) t[k] = __ldg(p + (long long)toff[k] * vstride);
+    }
     for (int r0 = 0; r0 < nrows; r0 += 6) {
 #pragma unroll
       for (int u = 0; u < 6; ++u) {
         const int r = r0 + u;
         if (r >= nrows) break;
-        const T *p = a + (long long)row * ystride + ixy;
-        T t[V + 5];
+        if (++row == nvy) row = 0;
+        T tn[V + 5], ln[V];
+        if (r + 1 < nrows) {
+          const T *p = a + (long long)row * ystride + ixy;
 #pragma unroll
-        for (int k = 0; k < V + 5; ++k) t[k] = __ldg(p + (long long)toff[k] * vstride);
+          for (int k = 0; k < V + 5; ++k) tn[k] = __ldg(p + (long long)toff[k] * vstride);
+          if (r + 1 >= 5) {
+            const T *lp = lcol + (long long)(ivy0 + r - 4) * ystride;
+#pragma unroll
+            for (int i = 0; i < V; ++i) ln[i] = __ldg(lp + (long long)i * vstride);
+          }
+        }
 #pragma unroll
         for (int i = 0; i < V; ++i) {
           T sa = wx[0] * t[i], sb = dx[0] * t[i];
@@ -245,22 +263,23 @@ __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const 
           A[u][i] = sa;
           B[u][i] = sb;
         }
-        if (++row == nvy) row = 0;
         if (r >= 5) {
-          const T *lp = lcol + (long long)(ivy0 + r - 5) * ystride;
 #pragma unroll
           for (int i = 0; i < V; ++i) {
-            const double l = (double)__ldg(lp + (long long)i * vstride);
-            double sx = 0., sy = 0.;
+            T sx = wy[0] * B[(u + 1) % 6][i], sy = dy[0] * A[(u + 1) % 6][i];
 #pragma unroll
-            for (int k = 0; k < 6; ++k) {
-              sx = fma(wy[k], (double)B[(u + 1 + k) % 6][i], sx);
-              sy = fma(dy[k], (double)A[(u + 1 + k) % 6][i], sy);
+            for (int k = 1; k < 6; ++k) {
+              sx = fma(wy[k], B[(u + 1 + k) % 6][i], sx);
+              sy = fma(dy[k], A[(u + 1 + k) % 6][i], sy);
             }
-            gx = fma(l, sx, gx);
-            gy = fma(l, sy, gy);
+            gx = fma((double)l[i], (double)sx, gx);
+            gy = fma((double)l[i], (double)sy, gy);
           }
         }
+#pragma unroll
+        for (int k = 0; k < V + 5; ++k) t[k] = tn[k];
+#pragma unroll
+        for (int i = 0; i < V; ++i) l[i] = ln[i];
       }
     }
   }
