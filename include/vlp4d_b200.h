@@ -151,6 +151,19 @@ int vlp4d_check(vlp4d_ctx *ctx);
 /* Synchronous read of the diagnostic history entries [0, count); includes
  * vlp4d_check. */
 int vlp4d_diags_read(vlp4d_ctx *ctx, double *nrj, double *mass, int count);
+/* The vlp4d_mpi diagnostics (miniapps/vlp4d_mpi/thrust/Diags.cpp:17-92),
+ * kept beside the vlp4d ones.  vlp4d_diags_compute also records, for the
+ * same iteration, nrjx = sqrt(0.5 * sum Ex^2 * dx*dy) and
+ * nrjy = sqrt(0.5 * sum Ey^2 * dx*dy) (Diags.cpp:63-64; Kahan-compensated
+ * FP64 sums).  vlp4d_diags_l2norm records
+ * l2norm = sqrt(sum f^2 * dx*dy*dvx*dvy) of the device state fn
+ * (Diags::computeL2norm, Diags.cpp:68-92; Kahan-compensated FP64 sums in a
+ * fixed order, FP32 or FP64 f, 16-byte aligned).  vlp4d_diags_read_ext
+ * synchronises and copies the first `count` values of the three histories
+ * (any pointer may be NULL). */
+int vlp4d_diags_l2norm(vlp4d_ctx *ctx, const void *fn, int iter, void *stream);
+int vlp4d_diags_read_ext(vlp4d_ctx *ctx, double *nrjx, double *nrjy, double *l2norm, int count);
+
 /* Diags::save (diags.cpp:57-68): "t nrj mass" per iteration into `path`. */
 int vlp4d_diags_save(vlp4d_ctx *ctx, const char *path);
 

@@ -76,6 +76,9 @@ class Restatement:
             lib.orc_rfft2.argtypes = [C.c_int, C.c_int, _dp, _dp]
             lib.orc_irfft2.argtypes = [C.c_int, C.c_int, _dp, _dp]
             lib.orc_step.argtypes = [P, _dp, _dp, _dp, _dp, _dp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+            lib.orc_diags_mpi.argtypes = [P, _dp, _dp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+            lib.orc_l2norm.argtypes = [P, _dp]
+            lib.orc_l2norm.restype = C.c_double
             lib.orc_run.argtypes = [P, _dp, _dp, _dp, _dp, _dp, C.c_int, _dp, _dp]
             lib.orc_init_case.argtypes = [P, _dp, C.c_int, C.c_double, C.c_double, C.c_double]
             # FP64 discrete adjoint (vlp4d_adjoint.c).
@@ -157,6 +160,15 @@ class Restatement:
         self.L.orc_diags(C.byref(self.d), np.ascontiguousarray(rho), np.ascontiguousarray(ex),
                          np.ascontiguousarray(ey), C.byref(nrj), C.byref(mass))
         return nrj.value, mass.value
+
+    def diags_mpi(self, ex, ey):
+        """(nrjx, nrjy) of miniapps/vlp4d_mpi/thrust/Diags.cpp:63-64."""
+        a, b = C.c_double(), C.c_double()
+        self.L.orc_diags_mpi(C.byref(self.d), np.ascontiguousarray(ex), np.ascontiguousarray(ey), C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def l2norm(self, f):
+        return self.L.orc_l2norm(C.byref(self.d), np.ascontiguousarray(f, dtype=np.float64))
 
     def rfft2(self, a):
         ny, nx = a.shape

@@ -382,6 +382,28 @@ void orc_diags(const orc_domain *d, const double *rho, const double *ex, const d
   *mass = m * d->dx[0] * d->dx[1];
 }
 
+/* The vlp4d_mpi diagnostics, miniapps/vlp4d_mpi/thrust/Diags.cpp:17-66:
+ * nrjx = sqrt(0.5 * sum Ex^2 * dx * dy), nrjy likewise with Ey. */
+void orc_diags_mpi(const orc_domain *d, const double *ex, const double *ey, double *nrjx, double *nrjy) {
+  const size_t n2 = (size_t)d->n[0] * d->n[1];
+  double sx = 0., sy = 0.;
+  for (size_t i = 0; i < n2; ++i) {
+    sx += ex[i] * ex[i];
+    sy += ey[i] * ey[i];
+  }
+  *nrjx = sqrt(0.5 * sx * d->dx[0] * d->dx[1]);
+  *nrjy = sqrt(0.5 * sy * d->dx[0] * d->dx[1]);
+}
+
+/* Diags::computeL2norm, miniapps/vlp4d_mpi/thrust/Diags.cpp:68-92:
+ * sqrt(sum f^2 * dx * dy * dvx * dvy) over the whole (single-rank) grid. */
+double orc_l2norm(const orc_domain *d, const double *f) {
+  const size_t n = (size_t)d->n[0] * d->n[1] * d->n[2] * d->n[3];
+  double s = 0.;
+  for (size_t i = 0; i < n; ++i) s += f[i] * f[i];
+  return sqrt(s * d->dx[0] * d->dx[1] * d->dx[2] * d->dx[3]);
+}
+
 /* miniapps/vlp4d/openmp/timestep.hpp:11-55. */
 void orc_step(const orc_domain *d, double *fn, double *fnp1, double *rho, double *ex, double *ey,
               double *nrj, double *mass) {

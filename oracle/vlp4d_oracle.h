@@ -51,6 +51,9 @@ void orc_field_rho(const orc_domain *d, const double *fn, double *rho);
 void orc_field_poisson(const orc_domain *d, double *rho, double *ex, double *ey);
 void orc_diags(const orc_domain *d, const double *rho, const double *ex, const double *ey,
                double *nrj, double *mass);
+/* The vlp4d_mpi diagnostics (miniapps/vlp4d_mpi/thrust/Diags.cpp:17-92). */
+void orc_diags_mpi(const orc_domain *d, const double *ex, const double *ey, double *nrjx, double *nrjy);
+double orc_l2norm(const orc_domain *d, const double *f);
 
 /* rfft2 / irfft2 of a (nx1, nx2) layout_left real array; `hat` is
  * (nx1/2+1, nx2) complex, interleaved (re, im). */

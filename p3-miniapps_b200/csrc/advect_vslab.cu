@@ -390,7 +390,9 @@ bool vslab_config(const vlp4d_ctx *c, VslabCfg &cfg) {
   }
   if (nvx % cfg.V || nxy % cfg.C) return false;
   cfg.threads = cfg.C * (nvx / cfg.V);
-  if (cfg.threads > 512 || cfg.threads < 32) return false;
+  // Whole warps only: every warp releases each slab once, and the last of
+  // blockDim/32 releases refills it.
+  if (cfg.threads > 512 || cfg.threads < 32 || cfg.threads % 32) return false;
   // Q: the tallest vy segment (fewest halo re-reads) that still leaves at
   // least six items per SM.
   const long long nchunks = nxy / cfg.C;

@@ -78,6 +78,8 @@ void free_ctx(vlp4d_ctx *c) {
   cudaFree(c->ex_hat);
   cudaFree(c->ey_hat);
   cudaFree(c->nrj);
+  cudaFree(c->nrjx);
+  cudaFree(c->l2_part);
   cudaFree(c->mass);
   cudaFree(c->rho_part);
   cudaFree(c->d_err);
@@ -184,6 +186,11 @@ int vlp4d_ctx_create(const vlp4d_domain *dom, int dtype, vlp4d_ctx **out) {
   c->hist_len = dom->nbiter + 1;
   CTX_ALLOC(c->nrj, sizeof(double) * c->hist_len);
   CTX_ALLOC(c->mass, sizeof(double) * c->hist_len);
+  CTX_ALLOC(c->nrjx, sizeof(double) * 3 * c->hist_len);
+  c->nrjy = c->nrjx + c->hist_len;
+  c->l2norm = c->nrjy + c->hist_len;
+  c->l2_blocks = 2 * c->num_sms;
+  CTX_ALLOC(c->l2_part, sizeof(double) * 2 * c->l2_blocks);
   // Enough (column block, plane group) blocks to fill the GPU a few times.
   long long groups = ((long long)c->num_sms * 8 * 256 + nxy - 1) / nxy;
   if (groups > c->g.nv()) groups = c->g.nv();
@@ -213,6 +220,7 @@ int vlp4d_ctx_create(const vlp4d_domain *dom, int dtype, vlp4d_ctx **out) {
       cudaMemset(c->ey, 0, sizeof(double) * nxy) != cudaSuccess ||
       cudaMemset(c->nrj, 0, sizeof(double) * c->hist_len) != cudaSuccess ||
       cudaMemset(c->mass, 0, sizeof(double) * c->hist_len) != cudaSuccess ||
+      cudaMemset(c->nrjx, 0, sizeof(double) * 3 * c->hist_len) != cudaSuccess ||
       cudaMemset(c->d_err, 0, sizeof(int)) != cudaSuccess)
     return bail(fail(VLP4D_ERR_CUDA, "cudaMemset failed"));
   // lib/Cuda_FFT.hpp:108-114: cufftPlan2d(nx2 = ny, nx1 = nx) on x-fastest data.
@@ -391,6 +399,25 @@ int vlp4d_diags_read(vlp4d_ctx *ctx, double *nrj, double *mass, int count) {
   if ((rc = vlp4d_check(ctx))) return rc;
   if (nrj) VLP4D_CUDA_TRY(cudaMemcpy(nrj, ctx->nrj, sizeof(double) * count, cudaMemcpyDeviceToHost));
   if (mass) VLP4D_CUDA_TRY(cudaMemcpy(mass, ctx->mass, sizeof(double) * count, cudaMemcpyDeviceToHost));
+  return VLP4D_OK;
+}
+
+int vlp4d_diags_l2norm(vlp4d_ctx *ctx, const void *fn, int iter, void *stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (!fn) return fail(VLP4D_ERR_INVALID_ARG, "fn is NULL");
+  if (iter < 0 || iter >= ctx->hist_len) return fail(VLP4D_ERR_INVALID_ARG, "iter outside [0, nbiter]");
+  return launch_l2norm(ctx, fn, iter, as_stream(stream));
+}
+
+int vlp4d_diags_read_ext(vlp4d_ctx *ctx, double *nrjx, double *nrjy, double *l2norm, int count) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (count < 0 || count > ctx->hist_len) return fail(VLP4D_ERR_INVALID_ARG, "count outside [0, nbiter+1]");
+  if ((rc = vlp4d_check(ctx))) return rc;
+  if (nrjx) VLP4D_CUDA_TRY(cudaMemcpy(nrjx, ctx->nrjx, sizeof(double) * count, cudaMemcpyDeviceToHost));
+  if (nrjy) VLP4D_CUDA_TRY(cudaMemcpy(nrjy, ctx->nrjy, sizeof(double) * count, cudaMemcpyDeviceToHost));
+  if (l2norm) VLP4D_CUDA_TRY(cudaMemcpy(l2norm, ctx->l2norm, sizeof(double) * count, cudaMemcpyDeviceToHost));
   return VLP4D_OK;
 }
 

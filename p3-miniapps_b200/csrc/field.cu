@@ -110,38 +110,85 @@ __device__ __forceinline__ void kahan_add(double &sum, double &c, double x) {
 
 __global__ void k_diags(const double *__restrict__ rho, const double *__restrict__ ex, const double *__restrict__ ey,
                         long long n, double dx, double dy, double *__restrict__ nrj_hist,
-                        double *__restrict__ mass_hist, int iter) {
-  double sm = 0., cm = 0., se = 0., ce = 0.;
+                        double *__restrict__ mass_hist, double *__restrict__ nrjx_hist,
+                        double *__restrict__ nrjy_hist, int iter) {
+  // Kahan sums of rho, Ex^2 + Ey^2, Ex^2, Ey^2.
+  double s[4] = {0., 0., 0., 0.}, c[4] = {0., 0., 0., 0.};
   for (long long i = threadIdx.x; i < n; i += blockDim.x) {
-    kahan_add(sm, cm, rho[i]);
     const double a = ex[i], b = ey[i];
-    kahan_add(se, ce, __dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)));
+    const double ax = __dmul_rn(a, a), by = __dmul_rn(b, b);
+    kahan_add(s[0], c[0], rho[i]);
+    kahan_add(s[1], c[1], __dadd_rn(ax, by));
+    kahan_add(s[2], c[2], ax);
+    kahan_add(s[3], c[3], by);
   }
-  sm -= cm;
-  se -= ce;
-  for (int o = 16; o > 0; o >>= 1) {
-    sm += __shfl_down_sync(0xffffffffu, sm, o);
-    se += __shfl_down_sync(0xffffffffu, se, o);
-  }
-  __shared__ double wm[32], we[32];
+  __shared__ double ws[4][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) { wm[warp] = sm; we[warp] = se; }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    double v = s[k] - c[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) ws[k][warp] = v;
+  }
   __syncthreads();
   if (warp == 0) {
     const int nw = (blockDim.x + 31) >> 5;
-    sm = lane < nw ? wm[lane] : 0.;
-    se = lane < nw ? we[lane] : 0.;
-    for (int o = 16; o > 0; o >>= 1) {
-      sm += __shfl_down_sync(0xffffffffu, sm, o);
-      se += __shfl_down_sync(0xffffffffu, se, o);
+    double v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      v[k] = lane < nw ? ws[k][lane] : 0.;
+      for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
     }
     if (lane == 0) {
-      double e = sqrt(se * dx * dy);
+      double e = sqrt(v[1] * dx * dy);
       e = e > 1.e-30 ? log(e) : -1.e9;
       nrj_hist[iter] = e;
-      mass_hist[iter] = sm * dx * dy;
+      mass_hist[iter] = v[0] * dx * dy;
+      // miniapps/vlp4d_mpi/thrust/Diags.cpp:63-64.
+      nrjx_hist[iter] = sqrt(0.5 * v[2] * dx * dy);
+      nrjy_hist[iter] = sqrt(0.5 * v[3] * dx * dy);
     }
   }
+}
+
+// ---- L2 norm of f (miniapps/vlp4d_mpi/thrust/Diags.cpp:68-92):
+// l2norm = sqrt(sum f^2 * dx dy dvx dvy).  Each block keeps Kahan sums per
+// thread (grid-stride, 16-byte loads), reduces them in a fixed order and
+// writes one (sum, compensation) pair; one block adds the pairs in order.
+template <typename T>
+__global__ void k_l2_partial(const T *__restrict__ f, long long n, double *__restrict__ part) {
+  double sum = 0., comp = 0.;
+  const long long n4 = n / 4;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
+    T v[4];
+    load4(f + 4 * i, v);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) kahan_add(sum, comp, (double)v[k] * (double)v[k]);
+  }
+  if (blockIdx.x == 0)
+    for (long long i = 4 * n4 + threadIdx.x; i < n; i += blockDim.x) kahan_add(sum, comp, (double)f[i] * (double)f[i]);
+  __shared__ double ws[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double v = sum - comp;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if (lane == 0) ws[warp] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s2 = 0., c2 = 0.;
+    for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) kahan_add(s2, c2, ws[w]);
+    part[2 * blockIdx.x] = s2;
+    part[2 * blockIdx.x + 1] = c2;
+  }
+}
+
+__global__ void k_l2_finish(const double *__restrict__ part, int blocks, double scale, double *__restrict__ out) {
+  if (threadIdx.x != 0) return;
+  double s = 0., c = 0.;
+  for (int b = 0; b < blocks; ++b) {
+    kahan_add(s, c, part[2 * b]);
+    kahan_add(s, c, -part[2 * b + 1]);
+  }
+  *out = sqrt((s - c) * scale);
 }
 
 // ---- initcase.
@@ -263,7 +310,22 @@ int launch_field_poisson(vlp4d_ctx *c, cudaStream_t s) {
 }
 
 int launch_diags(vlp4d_ctx *c, int iter, cudaStream_t s) {
-  k_diags<<<1, 1024, 0, s>>>(c->rho, c->ex, c->ey, c->g.nxy(), c->g.dx[0], c->g.dx[1], c->nrj, c->mass, iter);
+  k_diags<<<1, 1024, 0, s>>>(c->rho, c->ex, c->ey, c->g.nxy(), c->g.dx[0], c->g.dx[1], c->nrj, c->mass, c->nrjx,
+                             c->nrjy, iter);
+  VLP4D_LAUNCH_CHECK();
+  return VLP4D_OK;
+}
+
+int launch_l2norm(vlp4d_ctx *c, const void *fn, int iter, cudaStream_t s) {
+  const long long n = c->g.cells();
+  if ((uintptr_t)fn % 16) return fail_msg(VLP4D_ERR_INVALID_ARG, "diags_l2norm: f must be 16-byte aligned");
+  if (c->dtype == VLP4D_F64)
+    k_l2_partial<double><<<c->l2_blocks, 512, 0, s>>>((const double *)fn, n, c->l2_part);
+  else
+    k_l2_partial<float><<<c->l2_blocks, 512, 0, s>>>((const float *)fn, n, c->l2_part);
+  VLP4D_LAUNCH_CHECK();
+  const double scale = c->g.dx[0] * c->g.dx[1] * c->g.dx[2] * c->g.dx[3];
+  k_l2_finish<<<1, 32, 0, s>>>(c->l2_part, c->l2_blocks, scale, c->l2norm + iter);
   VLP4D_LAUNCH_CHECK();
   return VLP4D_OK;
 }

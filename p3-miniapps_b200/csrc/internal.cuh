@@ -91,6 +91,12 @@ struct vlp4d_ctx {
 
   // Diagnostics history (nbiter+1 entries each) and the reduction scratch.
   double *nrj = nullptr, *mass = nullptr;
+  // The vlp4d_mpi diagnostics (miniapps/vlp4d_mpi/thrust/Diags.cpp:17-92):
+  // per-component field energies and the L2 norm of f, one slot per iteration.
+  double *nrjx = nullptr, *nrjy = nullptr, *l2norm = nullptr;
+  // L2-norm partial sums (Kahan pairs, one per block of k_l2_partial).
+  double *l2_part = nullptr;
+  int l2_blocks = 0;
   int hist_len = 0;
 
   // Moment partials: rho_part_groups x nxy FP64.  The generic reduction
@@ -175,6 +181,7 @@ int launch_field_rho(vlp4d_ctx *c, const void *fn, cudaStream_t s);
 int launch_rho_finish(vlp4d_ctx *c, int groups, cudaStream_t s);
 int launch_field_poisson(vlp4d_ctx *c, cudaStream_t s);
 int launch_diags(vlp4d_ctx *c, int iter, cudaStream_t s);
+int launch_l2norm(vlp4d_ctx *c, const void *fn, int iter, cudaStream_t s);
 int launch_init_case(vlp4d_ctx *c, void *f, int ic, double amp, double k, double u, cudaStream_t s);
 int launch_transpose(const void *in, void *out, int rows, int cols, int elem, cudaStream_t s);
 int launch_wait_selftest(vlp4d_ctx *c, long long limit, cudaStream_t s);

@@ -37,7 +37,7 @@ EXPORTS = (
     "vlp4d_step_adjoint", "vlp4d_energy_grad",
     "vlp4d_ensemble_create", "vlp4d_ensemble_destroy", "vlp4d_ensemble_run", "vlp4d_ensemble_check",
     "vlp4d_ensemble_read", "vlp4d_ensemble_cells", "vlp4d_ensemble_set_tiles", "vlp4d_ensemble_get_tiles",
-    "vlp4d_ensemble_autotune", "vlp4d_selftest_wait_timeout",
+    "vlp4d_ensemble_autotune", "vlp4d_selftest_wait_timeout", "vlp4d_diags_l2norm", "vlp4d_diags_read_ext",
 )
 
 
@@ -127,6 +127,8 @@ def lib() -> C.CDLL:
         L.vlp4d_ensemble_get_tiles.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
         L.vlp4d_ensemble_autotune.argtypes = [vp, i, C.c_char_p, vp]
         L.vlp4d_selftest_wait_timeout.argtypes = [vp, C.c_longlong, vp]
+        L.vlp4d_diags_l2norm.argtypes = [vp, vp, i, vp]
+        L.vlp4d_diags_read_ext.argtypes = [vp, dp, dp, dp, i]
         for n in EXPORTS:
             if n not in ("vlp4d_last_error", "vlp4d_kernel_launches", "vlp4d_ensemble_cells"):
                 getattr(L, n).restype = C.c_int
@@ -315,6 +317,18 @@ class Context:
         mass = (C.c_double * max(count, 1))()
         _check(lib().vlp4d_diags_read(self.h, nrj, mass, count))
         return np.array(nrj[:count]), np.array(mass[:count])
+
+    def diags_l2norm(self, fn, it, stream=None):
+        _check(lib().vlp4d_diags_l2norm(self.h, self._f(fn), it, _stream_ptr(stream)))
+
+    def diags_read_ext(self, count=None):
+        """(nrjx, nrjy, l2norm) histories, the vlp4d_mpi diagnostics."""
+        import numpy as np
+
+        count = self.dom.nbiter + 1 if count is None else count
+        bufs = [(C.c_double * max(count, 1))() for _ in range(3)]
+        _check(lib().vlp4d_diags_read_ext(self.h, bufs[0], bufs[1], bufs[2], count))
+        return tuple(np.array(b[:count]) for b in bufs)
 
     def diags_save(self, path):
         _check(lib().vlp4d_diags_save(self.h, str(path).encode()))

@@ -116,8 +116,11 @@ def test_fused_moment_matches_generic_moment(pkg, cuda):
             assert abs(na[1] - nb[1]) < tol and abs(ma[1] - mb[1]) < tol
 
 
-def test_fused_only_mode_rejects_unsupported_shape(pkg, cuda):
-    dom = _dom(pkg, (12, 10, 14, 10))  # nvx = 14: no v-slab configuration
+@pytest.mark.parametrize("n", [(12, 10, 14, 10), (16, 12, 20, 16)])
+def test_fused_only_mode_rejects_unsupported_shape(pkg, cuda, n):
+    # nvx = 14: no v-slab configuration; nvx = 20 in FP64: 16 columns x 5
+    # row groups = 80 threads, not whole warps.
+    dom = _dom(pkg, n)
     with _ctx(pkg, dom, "f64", "fused") as ctx:
         f, g = ctx.empty_f(), ctx.empty_f()
         ctx.init_case(f, IC_LANDAU_SUM)

@@ -158,3 +158,19 @@ def test_reference_and_restatement_agree_live():
     f, nrj, mass, _, _ = R.run(f0, 3)
     assert np.abs(F.get_f(0) - f).max() < 1e-14
     assert np.abs(d[:, 1] - nrj).max() < 1e-12
+
+
+def test_mpi_diagnostics_restatement():
+    """orc_diags_mpi / orc_l2norm against their definitions
+    (miniapps/vlp4d_mpi/thrust/Diags.cpp:63-64, 68-92)."""
+    L = 4 * np.pi
+    o = Restatement((8, 6, 10, 8), [0, 0, -6, -6], [L, L, 6, 6], 0.125, 110)
+    rng = np.random.default_rng(2)
+    ex, ey = rng.normal(size=o.shape2), rng.normal(size=o.shape2)
+    f = rng.normal(size=o.shape4)
+    dx = o.dx
+    nx, ny = o.diags_mpi(ex, ey)
+    assert abs(nx - np.sqrt(0.5 * (ex ** 2).sum() * dx[0] * dx[1])) < 1e-14 * nx
+    assert abs(ny - np.sqrt(0.5 * (ey ** 2).sum() * dx[0] * dx[1])) < 1e-14 * ny
+    l2 = o.l2norm(f)
+    assert abs(l2 - np.sqrt((f ** 2).sum() * np.prod(dx))) < 1e-13 * l2

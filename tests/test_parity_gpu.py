@@ -317,3 +317,32 @@ def test_invalid_iter_rejected(pkg, cuda):
         f = ctx.empty_f()
         with pytest.raises(pkg.vlp4d.Vlp4dError):
             ctx.step(f, f, 1)
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_mpi_diagnostics_match_oracle(pkg, cuda, dtype):
+    """nrjx/nrjy (recorded by vlp4d_diags_compute) and the L2 norm of f
+    (vlp4d_diags_l2norm) against the oracle's restatement of the vlp4d_mpi
+    diagnostics, over three fused steps."""
+    torch = cuda
+    n, nsteps = (16, 12, 20, 16), 3
+    dom = pkg.Domain(list(n), [0.0, 0.0, -6.0, -6.0], [4 * np.pi, 4 * np.pi, 6.0, 6.0], 0.125, nsteps, 110)
+    ora = Restatement(dom.nxmax, dom.min_phy, dom.max_phy, dom.dt, 110)
+    v = pkg.vlp4d
+    with pkg.Context(dom, dtype) as ctx:
+        a, b = ctx.empty_f(), ctx.empty_f()
+        ctx.init_case(a, v.IC_LANDAU_SUM, 0.05, 0.5)
+        ctx.field_rho(a)
+        ctx.field_poisson()
+        ctx.diags_compute(0)
+        ctx.diags_l2norm(a, 0)
+        ref = [(ora.diags_mpi(ctx.ex.cpu().numpy(), ctx.ey.cpu().numpy()), ora.l2norm(a.double().cpu().numpy()))]
+        for it in range(1, nsteps + 1):
+            ctx.step(a, b, it)
+            ctx.diags_l2norm(b, it)
+            ref.append((ora.diags_mpi(ctx.ex.cpu().numpy(), ctx.ey.cpu().numpy()), ora.l2norm(b.double().cpu().numpy())))
+            a, b = b, a
+        nrjx, nrjy, l2 = ctx.diags_read_ext(nsteps + 1)
+    for it, ((rx, ry), rl) in enumerate(ref):
+        assert abs(nrjx[it] - rx) <= 1e-13 * rx and abs(nrjy[it] - ry) <= 1e-13 * ry, it
+        assert abs(l2[it] - rl) <= 1e-13 * rl, it
