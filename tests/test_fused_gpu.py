@@ -233,3 +233,35 @@ def test_advect_xyxy_matches_two_xy_passes(pkg, cuda, n, dtype):
             assert float((rho_one - rho_sep).abs().max()) <= (1e-13 if dtype == "f64" else 1e-6) * float(
                 rho_sep.abs().max())
             ctx.check()
+
+
+# Odd shapes: thin planes (ny below the stencil span), row widths that are
+# not powers of two (runtime-width paths), vx extents that give partial or
+# no v-slab configurations, tiny vy extents.
+ODD_SHAPES = [(4, 3, 8, 2), (8, 5, 12, 6), (12, 7, 24, 11), (20, 9, 40, 6), (36, 6, 16, 9), (24, 16, 8, 3)]
+
+
+@pytest.mark.parametrize("n", ODD_SHAPES)
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_odd_shapes_default_path_matches_generic(pkg, cuda, n, dtype):
+    """Two steps and a two-step time loop on the default path (fused kernels
+    where the shape allows, generic otherwise) against the generic kernels."""
+    torch = cuda
+    dom = pkg.Domain(list(n), [0.0, 0.0, -6.0, -6.0], [4 * np.pi, 4 * np.pi, 6.0, 6.0], 0.125, 4, 110)
+    res = {}
+    for kernels in ("", "generic"):
+        with _ctx(pkg, dom, dtype, kernels) as ctx:
+            f0 = ctx.empty_f()
+            ctx.init_case(f0, IC_LANDAU_SUM, 0.05, 0.5)
+            ctx.field_rho(f0)
+            ctx.field_poisson()
+            a, b = f0.clone(), ctx.empty_f()
+            ctx.step(a, b, 1)
+            ctx.step(b, a, 2)
+            c, d = f0.clone(), ctx.empty_f()
+            ctx.steps(c, d, 1, 2)
+            ctx.check()
+            res[kernels] = (a.clone(), d.clone())
+    tol = 1e-12 if dtype == "f64" else 2e-6
+    assert _rel(res[""][0], res["generic"][0]) < tol
+    assert _rel(res[""][1], res["generic"][1]) < tol
