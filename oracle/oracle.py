@@ -5,6 +5,13 @@
 * ``Reference`` wraps ``oracle/_ref/libvlp4d_ref.so``: the reference's own
   OpenMP vlp4d (miniapps/vlp4d/openmp) compiled from its sources by
   oracle/Makefile, driven through oracle/ref_driver.cpp.
+* ``MpiRestatement`` wraps the restatement of the one-process vlp4d_mpi
+  step (vlp4d_mpi_oracle.c, in the same library as ``Restatement``);
+  ``MpiReference`` wraps ``oracle/_ref/libvlp4d_mpi_ref.so``, the
+  reference's own OpenMP vlp4d_mpi (miniapps/vlp4d_mpi/openmp) driven
+  through oracle/ref_mpi_driver.cpp.  Their 4D arrays are the reference's
+  halo-extended views: numpy shape (nvy+6, nvx+6, ny+6, nx+6), index 3 is
+  grid point 0.
 
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
 this module; the CUDA library never does.  Arrays are numpy float64 in the
@@ -25,8 +32,11 @@ HERE = Path(__file__).resolve().parent
 RESTATEMENT_SO = HERE / "_build" / "liboracle_vlp4d.so"
 REFERENCE_SO = HERE / "_ref" / "libvlp4d_ref.so"
 REFERENCE_EXE = HERE / "_ref" / "vlp4d_ref"
+MPI_REFERENCE_SO = HERE / "_ref" / "libvlp4d_mpi_ref.so"
+HALO = 3
 
 IC_CYL02, IC_CYL05, IC_SLD10, IC_TSI20, IC_LANDAU_SUM, IC_TWO_STREAM = 2, 5, 10, 20, 110, 120
+IC_TSI20_MPI = 21
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 
@@ -91,6 +101,22 @@ class Restatement:
             lib.orc_energy_grad.argtypes = [P, _dp, C.POINTER(C.c_double), _dp]
             lib.orc_step_adjoint.argtypes = [P, _dp, _dp, _dp]
             lib.orc_adjoint_run.argtypes = [P, _dp, C.c_int, C.POINTER(C.c_double), _dp]
+            # One-process vlp4d_mpi step (vlp4d_mpi_oracle.c).
+            lib.orcm_size.argtypes = [P]
+            lib.orcm_size.restype = C.c_size_t
+            for name in ("orcm_halo_fill", "orcm_spline_xy", "orcm_spline_vxvy"):
+                getattr(lib, name).argtypes = [P, _dp]
+            lib.orcm_advect_2d.argtypes = [P, _dp, _dp, C.c_double]
+            lib.orcm_advect_2d.restype = C.c_int
+            lib.orcm_advect_4d.argtypes = [P, _dp, _dp, _dp, _dp]
+            lib.orcm_advect_4d.restype = C.c_int
+            lib.orcm_field_rho.argtypes = [P, _dp, _dp]
+            lib.orcm_l2norm.argtypes = [P, _dp]
+            lib.orcm_l2norm.restype = C.c_double
+            lib.orcm_start.argtypes = [P, _dp, _dp, _dp, _dp, _dp]
+            lib.orcm_step.argtypes = [P, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
+            lib.orcm_step.restype = C.c_int
+            lib.orcm_init_case.argtypes = [P, _dp, C.c_int]
             cls._lib = lib
         return cls._lib
 
@@ -402,3 +428,212 @@ class Reference:
         out = np.zeros((nb, ny, nx))
         L.ref_irfft2(nx, ny, nb, src, out)
         return out
+
+
+def interior(fh):
+    """The grid points of a halo-extended array (a view)."""
+    return fh[HALO:-HALO, HALO:-HALO, HALO:-HALO, HALO:-HALO]
+
+
+class MpiRestatement(Restatement):
+    """The plain-C restatement of the one-process vlp4d_mpi step."""
+
+    def __init__(self, n, minp, maxp, dt, idcase=10):
+        super().__init__(n, minp, maxp, dt, idcase)
+        self.hshape4 = tuple(v + 2 * HALO for v in self.shape4)
+
+    def empty_halo(self):
+        return np.zeros(self.hshape4, dtype=np.float64)
+
+    def init_halo(self, ic):
+        fh = self.empty_halo()
+        self.L.orcm_init_case(C.byref(self.d), fh, ic)
+        return fh
+
+    def halo_fill(self, fh):
+        out = np.array(fh, dtype=np.float64, copy=True)
+        self.L.orcm_halo_fill(C.byref(self.d), out)
+        return out
+
+    def spline_xy(self, fh):
+        out = np.array(fh, dtype=np.float64, copy=True)
+        self.L.orcm_spline_xy(C.byref(self.d), out)
+        return out
+
+    def spline_vxvy(self, fh):
+        out = np.array(fh, dtype=np.float64, copy=True)
+        self.L.orcm_spline_vxvy(C.byref(self.d), out)
+        return out
+
+    def advect_2d(self, coef, dt):
+        """(values on the interior + coef's halo, out-of-range count)."""
+        out = np.array(coef, dtype=np.float64, copy=True)
+        tmp = self.empty_halo()
+        err = self.L.orcm_advect_2d(C.byref(self.d), out, tmp, dt)
+        return out, err
+
+    def advect_4d(self, coef, ex, ey):
+        out = np.array(coef, dtype=np.float64, copy=True)
+        tmp = self.empty_halo()
+        err = self.L.orcm_advect_4d(C.byref(self.d), np.ascontiguousarray(ex), np.ascontiguousarray(ey), out, tmp)
+        return out, err
+
+    def field_rho_halo(self, fh):
+        rho = self.empty2()
+        self.L.orcm_field_rho(C.byref(self.d), np.ascontiguousarray(fh), rho)
+        return rho
+
+    def l2norm_halo(self, fh):
+        return float(self.L.orcm_l2norm(C.byref(self.d), np.ascontiguousarray(fh)))
+
+    def start(self, fh):
+        """Initial field and diagnostics: (phi, ex, ey, [nrj, nrjx, nrjy, mass, l2norm])."""
+        rho, ex, ey = self.empty2(), self.empty2(), self.empty2()
+        out = np.zeros(5)
+        self.L.orcm_start(C.byref(self.d), np.ascontiguousarray(fh), rho, ex, ey, out)
+        return rho, ex, ey, out
+
+    def step_mpi(self, fh):
+        """One step: (new state, ex, ey, half-step diags[4], end diags[5], out-of-range count)."""
+        fn = np.array(fh, dtype=np.float64, copy=True)
+        fnp1, tmp = self.empty_halo(), self.empty_halo()
+        rho, ex, ey = self.empty2(), self.empty2(), self.empty2()
+        half, out = np.zeros(4), np.zeros(5)
+        err = self.L.orcm_step(C.byref(self.d), fn, fnp1, tmp, rho, ex, ey, half, out)
+        return fn, ex, ey, half, out, err
+
+    def run_mpi(self, fh, nsteps):
+        """Initial solve + nsteps steps: (state, diags[nsteps+1, 5], ex, ey)."""
+        f = np.array(fh, dtype=np.float64, copy=True)
+        _, ex, ey, out = self.start(f)
+        rows = [out]
+        for _ in range(nsteps):
+            f, ex, ey, _, out, err = self.step_mpi(f)
+            if err:
+                raise RuntimeError("time step too large for the interpolation range")
+            rows.append(out)
+        return f, np.array(rows), ex, ey
+
+
+class MpiReference:
+    """The reference's own OpenMP vlp4d_mpi as one process (oracle/_ref)."""
+
+    _lib = None
+
+    @classmethod
+    def available(cls) -> bool:
+        return MPI_REFERENCE_SO.exists()
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            lib = C.CDLL(str(MPI_REFERENCE_SO))
+            lib.refm_create.restype = C.c_void_p
+            lib.refm_create.argtypes = [C.c_int * 4, C.c_double * 4, C.c_double * 4, C.c_double, C.c_int, C.c_int]
+            lib.refm_destroy.argtypes = [C.c_void_p]
+            for name in ("refm_set_f", "refm_get_f", "refm_set_field", "refm_get_field"):
+                getattr(lib, name).argtypes = [C.c_void_p, C.c_int, _dp]
+            for name in ("refm_initcase", "refm_exchange_halo", "refm_spline_xy", "refm_spline_vxvy",
+                         "refm_field", "refm_l2norm"):
+                getattr(lib, name).argtypes = [C.c_void_p, C.c_int] + ([C.c_int] if name == "refm_l2norm" else [])
+            lib.refm_advect_2d.argtypes = [C.c_void_p, C.c_int, C.c_double]
+            lib.refm_advect_4d.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double]
+            lib.refm_diags.argtypes = [C.c_void_p, C.c_int]
+            lib.refm_diags_save.argtypes = [C.c_void_p, C.c_char_p]
+            lib.refm_onetimestep.argtypes = [C.c_void_p, C.c_int]
+            lib.refm_run.argtypes = [C.c_void_p, C.c_int]
+            lib.refm_timer_seconds.restype = C.c_double
+            lib.refm_timer_seconds.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+            lib.refm_reset_timers.argtypes = [C.c_void_p]
+            lib.refm_max_threads.restype = C.c_int
+            cls._lib = lib
+        return cls._lib
+
+    TIMERS = ("total", "MainLoop", "pack", "comm", "unpack", "advec2D", "advec4D", "field", "all_reduce",
+              "Fourier", "diag", "splinecoeff_xy", "splinecoeff_vxvy")
+
+    def __init__(self, n, minp, maxp, dt, nbiter, idcase=10):
+        self.L = self.lib()
+        self.n = tuple(int(v) for v in n)
+        self.hshape4 = (self.n[3] + 2 * HALO, self.n[2] + 2 * HALO, self.n[1] + 2 * HALO, self.n[0] + 2 * HALO)
+        self.shape2 = (self.n[1], self.n[0])
+        self.nbiter = nbiter
+        self.h = self.L.refm_create(_c_arr(C.c_int, n), _c_arr(C.c_double, minp), _c_arr(C.c_double, maxp),
+                                    dt, nbiter, idcase)
+
+    def close(self):
+        if self.h:
+            self.L.refm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_f(self, which, fh):
+        self.L.refm_set_f(self.h, which, np.ascontiguousarray(fh, dtype=np.float64))
+
+    def get_f(self, which):
+        out = np.zeros(self.hshape4)
+        self.L.refm_get_f(self.h, which, out)
+        return out
+
+    def set_field(self, which, a):
+        self.L.refm_set_field(self.h, which, np.ascontiguousarray(a, dtype=np.float64))
+
+    def get_field(self, which):
+        out = np.zeros(self.shape2)
+        self.L.refm_get_field(self.h, which, out)
+        return out
+
+    def exchange_halo(self, which=0):
+        self.L.refm_exchange_halo(self.h, which)
+
+    def spline_xy(self, which=0):
+        self.L.refm_spline_xy(self.h, which)
+
+    def spline_vxvy(self, which=0):
+        self.L.refm_spline_vxvy(self.h, which)
+
+    def advect_2d(self, which, dt):
+        self.L.refm_advect_2d(self.h, which, dt)
+
+    def advect_4d(self, dst, src, dt):
+        self.L.refm_advect_4d(self.h, dst, src, dt)
+
+    def field(self, which=0):
+        self.L.refm_field(self.h, which)
+
+    def diags_compute(self, it):
+        self.L.refm_diags(self.h, it)
+
+    def l2norm(self, which, it):
+        self.L.refm_l2norm(self.h, which, it)
+
+    def diags(self):
+        """(nrj.out rows (t, nrj, nrjx, nrjy, mass), l2norm.out rows (t, l2norm)), nbiter+1 rows each."""
+        with tempfile.TemporaryDirectory() as d:
+            rc = self.L.refm_diags_save(self.h, d.encode())
+            if rc != 0:
+                raise RuntimeError(f"refm_diags_save failed ({rc})")
+            return (np.loadtxt(os.path.join(d, "nrj.out"), ndmin=2),
+                    np.loadtxt(os.path.join(d, "l2norm.out"), ndmin=2))
+
+    def onetimestep(self, it):
+        self.L.refm_onetimestep(self.h, it)
+
+    def run(self, nsteps):
+        self.L.refm_run(self.h, nsteps)
+
+    def timers(self):
+        out = {}
+        for i, name in enumerate(self.TIMERS):
+            calls = C.c_int()
+            s = self.L.refm_timer_seconds(self.h, i, C.byref(calls))
+            out[name] = (s, calls.value)
+        return out
+
+    def reset_timers(self):
+        self.L.refm_reset_timers(self.h)

@@ -428,6 +428,8 @@ void orc_run(const orc_domain *d, double *fn, double *fnp1, double *rho, double 
 }
 
 /* Initial conditions.  SLD10: init.cpp:237-258; TSI20: init.cpp:261-288;
+ * TSI20_MPI: miniapps/vlp4d_mpi/openmp/Init.cpp:249-277 (SLD10 there is
+ * the same function as here);
  * CYL02/CYL05: init.cpp:146-234.  LANDAU_SUM and TWO_STREAM are the
  * perturbed Maxwellians of the benchmark configurations (amplitude amp,
  * wave number k, beam speed u). */
@@ -453,6 +455,12 @@ void orc_init_case(const orc_domain *d, double *f, int ic, double amp, double k,
               const double sum = vx * vx + vy * vy;
               val = (1 + alpha * (cos(0.5 * x))) * 1 / (2 * ORC_PI) * ((2 - 2 * xi) / (3 - 2 * xi)) *
                     (1 + .5 * vx * vx / (1 - xi)) * exp(-.5 * sum);
+            } break;
+            case ORC_IC_TSI20_MPI: {
+              const double vd = 2.4, vthx = 1.0, vthy = 0.5, ax = 0.05, ay = 0.25, kx = 0.2, ky = 0.2;
+              val = 1. / (4 * ORC_PI * vthx * vthy) * (1 - ax * sin(kx * x) - ay * sin(ky * y)) *
+                    (exp(-.5 * (pow((vx - vd) / vthx, 2) + pow(vy / vthy, 2))) +
+                     exp(-.5 * (pow((vx + vd) / vthx, 2) + pow(vy / vthy, 2))));
             } break;
             case ORC_IC_CYL02:
             case ORC_IC_CYL05: {

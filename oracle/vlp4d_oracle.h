@@ -13,6 +13,8 @@
 #ifndef VLP4D_ORACLE_H
 #define VLP4D_ORACLE_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -33,6 +35,7 @@ enum {
   ORC_IC_CYL05 = 5,
   ORC_IC_SLD10 = 10,          /* (1+a cos(kx x) cos(ky y)) M(vx) M(vy), a=0.05, k=0.5 */
   ORC_IC_TSI20 = 20,
+  ORC_IC_TSI20_MPI = 21,      /* vlp4d_mpi's case 20 (miniapps/vlp4d_mpi/openmp/Init.cpp:249-277) */
   ORC_IC_LANDAU_SUM = 110,    /* (1+a cos(k x)+a cos(k y)) M(vx) M(vy) */
   ORC_IC_TWO_STREAM = 120     /* (1+a cos(k x)+a cos(k y)) 0.5[M(vx-u)+M(vx+u)] M(vy) */
 };
@@ -70,6 +73,23 @@ void orc_run(const orc_domain *d, double *fn, double *fnp1, double *rho, double 
              int nsteps, double *nrj, double *mass);
 
 void orc_init_case(const orc_domain *d, double *f, int ic, double amp, double k, double u);
+
+/* The vlp4d_mpi step for one process (vlp4d_mpi_oracle.c).  Halo arrays:
+ * extents n[d] + 6, first index -3, layout_left; orcm_size() doubles. */
+size_t orcm_size(const orc_domain *d);
+void orcm_get_interior(const orc_domain *d, const double *fh, double *f);
+void orcm_set_interior(const orc_domain *d, double *fh, const double *f);
+void orcm_halo_fill(const orc_domain *d, double *f);
+void orcm_spline_xy(const orc_domain *d, double *f);
+void orcm_spline_vxvy(const orc_domain *d, double *f);
+int orcm_advect_2d(const orc_domain *d, double *f, double *tmp, double dt);
+int orcm_advect_4d(const orc_domain *d, const double *ex, const double *ey, double *fn, double *tmp);
+void orcm_field_rho(const orc_domain *d, const double *f, double *rho);
+double orcm_l2norm(const orc_domain *d, const double *f);
+void orcm_start(const orc_domain *d, const double *fn, double *rho, double *ex, double *ey, double out[5]);
+int orcm_step(const orc_domain *d, double *fn, double *fnp1, double *tmp, double *rho, double *ex, double *ey,
+              double half[4], double out[5]);
+void orcm_init_case(const orc_domain *d, double *fh, int ic);
 
 /* FP64 discrete adjoint of the restated step (vlp4d_adjoint.c).  The
  * objective is J(f) = dx*dy * sum (Ex^2 + Ey^2), E solved from f. */

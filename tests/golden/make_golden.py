@@ -18,6 +18,13 @@ oracle/ref_driver.cpp) on small seeded inputs and stores what it computes:
   (tests/openmp/test_fft.cpp:7-71) through its Impl::FFT wrapper.
 * ``<deck>_nrj.out``: nrj.out written by the reference's own driver
   (oracle/_ref/vlp4d_ref) on the small decks in decks/.
+* ``mpi_stages_small.npz``: the reference's OpenMP vlp4d_mpi
+  (miniapps/vlp4d_mpi/openmp, one process, oracle/_ref/libvlp4d_mpi_ref.so
+  driven by oracle/ref_mpi_driver.cpp) on a 10x12x10x11 grid: digests of
+  the halo exchange, both spline prefilters, advect_2D_xy, the field,
+  advect_4D and one onetimestep (sum, sum of squares, the values at 400
+  seeded positions of the halo-extended array and one full x line through
+  the outer halo layers), plus the nrj.out / l2norm.out history of 12 steps.
 
 Usage (needs the reference tree, which only the build container has):
     python tests/golden/make_golden.py
@@ -32,7 +39,8 @@ import numpy as np
 ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
-from oracle.oracle import IC_LANDAU_SUM, IC_TWO_STREAM, Reference, Restatement, build  # noqa: E402
+from oracle.oracle import (IC_LANDAU_SUM, IC_SLD10, IC_TWO_STREAM, MpiReference, MpiRestatement,  # noqa: E402
+                           Reference, Restatement, build)
 
 OUT = Path(__file__).resolve().parent
 FOUR_PI = 4 * np.pi
@@ -159,6 +167,54 @@ def deck_runs():
         print("deck run:", name)
 
 
+MPI_SMALL = dict(n=(10, 12, 10, 11), minp=(0, 0, -6, -6), maxp=(FOUR_PI, FOUR_PI, 6, 6), dt=0.1, steps=12)
+
+
+def mpi_digest(a, seed):
+    """sum, sum of squares, 400 values at seeded flat positions, and the x
+    line at (iy, ivx, ivy) = (-3, 0, -3) of a halo-extended array."""
+    flat = np.ascontiguousarray(a).reshape(-1)
+    pos = np.random.default_rng(seed).choice(flat.size, 400, replace=False)
+    return {"sum": np.array(flat.sum()), "sq": np.array((flat * flat).sum()), "pos": pos,
+            "val": flat[pos], "line": np.array(a[0, 3, 0, :])}
+
+
+def mpi_stages():
+    c = MPI_SMALL
+    n, dt = c["n"], c["dt"]
+    ref = MpiReference(n, c["minp"], c["maxp"], dt, nbiter=c["steps"], idcase=10)
+    out = {"n": np.array(n), "minp": np.array(c["minp"]), "maxp": np.array(c["maxp"]), "dt": np.array(dt)}
+    stages = {}
+    stages["init"] = ref.get_f(0)
+    ref.exchange_halo(0)
+    stages["halo"] = ref.get_f(0)
+    ref.spline_xy(0)
+    stages["spline_xy"] = ref.get_f(0)
+    ref.set_f(1, stages["spline_xy"])
+    ref.advect_2d(0, 0.5 * dt)
+    stages["advect_2d"] = ref.get_f(0)
+    ref.field(0)
+    out["phi"], out["ex"], out["ey"] = ref.get_field(0), ref.get_field(1), ref.get_field(2)
+    ref.spline_vxvy(1)
+    stages["spline_vxvy"] = ref.get_f(1)
+    ref.advect_4d(1, 0, dt)
+    stages["advect_4d"] = ref.get_f(1)
+    for i, (k, v) in enumerate(stages.items()):
+        for dk, dv in mpi_digest(v, 100 + i).items():
+            out[f"{k}_{dk}"] = dv
+    ref.close()
+    # A run through the reference's main loop (Vlp4d.cpp:30-49).
+    ref = MpiReference(n, c["minp"], c["maxp"], dt, nbiter=c["steps"], idcase=10)
+    ref.run(c["steps"])
+    nrj, l2 = ref.diags()
+    out["run_nrj"], out["run_l2norm"] = nrj, l2
+    for dk, dv in mpi_digest(ref.get_f(0), 200).items():
+        out[f"run_{dk}"] = dv
+    ref.close()
+    np.savez_compressed(OUT / "mpi_stages_small.npz", **out)
+    print("mpi_stages_small:", n)
+
+
 def main():
     build(reference=True)
     if not Reference.available():
@@ -171,6 +227,8 @@ def main():
     initcases()
     fft_kat()
     deck_runs()
+    if MpiReference.available():
+        mpi_stages()
 
 
 if __name__ == "__main__":
