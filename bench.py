@@ -47,9 +47,9 @@ def parse_args(argv=None):
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end runs")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip timing the reference CPU build")
     ap.add_argument("--only-f32", action="store_true", help="FP32 storage only (no FP64 run, no e2e): profiling")
-    ap.add_argument("--case", choices=["main", "adjoint", "ensemble"], default="main",
-                    help="profiling cases: the reverse-mode or the ensemble arm alone (--steps steps, "
-                         "--members members, default tiles), one JSON line")
+    ap.add_argument("--case", choices=["main", "adjoint", "ensemble", "mpi"], default="main",
+                    help="profiling cases: the reverse-mode, the ensemble or the vlp4d_mpi arm alone "
+                         "(--steps steps, --members members, default tiles; --n for mpi), one JSON line")
     ap.add_argument("--members", type=int, default=256, help="ensemble members for --case ensemble")
     return ap.parse_args(argv)
 
@@ -434,6 +434,120 @@ def adjoint_arm(pkg, torch, stream, n=64, nsteps=200, every=8):
     return out
 
 
+MPI_L = 12.56637112  # wk/SLD10.dat: x, y in [0, 12.56637112), v in [-9, 9), dt 0.01
+
+
+def _mpi_init_sld10(torch, ctx, fn):
+    """SLD10 initial condition of vlp4d_mpi (Init.cpp:228-247) on the grid
+    points of a halo array: (1/2pi) exp(-(vx^2+vy^2)/2) (1 + 0.05 cos(x/2) cos(y/2))."""
+    nx, ny, nvx, nvy = ctx.dom.nxmax
+    dx = [(ctx.dom.max_phy[k] - ctx.dom.min_phy[k]) / ctx.dom.nxmax[k] for k in range(4)]
+    ar = lambda k, m: ctx.dom.min_phy[k] + torch.arange(m, dtype=torch.float64, device="cuda") * dx[k]
+    x, y, vx, vy = ar(0, nx), ar(1, ny), ar(2, nvx), ar(3, nvy)
+    sp = 1 + 0.05 * torch.cos(0.5 * y)[:, None] * torch.cos(0.5 * x)[None, :]
+    mv = torch.exp(-0.5 * (vy[:, None] ** 2 + vx[None, :] ** 2)) / (2 * math.pi)
+    fn.zero_()
+    fn[3:-3, 3:-3, 3:-3, 3:-3] = mv[:, :, None, None] * sp[None, None, :, :]
+
+
+def mpi_reference_cpu(n, budget_s=20.0):
+    """The reference's own OpenMP vlp4d_mpi (oracle/_ref/libvlp4d_mpi_ref.so,
+    one process) on an n^4 SLD10 grid: one untimed step, then steps while
+    the total stays within budget_s."""
+    sys.path.insert(0, str(ROOT))
+    from oracle.oracle import MpiReference
+
+    if not MpiReference.available():
+        return None
+    ref = MpiReference((n,) * 4, (0.0, 0.0, -9.0, -9.0), (MPI_L, MPI_L, 9.0, 9.0), 0.01, nbiter=64, idcase=10)
+    threads = int(ref.L.refm_max_threads())
+    ref.onetimestep(1)
+    times = []
+    for it in range(60):
+        t0 = time.perf_counter()
+        ref.onetimestep(2 + it)
+        times.append(time.perf_counter() - t0)
+        if sum(times) > budget_s:
+            break
+    ref.close()
+    secs = sum(times)
+    return {"value": n ** 4 * len(times) / secs / 1e9, "unit": METRIC, "cores": threads, "kind": "reference",
+            "sample": f"{len(times)} onetimestep calls of the {n}^4 SLD10 grid (after 1 untimed), reference "
+                      f"OpenMP build miniapps/vlp4d_mpi/openmp as one process, FP64, OMP_NUM_THREADS={threads}"}
+
+
+def mpi_arm(pkg, torch, stream, peak, n=128, nsteps=10, warmup=3):
+    """The vlp4d_mpi step (cubic splines, 4D advection) for one process on the
+    geometry of its reference deck wk/SLD10.dat (128^4, x, y in
+    [0, 12.566), v in [-9, 9), dt 0.01, SLD10 initial condition), FP64
+    halo-extended arrays.  Times vlp4d_mpi_step (fused: four passes over f)
+    and the reference-order sequence of the separate entry points (halo
+    fill, spline_xy, advect_2d, field, spline_vxvy, advect_4d, field,
+    diagnostics) with CUDA events."""
+    dom = pkg.Domain([n] * 4, [0.0, 0.0, -9.0, -9.0], [MPI_L, MPI_L, 9.0, 9.0], 0.01, nsteps + warmup + 8, 10)
+    cells = n ** 4
+    with pkg.Context(dom, "f64") as ctx:
+        fn, fnp1 = ctx.mpi_empty(), ctx.mpi_empty()
+        _mpi_init_sld10(torch, ctx, fn)
+        ctx.mpi_field(fn)
+        ctx.diags_compute(0)
+        ctx.mpi_l2norm(fn, 0)
+        bufs = [fn, fnp1]
+        it = [1]
+
+        def one():
+            ctx.mpi_step(bufs[0], bufs[1], min(it[0], dom.nbiter), stream)
+            bufs.reverse()
+            it[0] += 1
+
+        for _ in range(warmup):
+            one()
+        torch.cuda.synchronize()
+        e0, e1 = _events(torch)
+        e0.record(stream)
+        for _ in range(nsteps):
+            one()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ctx.check()
+        t = e0.elapsed_time(e1) / 1e3 / nsteps
+        finite = bool(torch.isfinite(bufs[0][3:-3, 3:-3, 3:-3, 3:-3]).all().item())
+        _, _, l2 = ctx.diags_read_ext(it[0])
+        # The separate entry points in the reference's order.
+        tmp = ctx.mpi_empty()
+
+        def seq():
+            a = bufs[0]
+            ctx.mpi_halo_fill(a, stream)
+            ctx.mpi_spline_xy(a, stream)
+            bufs[1].copy_(a)
+            ctx.mpi_advect_2d(a, tmp, 0.005, stream)
+            ctx.mpi_field(a, stream)
+            ctx.mpi_spline_vxvy(bufs[1], stream)
+            ctx.mpi_advect_4d(bufs[1], a, 0.01, stream)
+            ctx.mpi_field(bufs[1], stream)
+            ctx.diags_compute(1, stream)
+            ctx.mpi_l2norm(bufs[1], 1, stream)
+            bufs.reverse()
+
+        t_seq = time_calls(torch, stream, seq, 2)
+        ctx.check()
+        del tmp
+    torch.cuda.empty_cache()
+    # FP64 bytes the four fused passes read and write once each (E = n + 6):
+    # x/y: n^4 -> E^2 n^2; vx: E^2 n^2 -> E^3 n; vy: E^3 n -> E^4;
+    # 4D: E^4 -> n^4.
+    e = n + 6
+    bytes_step = 8.0 * 2 * (n ** 4 + e * e * n * n + e ** 3 * n + e ** 4)
+    return {"config": {"workload": "vlp4d_mpi one process, SLD10 deck geometry", "grid": [n] * 4, "dt": 0.01,
+                       "x": [0, MPI_L], "v": [-9, 9], "storage": "f64 halo-extended (n+6)^4"},
+            "ms_per_step": t * 1e3, "value": cells / t / 1e9, "unit": METRIC,
+            "reference_order_entry_points_ms_per_step": t_seq * 1e3,
+            "hbm_bytes_per_step_model": bytes_step, "hbm_gbs_model": bytes_step / t / 1e9,
+            "finite": finite, "l2norm_first_last": [float(l2[0]), float(l2[-1])],
+            "launches_per_step": 9}
+
+
 # ---------------------------------------------------------------- CPU reference
 def landau_f0_numpy(n):
     """The benchmark initial condition on the host, FP64, layout_left order."""
@@ -523,6 +637,11 @@ def main(argv=None):
         peak, _ = measured_hbm_peak()
         if args.case == "adjoint":
             out = adjoint_arm(pkg, torch, stream, nsteps=args.steps)
+        elif args.case == "mpi":
+            out = mpi_arm(pkg, torch, stream, peak, n=args.n, nsteps=args.steps, warmup=max(args.warmup, 1))
+            if not args.no_cpu_baseline:
+                _set_omp_env()
+                out["cpu_baseline"] = mpi_reference_cpu(32)
         else:
             out = ensemble_arm(pkg, torch, stream, peak, nruns=args.members, nsteps=args.steps, autotune=False)
         print(json.dumps({"case": args.case, **out}), flush=True)

@@ -43,6 +43,9 @@ extern "C" {
 #define VLP4D_ERR_NO_DEVICE 4
 #define VLP4D_ERR_IO 5
 #define VLP4D_ERR_TIMEOUT 6 /* a kernel's bounded wait for an async copy ran out */
+#define VLP4D_ERR_RANGE 7   /* a vlp4d_mpi foot left the interpolation range: the
+                               reference's "Time step is too large" exit
+                               (miniapps/vlp4d_mpi/thrust/Advection.hpp:21-26) */
 
 #define VLP4D_F64 0
 #define VLP4D_F32 1
@@ -306,6 +309,55 @@ long long vlp4d_ensemble_cells(const vlp4d_ensemble *ens);
 int vlp4d_ensemble_set_tiles(vlp4d_ensemble *ens, int threads, int cols_per_tile, int ctas_per_sm);
 int vlp4d_ensemble_get_tiles(const vlp4d_ensemble *ens, int *threads, int *cols_per_tile, int *ctas_per_sm);
 int vlp4d_ensemble_autotune(vlp4d_ensemble *ens, int steps, const char *csv_path, void *stream);
+
+/* ---- vlp4d_mpi, one process (miniapps/vlp4d_mpi, cubic-spline scheme).
+ *
+ * The arrays are the reference's halo-extended views (RealView4D with
+ * offsets, miniapps/vlp4d_mpi/openmp/Init.cpp:333-343): FP64, extents
+ * n[d] + 6 in every dimension, first index -3 (HALO_PTS = 3, Config.hpp:7),
+ * layout_left, vlp4d_mpi_size() elements, 16-byte aligned.  The context must
+ * be FP64 with every grid dimension at least 10 (MMAX + 2, Init.cpp:85-89).
+ * A foot outside the interpolation range sets the context's error word:
+ * vlp4d_check then returns VLP4D_ERR_RANGE (the reference exits with "Time
+ * step is too large", thrust/Advection.hpp:21-26).  All calls are
+ * asynchronous on `stream`. */
+size_t vlp4d_mpi_size(const vlp4d_ctx *ctx);
+/* Distrib::exchangeHalo for one process (thrust/Communication.cpp, with the
+ * spline boundary sums of Communication.hpp boundary_condition): periodic
+ * images in the halo, sum_{j=1..8} alpha^j f(...) in its outermost layer.
+ * Bit-identical to the reference. */
+int vlp4d_mpi_halo_fill(vlp4d_ctx *ctx, void *fn, void *stream);
+/* Spline::computeCoeff_xy / computeCoeff_vxvy (thrust/Spline.hpp:61-302):
+ * cubic B-spline prefilter along x then y / vx then vy, in place on a
+ * halo-filled array.  Bit-identical to the reference. */
+int vlp4d_mpi_spline_xy(vlp4d_ctx *ctx, void *fn, void *stream);
+int vlp4d_mpi_spline_vxvy(vlp4d_ctx *ctx, void *fn, void *stream);
+/* Advection::advect_2D_xy(conf, fn, fn_tmp, dt) (thrust/Advection.hpp:95-226):
+ * fn_tmp receives a copy of fn (spline coefficients), fn's grid points the
+ * 4x4 spline interpolation at (x - dt vx, y - dt vy).  Bit-identical. */
+int vlp4d_mpi_advect_2d(vlp4d_ctx *ctx, void *fn, void *fn_tmp, double dt, void *stream);
+/* Advection::advect_4D(conf, ef, fn, tmp_fn, dt) (thrust/Advection.hpp:228-415)
+ * with the context's Ex, Ey: tmp_fn receives a copy of fn (4D spline
+ * coefficients), fn's grid points the interpolation at the
+ * predictor-corrector feet.  Bit-identical. */
+int vlp4d_mpi_advect_4d(vlp4d_ctx *ctx, void *fn, void *tmp_fn, double dt, void *stream);
+/* field_rho + field_reduce + field_poisson (thrust/Field.cpp) on the grid
+ * points of a halo array: the context's rho (then phi), Ex, Ey. */
+int vlp4d_mpi_field(vlp4d_ctx *ctx, const void *fn, void *stream);
+/* Diags::computeL2norm (thrust/Diags.cpp:68-92) of the grid points of a halo
+ * array into history slot iter (read with vlp4d_diags_read_ext). */
+int vlp4d_mpi_l2norm(vlp4d_ctx *ctx, const void *fn, int iter, void *stream);
+/* onetimestep (thrust/Timestep.hpp:34-97) with dt = the domain's dt: the
+ * state in fn's grid points advances into fnp1's grid points; fn is
+ * overwritten (it ends holding the 4D spline coefficients, as in the
+ * reference) and neither halo is part of the state.  Diagnostic slot `iter`
+ * receives the end-of-step nrj, mass, nrjx, nrjy and l2norm (the reference
+ * records the mid-step values in the same slot first and then overwrites
+ * them).  Fused: four passes over f (x/y prefilter with the 2D advection's
+ * moment, vx prefilter, vy prefilter, 4D advection with the moment and the
+ * L2 norm); equal to the reference sequence up to FP64 rounding.  The caller
+ * swaps fn and fnp1 afterwards, as Vlp4d.cpp:46 does. */
+int vlp4d_mpi_step(vlp4d_ctx *ctx, void *fn, void *fnp1, int iter, void *stream);
 
 #ifdef __cplusplus
 }

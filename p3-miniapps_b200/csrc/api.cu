@@ -83,6 +83,7 @@ void free_ctx(vlp4d_ctx *c) {
   cudaFree(c->mass);
   cudaFree(c->rho_part);
   cudaFree(c->d_err);
+  cudaFree(c->mpi_part);
   cudaFree(c->vspan);
   for (StencilTable *t : {&c->tab_x[0], &c->tab_x[1], &c->tab_y[0], &c->tab_y[1], &c->tab_vx, &c->tab_vy,
                           &c->tab_x11, &c->tab_y11}) {
@@ -205,6 +206,8 @@ int vlp4d_ctx_create(const vlp4d_domain *dom, int dtype, vlp4d_ctx **out) {
   c->rho_part_groups = (int)(fused_groups > groups ? fused_groups : groups);
   CTX_ALLOC(c->rho_part, sizeof(double) * nxy * (size_t)c->rho_part_groups);
   CTX_ALLOC(c->d_err, sizeof(int));
+  c->mpi_part_cap = 8192;
+  CTX_ALLOC(c->mpi_part, sizeof(double) * 2 * (size_t)c->mpi_part_cap);
   c->vspan_cap = (int)(nxy / 8 + 1);
   CTX_ALLOC(c->vspan, sizeof(int2) * (size_t)c->vspan_cap);
   {
@@ -387,7 +390,8 @@ int vlp4d_check(vlp4d_ctx *ctx) {
   VLP4D_CUDA_TRY(cudaMemcpy(&flag, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (flag) {
     VLP4D_CUDA_TRY(cudaMemset(ctx->d_err, 0, sizeof(int)));
-    return fail(VLP4D_ERR_TIMEOUT, "an asynchronous copy did not complete within its time limit");
+    if (flag & 1) return fail(VLP4D_ERR_TIMEOUT, "an asynchronous copy did not complete within its time limit");
+    return fail(VLP4D_ERR_RANGE, "a foot left the interpolation range (the reference stops: time step is too large)");
   }
   return VLP4D_OK;
 }

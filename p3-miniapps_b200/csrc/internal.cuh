@@ -114,7 +114,9 @@ struct vlp4d_ctx {
   // (an unsupported shape is an error instead of a silent fallback).
   bool fused = true;
   bool fused_only = false;
-  // Set to 1 by a kernel whose bounded wait for an asynchronous copy ran out.
+  // Error word: bit 1 set by a kernel whose bounded wait for an asynchronous
+  // copy ran out, bit 2 by a vlp4d_mpi advection whose foot left the
+  // interpolation range.
   int *d_err = nullptr;
   // Per column chunk (min, max) signed vy offset for the fused v pass.
   int2 *vspan = nullptr;
@@ -131,6 +133,11 @@ struct vlp4d_ctx {
 
   // Pinned host staging for vlp4d_run's per-step diagnostic read-back.
   double *h_diag = nullptr;
+
+  // Per-block (sum, compensation) pairs of the vlp4d_mpi L2 norm and 4D
+  // pass (mpi.cu), mpi_part_cap pairs.
+  double *mpi_part = nullptr;
+  int mpi_part_cap = 0;
 };
 
 namespace vlp4d {

@@ -20,7 +20,7 @@ from typing import Optional, Sequence
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libvlp4d_b200.so"
 
-OK, ERR_INVALID_ARG, ERR_CUDA, ERR_UNSUPPORTED, ERR_NO_DEVICE, ERR_IO, ERR_TIMEOUT = 0, 1, 2, 3, 4, 5, 6
+OK, ERR_INVALID_ARG, ERR_CUDA, ERR_UNSUPPORTED, ERR_NO_DEVICE, ERR_IO, ERR_TIMEOUT, ERR_RANGE = 0, 1, 2, 3, 4, 5, 6, 7
 F64, F32 = 0, 1
 FIELD_RHO, FIELD_EX, FIELD_EY = 0, 1, 2
 IC_CYL02, IC_CYL05, IC_SLD10, IC_TSI20, IC_LANDAU_SUM, IC_TWO_STREAM = 2, 5, 10, 20, 110, 120
@@ -38,7 +38,10 @@ EXPORTS = (
     "vlp4d_ensemble_create", "vlp4d_ensemble_destroy", "vlp4d_ensemble_run", "vlp4d_ensemble_check",
     "vlp4d_ensemble_read", "vlp4d_ensemble_cells", "vlp4d_ensemble_set_tiles", "vlp4d_ensemble_get_tiles",
     "vlp4d_ensemble_autotune", "vlp4d_selftest_wait_timeout", "vlp4d_diags_l2norm", "vlp4d_diags_read_ext",
+    "vlp4d_mpi_size", "vlp4d_mpi_halo_fill", "vlp4d_mpi_spline_xy", "vlp4d_mpi_spline_vxvy", "vlp4d_mpi_advect_2d",
+    "vlp4d_mpi_advect_4d", "vlp4d_mpi_field", "vlp4d_mpi_l2norm", "vlp4d_mpi_step",
 )
+HALO = 3  # HALO_PTS of the vlp4d_mpi halo-extended arrays
 
 
 class Vlp4dError(RuntimeError):
@@ -129,9 +132,17 @@ def lib() -> C.CDLL:
         L.vlp4d_selftest_wait_timeout.argtypes = [vp, C.c_longlong, vp]
         L.vlp4d_diags_l2norm.argtypes = [vp, vp, i, vp]
         L.vlp4d_diags_read_ext.argtypes = [vp, dp, dp, dp, i]
+        L.vlp4d_mpi_size.argtypes = [vp]
+        for n in ("vlp4d_mpi_halo_fill", "vlp4d_mpi_spline_xy", "vlp4d_mpi_spline_vxvy", "vlp4d_mpi_field"):
+            getattr(L, n).argtypes = [vp, vp, vp]
+        L.vlp4d_mpi_advect_2d.argtypes = [vp, vp, vp, d, vp]
+        L.vlp4d_mpi_advect_4d.argtypes = [vp, vp, vp, d, vp]
+        L.vlp4d_mpi_l2norm.argtypes = [vp, vp, i, vp]
+        L.vlp4d_mpi_step.argtypes = [vp, vp, vp, i, vp]
         for n in EXPORTS:
-            if n not in ("vlp4d_last_error", "vlp4d_kernel_launches", "vlp4d_ensemble_cells"):
+            if n not in ("vlp4d_last_error", "vlp4d_kernel_launches", "vlp4d_ensemble_cells", "vlp4d_mpi_size"):
                 getattr(L, n).restype = C.c_int
+        L.vlp4d_mpi_size.restype = C.c_size_t
         L.vlp4d_ensemble_cells.restype = C.c_longlong
         L.vlp4d_kernel_launches.restype = C.c_ulonglong
         _lib = L
@@ -364,6 +375,63 @@ class Context:
 
     def print_fxvx(self, fn, path):
         _check(lib().vlp4d_print_fxvx(self.h, self._f(fn), str(path).encode()))
+
+    # -- vlp4d_mpi (one process): halo-extended FP64 arrays of shape
+    #    (nvy+6, nvx+6, ny+6, nx+6); index 3 is grid point 0.
+    @property
+    def mpi_shape(self):
+        nx, ny, nvx, nvy = self.dom.nxmax
+        return (nvy + 2 * HALO, nvx + 2 * HALO, ny + 2 * HALO, nx + 2 * HALO)
+
+    def mpi_empty(self):
+        import torch
+
+        return torch.zeros(self.mpi_shape, dtype=torch.float64, device="cuda")
+
+    def _h(self, t):
+        import torch
+
+        n = int(lib().vlp4d_mpi_size(self.h))
+        if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous() and t.numel() == n):
+            raise ValueError(f"a vlp4d_mpi array must be a contiguous CUDA float64 tensor of {n} elements")
+        return C.c_void_p(t.data_ptr())
+
+    def mpi_halo_fill(self, fn, stream=None):
+        _check(lib().vlp4d_mpi_halo_fill(self.h, self._h(fn), _stream_ptr(stream)))
+
+    def mpi_spline_xy(self, fn, stream=None):
+        _check(lib().vlp4d_mpi_spline_xy(self.h, self._h(fn), _stream_ptr(stream)))
+
+    def mpi_spline_vxvy(self, fn, stream=None):
+        _check(lib().vlp4d_mpi_spline_vxvy(self.h, self._h(fn), _stream_ptr(stream)))
+
+    def mpi_advect_2d(self, fn, fn_tmp, dt, stream=None):
+        _check(lib().vlp4d_mpi_advect_2d(self.h, self._h(fn), self._h(fn_tmp), dt, _stream_ptr(stream)))
+
+    def mpi_advect_4d(self, fn, tmp_fn, dt, stream=None):
+        _check(lib().vlp4d_mpi_advect_4d(self.h, self._h(fn), self._h(tmp_fn), dt, _stream_ptr(stream)))
+
+    def mpi_field(self, fn, stream=None):
+        _check(lib().vlp4d_mpi_field(self.h, self._h(fn), _stream_ptr(stream)))
+
+    def mpi_l2norm(self, fn, it, stream=None):
+        _check(lib().vlp4d_mpi_l2norm(self.h, self._h(fn), it, _stream_ptr(stream)))
+
+    def mpi_step(self, fn, fnp1, it, stream=None):
+        """One vlp4d_mpi step: state in fn's grid points -> fnp1's (fn is overwritten)."""
+        _check(lib().vlp4d_mpi_step(self.h, self._h(fn), self._h(fnp1), it, _stream_ptr(stream)))
+
+    def mpi_run(self, fn, fnp1, nsteps, stream=None):
+        """Initial field and diagnostics, then nsteps steps (Vlp4d.cpp:30-49);
+        returns the tensor that holds the final state (fn or fnp1)."""
+        self.mpi_field(fn, stream)
+        self.diags_compute(0, stream)
+        self.mpi_l2norm(fn, 0, stream)
+        a, b = fn, fnp1
+        for it in range(1, nsteps + 1):
+            self.mpi_step(a, b, it, stream)
+            a, b = b, a
+        return a
 
 
 def field_rho_noalloc(f, rho, nxmax, dvx, dvy, stream=None):
