@@ -31,6 +31,7 @@
 //   norm of the new state.  Its arithmetic uses FMA and its own summation
 //   order: equal to the reference up to rounding.
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "internal.cuh"
@@ -90,6 +91,17 @@ __device__ __forceinline__ int wrapi(int i, int n) { return ((i % n) + n) % n; }
 __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+
+// 8-byte asynchronous global-to-shared copies (through L1), one commit group
+// per call site, waited for before the data is read.
+__device__ __forceinline__ void cp_async8(double *dst, const double *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
 
 // ---------------------------------------------------------------------------
 // Halo fill of one process (Communication.hpp:713-754 through the local
@@ -271,7 +283,8 @@ __global__ void __launch_bounds__(256) k_mpi_spline_xy(double *__restrict__ f, H
   for (long long p = blockIdx.x; p < planes; p += gridDim.x) {
     double *g = f + p * h.s[2];
     for (int r = threadIdx.y; r < E1; r += blockDim.y)
-      for (int c = threadIdx.x; c < E0; c += blockDim.x) pl[r * P + c] = g[(long long)r * E0 + c];
+      for (int c = threadIdx.x; c < E0; c += blockDim.x) cp_async8(pl + r * P + c, g + (long long)r * E0 + c);
+    cp_async_wait_all();
     __syncthreads();
     // plane_prefilter indexes threads linearly.
     const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
@@ -359,7 +372,8 @@ __global__ void __launch_bounds__(512) k_mpi_xy_pass(const double *__restrict__ 
     const int ivx = (int)(p % nvx), ivy = (int)(p / nvx);
     const double *src = fn + h.at(0, 0, ivx, ivy);
     for (int iy = warp; iy < ny; iy += nwarps)
-      for (int ix = lane; ix < nx; ix += 32) pl[(iy + kH) * P + ix + kH] = __ldg(src + (long long)iy * E0 + ix);
+      for (int ix = lane; ix < nx; ix += 32) cp_async8(pl + (iy + kH) * P + ix + kH, src + (long long)iy * E0 + ix);
+    cp_async_wait_all();
     __syncthreads();
     plane_extend(pl, P, h);
     plane_prefilter<false>(pl, P, h);
@@ -439,11 +453,12 @@ __global__ void __launch_bounds__(128) k_mpi_vlines(const double *in, double *ou
     const long long base = (long long)(x + kH) + h.s[1] * (y + kH) + so * (o + kH);
     if (live) {
       if (EXTEND) {
-        for (int i = 0; i < n; ++i) tile[(i + kH) * 32 + lane] = in[base + (long long)(i + kH) * sl];
+        for (int i = 0; i < n; ++i) cp_async8(tile + (i + kH) * 32 + lane, in + base + (long long)(i + kH) * sl);
       } else {
-        for (int i = 0; i < E; ++i) tile[i * 32 + lane] = in[base + (long long)i * sl];
+        for (int i = 0; i < E; ++i) cp_async8(tile + i * 32 + lane, in + base + (long long)i * sl);
       }
     }
+    cp_async_wait_all();
     __syncwarp();
     if (live) {
       double *col = tile + lane;
@@ -704,6 +719,125 @@ __global__ void __launch_bounds__(256) k_mpi_advect_4d(const double *__restrict_
   }
 }
 
+// The fused step's 4D pass with R cells per thread at consecutive y (same
+// x, vx, vy).  Block (32 x, 4 rows of R y), blockIdx.z = plane group as in
+// k_mpi_advect_4d.  When the R feet share their x, vx and vy cells and
+// their y cells are consecutive (all but a few per mille of the groups),
+// the group reads each (vx, vy) slab's R + 3 rows of four x values once
+// and applies every cell's own weights from registers: 64 (R + 3) / R
+// loads per cell instead of 256.  Other groups interpolate cell by cell.
+template <int R>
+__global__ void __launch_bounds__(128) k_mpi_advect_4d_rows(const double *__restrict__ c, double *__restrict__ fn,
+                                                           const double *__restrict__ ex,
+                                                           const double *__restrict__ ey, HGrid h, double dt,
+                                                           double *__restrict__ part, double *__restrict__ l2,
+                                                           int *__restrict__ err) {
+  const int ix = blockIdx.x * 32 + threadIdx.x;
+  const int iy0 = (blockIdx.y * blockDim.y + threadIdx.y) * R;
+  const int G = gridDim.z;
+  const long long planes = (long long)h.n[2] * h.n[3];
+  const long long nx = h.n[0];
+  double racc[R], sq = 0.;
+#pragma unroll
+  for (int q = 0; q < R; ++q) racc[q] = 0.;
+  bool bad = false;
+  if (ix < h.n[0] && iy0 < h.n[1]) {
+    for (long long p = blockIdx.z; p < planes; p += G) {
+      const int ivx = (int)(p % h.n[2]), ivy = (int)(p / h.n[2]);
+      double g[R][4];
+      bool ok[R];
+      bool fast = true;
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int iy = iy0 + q;
+        ok[q] = iy < h.n[1] && foot4d<false>(h, ex, ey, ix, iy < h.n[1] ? iy : iy0, ivx, ivy, dt, g[q]);
+        fast &= ok[q];
+      }
+      int ip[R][4];
+#pragma unroll
+      for (int q = 0; q < R; ++q)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) ip[q][j] = (int)floor(g[q][j]);
+#pragma unroll
+      for (int q = 1; q < R; ++q)
+        fast &= ip[q][0] == ip[0][0] && ip[q][2] == ip[0][2] && ip[q][3] == ip[0][3] && ip[q][1] == ip[0][1] + q;
+      double val[R];
+      if (fast) {
+        double e0[R][4], e1[R][4], e2[R][4], e3[R][4];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          bspline_w<false>(g[q][0] - ip[q][0], e0[q]);
+          bspline_w<false>(g[q][1] - ip[q][1], e1[q]);
+          bspline_w<false>(g[q][2] - ip[q][2], e2[q]);
+          bspline_w<false>(g[q][3] - ip[q][3], e3[q]);
+          val[q] = 0.;
+        }
+        const double *b = c + h.at(ip[0][0] - 1, ip[0][1] - 1, ip[0][2] - 1, ip[0][3] - 1);
+#pragma unroll
+        for (int k3 = 0; k3 < 4; ++k3) {
+#pragma unroll
+          for (int k2 = 0; k2 < 4; ++k2) {
+            const double *slab = b + k2 * h.s[2] + k3 * h.s[3];
+            double s2[R];
+#pragma unroll
+            for (int q = 0; q < R; ++q) s2[q] = 0.;
+#pragma unroll
+            for (int r = 0; r < R + 3; ++r) {
+              const double *row = slab + r * h.s[1];
+              const double v0 = __ldg(row), v1 = __ldg(row + 1), v2 = __ldg(row + 2), v3 = __ldg(row + 3);
+#pragma unroll
+              for (int q = 0; q < R; ++q) {
+                const int k1 = r - q;
+                if (k1 >= 0 && k1 < 4) {
+                  const double x = e0[q][0] * v0 + e0[q][1] * v1 + e0[q][2] * v2 + e0[q][3] * v3;
+                  s2[q] = fma(x, e1[q][k1], s2[q]);
+                }
+              }
+            }
+#pragma unroll
+            for (int q = 0; q < R; ++q) val[q] = fma(s2[q] * e2[q][k2], e3[q][k3], val[q]);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          val[q] = 0.;
+          if (iy0 + q < h.n[1]) {
+            if (ok[q]) val[q] = interp4d<false>(h, c, g[q]);
+            else bad = true;
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        if (iy0 + q < h.n[1]) {
+          fn[h.at(ix, iy0 + q, ivx, ivy)] = val[q];
+          racc[q] += val[q];
+          sq = fma(val[q], val[q], sq);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q)
+      if (iy0 + q < h.n[1]) part[(long long)blockIdx.z * nx * h.n[1] + ix + nx * (iy0 + q)] = racc[q];
+  }
+  if (bad) atomicOr(err, 2);
+  // Block sum of sq in a fixed order.
+  __shared__ double ws[4];
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  double v = sq;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((tid & 31) == 0) ws[tid >> 5] = v;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0.;
+    for (int w = 0; w < (int)(blockDim.x * blockDim.y) / 32; ++w) t += ws[w];
+    const long long bl = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+    l2[2 * bl] = t;
+    l2[2 * bl + 1] = 0.;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Velocity moment of the grid points of a halo array (Field.cpp:5-55):
 // part[group][ixy] over the planes of the group.
@@ -913,6 +1047,46 @@ int launch_advect_4d(vlp4d_ctx *c, const HGrid &h, const double *c4, double *fn,
   return VLP4D_OK;
 }
 
+template <int R>
+int launch_advect_4d_rows_r(vlp4d_ctx *c, const HGrid &h, const double *c4, double *fn, double dt, int *groups,
+                            long long *blocks, cudaStream_t s) {
+  const dim3 block(32, 4);
+  const long long bx = (h.n[0] + 31) / 32, by = (h.n[1] + 4 * R - 1) / (4 * R);
+  const long long planes = (long long)h.n[2] * h.n[3];
+  long long G = ((long long)c->num_sms * 12 + bx * by - 1) / (bx * by);
+  if (G > planes) G = planes;
+  if (G > c->rho_part_groups) G = c->rho_part_groups;
+  if (G * bx * by > c->mpi_part_cap) G = c->mpi_part_cap / (bx * by);
+  if (G < 1) return fail_msg(VLP4D_ERR_UNSUPPORTED, "mpi 4D advection: too many (x, y) blocks for the partials");
+  k_mpi_advect_4d_rows<R><<<dim3((unsigned)bx, (unsigned)by, (unsigned)G), block, 0, s>>>(
+      c4, fn, c->ex, c->ey, h, dt, c->rho_part, c->mpi_part, c->d_err);
+  VLP4D_LAUNCH_CHECK();
+  *groups = (int)G;
+  *blocks = G * bx * by;
+  return VLP4D_OK;
+}
+
+// Cells per thread of the fused 4D pass (VLP4D_MPI_ROWS = 1..4 overrides;
+// 1 is the cell-per-thread kernel).
+int mpi_rows() {
+  static int r = [] {
+    const char *e = getenv("VLP4D_MPI_ROWS");
+    const int v = e && *e ? atoi(e) : 2;
+    return v < 1 ? 1 : (v > 4 ? 4 : v);
+  }();
+  return r;
+}
+
+int launch_advect_4d_fused(vlp4d_ctx *c, const HGrid &h, const double *c4, double *fn, double dt, int *groups,
+                           long long *blocks, cudaStream_t s) {
+  switch (mpi_rows()) {
+    case 2: return launch_advect_4d_rows_r<2>(c, h, c4, fn, dt, groups, blocks, s);
+    case 3: return launch_advect_4d_rows_r<3>(c, h, c4, fn, dt, groups, blocks, s);
+    case 4: return launch_advect_4d_rows_r<4>(c, h, c4, fn, dt, groups, blocks, s);
+    default: return launch_advect_4d<false, true>(c, h, c4, fn, dt, groups, blocks, s);
+  }
+}
+
 int launch_rho_halo(vlp4d_ctx *c, const HGrid &h, const double *f, cudaStream_t s) {
   const long long nxy = (long long)h.n[0] * h.n[1];
   const int groups = c->rho_groups;
@@ -1022,7 +1196,7 @@ int vlp4d_mpi_step(vlp4d_ctx *ctx, void *fn, void *fnp1, int iter, void *stream)
   if ((rc = launch_vlines<true, false>(ctx, h, f, f, 3, -kH, h.n[2] + 2 * kH, -kH + 1, h.n[2] + kH - 2, s)))
     return rc;
   long long blocks = 0;
-  if ((rc = launch_advect_4d<false, true>(ctx, h, f, g, dt, &groups, &blocks, s))) return rc;
+  if ((rc = launch_advect_4d_fused(ctx, h, f, g, dt, &groups, &blocks, s))) return rc;
   if ((rc = launch_rho_finish(ctx, groups, s))) return rc;
   if ((rc = launch_field_poisson(ctx, s))) return rc;
   if ((rc = launch_diags(ctx, iter, s))) return rc;
