@@ -47,6 +47,7 @@ struct HGrid {
   int n[4];
   long long e[4];  // n + 6
   long long s[4];  // strides: 1, e0, e0 e1, e0 e1 e2
+  int is[4];       // the same strides as int (an array has fewer than 2^31 elements)
   double minp[4], maxp[4], dx[4], inv_dx[4];
   // Admissible feet of the 4D advection (Advection.hpp thrust :249-250):
   // [min + local_min*h - h, min + local_max*h + h] with local = 0..n-1.
@@ -77,6 +78,7 @@ HGrid make_hgrid(const vlp4d_ctx *c) {
   h.s[1] = h.e[0];
   h.s[2] = h.e[0] * h.e[1];
   h.s[3] = h.s[2] * h.e[2];
+  for (int k = 0; k < 4; ++k) h.is[k] = (int)h.s[k];
   // Spline.hpp:21,36-37: sqrt3 = sqrt(3), alpha = sqrt3 - 2,
   // beta = sqrt3 * (1 - alpha*alpha) (host IEEE arithmetic).
   h.sqrt3 = std::sqrt(3.0);
@@ -204,22 +206,50 @@ __device__ __forceinline__ void spline_line(double *__restrict__ e, long long st
       e[(long long)i * st] = c;
     }
   } else {
+    // Chunks of 8 positions: the next chunk's values are loaded (in program
+    // order) before the current chunk's results are stored, so the loads
+    // are in flight while the recursion runs.
+    constexpr int C = 8;
     const double e1 = e[st];
     double t = e[0] + e1;
     double hsum = e1;  // Horner: sum_{i=1..L} alpha^(L-i) e[i]
     e[st] = t;
-    for (int k = 1; k < L - 1; ++k) {
-      const double v = e[(long long)(1 + k) * st];
-      hsum = fma(hsum, alpha, v);
-      t = fma(alpha, t, v);
-      e[(long long)(1 + k) * st] = t;
+    double buf[C], nxt[C];
+#pragma unroll
+    for (int j = 0; j < C; ++j) buf[j] = 2 + j <= L - 1 ? e[(long long)(2 + j) * st] : 0.;
+    for (int i = 2; i <= L - 1; i += C) {
+#pragma unroll
+      for (int j = 0; j < C; ++j) nxt[j] = i + C + j <= L - 1 ? e[(long long)(i + C + j) * st] : 0.;
+#pragma unroll
+      for (int j = 0; j < C; ++j) {
+        if (i + j <= L - 1) {
+          hsum = fma(hsum, alpha, buf[j]);
+          t = fma(alpha, t, buf[j]);
+          e[(long long)(i + j) * st] = t;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < C; ++j) buf[j] = nxt[j];
     }
     hsum = fma(hsum, alpha, e[(long long)L * st]);
     double c = (e[(long long)(L + 1) * st] + hsum) * sqrt3;
     e[(long long)L * st] = c;
-    for (int i = L - 1; i >= 1; --i) {
-      c = fma(beta, e[(long long)i * st], alpha * c);
-      e[(long long)i * st] = c;
+    // Anticausal: c[i] = beta t[i-1] + alpha c[i+1], the beta products off
+    // the chain.
+#pragma unroll
+    for (int j = 0; j < C; ++j) buf[j] = L - 1 - j >= 1 ? beta * e[(long long)(L - 1 - j) * st] : 0.;
+    for (int i = L - 1; i >= 1; i -= C) {
+#pragma unroll
+      for (int j = 0; j < C; ++j) nxt[j] = i - C - j >= 1 ? beta * e[(long long)(i - C - j) * st] : 0.;
+#pragma unroll
+      for (int j = 0; j < C; ++j) {
+        if (i - j >= 1) {
+          c = fma(alpha, c, buf[j]);
+          e[(long long)(i - j) * st] = c;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < C; ++j) buf[j] = nxt[j];
     }
   }
 }
@@ -381,32 +411,32 @@ __global__ void __launch_bounds__(512) k_mpi_xy_pass(const double *__restrict__ 
     for (int r = warp; r < E1; r += nwarps)
       for (int c = lane; c < E0; c += 32) dst[(long long)r * E0 + c] = pl[r * P + c];
     // 2D advection at the grid points of the plane, from the coefficients.
+    // The shift (dt vx, dt vy) is the same for the whole plane: one cell
+    // offset and one set of weights per direction (the reference evaluates
+    // them per cell; they differ only by the rounding of x_i - dt vx).
     const double vx = h.minp[2] + ivx * h.dx[2], vy = h.minp[3] + ivy * h.dx[3];
-    const double depx = dt * vx, depy = dt * vy;
+    const double fx = -dt * vx * h.inv_dx[0], fy = -dt * vy * h.inv_dx[1];
+    const int mx = (int)floor(fx), my = (int)floor(fy);
+    if (mx < -1 || mx > 0 || my < -1 || my > 0) bad = true;  // i0 = ix + mx must stay in [-1, nx-1]
+    double ex[4], ey[4];
+    bspline_w<false>(fx - mx, ex);
+    bspline_w<false>(fy - my, ey);
+    if (!bad) {
 #pragma unroll
-    for (int k = 0; k < CPT; ++k) {
-      const int q = threadIdx.x + k * blockDim.x;
-      if (q < nxy) {
-        const int ix = q % nx, iy = q / nx;
-        const double fx = (h.minp[0] + ix * h.dx[0] - depx - h.minp[0]) * h.inv_dx[0];
-        const double fy = (h.minp[1] + iy * h.dx[1] - depy - h.minp[1]) * h.inv_dx[1];
-        const int i0 = (int)floor(fx), i1 = (int)floor(fy);
-        if (i0 < -1 || i0 > nx - 1 || i1 < -1 || i1 > ny - 1) {
-          bad = true;
-          continue;
-        }
-        double ex[4], ey[4];
-        bspline_w<false>(fx - i0, ex);
-        bspline_w<false>(fy - i1, ey);
-        const double *b = pl + (i1 - 1 + kH) * P + (i0 - 1 + kH);
-        double v = 0.;
+      for (int k = 0; k < CPT; ++k) {
+        const int q = threadIdx.x + k * blockDim.x;
+        if (q < nxy) {
+          const int ix = q % nx, iy = q / nx;
+          const double *b = pl + (iy + my - 1 + kH) * P + (ix + mx - 1 + kH);
+          double v = 0.;
 #pragma unroll
-        for (int ky = 0; ky < 4; ++ky) {
-          const double *r = b + ky * P;
-          const double s = ex[0] * r[0] + ex[1] * r[1] + ex[2] * r[2] + ex[3] * r[3];
-          v = fma(ey[ky], s, v);
+          for (int ky = 0; ky < 4; ++ky) {
+            const double *r = b + ky * P;
+            const double s = ex[0] * r[0] + ex[1] * r[1] + ex[2] * r[2] + ex[3] * r[3];
+            v = fma(ey[ky], s, v);
+          }
+          acc[k] += v;
         }
-        acc[k] += v;
       }
     }
     __syncthreads();
@@ -588,13 +618,14 @@ __device__ __forceinline__ bool foot4d(const HGrid &h, const double *__restrict_
     lag3w<EXACT>(EXACT ? sub(t[j], (double)ip[j]) : t[j] - ip[j], c[j]);
   }
   double e1 = 0., e2 = 0.;
+  const int r0 = wrapi(ip[0], nx), r1 = wrapi(ip[1], ny);
 #pragma unroll
   for (int k1 = 0; k1 < 3; ++k1) {
-    const int jy = wrapi(ip[1] % ny + k1, ny);
+    const int jy = r1 + k1 >= ny ? r1 + k1 - ny : r1 + k1;
 #pragma unroll
     for (int k0 = 0; k0 < 3; ++k0) {
-      const int jx = wrapi(ip[0] % nx + k0, nx);
-      const long long q = jx + (long long)nx * jy;
+      const int jx = r0 + k0 >= nx ? r0 + k0 - nx : r0 + k0;
+      const int q = jx + nx * jy;
       if (EXACT) {
         const double w = mul(c[0][k0], c[1][k1]);
         e1 = add(e1, mul(w, __ldg(ex + q)));
@@ -726,8 +757,8 @@ __global__ void __launch_bounds__(256) k_mpi_advect_4d(const double *__restrict_
 // the group reads each (vx, vy) slab's R + 3 rows of four x values once
 // and applies every cell's own weights from registers: 64 (R + 3) / R
 // loads per cell instead of 256.  Other groups interpolate cell by cell.
-template <int R>
-__global__ void __launch_bounds__(128) k_mpi_advect_4d_rows(const double *__restrict__ c, double *__restrict__ fn,
+template <int R, bool UK3>
+__global__ void __launch_bounds__(128, R <= 2 ? 3 : 2) k_mpi_advect_4d_rows(const double *__restrict__ c, double *__restrict__ fn,
                                                            const double *__restrict__ ex,
                                                            const double *__restrict__ ey, HGrid h, double dt,
                                                            double *__restrict__ part, double *__restrict__ l2,
@@ -773,8 +804,13 @@ __global__ void __launch_bounds__(128) k_mpi_advect_4d_rows(const double *__rest
           val[q] = 0.;
         }
         const double *b = c + h.at(ip[0][0] - 1, ip[0][1] - 1, ip[0][2] - 1, ip[0][3] - 1);
-#pragma unroll
+#pragma unroll(UK3 ? 4 : 1)
         for (int k3 = 0; k3 < 4; ++k3) {
+          // The cells' k3 weights (a select chain when k3 is not a constant).
+          double w3[R];
+#pragma unroll
+          for (int q = 0; q < R; ++q)
+            w3[q] = k3 == 0 ? e3[q][0] : (k3 == 1 ? e3[q][1] : (k3 == 2 ? e3[q][2] : e3[q][3]));
 #pragma unroll
           for (int k2 = 0; k2 < 4; ++k2) {
             const double *slab = b + k2 * h.s[2] + k3 * h.s[3];
@@ -795,7 +831,7 @@ __global__ void __launch_bounds__(128) k_mpi_advect_4d_rows(const double *__rest
               }
             }
 #pragma unroll
-            for (int q = 0; q < R; ++q) val[q] = fma(s2[q] * e2[q][k2], e3[q][k3], val[q]);
+            for (int q = 0; q < R; ++q) val[q] = fma(s2[q] * e2[q][k2], w3[q], val[q]);
           }
         }
       } else {
@@ -823,6 +859,153 @@ __global__ void __launch_bounds__(128) k_mpi_advect_4d_rows(const double *__rest
   }
   if (bad) atomicOr(err, 2);
   // Block sum of sq in a fixed order.
+  __shared__ double ws[4];
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  double v = sq;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((tid & 31) == 0) ws[tid >> 5] = v;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0.;
+    for (int w = 0; w < (int)(blockDim.x * blockDim.y) / 32; ++w) t += ws[w];
+    const long long bl = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+    l2[2 * bl] = t;
+    l2[2 * bl + 1] = 0.;
+  }
+}
+
+// Cubic B-spline weight k at fractional offset w, in closed form (equal to
+// the reference's expressions in exact arithmetic): (1-w)^3/6,
+// (3w^3 - 6w^2 + 4)/6, (-3w^3 + 3w^2 + 3w + 1)/6, w^3/6.
+template <int K>
+__device__ __forceinline__ double bspline_k(double w) {
+  constexpr double s = 1. / 6.;
+  if (K == 0) {
+    const double u = 1. - w;
+    return u * u * u * s;
+  } else if (K == 1) {
+    return fma(w * w, fma(3., w, -6.), 4.) * s;
+  } else if (K == 2) {
+    return fma(w, fma(w, fma(-3., w, 3.), 3.), 1.) * s;
+  } else {
+    return w * w * w * s;
+  }
+}
+
+// The fused 4D pass with R cells per thread at consecutive y, as
+// k_mpi_advect_4d_rows, keeping only the x and y weights of each cell in
+// registers: a slab's vx and vy weights are evaluated from the cells'
+// fractional offsets when the slab is reached (a few FP64 operations per
+// cell and slab instead of eight registers per cell), which leaves room for
+// four cells per thread.
+template <int R>
+__global__ void __launch_bounds__(128, 3) k_mpi_advect_4d_rows_w(const double *__restrict__ c,
+                                                                 double *__restrict__ fn,
+                                                                 const double *__restrict__ ex,
+                                                                 const double *__restrict__ ey, HGrid h, double dt,
+                                                                 double *__restrict__ part, double *__restrict__ l2,
+                                                                 int *__restrict__ err) {
+  const int ix = blockIdx.x * 32 + threadIdx.x;
+  const int iy0 = (blockIdx.y * blockDim.y + threadIdx.y) * R;
+  const int G = gridDim.z;
+  const long long planes = (long long)h.n[2] * h.n[3];
+  const long long nx = h.n[0];
+  double racc[R], sq = 0.;
+#pragma unroll
+  for (int q = 0; q < R; ++q) racc[q] = 0.;
+  bool bad = false;
+  if (ix < h.n[0] && iy0 < h.n[1]) {
+    for (long long p = blockIdx.z; p < planes; p += G) {
+      const int ivx = (int)(p % h.n[2]), ivy = (int)(p / h.n[2]);
+      double g[R][4];
+      bool ok[R];
+      bool fast = true;
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int iy = iy0 + q;
+        ok[q] = iy < h.n[1] && foot4d<false>(h, ex, ey, ix, iy < h.n[1] ? iy : iy0, ivx, ivy, dt, g[q]);
+        fast &= ok[q];
+      }
+      int ip[R][4];
+#pragma unroll
+      for (int q = 0; q < R; ++q)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) ip[q][j] = (int)floor(g[q][j]);
+#pragma unroll
+      for (int q = 1; q < R; ++q)
+        fast &= ip[q][0] == ip[0][0] && ip[q][2] == ip[0][2] && ip[q][3] == ip[0][3] && ip[q][1] == ip[0][1] + q;
+      double val[R];
+      if (fast) {
+        double e0[R][4], e1[R][4], w2[R], w3[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          bspline_w<false>(g[q][0] - ip[q][0], e0[q]);
+          bspline_w<false>(g[q][1] - ip[q][1], e1[q]);
+          w2[q] = g[q][2] - ip[q][2];
+          w3[q] = g[q][3] - ip[q][3];
+          val[q] = 0.;
+        }
+        const double *b = c + h.at(ip[0][0] - 1, ip[0][1] - 1, ip[0][2] - 1, ip[0][3] - 1);
+#pragma unroll
+        for (int k3 = 0; k3 < 4; ++k3) {
+#pragma unroll
+          for (int k2 = 0; k2 < 4; ++k2) {
+            const double *slab = b + k2 * h.s[2] + k3 * h.s[3];
+            double s2[R];
+#pragma unroll
+            for (int q = 0; q < R; ++q) s2[q] = 0.;
+#pragma unroll
+            for (int r = 0; r < R + 3; ++r) {
+              const double *row = slab + r * h.s[1];
+              const double v0 = __ldg(row), v1 = __ldg(row + 1), v2 = __ldg(row + 2), v3 = __ldg(row + 3);
+#pragma unroll
+              for (int q = 0; q < R; ++q) {
+                const int k1 = r - q;
+                if (k1 >= 0 && k1 < 4) {
+                  const double x = e0[q][0] * v0 + e0[q][1] * v1 + e0[q][2] * v2 + e0[q][3] * v3;
+                  s2[q] = fma(x, e1[q][k1], s2[q]);
+                }
+              }
+            }
+#pragma unroll
+            for (int q = 0; q < R; ++q) {
+              double b2, b3;
+              if (k2 == 0) b2 = bspline_k<0>(w2[q]);
+              else if (k2 == 1) b2 = bspline_k<1>(w2[q]);
+              else if (k2 == 2) b2 = bspline_k<2>(w2[q]);
+              else b2 = bspline_k<3>(w2[q]);
+              if (k3 == 0) b3 = bspline_k<0>(w3[q]);
+              else if (k3 == 1) b3 = bspline_k<1>(w3[q]);
+              else if (k3 == 2) b3 = bspline_k<2>(w3[q]);
+              else b3 = bspline_k<3>(w3[q]);
+              val[q] = fma(s2[q] * b2, b3, val[q]);
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          val[q] = 0.;
+          if (iy0 + q < h.n[1]) {
+            if (ok[q]) val[q] = interp4d<false>(h, c, g[q]);
+            else bad = true;
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        if (iy0 + q < h.n[1]) {
+          fn[h.at(ix, iy0 + q, ivx, ivy)] = val[q];
+          racc[q] += val[q];
+          sq = fma(val[q], val[q], sq);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q)
+      if (iy0 + q < h.n[1]) part[(long long)blockIdx.z * nx * h.n[1] + ix + nx * (iy0 + q)] = racc[q];
+  }
+  if (bad) atomicOr(err, 2);
   __shared__ double ws[4];
   const int tid = threadIdx.y * 32 + threadIdx.x;
   double v = sq;
@@ -1031,7 +1214,11 @@ int launch_advect_4d(vlp4d_ctx *c, const HGrid &h, const double *c4, double *fn,
   const dim3 block(32, 8);
   const long long bx = (h.n[0] + 31) / 32, by = (h.n[1] + 7) / 8;
   const long long planes = (long long)h.n[2] * h.n[3];
-  long long G = ((long long)c->num_sms * 8 + bx * by - 1) / (bx * by);
+  // One resident wave (see launch_advect_4d_rows_r).
+  int per_sm = 0;
+  VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mpi_advect_4d<EXACT, MOMENT>, 256, 0));
+  long long G = ((long long)c->num_sms * (per_sm > 0 ? per_sm : 1)) / (bx * by);
+  if (G < 1) G = 1;
   if (G > planes) G = planes;
   if (MOMENT) {
     if (G > c->rho_part_groups) G = c->rho_part_groups;
@@ -1047,19 +1234,30 @@ int launch_advect_4d(vlp4d_ctx *c, const HGrid &h, const double *c4, double *fn,
   return VLP4D_OK;
 }
 
-template <int R>
+template <int R, bool UK3, bool W = false>
 int launch_advect_4d_rows_r(vlp4d_ctx *c, const HGrid &h, const double *c4, double *fn, double dt, int *groups,
                             long long *blocks, cudaStream_t s) {
   const dim3 block(32, 4);
   const long long bx = (h.n[0] + 31) / 32, by = (h.n[1] + 4 * R - 1) / (4 * R);
   const long long planes = (long long)h.n[2] * h.n[3];
-  long long G = ((long long)c->num_sms * 12 + bx * by - 1) / (bx * by);
+  // One resident wave: every block walks the planes p = z, z + G, ... at
+  // the same pace, so the blocks in flight read neighbouring (vx, vy)
+  // slabs and the coefficients come from DRAM about once.
+  int per_sm = 0;
+  if (W) VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mpi_advect_4d_rows_w<R>, 128, 0));
+  else VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mpi_advect_4d_rows<R, UK3>, 128, 0));
+  long long G = ((long long)c->num_sms * (per_sm > 0 ? per_sm : 1)) / (bx * by);
+  if (G < 1) G = 1;
   if (G > planes) G = planes;
   if (G > c->rho_part_groups) G = c->rho_part_groups;
   if (G * bx * by > c->mpi_part_cap) G = c->mpi_part_cap / (bx * by);
   if (G < 1) return fail_msg(VLP4D_ERR_UNSUPPORTED, "mpi 4D advection: too many (x, y) blocks for the partials");
-  k_mpi_advect_4d_rows<R><<<dim3((unsigned)bx, (unsigned)by, (unsigned)G), block, 0, s>>>(
-      c4, fn, c->ex, c->ey, h, dt, c->rho_part, c->mpi_part, c->d_err);
+  if (W)
+    k_mpi_advect_4d_rows_w<R><<<dim3((unsigned)bx, (unsigned)by, (unsigned)G), block, 0, s>>>(
+        c4, fn, c->ex, c->ey, h, dt, c->rho_part, c->mpi_part, c->d_err);
+  else
+    k_mpi_advect_4d_rows<R, UK3><<<dim3((unsigned)bx, (unsigned)by, (unsigned)G), block, 0, s>>>(
+        c4, fn, c->ex, c->ey, h, dt, c->rho_part, c->mpi_part, c->d_err);
   VLP4D_LAUNCH_CHECK();
   *groups = (int)G;
   *blocks = G * bx * by;
@@ -1067,22 +1265,44 @@ int launch_advect_4d_rows_r(vlp4d_ctx *c, const HGrid &h, const double *c4, doub
 }
 
 // Cells per thread of the fused 4D pass (VLP4D_MPI_ROWS = 1..4 overrides;
-// 1 is the cell-per-thread kernel).
+// 1 is the cell-per-thread kernel; 12..14 the per-slab-weight variant).
 int mpi_rows() {
   static int r = [] {
     const char *e = getenv("VLP4D_MPI_ROWS");
     const int v = e && *e ? atoi(e) : 2;
-    return v < 1 ? 1 : (v > 4 ? 4 : v);
+    return (v >= 1 && v <= 4) || (v >= 12 && v <= 14) ? v : 2;
   }();
   return r;
 }
 
+// Whether the fused 4D pass unrolls its k3 loop (VLP4D_MPI_UNROLL = 0/1;
+// unrolled: more loads in flight, more registers).
+bool mpi_unroll_k3() {
+  static bool u = [] {
+    const char *e = getenv("VLP4D_MPI_UNROLL");
+    return e && *e ? atoi(e) != 0 : true;
+  }();
+  return u;
+}
+
 int launch_advect_4d_fused(vlp4d_ctx *c, const HGrid &h, const double *c4, double *fn, double dt, int *groups,
                            long long *blocks, cudaStream_t s) {
+  const bool u = mpi_unroll_k3();
+  // VLP4D_MPI_ROWS = 12, 13, 14: 2, 3, 4 cells per thread with the vx, vy
+  // weights evaluated per slab.
   switch (mpi_rows()) {
-    case 2: return launch_advect_4d_rows_r<2>(c, h, c4, fn, dt, groups, blocks, s);
-    case 3: return launch_advect_4d_rows_r<3>(c, h, c4, fn, dt, groups, blocks, s);
-    case 4: return launch_advect_4d_rows_r<4>(c, h, c4, fn, dt, groups, blocks, s);
+    case 12: return launch_advect_4d_rows_r<2, true, true>(c, h, c4, fn, dt, groups, blocks, s);
+    case 13: return launch_advect_4d_rows_r<3, true, true>(c, h, c4, fn, dt, groups, blocks, s);
+    case 14: return launch_advect_4d_rows_r<4, true, true>(c, h, c4, fn, dt, groups, blocks, s);
+    case 2:
+      return u ? launch_advect_4d_rows_r<2, true>(c, h, c4, fn, dt, groups, blocks, s)
+               : launch_advect_4d_rows_r<2, false>(c, h, c4, fn, dt, groups, blocks, s);
+    case 3:
+      return u ? launch_advect_4d_rows_r<3, true>(c, h, c4, fn, dt, groups, blocks, s)
+               : launch_advect_4d_rows_r<3, false>(c, h, c4, fn, dt, groups, blocks, s);
+    case 4:
+      return u ? launch_advect_4d_rows_r<4, true>(c, h, c4, fn, dt, groups, blocks, s)
+               : launch_advect_4d_rows_r<4, false>(c, h, c4, fn, dt, groups, blocks, s);
     default: return launch_advect_4d<false, true>(c, h, c4, fn, dt, groups, blocks, s);
   }
 }
