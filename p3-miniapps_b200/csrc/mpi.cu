@@ -874,153 +874,6 @@ __global__ void __launch_bounds__(128, R <= 2 ? 3 : 2) k_mpi_advect_4d_rows(cons
   }
 }
 
-// Cubic B-spline weight k at fractional offset w, in closed form (equal to
-// the reference's expressions in exact arithmetic): (1-w)^3/6,
-// (3w^3 - 6w^2 + 4)/6, (-3w^3 + 3w^2 + 3w + 1)/6, w^3/6.
-template <int K>
-__device__ __forceinline__ double bspline_k(double w) {
-  constexpr double s = 1. / 6.;
-  if (K == 0) {
-    const double u = 1. - w;
-    return u * u * u * s;
-  } else if (K == 1) {
-    return fma(w * w, fma(3., w, -6.), 4.) * s;
-  } else if (K == 2) {
-    return fma(w, fma(w, fma(-3., w, 3.), 3.), 1.) * s;
-  } else {
-    return w * w * w * s;
-  }
-}
-
-// The fused 4D pass with R cells per thread at consecutive y, as
-// k_mpi_advect_4d_rows, keeping only the x and y weights of each cell in
-// registers: a slab's vx and vy weights are evaluated from the cells'
-// fractional offsets when the slab is reached (a few FP64 operations per
-// cell and slab instead of eight registers per cell), which leaves room for
-// four cells per thread.
-template <int R>
-__global__ void __launch_bounds__(128, 3) k_mpi_advect_4d_rows_w(const double *__restrict__ c,
-                                                                 double *__restrict__ fn,
-                                                                 const double *__restrict__ ex,
-                                                                 const double *__restrict__ ey, HGrid h, double dt,
-                                                                 double *__restrict__ part, double *__restrict__ l2,
-                                                                 int *__restrict__ err) {
-  const int ix = blockIdx.x * 32 + threadIdx.x;
-  const int iy0 = (blockIdx.y * blockDim.y + threadIdx.y) * R;
-  const int G = gridDim.z;
-  const long long planes = (long long)h.n[2] * h.n[3];
-  const long long nx = h.n[0];
-  double racc[R], sq = 0.;
-#pragma unroll
-  for (int q = 0; q < R; ++q) racc[q] = 0.;
-  bool bad = false;
-  if (ix < h.n[0] && iy0 < h.n[1]) {
-    for (long long p = blockIdx.z; p < planes; p += G) {
-      const int ivx = (int)(p % h.n[2]), ivy = (int)(p / h.n[2]);
-      double g[R][4];
-      bool ok[R];
-      bool fast = true;
-#pragma unroll
-      for (int q = 0; q < R; ++q) {
-        const int iy = iy0 + q;
-        ok[q] = iy < h.n[1] && foot4d<false>(h, ex, ey, ix, iy < h.n[1] ? iy : iy0, ivx, ivy, dt, g[q]);
-        fast &= ok[q];
-      }
-      int ip[R][4];
-#pragma unroll
-      for (int q = 0; q < R; ++q)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) ip[q][j] = (int)floor(g[q][j]);
-#pragma unroll
-      for (int q = 1; q < R; ++q)
-        fast &= ip[q][0] == ip[0][0] && ip[q][2] == ip[0][2] && ip[q][3] == ip[0][3] && ip[q][1] == ip[0][1] + q;
-      double val[R];
-      if (fast) {
-        double e0[R][4], e1[R][4], w2[R], w3[R];
-#pragma unroll
-        for (int q = 0; q < R; ++q) {
-          bspline_w<false>(g[q][0] - ip[q][0], e0[q]);
-          bspline_w<false>(g[q][1] - ip[q][1], e1[q]);
-          w2[q] = g[q][2] - ip[q][2];
-          w3[q] = g[q][3] - ip[q][3];
-          val[q] = 0.;
-        }
-        const double *b = c + h.at(ip[0][0] - 1, ip[0][1] - 1, ip[0][2] - 1, ip[0][3] - 1);
-#pragma unroll
-        for (int k3 = 0; k3 < 4; ++k3) {
-#pragma unroll
-          for (int k2 = 0; k2 < 4; ++k2) {
-            const double *slab = b + k2 * h.s[2] + k3 * h.s[3];
-            double s2[R];
-#pragma unroll
-            for (int q = 0; q < R; ++q) s2[q] = 0.;
-#pragma unroll
-            for (int r = 0; r < R + 3; ++r) {
-              const double *row = slab + r * h.s[1];
-              const double v0 = __ldg(row), v1 = __ldg(row + 1), v2 = __ldg(row + 2), v3 = __ldg(row + 3);
-#pragma unroll
-              for (int q = 0; q < R; ++q) {
-                const int k1 = r - q;
-                if (k1 >= 0 && k1 < 4) {
-                  const double x = e0[q][0] * v0 + e0[q][1] * v1 + e0[q][2] * v2 + e0[q][3] * v3;
-                  s2[q] = fma(x, e1[q][k1], s2[q]);
-                }
-              }
-            }
-#pragma unroll
-            for (int q = 0; q < R; ++q) {
-              double b2, b3;
-              if (k2 == 0) b2 = bspline_k<0>(w2[q]);
-              else if (k2 == 1) b2 = bspline_k<1>(w2[q]);
-              else if (k2 == 2) b2 = bspline_k<2>(w2[q]);
-              else b2 = bspline_k<3>(w2[q]);
-              if (k3 == 0) b3 = bspline_k<0>(w3[q]);
-              else if (k3 == 1) b3 = bspline_k<1>(w3[q]);
-              else if (k3 == 2) b3 = bspline_k<2>(w3[q]);
-              else b3 = bspline_k<3>(w3[q]);
-              val[q] = fma(s2[q] * b2, b3, val[q]);
-            }
-          }
-        }
-      } else {
-#pragma unroll
-        for (int q = 0; q < R; ++q) {
-          val[q] = 0.;
-          if (iy0 + q < h.n[1]) {
-            if (ok[q]) val[q] = interp4d<false>(h, c, g[q]);
-            else bad = true;
-          }
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < R; ++q) {
-        if (iy0 + q < h.n[1]) {
-          fn[h.at(ix, iy0 + q, ivx, ivy)] = val[q];
-          racc[q] += val[q];
-          sq = fma(val[q], val[q], sq);
-        }
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < R; ++q)
-      if (iy0 + q < h.n[1]) part[(long long)blockIdx.z * nx * h.n[1] + ix + nx * (iy0 + q)] = racc[q];
-  }
-  if (bad) atomicOr(err, 2);
-  __shared__ double ws[4];
-  const int tid = threadIdx.y * 32 + threadIdx.x;
-  double v = sq;
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  if ((tid & 31) == 0) ws[tid >> 5] = v;
-  __syncthreads();
-  if (tid == 0) {
-    double t = 0.;
-    for (int w = 0; w < (int)(blockDim.x * blockDim.y) / 32; ++w) t += ws[w];
-    const long long bl = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
-    l2[2 * bl] = t;
-    l2[2 * bl + 1] = 0.;
-  }
-}
-
 // ---------------------------------------------------------------------------
 // Velocity moment of the grid points of a halo array (Field.cpp:5-55):
 // part[group][ixy] over the planes of the group.
@@ -1234,7 +1087,7 @@ int launch_advect_4d(vlp4d_ctx *c, const HGrid &h, const double *c4, double *fn,
   return VLP4D_OK;
 }
 
-template <int R, bool UK3, bool W = false>
+template <int R, bool UK3>
 int launch_advect_4d_rows_r(vlp4d_ctx *c, const HGrid &h, const double *c4, double *fn, double dt, int *groups,
                             long long *blocks, cudaStream_t s) {
   const dim3 block(32, 4);
@@ -1244,20 +1097,15 @@ int launch_advect_4d_rows_r(vlp4d_ctx *c, const HGrid &h, const double *c4, doub
   // the same pace, so the blocks in flight read neighbouring (vx, vy)
   // slabs and the coefficients come from DRAM about once.
   int per_sm = 0;
-  if (W) VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mpi_advect_4d_rows_w<R>, 128, 0));
-  else VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mpi_advect_4d_rows<R, UK3>, 128, 0));
+  VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mpi_advect_4d_rows<R, UK3>, 128, 0));
   long long G = ((long long)c->num_sms * (per_sm > 0 ? per_sm : 1)) / (bx * by);
   if (G < 1) G = 1;
   if (G > planes) G = planes;
   if (G > c->rho_part_groups) G = c->rho_part_groups;
   if (G * bx * by > c->mpi_part_cap) G = c->mpi_part_cap / (bx * by);
   if (G < 1) return fail_msg(VLP4D_ERR_UNSUPPORTED, "mpi 4D advection: too many (x, y) blocks for the partials");
-  if (W)
-    k_mpi_advect_4d_rows_w<R><<<dim3((unsigned)bx, (unsigned)by, (unsigned)G), block, 0, s>>>(
-        c4, fn, c->ex, c->ey, h, dt, c->rho_part, c->mpi_part, c->d_err);
-  else
-    k_mpi_advect_4d_rows<R, UK3><<<dim3((unsigned)bx, (unsigned)by, (unsigned)G), block, 0, s>>>(
-        c4, fn, c->ex, c->ey, h, dt, c->rho_part, c->mpi_part, c->d_err);
+  k_mpi_advect_4d_rows<R, UK3><<<dim3((unsigned)bx, (unsigned)by, (unsigned)G), block, 0, s>>>(
+      c4, fn, c->ex, c->ey, h, dt, c->rho_part, c->mpi_part, c->d_err);
   VLP4D_LAUNCH_CHECK();
   *groups = (int)G;
   *blocks = G * bx * by;
@@ -1265,12 +1113,12 @@ int launch_advect_4d_rows_r(vlp4d_ctx *c, const HGrid &h, const double *c4, doub
 }
 
 // Cells per thread of the fused 4D pass (VLP4D_MPI_ROWS = 1..4 overrides;
-// 1 is the cell-per-thread kernel; 12..14 the per-slab-weight variant).
+// 1 is the cell-per-thread kernel).
 int mpi_rows() {
   static int r = [] {
     const char *e = getenv("VLP4D_MPI_ROWS");
     const int v = e && *e ? atoi(e) : 2;
-    return (v >= 1 && v <= 4) || (v >= 12 && v <= 14) ? v : 2;
+    return v >= 1 && v <= 4 ? v : 2;
   }();
   return r;
 }
@@ -1288,12 +1136,7 @@ bool mpi_unroll_k3() {
 int launch_advect_4d_fused(vlp4d_ctx *c, const HGrid &h, const double *c4, double *fn, double dt, int *groups,
                            long long *blocks, cudaStream_t s) {
   const bool u = mpi_unroll_k3();
-  // VLP4D_MPI_ROWS = 12, 13, 14: 2, 3, 4 cells per thread with the vx, vy
-  // weights evaluated per slab.
   switch (mpi_rows()) {
-    case 12: return launch_advect_4d_rows_r<2, true, true>(c, h, c4, fn, dt, groups, blocks, s);
-    case 13: return launch_advect_4d_rows_r<3, true, true>(c, h, c4, fn, dt, groups, blocks, s);
-    case 14: return launch_advect_4d_rows_r<4, true, true>(c, h, c4, fn, dt, groups, blocks, s);
     case 2:
       return u ? launch_advect_4d_rows_r<2, true>(c, h, c4, fn, dt, groups, blocks, s)
                : launch_advect_4d_rows_r<2, false>(c, h, c4, fn, dt, groups, blocks, s);
