@@ -116,59 +116,77 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // loop and the powers of alpha built by repeated products, as the
 // reference does.  Every grid dimension is at least MMAX + 2 = 10, so the
 // sums read interior points only.
-__global__ void k_mpi_halo(double *__restrict__ f, HGrid h) {
-  const long long total = h.total();
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x) {
-    long long r0 = i;
-    int c[4];
+// The value of halo point c (not a grid point) of a halo-filled array.
+__device__ double halo_value(const double *__restrict__ f, const HGrid &h, const int c[4]) {
+  int B[4], sg[4], r[4], m = 0;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      c[k] = (int)(r0 % h.e[k]) - kH;
-      r0 /= h.e[k];
-    }
-    bool inside = true;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) inside &= (c[k] >= 0 && c[k] < h.n[k]);
-    if (inside) continue;
-    int B[4], sg[4], r[4], m = 0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (c[k] == -kH || c[k] == h.n[k] + kH - 1) {
-        sg[k] = c[k] == -kH ? -1 : 1;
-        B[m++] = k;
-        r[k] = wrapi(c[k] - sg[k], h.n[k]);
-      } else {
-        sg[k] = 0;
-        r[k] = wrapi(c[k], h.n[k]);
-      }
-    }
-    double val;
-    if (m == 0) {
-      val = f[h.at(r[0], r[1], r[2], r[3])];
+  for (int k = 0; k < 4; ++k) {
+    if (c[k] == -kH || c[k] == h.n[k] + kH - 1) {
+      sg[k] = c[k] == -kH ? -1 : 1;
+      B[m++] = k;
+      r[k] = wrapi(c[k] - sg[k], h.n[k]);
     } else {
-      int j[4] = {1, 1, 1, 1};
-      double w[4];
-      w[m - 1] = h.alpha;
-      for (int l = m - 2; l >= 0; --l) w[l] = mul(h.alpha, w[l + 1]);
-      double sum = 0.;
-      for (;;) {
-        int p[4] = {r[0], r[1], r[2], r[3]};
-        for (int l = 0; l < m; ++l) p[B[l]] += sg[B[l]] * j[l];
-        sum = add(sum, mul(f[h.at(p[0], p[1], p[2], p[3])], w[0]));
-        int l = 0;
-        w[0] = mul(w[0], h.alpha);
-        while (l < m && ++j[l] > kMmax) {
-          j[l] = 1;
-          ++l;
-          if (l < m) w[l] = mul(w[l], h.alpha);
-        }
-        if (l == m) break;
-        for (int q = l - 1; q >= 0; --q) w[q] = mul(h.alpha, w[q + 1]);
-      }
-      val = sum;
+      sg[k] = 0;
+      r[k] = wrapi(c[k], h.n[k]);
     }
-    f[i] = val;
+  }
+  if (m == 0) return f[h.at(r[0], r[1], r[2], r[3])];
+  int j[4] = {1, 1, 1, 1};
+  double w[4];
+  w[m - 1] = h.alpha;
+  for (int l = m - 2; l >= 0; --l) w[l] = mul(h.alpha, w[l + 1]);
+  double sum = 0.;
+  for (;;) {
+    int p[4] = {r[0], r[1], r[2], r[3]};
+    for (int l = 0; l < m; ++l) p[B[l]] += sg[B[l]] * j[l];
+    sum = add(sum, mul(f[h.at(p[0], p[1], p[2], p[3])], w[0]));
+    int l = 0;
+    w[0] = mul(w[0], h.alpha);
+    while (l < m && ++j[l] > kMmax) {
+      j[l] = 1;
+      ++l;
+      if (l < m) w[l] = mul(w[l], h.alpha);
+    }
+    if (l == m) break;
+    for (int q = l - 1; q >= 0; --q) w[q] = mul(h.alpha, w[q + 1]);
+  }
+  return sum;
+}
+
+// One block per extended (vx, vy) plane: a plane with vx, vy both grid
+// coordinates has only its x/y ring (e0 e1 - n0 n1 points) in the halo,
+// any other plane is halo throughout.  Halo points only read grid points,
+// so the order of the writes does not matter.
+__global__ void k_mpi_halo(double *__restrict__ f, HGrid h) {
+  const long long planes = h.e[2] * h.e[3];
+  const int e0 = (int)h.e[0], e1 = (int)h.e[1];
+  const int ring = e0 * e1 - h.n[0] * h.n[1];
+  for (long long pl = blockIdx.x; pl < planes; pl += gridDim.x) {
+    const int cvx = (int)(pl % h.e[2]) - kH, cvy = (int)(pl / h.e[2]) - kH;
+    const bool vin = cvx >= 0 && cvx < h.n[2] && cvy >= 0 && cvy < h.n[3];
+    const int count = vin ? ring : e0 * e1;
+    for (int t = threadIdx.x; t < count; t += blockDim.x) {
+      int cx, cy;
+      if (vin) {
+        // The ring: rows -3..-1 and n1..n1+2 in full, then the six halo
+        // columns of the interior rows.
+        const int full = 2 * kH * e0;
+        if (t < full) {
+          const int rr = t / e0;
+          cy = rr < kH ? rr - kH : h.n[1] + rr - kH;
+          cx = t % e0 - kH;
+        } else {
+          const int u = t - full, k = u % (2 * kH);
+          cy = u / (2 * kH);
+          cx = k < kH ? k - kH : h.n[0] + k - kH;
+        }
+      } else {
+        cx = t % e0 - kH;
+        cy = t / e0 - kH;
+      }
+      const int c[4] = {cx, cy, cvx, cvy};
+      f[h.at(cx, cy, cvx, cvy)] = halo_value(f, h, c);
+    }
   }
 }
 
@@ -901,13 +919,16 @@ __device__ __forceinline__ void kahan(double &s, double &c, double x) {
 // (sum, compensation) pair, threads reduced in a fixed order.
 __global__ void __launch_bounds__(256) k_mpi_l2_partial(const double *__restrict__ f, HGrid h,
                                                         double *__restrict__ l2) {
+  // A warp walks rows (32 x positions at a time); the block's 8 warps take
+  // rows r = 8 * blockIdx + warp, stepping by 8 * gridDim.
   const long long rows = (long long)h.n[1] * h.n[2] * h.n[3];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   double s = 0., cp = 0.;
-  for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+  for (long long r = (long long)blockIdx.x * nw + warp; r < rows; r += (long long)gridDim.x * nw) {
     const int iy = (int)(r % h.n[1]);
     const long long rv = r / h.n[1];
     const double *row = f + h.at(0, iy, (int)(rv % h.n[2]), (int)(rv / h.n[2]));
-    for (int ix = threadIdx.x; ix < h.n[0]; ix += blockDim.x) {
+    for (int ix = lane; ix < h.n[0]; ix += 32) {
       const double v = __ldg(row + ix);
       kahan(s, cp, v * v);
     }
@@ -972,7 +993,9 @@ int smem_limit(const vlp4d_ctx *c) {
 }
 
 int launch_halo(vlp4d_ctx *c, const HGrid &h, double *f, cudaStream_t s) {
-  k_mpi_halo<<<c->num_sms * 8, 256, 0, s>>>(f, h);
+  long long grid = (long long)c->num_sms * 8;
+  if (grid > h.e[2] * h.e[3]) grid = h.e[2] * h.e[3];
+  k_mpi_halo<<<(unsigned)grid, 256, 0, s>>>(f, h);
   VLP4D_LAUNCH_CHECK();
   return VLP4D_OK;
 }

@@ -198,3 +198,54 @@ def test_argument_checks(pkg, cuda):
         with pytest.raises(vl.Vlp4dError) as e:
             ctx.mpi_step(a, a, 1)
         assert e.value.code == vl.ERR_INVALID_ARG
+
+
+def test_fused_step_matches_entry_point_sequence_64(pkg, cuda):
+    """At 64^4 (beyond what the CPU checker covers quickly) the fused step
+    against the reference-order entry points on the GPU, which are
+    bit-identical to the reference stage by stage: three steps on the SLD10
+    deck geometry, states within 1e-12 of max|f| and equal diagnostics."""
+    torch = cuda
+    n, L, dt, steps = 64, 12.56637112, 0.01, 3
+    dom = _dom(pkg, (n,) * 4, (0, 0, -9, -9), (L, L, 9, 9), dt, 10, steps)
+    with pkg.Context(dom, "f64") as ctx:
+        # SLD10 initial condition on the device (Init.cpp:228-247).
+        dx = [(dom.max_phy[k] - dom.min_phy[k]) / n for k in range(4)]
+        ar = lambda k: dom.min_phy[k] + torch.arange(n, dtype=torch.float64, device="cuda") * dx[k]
+        x, y, vx, vy = ar(0), ar(1), ar(2), ar(3)
+        f0 = ctx.mpi_empty()
+        f0[3:-3, 3:-3, 3:-3, 3:-3] = (torch.exp(-0.5 * (vy[:, None] ** 2 + vx[None, :] ** 2)) / (2 * np.pi))[
+            :, :, None, None] * (1 + 0.05 * torch.cos(0.5 * y)[:, None] * torch.cos(0.5 * x)[None, :])[None, None]
+        # Fused.
+        a, b = f0.clone(), ctx.mpi_empty()
+        fused = ctx.mpi_run(a, b, steps)
+        ctx.check()
+        nrj_f, _ = ctx.diags_read()
+        _, _, l2_f = ctx.diags_read_ext()
+        got = fused[3:-3, 3:-3, 3:-3, 3:-3].clone()
+        del a, b, fused
+        # Reference order.
+        fn, fnp1, tmp = f0.clone(), ctx.mpi_empty(), ctx.mpi_empty()
+        ctx.mpi_field(fn)
+        ctx.diags_compute(0)
+        ctx.mpi_l2norm(fn, 0)
+        for it in range(1, steps + 1):
+            ctx.mpi_halo_fill(fn)
+            ctx.mpi_spline_xy(fn)
+            fnp1.copy_(fn)
+            ctx.mpi_advect_2d(fn, tmp, 0.5 * dt)
+            ctx.mpi_field(fn)
+            ctx.mpi_spline_vxvy(fnp1)
+            ctx.mpi_advect_4d(fnp1, fn, dt)
+            ctx.mpi_field(fnp1)
+            ctx.diags_compute(it)
+            ctx.mpi_l2norm(fnp1, it)
+            fn, fnp1 = fnp1, fn
+        ctx.check()
+        nrj_r, _ = ctx.diags_read()
+        _, _, l2_r = ctx.diags_read_ext()
+        want = fn[3:-3, 3:-3, 3:-3, 3:-3]
+        err = float((got - want).abs().max() / want.abs().max())
+    assert err <= 1e-12
+    np.testing.assert_allclose(nrj_f, nrj_r, rtol=0, atol=1e-11)
+    np.testing.assert_allclose(l2_f, l2_r, rtol=1e-12)
