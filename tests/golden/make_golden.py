@@ -18,6 +18,10 @@ oracle/ref_driver.cpp) on small seeded inputs and stores what it computes:
   (tests/openmp/test_fft.cpp:7-71) through its Impl::FFT wrapper.
 * ``<deck>_nrj.out``: nrj.out written by the reference's own driver
   (oracle/_ref/vlp4d_ref) on the small decks in decks/.
+* ``<deck>_nrj.out`` / ``<deck>_l2norm.out`` for the vlp4d_mpi decks
+  ``sld10_mpi_12`` and ``tsi20_mpi_32x10``: written by the reference's own
+  vlp4d_mpi driver (oracle/_ref/vlp4d_mpi_ref, main() of
+  miniapps/vlp4d_mpi/openmp/Vlp4d.cpp, one process).
 * ``mpi_stages_small.npz``: the reference's OpenMP vlp4d_mpi
   (miniapps/vlp4d_mpi/openmp, one process, oracle/_ref/libvlp4d_mpi_ref.so
   driven by oracle/ref_mpi_driver.cpp) on a 10x12x10x11 grid: digests of
@@ -215,6 +219,29 @@ def mpi_stages():
     print("mpi_stages_small:", n)
 
 
+def mpi_deck_runs():
+    """The reference's own vlp4d_mpi driver on two small decks (every
+    dimension at least 10); keeps its nrj.out and l2norm.out."""
+    import shutil
+    import subprocess
+    import tempfile
+
+    exe = ROOT / "oracle" / "_ref" / "vlp4d_mpi_ref"
+    decks = OUT / "decks"
+    write_deck(decks / "sld10_mpi_12.dat", [12] * 4, ["0.", "0.", "-9.", "-9."], ["12.56637112"] * 2 + ["9.", "9."],
+               10, 0.05, 20, 4, 0)
+    write_deck(decks / "tsi20_mpi_32x10.dat", [32, 10, 32, 10], ["0.", "0.", "-9.", "-9."],
+               ["25.13274122871834590"] * 2 + ["9.", "9."], 20, 0.05, 20, 4, 0)
+    for name in ("sld10_mpi_12", "tsi20_mpi_32x10"):
+        with tempfile.TemporaryDirectory() as d:
+            shutil.copy(decks / f"{name}.dat", Path(d) / "deck.dat")
+            subprocess.run([str(exe), "-f", "deck.dat"], cwd=d, check=True, capture_output=True,
+                           env={"OMP_NUM_THREADS": "4", "PATH": "/usr/bin:/bin"})
+            shutil.copy(Path(d) / "nrj.out", OUT / f"{name}_nrj.out")
+            shutil.copy(Path(d) / "l2norm.out", OUT / f"{name}_l2norm.out")
+        print("mpi deck run:", name)
+
+
 def main():
     build(reference=True)
     if not Reference.available():
@@ -229,6 +256,7 @@ def main():
     deck_runs()
     if MpiReference.available():
         mpi_stages()
+        mpi_deck_runs()
 
 
 if __name__ == "__main__":

@@ -249,3 +249,27 @@ def test_fused_step_matches_entry_point_sequence_64(pkg, cuda):
     assert err <= 1e-12
     np.testing.assert_allclose(nrj_f, nrj_r, rtol=0, atol=1e-11)
     np.testing.assert_allclose(l2_f, l2_r, rtol=1e-12)
+
+
+@pytest.mark.parametrize("deck", ["sld10_mpi_12", "tsi20_mpi_32x10"])
+def test_decks_match_reference_main(pkg, cuda, deck):
+    """The fused step on the decks the reference's own vlp4d_mpi main() ran
+    (nrj.out / l2norm.out in tests/golden, 13 printed digits)."""
+    torch = cuda
+    from conftest import GOLDEN
+
+    dom = pkg.Domain.from_deck(GOLDEN / "decks" / f"{deck}.dat")
+    ic = IC_SLD10 if dom.idcase == 10 else IC_TSI20_MPI
+    rest = MpiRestatement(dom.nxmax, dom.min_phy, dom.max_phy, dom.dt, dom.idcase)
+    with pkg.Context(dom, "f64") as ctx:
+        fn, fnp1 = _dev(torch, rest.init_halo(ic)), ctx.mpi_empty()
+        ctx.mpi_run(fn, fnp1, dom.nbiter)
+        ctx.check()
+        nrj, _ = ctx.diags_read()
+        nrjx, nrjy, l2 = ctx.diags_read_ext()
+    ref = np.loadtxt(GOLDEN / f"{deck}_nrj.out")
+    ref_l2 = np.loadtxt(GOLDEN / f"{deck}_l2norm.out")
+    np.testing.assert_allclose(nrj, ref[:, 1], rtol=1e-11)
+    np.testing.assert_allclose(nrjx, ref[:, 2], rtol=1e-11)
+    np.testing.assert_allclose(nrjy, ref[:, 3], rtol=1e-11)
+    np.testing.assert_allclose(l2, ref_l2[:, 1], rtol=1e-12)

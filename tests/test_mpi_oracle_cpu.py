@@ -159,3 +159,26 @@ def test_halo_fill_periodic_images_and_outer_sums():
     right = sum(alpha ** j * inner[:, :, :, (1 + j) % n[0]] for j in range(1, 9))
     np.testing.assert_allclose(h[3:-3, 3:-3, 3:-3, 0], left, rtol=1e-13, atol=1e-15)
     np.testing.assert_allclose(h[3:-3, 3:-3, 3:-3, -1], right, rtol=1e-13, atol=1e-15)
+
+
+def _read_deck(path):
+    """Values after each ':' of a reference deck (Init.cpp:12-90 order)."""
+    vals = [line.split(":", 1)[1].strip() for line in Path(path).read_text().splitlines() if ":" in line]
+    n = [int(v) for v in vals[0:4]]
+    mm = [float(v) for v in vals[4:12]]
+    minp, maxp = mm[0::2], mm[1::2]
+    return n, minp, maxp, int(vals[12]), float(vals[13]), int(vals[14])
+
+
+@pytest.mark.parametrize("deck", ["sld10_mpi_12", "tsi20_mpi_32x10"])
+def test_restatement_matches_reference_main_decks(deck):
+    """nrj.out and l2norm.out written by the reference's own vlp4d_mpi
+    main() (Vlp4d.cpp, one process) on two small decks."""
+    n, minp, maxp, case, dt, steps = _read_deck(GOLDEN / "decks" / f"{deck}.dat")
+    ic = IC_SLD10 if case == 10 else IC_TSI20_MPI
+    rest = MpiRestatement(n, minp, maxp, dt, case)
+    _, diags, _, _ = rest.run_mpi(rest.init_halo(ic), steps)
+    nrj = np.loadtxt(GOLDEN / f"{deck}_nrj.out")
+    l2 = np.loadtxt(GOLDEN / f"{deck}_l2norm.out")
+    np.testing.assert_allclose(nrj[:, 1:4], diags[:, 0:3], rtol=1e-12, atol=0)
+    np.testing.assert_allclose(l2[:, 1], diags[:, 4], rtol=1e-12, atol=0)
