@@ -398,10 +398,13 @@ __device__ void plane_extend(double *pl, int P, const HGrid &h) {
 // plane's grid points from fn, builds its halo, prefilters it, writes the
 // coefficients of the whole extended plane into cxy, and evaluates the 2D
 // advection by dt (Advection.hpp thrust :131-214) at every grid point,
-// adding it to the thread's moment accumulators (cell q = tid + k*blockDim
-// of the plane, planes in a fixed order).  The accumulators go to
-// part[blockIdx.x][q] at the end.  A foot outside the spline's range sets
-// bit 2 of *err (the reference stops: "Time step is too large").
+// adding it to the thread's moment accumulators, planes in a fixed order.
+// Thread t owns the CPT cells of column t % nx, rows (t / nx) * CPT ..;
+// it walks them with a sliding window of four x sums, so a cell costs
+// about 4 shared-memory loads instead of 16.  The accumulators go to
+// part[blockIdx.x][ix + nx*iy] at the end.  A foot outside the spline's
+// range sets bit 2 of *err (the reference stops: "Time step is too
+// large").
 template <int CPT>
 __global__ void __launch_bounds__(512) k_mpi_xy_pass(const double *__restrict__ fn, double *__restrict__ cxy,
                                                      HGrid h, int P, double dt, double *__restrict__ part,
@@ -415,6 +418,9 @@ __global__ void __launch_bounds__(512) k_mpi_xy_pass(const double *__restrict__ 
 #pragma unroll
   for (int k = 0; k < CPT; ++k) acc[k] = 0.;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  // This thread's strip of the 2D advection: column ix, rows iy0 .. iy0+CPT-1.
+  const int ix = threadIdx.x % nx, iy0 = (threadIdx.x / nx) * CPT;
+  const bool own = iy0 < ny;
   bool bad = false;
   for (long long p = blockIdx.x; p < planes; p += gridDim.x) {
     const int ivx = (int)(p % nvx), ivy = (int)(p / nvx);
@@ -439,31 +445,33 @@ __global__ void __launch_bounds__(512) k_mpi_xy_pass(const double *__restrict__ 
     double ex[4], ey[4];
     bspline_w<false>(fx - mx, ex);
     bspline_w<false>(fy - my, ey);
-    if (!bad) {
+    if (!bad && own) {
+      // x sums of rows iy0 + my - 1 + r (r = 0 .. CPT + 2), a window of four.
+      const double *b = pl + (iy0 + my - 1 + kH) * P + (ix + mx - 1 + kH);
+      double w0 = 0., w1 = 0., w2 = 0.;
 #pragma unroll
-      for (int k = 0; k < CPT; ++k) {
-        const int q = threadIdx.x + k * blockDim.x;
-        if (q < nxy) {
-          const int ix = q % nx, iy = q / nx;
-          const double *b = pl + (iy + my - 1 + kH) * P + (ix + mx - 1 + kH);
-          double v = 0.;
-#pragma unroll
-          for (int ky = 0; ky < 4; ++ky) {
-            const double *r = b + ky * P;
-            const double s = ex[0] * r[0] + ex[1] * r[1] + ex[2] * r[2] + ex[3] * r[3];
-            v = fma(ey[ky], s, v);
-          }
-          acc[k] += v;
+      for (int r = 0; r < CPT + 3; ++r) {
+        double w3 = 0.;
+        if (iy0 + r - 3 < ny) {  // row needed by some cell of the strip
+          const double *row = b + r * P;
+          w3 = ex[0] * row[0] + ex[1] * row[1] + ex[2] * row[2] + ex[3] * row[3];
         }
+        if (r >= 3) {
+          const int j = r - 3;
+          if (iy0 + j < ny) acc[j] += ey[0] * w0 + ey[1] * w1 + ey[2] * w2 + ey[3] * w3;
+        }
+        w0 = w1;
+        w1 = w2;
+        w2 = w3;
       }
     }
     __syncthreads();
   }
   if (bad) atomicOr(err, 2);
+  if (own) {
 #pragma unroll
-  for (int k = 0; k < CPT; ++k) {
-    const int q = threadIdx.x + k * blockDim.x;
-    if (q < nxy) part[(long long)blockIdx.x * nxy + q] = acc[k];
+    for (int j = 0; j < CPT; ++j)
+      if (iy0 + j < ny) part[(long long)blockIdx.x * nxy + ix + (long long)nx * (iy0 + j)] = acc[j];
   }
 }
 
@@ -1070,15 +1078,18 @@ int launch_xy_pass(vlp4d_ctx *c, const HGrid &h, const double *fn, double *cxy, 
                    cudaStream_t s) {
   if (plane_bytes(h) > (size_t)smem_limit(c))
     return fail_msg(VLP4D_ERR_UNSUPPORTED, "mpi_step: the (x, y) plane does not fit in shared memory");
-  const long long nxy = (long long)h.n[0] * h.n[1];
-  const long long cpt = (nxy + 511) / 512;
-  if (cpt <= 1) return launch_xy_pass_cpt<1>(c, h, fn, cxy, dt, groups, s);
-  if (cpt <= 2) return launch_xy_pass_cpt<2>(c, h, fn, cxy, dt, groups, s);
-  if (cpt <= 4) return launch_xy_pass_cpt<4>(c, h, fn, cxy, dt, groups, s);
-  if (cpt <= 8) return launch_xy_pass_cpt<8>(c, h, fn, cxy, dt, groups, s);
-  if (cpt <= 16) return launch_xy_pass_cpt<16>(c, h, fn, cxy, dt, groups, s);
-  if (cpt <= 32) return launch_xy_pass_cpt<32>(c, h, fn, cxy, dt, groups, s);
-  return fail_msg(VLP4D_ERR_UNSUPPORTED, "mpi_step: nx*ny above 16384");
+  // Cells per thread: the smallest CPT whose strips (nx columns of
+  // ceil(ny / CPT) strips) fit in the 512 threads.
+  const long long nx = h.n[0], ny = h.n[1];
+  auto fits = [&](long long cpt) { return nx * ((ny + cpt - 1) / cpt) <= 512; };
+  if (nx > 512) return fail_msg(VLP4D_ERR_UNSUPPORTED, "mpi_step: nx above 512");
+  if (fits(1)) return launch_xy_pass_cpt<1>(c, h, fn, cxy, dt, groups, s);
+  if (fits(2)) return launch_xy_pass_cpt<2>(c, h, fn, cxy, dt, groups, s);
+  if (fits(4)) return launch_xy_pass_cpt<4>(c, h, fn, cxy, dt, groups, s);
+  if (fits(8)) return launch_xy_pass_cpt<8>(c, h, fn, cxy, dt, groups, s);
+  if (fits(16)) return launch_xy_pass_cpt<16>(c, h, fn, cxy, dt, groups, s);
+  if (fits(32)) return launch_xy_pass_cpt<32>(c, h, fn, cxy, dt, groups, s);
+  return fail_msg(VLP4D_ERR_UNSUPPORTED, "mpi_step: the x/y plane needs more than 32 cells per thread");
 }
 
 // 4D advection of the coefficients c4 into fn's grid points; MOMENT: with
