@@ -437,19 +437,6 @@ def adjoint_arm(pkg, torch, stream, n=64, nsteps=200, every=8):
 MPI_L = 12.56637112  # wk/SLD10.dat: x, y in [0, 12.56637112), v in [-9, 9), dt 0.01
 
 
-def _mpi_init_sld10(torch, ctx, fn):
-    """SLD10 initial condition of vlp4d_mpi (Init.cpp:228-247) on the grid
-    points of a halo array: (1/2pi) exp(-(vx^2+vy^2)/2) (1 + 0.05 cos(x/2) cos(y/2))."""
-    nx, ny, nvx, nvy = ctx.dom.nxmax
-    dx = [(ctx.dom.max_phy[k] - ctx.dom.min_phy[k]) / ctx.dom.nxmax[k] for k in range(4)]
-    ar = lambda k, m: ctx.dom.min_phy[k] + torch.arange(m, dtype=torch.float64, device="cuda") * dx[k]
-    x, y, vx, vy = ar(0, nx), ar(1, ny), ar(2, nvx), ar(3, nvy)
-    sp = 1 + 0.05 * torch.cos(0.5 * y)[:, None] * torch.cos(0.5 * x)[None, :]
-    mv = torch.exp(-0.5 * (vy[:, None] ** 2 + vx[None, :] ** 2)) / (2 * math.pi)
-    fn.zero_()
-    fn[3:-3, 3:-3, 3:-3, 3:-3] = mv[:, :, None, None] * sp[None, None, :, :]
-
-
 def mpi_reference_cpu(n, budget_s=20.0):
     """The reference's own OpenMP vlp4d_mpi (oracle/_ref/libvlp4d_mpi_ref.so,
     one process) on an n^4 SLD10 grid: one untimed step, then steps while
@@ -488,7 +475,7 @@ def mpi_arm(pkg, torch, stream, peak, n=128, nsteps=10, warmup=3):
     cells = n ** 4
     with pkg.Context(dom, "f64") as ctx:
         fn, fnp1 = ctx.mpi_empty(), ctx.mpi_empty()
-        _mpi_init_sld10(torch, ctx, fn)
+        ctx.mpi_init_case(fn)  # SLD10 (Init.cpp:228-247) on the device
         ctx.mpi_field(fn)
         ctx.diags_compute(0)
         ctx.mpi_l2norm(fn, 0)

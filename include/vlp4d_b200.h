@@ -322,6 +322,11 @@ int vlp4d_ensemble_autotune(vlp4d_ensemble *ens, int steps, const char *csv_path
  * step is too large", thrust/Advection.hpp:21-26).  All calls are
  * asynchronous on `stream`. */
 size_t vlp4d_mpi_size(const vlp4d_ctx *ctx);
+/* initcase of vlp4d_mpi (miniapps/vlp4d_mpi/openmp/Init.cpp:126-277) for the
+ * domain's idcase: 10 SLD10, 20 TSI20 (vlp4d_mpi's own formula), 2/5 CYL02/
+ * CYL05, on the grid points of fn; the halo is zero (Init.cpp:370-372).
+ * Another idcase is VLP4D_ERR_INVALID_ARG (the reference aborts). */
+int vlp4d_mpi_init_case(vlp4d_ctx *ctx, void *fn, void *stream);
 /* Distrib::exchangeHalo for one process (thrust/Communication.cpp, with the
  * spline boundary sums of Communication.hpp boundary_condition): periodic
  * images in the halo, sum_{j=1..8} alpha^j f(...) in its outermost layer.

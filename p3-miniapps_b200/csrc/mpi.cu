@@ -901,6 +901,61 @@ __global__ void __launch_bounds__(128, R <= 2 ? 3 : 2) k_mpi_advect_4d_rows(cons
 }
 
 // ---------------------------------------------------------------------------
+// initcase of vlp4d_mpi (Init.cpp:126-277) on a halo array: the halo is
+// zero, as after init() (Init.cpp:370-372); grid points get
+//   10 SLD10: (1/2pi) exp(-(vx^2+vy^2)/2) (1 + 0.05 cos(x/2) cos(y/2))
+//   20 TSI20: 1/(4 pi vthx vthy) (1 - ax sin(kx x) - ay sin(ky y))
+//             [exp(-((vx-vd)/vthx)^2/2 - (vy/vthy)^2/2) + (vx+vd) term],
+//             vd 2.4, vthx 1, vthy 0.5, ax 0.05, ay 0.25, kx = ky = 0.2
+//   2, 5 CYL02 / CYL05: AMPLI hx hv with the cosine bumps of x, vx (2) or
+//             y, vy (5); case 5 leaves the last vx, y and x index at 0, as
+//             the reference's loops do (Init.cpp:198-202 stop before
+//             local_nxmax).
+__global__ void k_mpi_init_case(double *__restrict__ f, HGrid h, int idcase) {
+  const long long total = h.total();
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    long long r0 = i;
+    int c[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      c[k] = (int)(r0 % h.e[k]) - kH;
+      r0 /= h.e[k];
+    }
+    bool inside = true;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) inside &= (c[k] >= 0 && c[k] < h.n[k]);
+    double v = 0.;
+    if (inside) {
+      const double x = h.minp[0] + c[0] * h.dx[0], y = h.minp[1] + c[1] * h.dx[1];
+      const double vx = h.minp[2] + c[2] * h.dx[2], vy = h.minp[3] + c[3] * h.dx[3];
+      if (idcase == 10) {
+        const double sum = vx * vx + vy * vy;
+        v = (1. / (2 * M_PI)) * exp(-0.5 * sum) * (1 + 0.05 * (cos(0.5 * x) * cos(0.5 * y)));
+      } else if (idcase == 20) {
+        const double vd = 2.4, vthx = 1.0, vthy = 0.5, ax = 0.05, ay = 0.25, kx = 0.2, ky = 0.2;
+        const double a = (vx - vd) / vthx, b = (vx + vd) / vthx, q = vy / vthy;
+        v = 1. / (4 * M_PI * vthx * vthy) * (1 - ax * sin(kx * x) - ay * sin(ky * y)) *
+            (exp(-.5 * (a * a + q * q)) + exp(-.5 * (b * b + q * q)));
+      } else if (idcase == 2 || idcase == 5) {
+        const bool skip = idcase == 5 && (c[2] == h.n[2] - 1 || c[1] == h.n[1] - 1 || c[0] == h.n[0] - 1);
+        if (!skip) {
+          const double PERIOD = 0.5 * M_PI, AMPLI = 4, cc = 0.50 * (6. / 16.), rc = 0.50 * (4. / 16.);
+          const double xx = idcase == 2 ? x : y, vv = idcase == 2 ? vx : vy;
+          double hv = 0.0, hx = 0.0;
+          if ((vv <= cc + rc) && (vv >= cc - rc)) hv = cos(PERIOD * ((vv - cc) / rc));
+          else if ((vv <= -cc + rc) && (vv >= -cc - rc)) hv = -cos(PERIOD * ((vv + cc) / rc));
+          if ((xx <= cc + rc) && (xx >= cc - rc)) hx = cos(PERIOD * ((xx - cc) / rc));
+          else if ((xx <= -cc + rc) && (xx >= -cc - rc)) hx = -cos(PERIOD * ((xx + cc) / rc));
+          v = AMPLI * hx * hv;
+        }
+      }
+    }
+    f[i] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Velocity moment of the grid points of a halo array (Field.cpp:5-55):
 // part[group][ixy] over the planes of the group.
 __global__ void k_mpi_rho_partial(const double *__restrict__ f, double *__restrict__ part, HGrid h, int groups) {
@@ -1215,6 +1270,17 @@ size_t vlp4d_mpi_size(const vlp4d_ctx *ctx) {
   size_t n = 1;
   for (int k = 0; k < 4; ++k) n *= (size_t)(ctx->g.n[k] + 2 * kH);
   return n;
+}
+
+int vlp4d_mpi_init_case(vlp4d_ctx *ctx, void *fn, void *stream) {
+  int rc = mpi_check(ctx, "mpi_init_case");
+  if (rc || (rc = mpi_check_ptr(fn, "mpi_init_case"))) return rc;
+  const int ic = ctx->dom.idcase;
+  if (ic != 2 && ic != 5 && ic != 10 && ic != 20)
+    return fail_msg(VLP4D_ERR_INVALID_ARG, "mpi_init_case: unknown test case (the reference aborts, Init.cpp:142-145)");
+  k_mpi_init_case<<<ctx->num_sms * 8, 256, 0, (cudaStream_t)stream>>>((double *)fn, make_hgrid(ctx), ic);
+  VLP4D_LAUNCH_CHECK();
+  return VLP4D_OK;
 }
 
 int vlp4d_mpi_halo_fill(vlp4d_ctx *ctx, void *fn, void *stream) {

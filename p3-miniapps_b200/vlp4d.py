@@ -38,7 +38,7 @@ EXPORTS = (
     "vlp4d_ensemble_create", "vlp4d_ensemble_destroy", "vlp4d_ensemble_run", "vlp4d_ensemble_check",
     "vlp4d_ensemble_read", "vlp4d_ensemble_cells", "vlp4d_ensemble_set_tiles", "vlp4d_ensemble_get_tiles",
     "vlp4d_ensemble_autotune", "vlp4d_selftest_wait_timeout", "vlp4d_diags_l2norm", "vlp4d_diags_read_ext",
-    "vlp4d_mpi_size", "vlp4d_mpi_halo_fill", "vlp4d_mpi_spline_xy", "vlp4d_mpi_spline_vxvy", "vlp4d_mpi_advect_2d",
+    "vlp4d_mpi_size", "vlp4d_mpi_init_case", "vlp4d_mpi_halo_fill", "vlp4d_mpi_spline_xy", "vlp4d_mpi_spline_vxvy", "vlp4d_mpi_advect_2d",
     "vlp4d_mpi_advect_4d", "vlp4d_mpi_field", "vlp4d_mpi_l2norm", "vlp4d_mpi_step",
 )
 HALO = 3  # HALO_PTS of the vlp4d_mpi halo-extended arrays
@@ -133,7 +133,8 @@ def lib() -> C.CDLL:
         L.vlp4d_diags_l2norm.argtypes = [vp, vp, i, vp]
         L.vlp4d_diags_read_ext.argtypes = [vp, dp, dp, dp, i]
         L.vlp4d_mpi_size.argtypes = [vp]
-        for n in ("vlp4d_mpi_halo_fill", "vlp4d_mpi_spline_xy", "vlp4d_mpi_spline_vxvy", "vlp4d_mpi_field"):
+        for n in ("vlp4d_mpi_init_case", "vlp4d_mpi_halo_fill", "vlp4d_mpi_spline_xy", "vlp4d_mpi_spline_vxvy",
+                  "vlp4d_mpi_field"):
             getattr(L, n).argtypes = [vp, vp, vp]
         L.vlp4d_mpi_advect_2d.argtypes = [vp, vp, vp, d, vp]
         L.vlp4d_mpi_advect_4d.argtypes = [vp, vp, vp, d, vp]
@@ -395,6 +396,10 @@ class Context:
         if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous() and t.numel() == n):
             raise ValueError(f"a vlp4d_mpi array must be a contiguous CUDA float64 tensor of {n} elements")
         return C.c_void_p(t.data_ptr())
+
+    def mpi_init_case(self, fn, stream=None):
+        """The domain's vlp4d_mpi initial condition (idcase 10, 20, 2, 5) on fn's grid points, halo zero."""
+        _check(lib().vlp4d_mpi_init_case(self.h, self._h(fn), _stream_ptr(stream)))
 
     def mpi_halo_fill(self, fn, stream=None):
         _check(lib().vlp4d_mpi_halo_fill(self.h, self._h(fn), _stream_ptr(stream)))
