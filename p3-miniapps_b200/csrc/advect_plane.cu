@@ -442,6 +442,33 @@ __device__ __forceinline__ void x11_from(const double (&t)[20], const W11<double
     o[q] = acc;
   }
 }
+// X11 of eight outputs from t[0..23] (FP32): the two quads' loads, column
+// differences and register pairs are shared; each output is computed
+// exactly as x11_from computes it.
+template <int R_>
+__device__ __forceinline__ void x11_from8(const float (&t)[24], const W11<float> &w, float (&o)[8]) {
+  float d[17];
+#pragma unroll
+  for (int j = 0; j < 17; ++j) d[j] = t[R_ + j + 1] - t[R_ + j];
+  float2 dp[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) dp[j] = make_float2(d[j], d[j + 1]);
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const float2 r = interp11_2(w.u, make_float2(t[R_ + 5 + 2 * p], t[R_ + 6 + 2 * p]), dp + 2 * p);
+    o[2 * p] = r.x;
+    o[2 * p + 1] = r.y;
+  }
+}
+__device__ __forceinline__ void sweep_x11_8(const float (&t)[24], int r, const W11<float> &w, float (&o)[8]) {
+  switch (r) {
+    case 0: x11_from8<0>(t, w, o); break;
+    case 1: x11_from8<1>(t, w, o); break;
+    case 2: x11_from8<2>(t, w, o); break;
+    default: x11_from8<3>(t, w, o); break;
+  }
+}
+
 template <typename T>
 __device__ __forceinline__ void sweep_x11(const T (&t)[20], int r, const W11<T> &w, T (&o)[4]) {
   switch (r) {
@@ -452,7 +479,11 @@ __device__ __forceinline__ void sweep_x11(const T (&t)[20], int r, const W11<T> 
   }
 }
 
-template <typename T, int NX, int RT>
+// X8 (FP32, RT = 4, nx a multiple of 8): the X11 phase maps thread t to
+// the column octet 8*(t mod nx/8) and the two rows 2*(t / (nx/8)) + {0, 1}
+// of the chunk (as many threads as the Y11 mapping), so that neighbouring
+// outputs share their loads, differences and register pairs.
+template <typename T, int NX, int RT, bool X8 = false>
 __global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int nx = NX ? NX : a.nx;
@@ -511,6 +542,9 @@ __global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
   for (int i = 0; i < RT; ++i)
 #pragma unroll
     for (int q = 0; q < 4; ++q) racc[i][q] = 0.0;
+  // X8 mapping (racc[2 * i + h][q] holds row i, column c8 + 4h + q).
+  const int c8 = X8 ? 8 * (threadIdx.x % (nx >> 3)) : 0;
+  const int r8 = X8 ? 2 * (threadIdx.x / (nx >> 3)) : 0;
 
   const int gdx = G % a.nvx, gdy = G / a.nvx;
   int ivx = g % a.nvx, ivy = g / a.nvx;
@@ -534,7 +568,42 @@ __global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
       return;
     }
     if (threadIdx.x == 0 && it + S < n_items) issue(it + S);
-    {  // X11 of the thread's rows, the moment.
+    if constexpr (X8) {  // X11 of the thread's column octet and two rows, the moment.
+      W11<T> wx;
+      int base = c8 + read_line11(xrec[ivx], wx);
+      base = base % nx;
+      const int rr = base & 3;
+      int o[6];
+      o[0] = base - rr;
+#pragma unroll
+      for (int k = 1; k < 6; ++k) {
+        o[k] = o[k - 1] + 4;
+        if (o[k] >= nx) o[k] -= nx;
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const T *row = ys + (size_t)(r8 + i) * nx;
+        float t[24], q4[4];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          load4(row + o[k], q4);
+          t[4 * k] = q4[0];
+          t[4 * k + 1] = q4[1];
+          t[4 * k + 2] = q4[2];
+          t[4 * k + 3] = q4[3];
+        }
+        float out[8];
+        sweep_x11_8(t, rr, wx, out);
+        const float lo[4] = {out[0], out[1], out[2], out[3]}, hi[4] = {out[4], out[5], out[6], out[7]};
+        store4(outp + (size_t)(r8 + i) * nx + c8, lo);
+        store4(outp + (size_t)(r8 + i) * nx + c8 + 4, hi);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          racc[2 * i][q] += (double)lo[q];
+          racc[2 * i + 1][q] += (double)hi[q];
+        }
+      }
+    } else {  // X11 of the thread's rows, the moment.
       W11<T> wx;
       int base = c0 + read_line11(xrec[ivx], wx);
       base = base % nx;
@@ -576,11 +645,23 @@ __global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
       parity ^= 1u;
     }
   }
-  double *rdst = a.rho_part + (long long)g * plane_elems + ((long long)chunk * R + r0) * nx + c0;
+  if constexpr (X8) {
+    double *rdst = a.rho_part + (long long)g * plane_elems + ((long long)chunk * R + r8) * nx + c8;
 #pragma unroll
-  for (int i = 0; i < RT; ++i) {
-    reinterpret_cast<double2 *>(rdst + (size_t)i * nx)[0] = make_double2(racc[i][0], racc[i][1]);
-    reinterpret_cast<double2 *>(rdst + (size_t)i * nx)[1] = make_double2(racc[i][2], racc[i][3]);
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        double2 *p2 = reinterpret_cast<double2 *>(rdst + (size_t)i * nx + 4 * h);
+        p2[0] = make_double2(racc[2 * i + h][0], racc[2 * i + h][1]);
+        p2[1] = make_double2(racc[2 * i + h][2], racc[2 * i + h][3]);
+      }
+  } else {
+    double *rdst = a.rho_part + (long long)g * plane_elems + ((long long)chunk * R + r0) * nx + c0;
+#pragma unroll
+    for (int i = 0; i < RT; ++i) {
+      reinterpret_cast<double2 *>(rdst + (size_t)i * nx)[0] = make_double2(racc[i][0], racc[i][1]);
+      reinterpret_cast<double2 *>(rdst + (size_t)i * nx)[1] = make_double2(racc[i][2], racc[i][3]);
+    }
   }
 }
 
@@ -753,9 +834,18 @@ bool xyxy_config(const vlp4d_ctx *c, PlaneCfg &cfg) {
   return true;
 }
 
+// The X8 mapping for FP32 (VLP4D_XYXY_X8 = 0 turns it off).
+bool xyxy_x8(int nx) {
+  static const int env = env_int("VLP4D_XYXY_X8", 1);
+  return env != 0 && nx % 8 == 0;
+}
+
 template <typename T, int NX, int RT>
 int run_xyxy(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, cudaStream_t s) {
   auto kern = k_plane_xyxy<T, NX, RT>;
+  if constexpr (sizeof(T) == 4 && RT == 4) {
+    if (xyxy_x8(args.nx)) kern = k_plane_xyxy<T, NX, RT, true>;
+  }
   VLP4D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
   int per_sm = 0;
   VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, cfg.threads, cfg.smem));
