@@ -806,16 +806,20 @@ size_t xyxy_smem(int R, int nx, size_t elem, int stages, int nvx, int nvy) {
 // Chunk height (the tallest divisor of ny up to 32 rows whose block and
 // shared memory fit), rows per thread (4 in FP32 when R allows, 1 in FP64)
 // and pipeline depth (3 stages if two CTAs then share an SM, else 2) of
-// k_plane_xyxy.  VLP4D_XYXY_STAGES overrides the depth.
+// k_plane_xyxy.  VLP4D_XYXY_STAGES overrides the depth, VLP4D_XYXY_R the
+// chunk height (tuning sweeps).
 bool xyxy_config(const vlp4d_ctx *c, PlaneCfg &cfg) {
   const int nx = c->g.n[0], ny = c->g.n[1];
   if (nx % 4 != 0 || nx > 2048) return false;
   const int ncg = nx / 4;
   const int forced = env_int("VLP4D_XYXY_STAGES", 0);
+  const int forced_r = env_int("VLP4D_XYXY_R", 0);
   if (forced && (forced < 2 || forced > kMaxStages)) return false;
   cfg.R = 0;
-  for (int r = ny < 32 ? ny : 32; r >= 1 && !cfg.R; --r) {
+  const int rmax = forced_r > 0 ? forced_r : 32;
+  for (int r = ny < rmax ? ny : rmax; r >= 1 && !cfg.R; --r) {
     if (ny % r) continue;
+    if (forced_r && r != forced_r) continue;
     const int t = (c->elem == 4 && r % 4 == 0) ? 4 : 1;
     if (ncg * (r / t) > 512 || ncg * (r / t) < 1) continue;
     int st = forced;
