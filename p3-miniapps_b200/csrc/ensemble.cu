@@ -105,82 +105,104 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+// Shared memory of the plane stages: the moment (FP64, maxnxy cells), a ring
+// of kEnsRing raw plane groups, the x-swept group, the x lines of the row.
+constexpr int kEnsGroupCells = 4608;  // cells of one plane group (18 KB FP32)
+constexpr int kEnsRing = 3;           // raw group buffers: two groups in flight
+
+// a / n for 0 <= a < 2^22, n >= 1, inv = 1.f / n: the float quotient is
+// within one of the integer one, and one correction step fixes it.
+__device__ __forceinline__ int div_small(int a, int n, float inv) {
+  int q = __float2int_rz((float)a * inv);
+  const int r = a - q * n;
+  q += r >= n ? 1 : 0;
+  q -= r < 0 ? 1 : 0;
+  return q;
+}
+
 // Moment of f0 (stage 0) or x/y half step (+ moment) of the vy row `ivy`.
 // The row's nvx planes are contiguous; they are processed in groups of P
-// planes (P * nx*ny <= maxnxy cells) so that small planes share the loads
-// and barriers.  Shared memory: the moment (FP64, one per cell), the loaded
-// group, its x-swept copy, the x lines of the row.  The thread that owns
-// cell q of a plane owns it in every plane of the row, so the moment adds
-// the planes in ivx order whatever the block size.
+// planes (P * nx*ny <= kEnsGroupCells), streamed through a ring of
+// kEnsRing shared buffers with cp.async (two groups in flight while one is
+// swept).  Per group: the x sweep into the swept buffer, one barrier, the
+// y sweep to global memory (items: every (plane, column quad) of the
+// group, so that small planes keep all threads busy).  With the moment the
+// y sweep also leaves its output in the group's raw buffer (no longer read
+// after the barrier), and after a second barrier the thread that owns cell
+// q adds the group's planes to the cell's FP64 sum in ivx order: the sums
+// do not depend on the block size or the tile configuration.
 template <bool SWEEP, bool MOMENT>
 __device__ void ens_planes(const EnsArgs &a, const EnsRun &R, const float *fin, float *fout, int ivy,
                            unsigned char *smem) {
   const int nx = R.n[0], ny = R.n[1], nvx = R.n[2];
   const int nxy = nx * ny;
-  // Layout: acc (maxnxy doubles) | two load buffers | x-swept buffer | x lines.
+  const long long row0 = R.f_off + (long long)ivy * nvx * nxy;
   double *acc = reinterpret_cast<double *>(smem);
-  float *bin[2] = {reinterpret_cast<float *>(acc + a.maxnxy), reinterpret_cast<float *>(acc + a.maxnxy) + a.maxnxy};
-  float *b1 = bin[1] + a.maxnxy;
-  EnsLine *xl = reinterpret_cast<EnsLine *>(b1 + a.maxnxy);
+  if (!SWEEP) {
+    double *pp = a.part + R.p_off + (long long)ivy * nxy;
+    for (int q = threadIdx.x; q < nxy; q += blockDim.x) {
+      double s = 0.;
+      for (int p = 0; p < nvx; ++p) s += (double)__ldcg(fin + row0 + (long long)p * nxy + q);
+      pp[q] = s;
+    }
+    return;
+  }
+  float *raw0 = reinterpret_cast<float *>(acc + a.maxnxy);
+  float *b1 = raw0 + (size_t)kEnsRing * kEnsGroupCells;
+  EnsLine *xl = reinterpret_cast<EnsLine *>(b1 + kEnsGroupCells);
   __shared__ EnsLine yl;
   const double hdt = 0.5 * R.dt;
-  int P = a.maxnxy / nxy;
+  int P = kEnsGroupCells / nxy;
   P = P < 1 ? 1 : (P > nvx ? nvx : P);
-  if (SWEEP) {
-    for (int l = threadIdx.x; l < nvx; l += blockDim.x)
-      xl[l] = ens_line(hdt * (R.minp[2] + l * R.dx[2]), R.minp[0], R.maxp[0], nx);
-    if (threadIdx.x == 0) yl = ens_line(hdt * (R.minp[3] + ivy * R.dx[3]), R.minp[1], R.maxp[1], ny);
-  }
+  const int ngroups = (nvx + P - 1) / P;
+  for (int l = threadIdx.x; l < nvx; l += blockDim.x)
+    xl[l] = ens_line(hdt * (R.minp[2] + l * R.dx[2]), R.minp[0], R.maxp[0], nx);
+  if (threadIdx.x == 0) yl = ens_line(hdt * (R.minp[3] + ivy * R.dx[3]), R.minp[1], R.maxp[1], ny);
   if (MOMENT)
     for (int q = threadIdx.x; q < nxy; q += blockDim.x) acc[q] = 0.;
-  __syncthreads();
-  const long long row0 = R.f_off + (long long)ivy * nvx * nxy;
-  const bool vec = (nxy & 3) == 0;  // f_off is a multiple of 64 elements
-  // Group p0's copies into bin[buf]: asynchronous (vec) or plain loads.
-  auto load_group = [&](int p0, int buf) {
-    const int np = nvx - p0 < P ? nvx - p0 : P;
-    const long long gbase = row0 + (long long)p0 * nxy;
-    if (vec) {
-      const float4 *src = reinterpret_cast<const float4 *>(fin + gbase);
-      float4 *dst = reinterpret_cast<float4 *>(bin[buf]);
-      for (int c = threadIdx.x; c < np * nxy / 4; c += blockDim.x) cp_async16(dst + c, src + c);
-    } else {
-      for (int c = threadIdx.x; c < np * nxy; c += blockDim.x) bin[buf][c] = __ldcg(fin + gbase + c);
+  // Column quads when the rows are multiples of four floats (f_off is a
+  // multiple of 64 elements, so every plane starts 16-byte aligned).
+  const bool quad = (nx & 3) == 0;
+  auto load_group = [&](int gi) {
+    if (gi < ngroups) {
+      const int p0 = gi * P;
+      const int np = nvx - p0 < P ? nvx - p0 : P;
+      float *dst = raw0 + (size_t)(gi % kEnsRing) * kEnsGroupCells;
+      const long long gbase = row0 + (long long)p0 * nxy;
+      if (quad) {
+        const float4 *src = reinterpret_cast<const float4 *>(fin + gbase);
+        float4 *d4 = reinterpret_cast<float4 *>(dst);
+        for (int c = threadIdx.x; c < (np * nxy) >> 2; c += blockDim.x) cp_async16(d4 + c, src + c);
+      } else {
+        for (int c = threadIdx.x; c < np * nxy; c += blockDim.x) dst[c] = __ldcg(fin + gbase + c);
+      }
     }
     cp_async_commit();
   };
-  if (SWEEP) load_group(0, 0);
-  int buf = 0;
-  for (int p0 = 0; p0 < nvx; p0 += P, buf ^= 1) {
-    const int np = nvx - p0 < P ? nvx - p0 : P;
-    const int cells = np * nxy;
-    const long long gbase = row0 + (long long)p0 * nxy;
-    if (!SWEEP) {
-      for (int q = threadIdx.x; q < nxy; q += blockDim.x) {
-        double s = acc[q];
-        for (int p = 0; p < np; ++p) s += (double)__ldcg(fin + gbase + (long long)p * nxy + q);
-        acc[q] = s;
-      }
-      continue;
-    }
-    // Next group in flight while this one is swept.
-    if (p0 + P < nvx) {
-      load_group(p0 + P, buf ^ 1);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
+  __syncthreads();
+#pragma unroll
+  for (int gi = 0; gi < kEnsRing - 1; ++gi) load_group(gi);
+  const int my = yl.m;
+  for (int gi = 0; gi < ngroups; ++gi) {
+    cp_async_wait<kEnsRing - 2>();
+    // Group gi has landed (every thread's copies); every thread is done
+    // with group gi - 1, whose buffer the next load reuses.
     __syncthreads();
-    const float *b0 = bin[buf];
-    if (vec && (nx & 3) == 0) {
-      // Column quads (the planes' rows are multiples of four floats): three
-      // 16-byte taps per quad in x and six rows of quads in y, packed f32x2
-      // arithmetic, as the single-run plane pass does.
-      const int nq = nx >> 2;
-      for (int qd = threadIdx.x; qd < (cells >> 2); qd += blockDim.x) {
-        const int c = qd << 2;
-        const int p = c / nxy, qc = c - p * nxy;
-        const int ix0 = qc % nx, row = c - ix0;
+    load_group(gi + kEnsRing - 1);
+    const int p0 = gi * P;
+    const int np = nvx - p0 < P ? nvx - p0 : P;
+    float *b0 = raw0 + (size_t)(gi % kEnsRing) * kEnsGroupCells;
+    const long long gbase = row0 + (long long)p0 * nxy;
+    if (quad) {
+      const int nq = nx >> 2, nqp = nxy >> 2;
+      const float inv_nq = 1.f / (float)nq, inv_nqp = 1.f / (float)nqp;
+      const int items = np * nqp;
+      for (int it = threadIdx.x; it < items; it += blockDim.x) {
+        const int p = div_small(it, nqp, inv_nqp);
+        const int qi = it - p * nqp;
+        const int iy = div_small(qi, nq, inv_nq);
+        const int ix0 = (qi - iy * nq) << 2;
+        const int row = p * nxy + iy * nx;
         const EnsLine &lx = xl[p0 + p];
         int base = ix0 + lx.m;
         base = base >= nx ? base - nx : base;
@@ -202,80 +224,64 @@ __device__ void ens_planes(const EnsArgs &a, const EnsRun &R, const float *fin, 
         make_sweep_w(lx.v, w);
         float out[4];
         sweep_x4(t, rr, w, out);
-        *reinterpret_cast<float4 *>(b1 + c) = make_float4(out[0], out[1], out[2], out[3]);
+        *reinterpret_cast<float4 *>(b1 + row + ix0) = make_float4(out[0], out[1], out[2], out[3]);
       }
       __syncthreads();
       SweepW<float> wy;
       make_sweep_w(yl.v, wy);
-      const int my = yl.m;
-      for (int qi = threadIdx.x; qi < (nxy >> 2); qi += blockDim.x) {
-        const int iy = qi / nq, ix0 = (qi - iy * nq) << 2;
-        int rows[6];
+      for (int it = threadIdx.x; it < items; it += blockDim.x) {
+        const int p = div_small(it, nqp, inv_nqp);
+        const int qi = it - p * nqp;
+        const int iy = div_small(qi, nq, inv_nq);
+        const int ix0 = (qi - iy * nq) << 2;
+        const float *pl = b1 + p * nxy + ix0;
         int j = iy + my;
         j = j >= ny ? j - ny : j;
+        float2 y[6][2];
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
-          rows[k] = j * nx + ix0;
+          const float4 v = *reinterpret_cast<const float4 *>(pl + j * nx);
+          y[k][0] = make_float2(v.x, v.y);
+          y[k][1] = make_float2(v.z, v.w);
           if (++j == ny) j = 0;
         }
-        double s4[4];
+        float2 o2[2];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) s4[q] = MOMENT ? acc[(qi << 2) + q] : 0.;
-        for (int p = 0; p < np; ++p) {
-          const float *pl = b1 + p * nxy;
-          float2 y[6][2];
+        for (int h = 0; h < 2; ++h)
+          o2[h] = interp_diff2(wy.v, y[2][h], sub2(y[1][h], y[0][h]), sub2(y[2][h], y[1][h]), sub2(y[3][h], y[2][h]),
+                               sub2(y[4][h], y[3][h]), sub2(y[5][h], y[4][h]));
+        const float4 o4 = make_float4(o2[0].x, o2[0].y, o2[1].x, o2[1].y);
+        *reinterpret_cast<float4 *>(fout + gbase + (long long)it * 4) = o4;
+        if (MOMENT) *reinterpret_cast<float4 *>(b0 + it * 4) = o4;
+      }
+    } else {
+      const float inv_nx = 1.f / (float)nx, inv_nxy = 1.f / (float)nxy;
+      const int cells = np * nxy;
+      for (int c = threadIdx.x; c < cells; c += blockDim.x) {
+        const int p = div_small(c, nxy, inv_nxy);
+        const int qc = c - p * nxy;
+        const int ix = qc - div_small(qc, nx, inv_nx) * nx;
+        const int row = c - ix;
+        const EnsLine &lx = xl[p0 + p];
+        int j = ix + lx.m;
+        j = j >= nx ? j - nx : j;
+        float t[6];
 #pragma unroll
-          for (int k = 0; k < 6; ++k) {
-            const float4 v = *reinterpret_cast<const float4 *>(pl + rows[k]);
-            y[k][0] = make_float2(v.x, v.y);
-            y[k][1] = make_float2(v.z, v.w);
-          }
-          float2 o2[2];
-#pragma unroll
-          for (int h = 0; h < 2; ++h)
-            o2[h] = interp_diff2(wy.v, y[2][h], sub2(y[1][h], y[0][h]), sub2(y[2][h], y[1][h]), sub2(y[3][h], y[2][h]),
-                                 sub2(y[4][h], y[3][h]), sub2(y[5][h], y[4][h]));
-          *reinterpret_cast<float4 *>(fout + gbase + (long long)p * nxy + (qi << 2)) =
-              make_float4(o2[0].x, o2[0].y, o2[1].x, o2[1].y);
-          if (MOMENT) {
-            s4[0] += (double)o2[0].x;
-            s4[1] += (double)o2[0].y;
-            s4[2] += (double)o2[1].x;
-            s4[3] += (double)o2[1].y;
-          }
+        for (int k = 0; k < 6; ++k) {
+          t[k] = b0[row + j];
+          if (++j == nx) j = 0;
         }
-        if (MOMENT) {
-#pragma unroll
-          for (int q = 0; q < 4; ++q) acc[(qi << 2) + q] = s4[q];
-        }
+        b1[c] = interp6(lx.v, t[0], t[1], t[2], t[3], t[4], t[5]);
       }
       __syncthreads();
-      continue;
-    }
-    for (int c = threadIdx.x; c < cells; c += blockDim.x) {
-      const int p = c / nxy, qc = c - p * nxy;
-      const int ix = qc % nx, row = c - ix;
-      const EnsLine &lx = xl[p0 + p];
-      int j = ix + lx.m;
-      j = j >= nx ? j - nx : j;
-      float t[6];
-#pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        t[k] = b0[row + j];
-        if (++j == nx) j = 0;
-      }
-      b1[c] = interp6(lx.v, t[0], t[1], t[2], t[3], t[4], t[5]);
-    }
-    __syncthreads();
-    const EnsLine ly = yl;
-    for (int q = threadIdx.x; q < nxy; q += blockDim.x) {
-      const int ix = q % nx, iy = q / nx;
-      int j0 = iy + ly.m;
-      j0 = j0 >= ny ? j0 - ny : j0;
-      double s = MOMENT ? acc[q] : 0.;
-      for (int p = 0; p < np; ++p) {
-        const float *pl = b1 + p * nxy + ix;
-        int j = j0;
+      const EnsLine ly = yl;
+      for (int c = threadIdx.x; c < cells; c += blockDim.x) {
+        const int p = div_small(c, nxy, inv_nxy);
+        const int qc = c - p * nxy;
+        const int iy = div_small(qc, nx, inv_nx);
+        const float *pl = b1 + p * nxy + (qc - iy * nx);
+        int j = iy + my;
+        j = j >= ny ? j - ny : j;
         float t[6];
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
@@ -283,13 +289,20 @@ __device__ void ens_planes(const EnsArgs &a, const EnsRun &R, const float *fin, 
           if (++j == ny) j = 0;
         }
         const float o = interp6(ly.v, t[0], t[1], t[2], t[3], t[4], t[5]);
-        fout[gbase + (long long)p * nxy + q] = o;
-        if (MOMENT) s += (double)o;
+        fout[gbase + c] = o;
+        if (MOMENT) b0[c] = o;
       }
-      if (MOMENT) acc[q] = s;
     }
-    __syncthreads();
+    if (MOMENT) {
+      __syncthreads();  // the group's outputs are in b0
+      for (int q = threadIdx.x; q < nxy; q += blockDim.x) {
+        double s = acc[q];
+        for (int p = 0; p < np; ++p) s += (double)b0[p * nxy + q];
+        acc[q] = s;
+      }
+    }
   }
+  cp_async_wait<0>();
   if (MOMENT) {
     __syncthreads();
     double *pp = a.part + R.p_off + (long long)ivy * nxy;
@@ -300,8 +313,11 @@ __device__ void ens_planes(const EnsArgs &a, const EnsRun &R, const float *fin, 
 // vx then vy (dt) of the columns [tile*cc, tile*cc + cc).  Thread (col, g)
 // handles the groups of V consecutive output vx rows g, g+G, ...; for each
 // group it streams the vy rows from the column's vy offset (V+5 vx taps per
-// row, shared by the V outputs), keeping six vx-swept rows in a ring.
+// row, shared by the V outputs), keeping six vx-swept rows in a ring, with
+// the taps of the next D rows in flight.
+template <int D>
 __device__ void ens_vxvy(const EnsArgs &a, const EnsRun &R, const float *fin, float *fout, int tile) {
+  static_assert(6 % D == 0, "the tap ring is indexed by the unrolled row");
   constexpr int V = 4;
   const int nx = R.n[0], ny = R.n[1], nvx = R.n[2], nvy = R.n[3];
   const int nxy = nx * ny;
@@ -313,50 +329,54 @@ __device__ void ens_vxvy(const EnsArgs &a, const EnsRun &R, const float *fin, fl
   const double *ex = a.fld + R.e_off, *ey = ex + nxy;
   const EnsLine lx = ens_line(R.dt * __ldcg(ex + col), R.minp[2], R.maxp[2], nvx);
   const EnsLine ly = ens_line(R.dt * __ldcg(ey + col), R.minp[3], R.maxp[3], nvy);
-  const long long vstride = nxy, ystride = (long long)nxy * nvx;
+  // Offsets within the member's f (< 64^4 elements) fit 32 bits.
+  const int ystride = nxy * nvx;
   const float *src = fin + R.f_off + col;
   float *dst = fout + R.f_off + col;
+  const int nrows = nvy + 5;
   for (int v0 = g * V; v0 < nvx; v0 += G * V) {
-    long long toff[V + 5];
+    int toff[V + 5];
     int j = v0 + lx.m;
     while (j >= nvx) j -= nvx;
 #pragma unroll
     for (int k = 0; k < V + 5; ++k) {
-      toff[k] = (long long)j * vstride;
+      toff[k] = j * nxy;
       if (++j == nvx) j = 0;
     }
     float ring[6][V];
-    int row = ly.m;
-    const int nrows = nvy + 5;
-    // Row r's taps are loaded one row ahead (tn) so their latency overlaps
-    // the arithmetic of the row before.
-    float t[V + 5];
+    float t[D][V + 5];
+    int lrow = ly.m;  // the next vy row to load
 #pragma unroll
-    for (int k = 0; k < V + 5; ++k) t[k] = __ldcg(src + (long long)row * ystride + toff[k]);
+    for (int d = 0; d < D; ++d) {
+      if (d < nrows) {
+        const float *pn = src + lrow * ystride;
+#pragma unroll
+        for (int k = 0; k < V + 5; ++k) t[d][k] = __ldcg(pn + toff[k]);
+        if (++lrow == nvy) lrow = 0;
+      }
+    }
     for (int r0 = 0; r0 < nrows; r0 += 6) {
 #pragma unroll
       for (int u = 0; u < 6; ++u) {
         const int r = r0 + u;
         if (r >= nrows) break;
-        if (++row == nvy) row = 0;
-        float tn[V + 5];
-        if (r + 1 < nrows) {
-          const float *pn = src + (long long)row * ystride;
+        float(&cur)[V + 5] = t[u % D];
 #pragma unroll
-          for (int k = 0; k < V + 5; ++k) tn[k] = __ldcg(pn + toff[k]);
+        for (int i = 0; i < V; ++i)
+          ring[u][i] = interp6(lx.v, cur[i], cur[i + 1], cur[i + 2], cur[i + 3], cur[i + 4], cur[i + 5]);
+        if (r + D < nrows) {
+          const float *pn = src + lrow * ystride;
+#pragma unroll
+          for (int k = 0; k < V + 5; ++k) cur[k] = __ldcg(pn + toff[k]);
+          if (++lrow == nvy) lrow = 0;
         }
-#pragma unroll
-        for (int i = 0; i < V; ++i) ring[u][i] = interp6(lx.v, t[i], t[i + 1], t[i + 2], t[i + 3], t[i + 4], t[i + 5]);
-#pragma unroll
-        for (int k = 0; k < V + 5; ++k) t[k] = tn[k];
         if (r >= 5) {
-          float *orow = dst + (long long)(r - 5) * ystride;
+          float *orow = dst + (r - 5) * ystride;
 #pragma unroll
           for (int i = 0; i < V; ++i) {
             if (v0 + i < nvx)
-              orow[(long long)(v0 + i) * vstride] =
-                  interp6(ly.v, ring[(u + 1) % 6][i], ring[(u + 2) % 6][i], ring[(u + 3) % 6][i],
-                          ring[(u + 4) % 6][i], ring[(u + 5) % 6][i], ring[u][i]);
+              orow[(v0 + i) * nxy] = interp6(ly.v, ring[(u + 1) % 6][i], ring[(u + 2) % 6][i], ring[(u + 3) % 6][i],
+                                             ring[(u + 4) % 6][i], ring[(u + 5) % 6][i], ring[u][i]);
           }
         }
       }
@@ -490,10 +510,7 @@ __global__ void __launch_bounds__(512) k_ensemble(EnsArgs a) {
       // got_run: -1 leave (all members done, or no work for idle_limit
       // cycles); -2 nothing taken; >= 0 a tile of that member.
       int got_run = -2, got_stage = 0, got_tile = 0;
-      const int rem = __shfl_sync(0xffffffffu, lane == 0 ? *(volatile int *)a.remaining : 0, 0);
-      if (rem <= 0) {
-        got_run = -1;
-      } else {
+      {
         const int rounds = (a.nruns + 31) / 32;
         for (int rd = 0; rd < rounds && got_run == -2; ++rd) {
           const int idx = rd * 32 + lane;
@@ -528,6 +545,8 @@ __global__ void __launch_bounds__(512) k_ensemble(EnsArgs a) {
         if (got_run >= 0) {
           r = got_run;
           idle_start = clock64();
+        } else if (__shfl_sync(0xffffffffu, lane == 0 ? *(volatile int *)a.remaining : 0, 0) <= 0) {
+          got_run = -1;  // every member has finished
         } else {
           __nanosleep(256);
           if (clock64() - idle_start > a.idle_limit) {
@@ -558,7 +577,7 @@ __global__ void __launch_bounds__(512) k_ensemble(EnsArgs a) {
         float *fa = (t & 1) ? a.F1 : a.F0, *fb = (t & 1) ? a.F0 : a.F1;
         if (sub == 0) ens_planes<true, true>(a, R, fa, fb, tile, smem);
         else if (sub == 1) ens_field(a, R, t + 1, smem);
-        else if (sub == 2) ens_vxvy(a, R, fb, fa, tile);
+        else if (sub == 2) ens_vxvy<3>(a, R, fb, fa, tile);
         else ens_planes<true, false>(a, R, fa, fb, tile, smem);
       }
       // Every thread's writes, then the tile count.
@@ -636,7 +655,8 @@ namespace vlp4d {
 namespace {
 
 size_t ens_smem(int maxnxy) {
-  const size_t planes = sizeof(double) * maxnxy + 3 * sizeof(float) * maxnxy + sizeof(EnsLine) * kEnsMaxN;
+  const size_t planes = sizeof(double) * maxnxy + (kEnsRing + 1) * sizeof(float) * kEnsGroupCells +
+                        sizeof(EnsLine) * kEnsMaxN;
   const size_t field = 2 * sizeof(double2) * maxnxy + 2 * sizeof(double2) * kEnsMaxN;
   return ((planes > field ? planes : field) + 255) / 256 * 256;
 }
