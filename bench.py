@@ -376,8 +376,11 @@ def ensemble_arm(pkg, torch, stream, peak, nruns=256, nsteps=50, autotune=True):
     """The batched-ensemble configuration: 256 Landau members, N per dimension
     drawn from {16, 24, 32, 48}, amp ~ U[0.01, 0.1], k in {0.3, 0.5}, 50 steps
     of dt 0.1, FP32 f, in one persistent launch replayed from a CUDA graph.
-    Tiles from the autotuner (3 steps per configuration).  Algorithmic bytes:
-    f read and written by each of the three passes of a step."""
+    Tiles from the autotuner (3 steps per configuration).  Algorithmic bytes
+    per cell of a run: the moment of f0 reads f once (4 B), each step's x/y
+    pass (the first one alone, later ones joined with the previous step's
+    closing half step) and vx/vy pass read and write it (16 B per step), and
+    the closing x/y pass of the last step reads and writes it (8 B)."""
     v = pkg.vlp4d
     members = v.landau_ensemble_members(nruns)
     with v.Ensemble(members, nsteps) as ens:
@@ -387,12 +390,13 @@ def ensemble_arm(pkg, torch, stream, peak, nruns=256, nsteps=50, autotune=True):
         t = time_calls(torch, stream, lambda: ens.run(stream), 3)
         ens.check()
         cells = ens.cells
-        gbs = 3 * 2 * 4.0 * cells * nsteps / t / 1e9
+        run_bytes = (16.0 * nsteps + 12.0) * cells
+        gbs = run_bytes / t / 1e9
         return {"config": {"members": nruns, "sizes": [16, 24, 32, 48], "steps": nsteps, "dt": 0.1,
                            "amp": [0.01, 0.1], "k": [0.3, 0.5], "storage": "f32 f, f64 fields"},
                 "cells": cells, "ms": t * 1e3, "value": cells * nsteps / t / 1e9, "unit": METRIC,
                 "tiles": {"threads": tiles[0], "cols_per_tile": tiles[1], "ctas_per_sm": tiles[2]},
-                "hbm": {"achieved_gbs": gbs, "frac": gbs / peak, "bytes_per_step": 3 * 2 * 4 * cells},
+                "hbm": {"achieved_gbs": gbs, "frac": gbs / peak, "bytes_per_run": run_bytes},
                 "launches_per_run": 3}
 
 

@@ -10,11 +10,14 @@
 // Work decomposition.  Member r's run is a sequence of stages
 //   0: moment of f0                     tiles: nvy  (one vy row of planes each)
 //   1: field solve, diagnostic 0        tiles: 1
-//   per step t (stage 2 + 4t + sub):
+//   per step t (stage 2 + 3t + sub):
 //   sub 0: x, y (dt/2) + moment         tiles: nvy
+//          for t > 0 joined with the closing x, y (dt/2) of step t - 1
+//          (no field solve separates them): x, y, x, y as the composed
+//          11-tap stencils, as the single-run time loop does in FP32
 //   sub 1: field solve, diagnostic t+1  tiles: 1
 //   sub 2: vx, vy (dt)                  tiles: ceil(nx*ny / cc)   (cc columns each)
-//   sub 3: x, y (dt/2)                  tiles: nvy
+//   last:  x, y (dt/2), the closing half step of the last step   tiles: nvy
 // A stage's tiles may start only when the member's previous stage is
 // complete; different members are independent.  Scheduling is dynamic and
 // wait-free: a CTA picks a member, atomically takes the next tile of the
@@ -74,13 +77,17 @@ struct EnsArgs {
   long long idle_limit;
 };
 
+// Stages of a run of nsteps steps (none but the moment and field solve of
+// f0 when nsteps is 0).
+__host__ __device__ __forceinline__ int total_stages_of(int nsteps) { return nsteps > 0 ? 3 + 3 * nsteps : 2; }
+
 __device__ __forceinline__ int stage_tiles(const EnsRun &R, int S, int cc) {
   if (S == 0) return R.n[3];
   if (S == 1) return 1;
-  const int sub = (S - 2) & 3;
+  const int sub = (S - 2) % 3;
   if (sub == 1) return 1;
   if (sub == 2) return (R.n[0] * R.n[1] + cc - 1) / cc;
-  return R.n[3];
+  return R.n[3];  // sub 0 and the closing x, y stage
 }
 
 // Stencil record of one line: FP32 difference weights and the tap offset.
@@ -310,6 +317,256 @@ __device__ void ens_planes(const EnsArgs &a, const EnsRun &R, const float *fin, 
   }
 }
 
+// Composed 11-tap line of two shifts by the same displacement (the closing
+// x/y half step of one step and the opening one of the next): out[i] =
+// sum_q W_q in[(i + 2m + q) mod n], W = w * w, as FP32 difference weights
+// about tap 5: out = f5 + sum_j u_j (f_{j+1} - f_j), u_j = -(W_0+..+W_j)
+// for j < 5 and W_{j+1}+..+W_10 for j >= 5 (the weights sum to one).  FP64
+// products and sums in the order of the single-run table, unfused.
+struct EnsLine11 {
+  float u[10];
+  int m;
+};
+
+__device__ __forceinline__ EnsLine11 ens_line11(double disp, double hmin, double hmax, int n) {
+  const LineStencil s = line_stencil(disp, hmin, hmax, n);
+  double W[11];
+#pragma unroll
+  for (int q = 0; q < 11; ++q) W[q] = 0.;
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+#pragma unroll
+    for (int j = 0; j < 6; ++j) W[k + j] = __dadd_rn(W[k + j], __dmul_rn(s.w[k], s.w[j]));
+  EnsLine11 l;
+  double acc = 0.;
+#pragma unroll
+  for (int j = 0; j < 5; ++j) {
+    acc = __dadd_rn(acc, W[j]);
+    l.u[j] = (float)-acc;
+  }
+  acc = 0.;
+#pragma unroll
+  for (int j = 9; j >= 5; --j) {
+    acc = __dadd_rn(acc, W[j + 1]);
+    l.u[j] = (float)acc;
+  }
+  l.m = (int)((2LL * s.m) % n);
+  return l;
+}
+
+// f5 + sum_j u_j d_j on packed pairs.
+__device__ __forceinline__ float2 ens_interp11(const float2 (&u)[10], float2 f5, const float2 *d) {
+  float2 acc = __fmul2_rn(u[0], d[0]);
+#pragma unroll
+  for (int j = 1; j < 10; ++j) acc = __ffma2_rn(u[j], d[j], acc);
+  return __fadd2_rn(f5, acc);
+}
+
+// Four X11 outputs from t[0..19] starting at the aligned column base - r:
+// output q uses t[r+q .. r+q+10].
+template <int R_>
+__device__ __forceinline__ void ens_x11_from(const float (&t)[20], const float2 (&u)[10], float (&o)[4]) {
+  float d[13];
+#pragma unroll
+  for (int j = 0; j < 13; ++j) d[j] = t[R_ + j + 1] - t[R_ + j];
+  float2 dp[12];
+#pragma unroll
+  for (int j = 0; j < 12; ++j) dp[j] = make_float2(d[j], d[j + 1]);
+  const float2 lo = ens_interp11(u, make_float2(t[R_ + 5], t[R_ + 6]), dp);
+  const float2 hi = ens_interp11(u, make_float2(t[R_ + 7], t[R_ + 8]), dp + 2);
+  o[0] = lo.x;
+  o[1] = lo.y;
+  o[2] = hi.x;
+  o[3] = hi.y;
+}
+
+// One scalar output f5 + sum_j u_j (f_{j+1} - f_j).
+__device__ __forceinline__ float ens_interp11_1(const float (&u)[10], const float (&t)[11]) {
+  float acc = u[0] * (t[1] - t[0]);
+#pragma unroll
+  for (int j = 1; j < 10; ++j) acc = fmaf(u[j], t[j + 1] - t[j], acc);
+  return t[5] + acc;
+}
+
+// x, y, x, y (dt/2 each) + moment of the vy row `ivy`: X11 then Y11 (the x
+// and y shifts commute), otherwise as ens_planes: plane groups through the
+// cp.async ring, X11 into the swept buffer, one barrier, Y11 per (plane,
+// column quad) to global memory and in place into the raw buffer, a
+// barrier, the moment in ivx order per cell.
+__device__ void ens_planes11(const EnsArgs &a, const EnsRun &R, const float *fin, float *fout, int ivy,
+                             unsigned char *smem) {
+  const int nx = R.n[0], ny = R.n[1], nvx = R.n[2];
+  const int nxy = nx * ny;
+  const long long row0 = R.f_off + (long long)ivy * nvx * nxy;
+  double *acc = reinterpret_cast<double *>(smem);
+  float *raw0 = reinterpret_cast<float *>(acc + a.maxnxy);
+  float *b1 = raw0 + (size_t)kEnsRing * kEnsGroupCells;
+  EnsLine11 *xl = reinterpret_cast<EnsLine11 *>(b1 + kEnsGroupCells);
+  __shared__ EnsLine11 yl;
+  const double hdt = 0.5 * R.dt;
+  int P = kEnsGroupCells / nxy;
+  P = P < 1 ? 1 : (P > nvx ? nvx : P);
+  const int ngroups = (nvx + P - 1) / P;
+  for (int l = threadIdx.x; l < nvx; l += blockDim.x)
+    xl[l] = ens_line11(hdt * (R.minp[2] + l * R.dx[2]), R.minp[0], R.maxp[0], nx);
+  if (threadIdx.x == 0) yl = ens_line11(hdt * (R.minp[3] + ivy * R.dx[3]), R.minp[1], R.maxp[1], ny);
+  for (int q = threadIdx.x; q < nxy; q += blockDim.x) acc[q] = 0.;
+  const bool quad = (nx & 3) == 0;
+  auto load_group = [&](int gi) {
+    if (gi < ngroups) {
+      const int p0 = gi * P;
+      const int np = nvx - p0 < P ? nvx - p0 : P;
+      float *dst = raw0 + (size_t)(gi % kEnsRing) * kEnsGroupCells;
+      const long long gbase = row0 + (long long)p0 * nxy;
+      if (quad) {
+        const float4 *src = reinterpret_cast<const float4 *>(fin + gbase);
+        float4 *d4 = reinterpret_cast<float4 *>(dst);
+        for (int c = threadIdx.x; c < (np * nxy) >> 2; c += blockDim.x) cp_async16(d4 + c, src + c);
+      } else {
+        for (int c = threadIdx.x; c < np * nxy; c += blockDim.x) dst[c] = __ldcg(fin + gbase + c);
+      }
+    }
+    cp_async_commit();
+  };
+  __syncthreads();
+#pragma unroll
+  for (int gi = 0; gi < kEnsRing - 1; ++gi) load_group(gi);
+  const int my = yl.m;
+  float2 uy[10];
+  float uys[10];
+#pragma unroll
+  for (int k = 0; k < 10; ++k) {
+    uys[k] = yl.u[k];
+    uy[k] = make_float2(uys[k], uys[k]);
+  }
+  for (int gi = 0; gi < ngroups; ++gi) {
+    cp_async_wait<kEnsRing - 2>();
+    __syncthreads();  // group gi landed; group gi - 1 is done with
+    load_group(gi + kEnsRing - 1);
+    const int p0 = gi * P;
+    const int np = nvx - p0 < P ? nvx - p0 : P;
+    float *b0 = raw0 + (size_t)(gi % kEnsRing) * kEnsGroupCells;
+    const long long gbase = row0 + (long long)p0 * nxy;
+    if (quad) {
+      const int nq = nx >> 2, nqp = nxy >> 2;
+      const float inv_nq = 1.f / (float)nq, inv_nqp = 1.f / (float)nqp;
+      const int items = np * nqp;
+      for (int it = threadIdx.x; it < items; it += blockDim.x) {
+        const int p = div_small(it, nqp, inv_nqp);
+        const int qi = it - p * nqp;
+        const int iy = div_small(qi, nq, inv_nq);
+        const int ix0 = (qi - iy * nq) << 2;
+        const int row = p * nxy + iy * nx;
+        const EnsLine11 &lx = xl[p0 + p];
+        int base = ix0 + lx.m;
+        base = base >= nx ? base - nx : base;
+        const int rr = base & 3;
+        int o = base - rr;
+        float t[20];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+          const float4 v = *reinterpret_cast<const float4 *>(b0 + row + o);
+          t[4 * k] = v.x;
+          t[4 * k + 1] = v.y;
+          t[4 * k + 2] = v.z;
+          t[4 * k + 3] = v.w;
+          o += 4;
+          if (o >= nx) o -= nx;
+        }
+        float2 u[10];
+#pragma unroll
+        for (int k = 0; k < 10; ++k) u[k] = make_float2(lx.u[k], lx.u[k]);
+        float out[4];
+        switch (rr) {
+          case 0: ens_x11_from<0>(t, u, out); break;
+          case 1: ens_x11_from<1>(t, u, out); break;
+          case 2: ens_x11_from<2>(t, u, out); break;
+          default: ens_x11_from<3>(t, u, out); break;
+        }
+        *reinterpret_cast<float4 *>(b1 + row + ix0) = make_float4(out[0], out[1], out[2], out[3]);
+      }
+      __syncthreads();
+      for (int it = threadIdx.x; it < items; it += blockDim.x) {
+        const int p = div_small(it, nqp, inv_nqp);
+        const int qi = it - p * nqp;
+        const int iy = div_small(qi, nq, inv_nq);
+        const int ix0 = (qi - iy * nq) << 2;
+        const float *pl = b1 + p * nxy + ix0;
+        int j = iy + my;
+        j = j >= ny ? j - ny : j;
+        float2 y[11][2];
+#pragma unroll
+        for (int k = 0; k < 11; ++k) {
+          const float4 v = *reinterpret_cast<const float4 *>(pl + j * nx);
+          y[k][0] = make_float2(v.x, v.y);
+          y[k][1] = make_float2(v.z, v.w);
+          if (++j == ny) j = 0;
+        }
+        float2 o2[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          float2 d[10];
+#pragma unroll
+          for (int k = 0; k < 10; ++k) d[k] = sub2(y[k + 1][h], y[k][h]);
+          o2[h] = ens_interp11(uy, y[5][h], d);
+        }
+        const float4 o4 = make_float4(o2[0].x, o2[0].y, o2[1].x, o2[1].y);
+        *reinterpret_cast<float4 *>(fout + gbase + (long long)it * 4) = o4;
+        *reinterpret_cast<float4 *>(b0 + it * 4) = o4;
+      }
+    } else {
+      const float inv_nx = 1.f / (float)nx, inv_nxy = 1.f / (float)nxy;
+      const int cells = np * nxy;
+      for (int c = threadIdx.x; c < cells; c += blockDim.x) {
+        const int p = div_small(c, nxy, inv_nxy);
+        const int qc = c - p * nxy;
+        const int ix = qc - div_small(qc, nx, inv_nx) * nx;
+        const int row = c - ix;
+        const EnsLine11 &lx = xl[p0 + p];
+        int j = ix + lx.m;
+        j = j >= nx ? j - nx : j;
+        float t[11], u[10];
+#pragma unroll
+        for (int k = 0; k < 11; ++k) {
+          t[k] = b0[row + j];
+          if (++j == nx) j = 0;
+        }
+#pragma unroll
+        for (int k = 0; k < 10; ++k) u[k] = lx.u[k];
+        b1[c] = ens_interp11_1(u, t);
+      }
+      __syncthreads();
+      for (int c = threadIdx.x; c < cells; c += blockDim.x) {
+        const int p = div_small(c, nxy, inv_nxy);
+        const int qc = c - p * nxy;
+        const int iy = div_small(qc, nx, inv_nx);
+        const float *pl = b1 + p * nxy + (qc - iy * nx);
+        int j = iy + my;
+        j = j >= ny ? j - ny : j;
+        float t[11];
+#pragma unroll
+        for (int k = 0; k < 11; ++k) {
+          t[k] = pl[j * nx];
+          if (++j == ny) j = 0;
+        }
+        const float o = ens_interp11_1(uys, t);
+        fout[gbase + c] = o;
+        b0[c] = o;
+      }
+    }
+    __syncthreads();  // the group's outputs are in b0
+    for (int q = threadIdx.x; q < nxy; q += blockDim.x) {
+      double s = acc[q];
+      for (int p = 0; p < np; ++p) s += (double)b0[p * nxy + q];
+      acc[q] = s;
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  double *pp = a.part + R.p_off + (long long)ivy * nxy;
+  for (int q = threadIdx.x; q < nxy; q += blockDim.x) pp[q] = acc[q];
+}
+
 // vx then vy (dt) of the columns [tile*cc, tile*cc + cc).  Thread (col, g)
 // handles the groups of V consecutive output vx rows g, g+G, ...; for each
 // group it streams the vy rows from the column's vy offset (V+5 vx taps per
@@ -498,7 +755,7 @@ __device__ void ens_field(const EnsArgs &a, const EnsRun &R, int iter, unsigned 
 __global__ void __launch_bounds__(512) k_ensemble(EnsArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_run, s_stage, s_tile;
-  const int total_stages = 2 + 4 * a.nsteps;
+  const int total_stages = total_stages_of(a.nsteps);
   // Scheduler state, kept (identically) by the lanes of warp 0.
   int r = (int)((blockIdx.x * 7919LL) % a.nruns);
   long long idle_start = clock64();
@@ -572,13 +829,19 @@ __global__ void __launch_bounds__(512) k_ensemble(EnsArgs a) {
         ens_planes<false, true>(a, R, a.F0, nullptr, tile, smem);
       } else if (S == 1) {
         ens_field(a, R, 0, smem);
+      } else if (S + 1 == total_stages) {
+        ens_planes<true, false>(a, R, a.F0, a.F1, tile, smem);  // closing half step
       } else {
-        const int t = (S - 2) >> 2, sub = (S - 2) & 3;
-        float *fa = (t & 1) ? a.F1 : a.F0, *fb = (t & 1) ? a.F0 : a.F1;
-        if (sub == 0) ens_planes<true, true>(a, R, fa, fb, tile, smem);
-        else if (sub == 1) ens_field(a, R, t + 1, smem);
-        else if (sub == 2) ens_vxvy<3>(a, R, fb, fa, tile);
-        else ens_planes<true, false>(a, R, fa, fb, tile, smem);
+        // The state lives in F0 between steps; sub 0 writes F1, vx/vy F0.
+        const int t = (S - 2) / 3, sub = (S - 2) % 3;
+        if (sub == 0) {
+          if (t == 0) ens_planes<true, true>(a, R, a.F0, a.F1, tile, smem);
+          else ens_planes11(a, R, a.F0, a.F1, tile, smem);
+        } else if (sub == 1) {
+          ens_field(a, R, t + 1, smem);
+        } else {
+          ens_vxvy<3>(a, R, a.F1, a.F0, tile);
+        }
       }
       // Every thread's writes, then the tile count.
       __threadfence();
@@ -655,8 +918,8 @@ namespace vlp4d {
 namespace {
 
 size_t ens_smem(int maxnxy) {
-  const size_t planes = sizeof(double) * maxnxy + (kEnsRing + 1) * sizeof(float) * kEnsGroupCells +
-                        sizeof(EnsLine) * kEnsMaxN;
+  const size_t line = sizeof(EnsLine11) > sizeof(EnsLine) ? sizeof(EnsLine11) : sizeof(EnsLine);
+  const size_t planes = sizeof(double) * maxnxy + (kEnsRing + 1) * sizeof(float) * kEnsGroupCells + line * kEnsMaxN;
   const size_t field = 2 * sizeof(double2) * maxnxy + 2 * sizeof(double2) * kEnsMaxN;
   return ((planes > field ? planes : field) + 255) / 256 * 256;
 }
@@ -891,7 +1154,7 @@ int vlp4d_ensemble_read(vlp4d_ensemble *ens, int run, void *f_out, double *nrj, 
   cudaStream_t s = (cudaStream_t)stream;
   const long long cells = (long long)R.n[0] * R.n[1] * R.n[2] * R.n[3];
   if (f_out)
-    VLP4D_CUDA_TRY(cudaMemcpyAsync(f_out, ens->F[ens->nsteps & 1] + R.f_off, sizeof(float) * cells,
+    VLP4D_CUDA_TRY(cudaMemcpyAsync(f_out, ens->F[ens->nsteps > 0 ? 1 : 0] + R.f_off, sizeof(float) * cells,
                                    cudaMemcpyDeviceToDevice, s));
   if (nrj) {
     VLP4D_CUDA_TRY(cudaMemcpyAsync(nrj, ens->nrj + R.d_off, sizeof(double) * (ens->nsteps + 1),

@@ -39,8 +39,10 @@ def _members(pkg, dims, nsteps_dt=0.1):
     return out
 
 
+# (10, 12, 16, 14): rows that are not a multiple of four floats (the scalar
+# plane sweeps).
 DIMS = [(16, 24, 32, 16), (24, 16, 16, 32), (32, 32, 24, 24), (16, 16, 16, 16), (48, 24, 16, 24),
-        (24, 48, 48, 16), (8, 12, 20, 10), (40, 16, 24, 36)]
+        (24, 48, 48, 16), (8, 12, 20, 10), (40, 16, 24, 36), (10, 12, 16, 14)]
 
 
 def test_members_match_single_runs(pkg, cuda):
