@@ -482,7 +482,14 @@ __device__ __forceinline__ void sweep_x11(const T (&t)[20], int r, const W11<T> 
 // X8 (FP32, RT = 4, nx a multiple of 8): the X11 phase maps thread t to
 // the column octet 8*(t mod nx/8) and the two rows 2*(t / (nx/8)) + {0, 1}
 // of the chunk (as many threads as the Y11 mapping), so that neighbouring
-// outputs share their loads, differences and register pairs.
+// outputs share their loads, differences and register pairs.  Its 16-byte
+// loads of neighbouring lanes lie 32 bytes apart, which would put two lanes
+// of each quarter-warp phase on the same banks; the intermediate tile
+// therefore stores 16-byte chunk c of a row at chunk c ^ ((c >> 3) & 1),
+// which maps the eight chunks one phase reads (2t + s for t = 0..7, any s)
+// to eight different bank groups, and keeps the Y11 stores (eight
+// consecutive chunks per phase) conflict-free.
+__device__ __forceinline__ int xyxy_swz(int chunk) { return chunk ^ ((chunk >> 3) & 1); }
 template <typename T, int NX, int RT, bool X8 = false>
 __global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -560,7 +567,10 @@ __global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
       W11<T> wy;
       read_line11(yrec[ivy], wy);
       sweep_y11<RT>(in + (size_t)r0 * nx + c0, nx, wy,
-                    [&](int i, const T (&o)[4]) { store4(ys + (size_t)(r0 + i) * nx + c0, o); });
+                    [&](int i, const T (&o)[4]) {
+                      const int cs = X8 ? 4 * xyxy_swz(c0 >> 2) : c0;
+                      store4(ys + (size_t)(r0 + i) * nx + cs, o);
+                    });
     }
     // ys is complete and the staged slot is no longer read: refill it.
     if (__syncthreads_or(!ok)) {
@@ -586,7 +596,7 @@ __global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
         float t[24], q4[4];
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
-          load4(row + o[k], q4);
+          load4(row + 4 * xyxy_swz(o[k] >> 2), q4);
           t[4 * k] = q4[0];
           t[4 * k + 1] = q4[1];
           t[4 * k + 2] = q4[2];

@@ -70,13 +70,10 @@ void free_ctx(vlp4d_ctx *c) {
   if (c->plans) {
     cufftDestroy(c->plan_fwd);
     cufftDestroy(c->plan_bwd);
+    cufftDestroy(c->plan_bwd3);
   }
-  cudaFree(c->rho);
-  cudaFree(c->ex);
-  cudaFree(c->ey);
-  cudaFree(c->rho_hat);
-  cudaFree(c->ex_hat);
-  cudaFree(c->ey_hat);
+  cudaFree(c->rho);  // ex, ey are slices of this allocation
+  cudaFree(c->rho_hat);  // ex_hat, ey_hat likewise
   cudaFree(c->nrj);
   cudaFree(c->nrjx);
   cudaFree(c->l2_part);
@@ -178,12 +175,16 @@ int vlp4d_ctx_create(const vlp4d_domain *dom, int dtype, vlp4d_ctx **out) {
     cudaError_t e_ = cudaMalloc(&(ptr), (bytes));                                            \
     if (e_ != cudaSuccess) return bail(fail(VLP4D_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e_))); \
   } while (0)
-  CTX_ALLOC(c->rho, sizeof(double) * nxy);
-  CTX_ALLOC(c->ex, sizeof(double) * nxy);
-  CTX_ALLOC(c->ey, sizeof(double) * nxy);
-  CTX_ALLOC(c->rho_hat, sizeof(cufftDoubleComplex) * nh);
-  CTX_ALLOC(c->ex_hat, sizeof(cufftDoubleComplex) * nh);
-  CTX_ALLOC(c->ey_hat, sizeof(cufftDoubleComplex) * nh);
+  // rho, ex, ey (and their spectra) as 256-byte aligned slices of one
+  // allocation, so that one batched inverse transform writes all three.
+  c->fstride = (size_t)(nxy + 31) / 32 * 32;
+  c->hstride = (nh + 15) / 16 * 16;
+  CTX_ALLOC(c->rho, sizeof(double) * 3 * c->fstride);
+  c->ex = c->rho + c->fstride;
+  c->ey = c->ex + c->fstride;
+  CTX_ALLOC(c->rho_hat, sizeof(cufftDoubleComplex) * 3 * c->hstride);
+  c->ex_hat = c->rho_hat + c->hstride;
+  c->ey_hat = c->ex_hat + c->hstride;
   c->hist_len = dom->nbiter + 1;
   CTX_ALLOC(c->nrj, sizeof(double) * c->hist_len);
   CTX_ALLOC(c->mass, sizeof(double) * c->hist_len);
@@ -232,6 +233,16 @@ int vlp4d_ctx_create(const vlp4d_domain *dom, int dtype, vlp4d_ctx **out) {
   if (cufftPlan2d(&c->plan_bwd, c->g.n[1], c->g.n[0], CUFFT_Z2D) != CUFFT_SUCCESS) {
     cufftDestroy(c->plan_fwd);
     return bail(fail(VLP4D_ERR_CUDA, "cufftPlan2d Z2D failed"));
+  }
+  {
+    int n[2] = {c->g.n[1], c->g.n[0]};
+    int inembed[2] = {c->g.n[1], nx1h}, onembed[2] = {c->g.n[1], c->g.n[0]};
+    if (cufftPlanMany(&c->plan_bwd3, 2, n, inembed, 1, (int)c->hstride, onembed, 1, (int)c->fstride, CUFFT_Z2D, 3) !=
+        CUFFT_SUCCESS) {
+      cufftDestroy(c->plan_fwd);
+      cufftDestroy(c->plan_bwd);
+      return bail(fail(VLP4D_ERR_CUDA, "cufftPlanMany Z2D (batch 3) failed"));
+    }
   }
   c->plans = true;
   if (cudaMallocHost(&c->h_diag, sizeof(double) * 2 * c->hist_len) != cudaSuccess)

@@ -303,9 +303,10 @@ int launch_field_poisson(vlp4d_ctx *c, cudaStream_t s) {
   k_poisson_solve<<<(nh + threads - 1) / threads, threads, 0, s>>>(c->rho_hat, c->ex_hat, c->ey_hat, nx1h, ny, kx0,
                                                                     ky0, normcoeff);
   VLP4D_LAUNCH_CHECK();
-  VLP4D_CUFFT_TRY(cufftExecZ2D(c->plan_bwd, c->rho_hat, c->rho));
-  VLP4D_CUFFT_TRY(cufftExecZ2D(c->plan_bwd, c->ex_hat, c->ex));
-  VLP4D_CUFFT_TRY(cufftExecZ2D(c->plan_bwd, c->ey_hat, c->ey));
+  // phi (into rho), ex, ey: one batched inverse transform over the three
+  // spectra (slices of one allocation at the same strides as the outputs).
+  VLP4D_CUFFT_TRY(cufftSetStream(c->plan_bwd3, s));
+  VLP4D_CUFFT_TRY(cufftExecZ2D(c->plan_bwd3, c->rho_hat, c->rho));
   return VLP4D_OK;
 }
 

@@ -87,6 +87,11 @@ struct vlp4d_ctx {
   // Spectral work arrays ((nx/2+1)*ny complex).
   cufftDoubleComplex *rho_hat = nullptr, *ex_hat = nullptr, *ey_hat = nullptr;
   cufftHandle plan_fwd = 0, plan_bwd = 0;
+  // The three inverse transforms of the field solve (phi, ex, ey) as one
+  // batched plan: rho/ex/ey and their spectra are slices of one allocation
+  // each, at the strides below.
+  cufftHandle plan_bwd3 = 0;
+  size_t fstride = 0, hstride = 0;
   bool plans = false;
 
   // Diagnostics history (nbiter+1 entries each) and the reduction scratch.
