@@ -16,18 +16,28 @@ namespace vlp4d {
 namespace {
 
 // One v-line per (ix, iy): displacement dt*E(ix, iy) (advection.hpp:243, 306).
-__global__ void k_build_vtable(const double *__restrict__ e, int lines, double dt, double hmin, double hmax,
-                               int n, int *__restrict__ m, double *__restrict__ w, float *__restrict__ wf) {
+// blockIdx.y selects the table (vx from Ex, vy from Ey), so that both are
+// built by one launch.
+struct VtableJob {
+  const double *e;
+  double hmin, hmax;
+  int n;
+  int *m;
+  double *w;
+  float *wf;
+};
+__global__ void k_build_vtable(VtableJob j0, VtableJob j1, int lines, double dt) {
   const int line = blockIdx.x * blockDim.x + threadIdx.x;
   if (line >= lines) return;
-  const LineStencil s = line_stencil(__dmul_rn(dt, e[line]), hmin, hmax, n);
-  m[line] = s.m;
+  const VtableJob j = blockIdx.y ? j1 : j0;
+  const LineStencil s = line_stencil(__dmul_rn(dt, j.e[line]), j.hmin, j.hmax, j.n);
+  j.m[line] = s.m;
   float f[6];
   weights_to_f32(s.w, f);
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
-    w[6 * line + k] = s.w[k];
-    wf[6 * line + k] = f[k];
+    j.w[6 * line + k] = s.w[k];
+    j.wf[6 * line + k] = f[k];
   }
 }
 
@@ -251,22 +261,23 @@ int ensure_xy11_table(vlp4d_ctx *c, int dim, double dt, StencilTable **out, cuda
 int build_v_tables(vlp4d_ctx *c, double dt, bool vx, bool vy, cudaStream_t s) {
   const int lines = (int)c->g.nxy();
   const int threads = 256, blocks = (lines + threads - 1) / threads;
+  VtableJob jobs[2];
+  int njobs = 0;
   if (vx) {
     int rc = alloc_table(c->tab_vx, lines);
     if (rc) return rc;
-    k_build_vtable<<<blocks, threads, 0, s>>>(c->ex, lines, dt, c->g.minp[2], c->g.maxp[2], c->g.n[2],
-                                               c->tab_vx.m, c->tab_vx.w, c->tab_vx.wf);
-    VLP4D_LAUNCH_CHECK();
-    c->tab_vx.valid = true;
+    jobs[njobs++] = {c->ex, c->g.minp[2], c->g.maxp[2], c->g.n[2], c->tab_vx.m, c->tab_vx.w, c->tab_vx.wf};
   }
   if (vy) {
     int rc = alloc_table(c->tab_vy, lines);
     if (rc) return rc;
-    k_build_vtable<<<blocks, threads, 0, s>>>(c->ey, lines, dt, c->g.minp[3], c->g.maxp[3], c->g.n[3],
-                                               c->tab_vy.m, c->tab_vy.w, c->tab_vy.wf);
-    VLP4D_LAUNCH_CHECK();
-    c->tab_vy.valid = true;
+    jobs[njobs++] = {c->ey, c->g.minp[3], c->g.maxp[3], c->g.n[3], c->tab_vy.m, c->tab_vy.w, c->tab_vy.wf};
   }
+  if (!njobs) return VLP4D_OK;
+  k_build_vtable<<<dim3((unsigned)blocks, (unsigned)njobs), threads, 0, s>>>(jobs[0], jobs[njobs - 1], lines, dt);
+  VLP4D_LAUNCH_CHECK();
+  if (vx) c->tab_vx.valid = true;
+  if (vy) c->tab_vy.valid = true;
   return VLP4D_OK;
 }
 

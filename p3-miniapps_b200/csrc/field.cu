@@ -34,8 +34,18 @@ __global__ void k_rho_finish(const double *__restrict__ part, double *__restrict
                              double dvx, double dvy) {
   const long long ixy = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (ixy >= nxy) return;
+  // Groups added in order; the loads of 16 groups are issued before their
+  // adds so that their latencies overlap.
   double s = 0.0;
-  for (int g = 0; g < groups; ++g) s += part[(long long)g * nxy + ixy];
+  int g = 0;
+  for (; g + 16 <= groups; g += 16) {
+    double v[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k] = part[(long long)(g + k) * nxy + ixy];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) s += v[k];
+  }
+  for (; g < groups; ++g) s += part[(long long)g * nxy + ixy];
   rho[ixy] = s * dvx * dvy;  // field.cpp:23 (sum * dvx * dvy)
 }
 
@@ -113,8 +123,29 @@ __global__ void k_diags(const double *__restrict__ rho, const double *__restrict
                         double *__restrict__ mass_hist, double *__restrict__ nrjx_hist,
                         double *__restrict__ nrjy_hist, int iter) {
   // Kahan sums of rho, Ex^2 + Ey^2, Ex^2, Ey^2.
+  // Each thread's elements in order; the loads of four of them are issued
+  // before their adds so that their latencies overlap.
   double s[4] = {0., 0., 0., 0.}, c[4] = {0., 0., 0., 0.};
-  for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+  const long long step = blockDim.x;
+  long long i = threadIdx.x;
+  for (; i + 3 * step < n; i += 4 * step) {
+    double r[4], a[4], b[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      r[u] = rho[i + u * step];
+      a[u] = ex[i + u * step];
+      b[u] = ey[i + u * step];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const double ax = __dmul_rn(a[u], a[u]), by = __dmul_rn(b[u], b[u]);
+      kahan_add(s[0], c[0], r[u]);
+      kahan_add(s[1], c[1], __dadd_rn(ax, by));
+      kahan_add(s[2], c[2], ax);
+      kahan_add(s[3], c[3], by);
+    }
+  }
+  for (; i < n; i += step) {
     const double a = ex[i], b = ey[i];
     const double ax = __dmul_rn(a, a), by = __dmul_rn(b, b);
     kahan_add(s[0], c[0], rho[i]);
