@@ -763,7 +763,10 @@ __global__ void __launch_bounds__(512) k_ensemble(EnsArgs a) {
   while (true) {
     if (threadIdx.x < 32) {
       // Warp 0 looks for a tile: 32 members per round, starting at r (the
-      // member last worked on), one sweep over all members at most.
+      // member last worked on), one sweep over all members at most.  Among
+      // the members of a round with free tiles it tries the one with the
+      // most work left first (stages left x cells), so that the largest
+      // members do not finish alone at the end of the run.
       // got_run: -1 leave (all members done, or no work for idle_limit
       // cycles); -2 nothing taken; >= 0 a tile of that member.
       int got_run = -2, got_stage = 0, got_tile = 0;
@@ -773,14 +776,23 @@ __global__ void __launch_bounds__(512) k_ensemble(EnsArgs a) {
           const int idx = rd * 32 + lane;
           const int cand = (int)(((long long)r + idx) % a.nruns);
           bool avail = false;
+          unsigned key = 0;  // work left, 26 bits, at least 1 when avail
           if (idx < a.nruns) {
             const unsigned long long w = *(volatile unsigned long long *)(a.word + cand);
             const int stage = (int)(w >> 32);
-            avail = stage < total_stages && (int)(w & 0xffffffffu) < stage_tiles(a.runs[cand], stage, a.cc);
+            const EnsRun &Rc = a.runs[cand];
+            avail = stage < total_stages && (int)(w & 0xffffffffu) < stage_tiles(Rc, stage, a.cc);
+            if (avail) {
+              const unsigned long long cells = (unsigned long long)Rc.n[0] * Rc.n[1] * Rc.n[2] * Rc.n[3];
+              const unsigned long long work = (unsigned long long)(total_stages - stage) * ((cells >> 10) + 1);
+              key = (unsigned)(work < (1ull << 26) - 1 ? work : (1ull << 26) - 2) + 1u;
+            }
           }
           unsigned ballot = __ballot_sync(0xffffffffu, avail);
           while (ballot) {
-            const int leader = __ffs(ballot) - 1;
+            // Most work left first; lower lanes on ties.
+            const unsigned mine = (ballot >> lane) & 1u ? (key << 5) | (31u - (unsigned)lane) : 0u;
+            const int leader = 31 - (int)(__reduce_max_sync(0xffffffffu, mine) & 31u);
             int ok = 0, st = 0, tl = 0;
             if (lane == leader) {
               const unsigned long long got = atomicAdd(a.word + cand, 1ULL);
@@ -796,7 +808,7 @@ __global__ void __launch_bounds__(512) k_ensemble(EnsArgs a) {
               got_tile = __shfl_sync(0xffffffffu, tl, leader);
               break;
             }
-            ballot &= ballot - 1;
+            ballot &= ~(1u << leader);
           }
         }
         if (got_run >= 0) {
