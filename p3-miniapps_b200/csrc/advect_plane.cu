@@ -127,20 +127,29 @@ __device__ __forceinline__ int read_line(const LineRec<T> &r, T (&w)[6]) {
 
 // Error exit after a copy timed out: flag it, let the copies already issued
 // for items it .. it+S-1 land (bounded waits), then leave.
-__device__ __noinline__ void plane_abort(const PlaneArgs &a, uint64_t *bars, long long it, long long n_items, int S) {
+__device__ __noinline__ void plane_abort(const PlaneArgs &a, uint64_t *bars, long long it, long long n_items, int S,
+                                         long long issued_end = -1) {
   if (threadIdx.x == 0) {
     atomicExch(a.err, 1);
-    const long long last = n_items < it + S ? n_items : it + S;
+    const long long end = issued_end >= 0 ? issued_end : it + S;
+    const long long last = n_items < end ? n_items : end;
     for (long long k = it; k < last; ++k) mbar_wait_bounded(&bars[k % S], (uint32_t)((k / S) & 1));
   }
   __syncthreads();
 }
 
 // Template parameters: element type, row width (0 = runtime a.nx), output
-// rows per thread in the y phase, which sweeps run, moment epilogue.
+// rows per thread in the y phase, which sweeps run, moment epilogue, and
+// INPLACE (x and y both on, nx/4 dividing 32): phase X writes the x-swept
+// rows back into the staged slot instead of a separate tile.  A row's
+// column quads then all belong to one warp, which reads the whole row
+// before any lane writes it (__syncwarp); phase Y reads the slot; the slot
+// of item it - 1 is refilled at the barrier of item it (one item later than
+// with the separate tile).  Without the two x-swept tiles an FP64 pass at
+// 128^4 fits two CTAs per SM.
 // Thread t owns column quad c0 = 4*(t % (nx/4)) and row group t / (nx/4)
 // for the whole kernel; blockDim = (nx/4) * (R/RT).
-template <typename T, int NX, int RT, bool DX, bool DY, bool RHO>
+template <typename T, int NX, int RT, bool DX, bool DY, bool RHO, bool INPLACE = false>
 __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int nx = NX ? NX : a.nx;
@@ -156,7 +165,7 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
   T *slots = reinterpret_cast<T *>(yrec + (DY ? a.nvy : 0));
   // Two x-swept buffers (x and y both on): item it writes xs[it & 1], so the
   // only barrier per item is the one between phase X and phase Y.
-  T *xs_base = slots + (size_t)S * slot_elems;
+  T *xs_base = slots + (size_t)S * slot_elems;  // unused when INPLACE
 
   const int cg = threadIdx.x % ncg;
   const int rg = threadIdx.x / ncg;
@@ -231,38 +240,74 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
       base = wrap_col<NX>(base, nx);
       const int rr = base & 3;
       const int o0 = base - rr, o1 = wrap_col<NX>(o0 + 4, nx), o2 = wrap_col<NX>(o0 + 8, nx);
-      for (int v = rg; v < vrows; v += RG) {
-        const T *row = in + (size_t)v * nx;
-        T t[12], q4[4];
-        load4(row + o0, q4);
-        t[0] = q4[0]; t[1] = q4[1]; t[2] = q4[2]; t[3] = q4[3];
-        load4(row + o1, q4);
-        t[4] = q4[0]; t[5] = q4[1]; t[6] = q4[2]; t[7] = q4[3];
-        load4(row + o2, q4);
-        t[8] = q4[0]; t[9] = q4[1]; t[10] = q4[2]; t[11] = q4[3];
-        T o[4];
-        sweep_x4(t, rr, wx, o);
-        if (DY) {
-          store4(xs + (size_t)v * nx + c0, o);
-        } else {
-          store4(outp + (size_t)v * nx + c0, o);
+      if constexpr (INPLACE) {
+        // Trip count of the warp's first row group, so that every lane
+        // reaches each __syncwarp.
+        const int rgw = (int)((threadIdx.x & ~31u) / (unsigned)ncg);
+        const int trips = (vrows - rgw + RG - 1) / RG;
+        for (int k = 0; k < trips; ++k) {
+          const int v = rg + k * RG;
+          T *row = const_cast<T *>(in) + (size_t)v * nx;
+          T t[12], q4[4], o[4];
+          if (v < vrows) {
+            load4(row + o0, q4);
+            t[0] = q4[0]; t[1] = q4[1]; t[2] = q4[2]; t[3] = q4[3];
+            load4(row + o1, q4);
+            t[4] = q4[0]; t[5] = q4[1]; t[6] = q4[2]; t[7] = q4[3];
+            load4(row + o2, q4);
+            t[8] = q4[0]; t[9] = q4[1]; t[10] = q4[2]; t[11] = q4[3];
+            sweep_x4(t, rr, wx, o);
+          }
+          __syncwarp();  // the row is read by all its lanes
+          if (v < vrows) store4(row + c0, o);
+        }
+        // These generic writes precede the slot's next bulk copy.
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      } else {
+        for (int v = rg; v < vrows; v += RG) {
+          const T *row = in + (size_t)v * nx;
+          T t[12], q4[4];
+          load4(row + o0, q4);
+          t[0] = q4[0]; t[1] = q4[1]; t[2] = q4[2]; t[3] = q4[3];
+          load4(row + o1, q4);
+          t[4] = q4[0]; t[5] = q4[1]; t[6] = q4[2]; t[7] = q4[3];
+          load4(row + o2, q4);
+          t[8] = q4[0]; t[9] = q4[1]; t[10] = q4[2]; t[11] = q4[3];
+          T o[4];
+          sweep_x4(t, rr, wx, o);
+          if (DY) {
+            store4(xs + (size_t)v * nx + c0, o);
+          } else {
+            store4(outp + (size_t)v * nx + c0, o);
+          }
         }
       }
     }
     if (DX && DY) {
-      // xs is complete and the staged slot is no longer read: refill it.
-      if (__syncthreads_or(!ok)) {
-        plane_abort(a, bars, it, n_items, S);
-        return;
+      if constexpr (INPLACE) {
+        // The x-swept rows are complete; every thread is done with item
+        // it - 1, whose slot now takes item it - 1 + S.
+        const long long issued_end = it == 0 ? (long long)S : it - 1 + S;
+        if (__syncthreads_or(!ok)) {
+          plane_abort(a, bars, it, n_items, S, issued_end);
+          return;
+        }
+        if (threadIdx.x == 0 && it > 0 && it - 1 + S < n_items) issue(it - 1 + S);
+      } else {
+        // xs is complete and the staged slot is no longer read: refill it.
+        if (__syncthreads_or(!ok)) {
+          plane_abort(a, bars, it, n_items, S);
+          return;
+        }
+        if (threadIdx.x == 0 && it + S < n_items) issue(it + S);
       }
-      if (threadIdx.x == 0 && it + S < n_items) issue(it + S);
     }
     if (DY) {  // Phase Y: rows r0 .. r0+RT-1 of this thread's column quad.
       T wl[6];
       read_line(yrec[ivy], wl);
       SweepW<T> wy;
       make_sweep_w(wl, wy);
-      const T *src = (DX ? xs : in) + (size_t)r0 * nx + c0;
+      const T *src = ((DX && !INPLACE) ? xs : in) + (size_t)r0 * nx + c0;
       T *dst = outp + (size_t)r0 * nx + c0;
       sweep_y<RT>(src, nx, wy, [&](int i, const T (&o)[4]) {
         store4(dst + (size_t)i * nx, o);
@@ -686,6 +731,7 @@ struct PlaneCfg {
   int R = 0, rt = 1, stages = 3, threads = 0, cpp = 1, grid = 0, G = 0;
   size_t smem = 0;
   int per_sm = 0;
+  bool inplace = false;
 };
 
 int env_int(const char *name, int dflt) {
@@ -693,10 +739,11 @@ int env_int(const char *name, int dflt) {
   return v && *v ? atoi(v) : dflt;
 }
 
-size_t plane_smem(int R, int halo, int nx, size_t elem, int stages, bool dx, bool dy, int nvx, int nvy) {
+size_t plane_smem(int R, int halo, int nx, size_t elem, int stages, bool dx, bool dy, int nvx, int nvy,
+                  bool inplace = false) {
   const size_t slot = (size_t)(R + halo) * nx * elem;
   const size_t rec = elem == 4 ? 32 : 64;
-  return kBarBytes + rec * ((dx ? nvx : 0) + (dy ? nvy : 0)) + stages * slot + ((dx && dy) ? 2 * slot : 0);
+  return kBarBytes + rec * ((dx ? nvx : 0) + (dy ? nvy : 0)) + stages * slot + ((dx && dy && !inplace) ? 2 * slot : 0);
 }
 
 // Chooses the chunk height R, rows per thread RT, the pipeline depth and the
@@ -726,17 +773,20 @@ bool plane_config(const vlp4d_ctx *c, bool dx, bool dy, PlaneCfg &cfg) {
     break;
   }
   if (!R) return false;
+  // FP64 x+y: x-swept rows in place (no separate tiles) when a warp holds
+  // whole rows; VLP4D_PLANE_INPLACE=0 turns it off.
+  const bool inplace = elem == 8 && dx && dy && 32 % ncg == 0 && env_int("VLP4D_PLANE_INPLACE", 1) != 0;
   const size_t two_per_sm = 112 * 1024, one_per_sm = 224 * 1024;
   int stages = 0;
   if (forced_s) {
     stages = forced_s;
   } else {
     for (int st = 3; st >= 2 && !stages; --st)
-      if (plane_smem(R, halo, nx, elem, st, dx, dy, c->g.n[2], c->g.n[3]) <= two_per_sm) stages = st;
+      if (plane_smem(R, halo, nx, elem, st, dx, dy, c->g.n[2], c->g.n[3], inplace) <= two_per_sm) stages = st;
     if (!stages) stages = 3;
   }
   if (stages < 2 || stages > kMaxStages) return false;
-  const size_t smem = plane_smem(R, halo, nx, elem, stages, dx, dy, c->g.n[2], c->g.n[3]);
+  const size_t smem = plane_smem(R, halo, nx, elem, stages, dx, dy, c->g.n[2], c->g.n[3], inplace);
   if (smem > one_per_sm) return false;
   cfg.R = R;
   cfg.rt = rt;
@@ -744,12 +794,19 @@ bool plane_config(const vlp4d_ctx *c, bool dx, bool dy, PlaneCfg &cfg) {
   cfg.cpp = ny / R;
   cfg.threads = ncg * (R / rt);
   cfg.smem = smem;
+  cfg.inplace = inplace;
   return true;
 }
+
+// Widths whose rows a warp holds whole (nx/4 divides 32), or the run-time width.
+constexpr bool inplace_width(int nx) { return nx == 0 || (nx % 4 == 0 && nx / 4 <= 32 && 32 % (nx / 4) == 0); }
 
 template <typename T, int NX, int RT, bool DX, bool DY, bool RHO>
 int run_plane(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, cudaStream_t s) {
   auto kern = k_plane<T, NX, RT, DX, DY, RHO>;
+  if constexpr (sizeof(T) == 8 && DX && DY && inplace_width(NX)) {
+    if (cfg.inplace) kern = k_plane<T, NX, RT, DX, DY, RHO, true>;
+  }
   VLP4D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
   int per_sm = 0;
   VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, cfg.threads, cfg.smem));
