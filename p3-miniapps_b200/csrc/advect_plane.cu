@@ -245,6 +245,9 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
         // reaches each __syncwarp.
         const int rgw = (int)((threadIdx.x & ~31u) / (unsigned)ncg);
         const int trips = (vrows - rgw + RG - 1) / RG;
+        // The lanes this warp has (small grids give blocks below 32 threads).
+        const unsigned wl = blockDim.x - (threadIdx.x & ~31u);
+        const unsigned wmask = wl >= 32 ? 0xffffffffu : (1u << wl) - 1u;
         for (int k = 0; k < trips; ++k) {
           const int v = rg + k * RG;
           T *row = const_cast<T *>(in) + (size_t)v * nx;
@@ -258,7 +261,7 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
             t[8] = q4[0]; t[9] = q4[1]; t[10] = q4[2]; t[11] = q4[3];
             sweep_x4(t, rr, wx, o);
           }
-          __syncwarp();  // the row is read by all its lanes
+          __syncwarp(wmask);  // the row is read by all its lanes
           if (v < vrows) store4(row + c0, o);
         }
         // These generic writes precede the slot's next bulk copy.
