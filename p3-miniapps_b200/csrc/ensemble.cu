@@ -441,7 +441,7 @@ __device__ void ens_planes11(const EnsArgs &a, const EnsRun &R, const float *fin
   }
   for (int gi = 0; gi < ngroups; ++gi) {
     cp_async_wait<kEnsRing - 2>();
-    __syncthreads();  // group gi landed; group gi - 1 is done with
+    __syncthreads();  // group gi landed; every thread is done with group gi - 1
     load_group(gi + kEnsRing - 1);
     const int p0 = gi * P;
     const int np = nvx - p0 < P ? nvx - p0 : P;
