@@ -335,7 +335,8 @@ int launch_field_poisson(vlp4d_ctx *c, cudaStream_t s) {
                                                                     ky0, normcoeff);
   VLP4D_LAUNCH_CHECK();
   // phi (into rho), ex, ey: one batched inverse transform over the three
-  // spectra (slices of one allocation at the same strides as the outputs).
+  // spectra (slices of one allocation; the plan's input and output batch
+  // distances are the spectrum and field slice strides).
   VLP4D_CUFFT_TRY(cufftSetStream(c->plan_bwd3, s));
   VLP4D_CUFFT_TRY(cufftExecZ2D(c->plan_bwd3, c->rho_hat, c->rho));
   return VLP4D_OK;
