@@ -59,6 +59,10 @@ struct vlp4d_adjoint {
   double *gpart = nullptr;  // per-segment partial sums of gE
   int gsegs = 0;
   cufftDoubleComplex *hx_hat = nullptr, *hy_hat = nullptr;  // spectra of the impulse responses
+  // Forward transforms of gex and gey (adjacent, n2 apart) into the
+  // context's ex_hat and ey_hat as one batched plan.
+  cufftHandle plan_g2 = 0;
+  bool have_plan_g2 = false;
   bool field_linear = true;  // false for the analytic-field cases 2 and 6
   StencilTable tab_x_adj, tab_y_adj, tab_vx_adj, tab_vy_adj;
   double *dw_vx = nullptr, *dw_vy = nullptr;  // dw/dE per v line (6 each, FP64)
@@ -416,6 +420,14 @@ int field_transpose_setup(vlp4d_adjoint *A, cudaStream_t s) {
     A->field_linear = false;
     return VLP4D_OK;
   }
+  {
+    int n[2] = {c->g.n[1], c->g.n[0]};
+    int inembed[2] = {c->g.n[1], c->g.n[0]}, onembed[2] = {c->g.n[1], c->g.n[0] / 2 + 1};
+    if (cufftPlanMany(&A->plan_g2, 2, n, inembed, 1, (int)n2, onembed, 1, (int)c->hstride, CUFFT_D2Z, 2) !=
+        CUFFT_SUCCESS)
+      return fail_msg(VLP4D_ERR_CUDA, "adjoint: cufftPlanMany D2Z (batch 2) failed");
+    A->have_plan_g2 = true;
+  }
   VLP4D_CUDA_TRY(cudaMemcpyAsync(A->save, c->rho, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
   VLP4D_CUDA_TRY(cudaMemcpyAsync(A->save + n2, c->ex, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
   VLP4D_CUDA_TRY(cudaMemcpyAsync(A->save + 2 * n2, c->ey, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
@@ -442,10 +454,9 @@ int field_transpose(vlp4d_adjoint *A, cudaStream_t s) {
     VLP4D_CUDA_TRY(cudaMemsetAsync(A->lam_rho, 0, sizeof(double) * c->g.nxy(), s));
     return VLP4D_OK;
   }
-  VLP4D_CUFFT_TRY(cufftSetStream(c->plan_fwd, s));
+  VLP4D_CUFFT_TRY(cufftSetStream(A->plan_g2, s));
   VLP4D_CUFFT_TRY(cufftSetStream(c->plan_bwd, s));
-  VLP4D_CUFFT_TRY(cufftExecD2Z(c->plan_fwd, A->gex, c->ex_hat));
-  VLP4D_CUFFT_TRY(cufftExecD2Z(c->plan_fwd, A->gey, c->ey_hat));
+  VLP4D_CUFFT_TRY(cufftExecD2Z(A->plan_g2, A->gex, c->ex_hat));  // gex, gey -> ex_hat, ey_hat
   const int nh = (nx / 2 + 1) * ny;
   k_field_transpose<<<(nh + 255) / 256, 256, 0, s>>>(c->ex_hat, c->ey_hat, A->hx_hat, A->hy_hat, c->rho_hat, nh,
                                                      1.0 / ((double)nx * ny));
@@ -703,6 +714,7 @@ int run_graph(vlp4d_adjoint *A, cudaGraphExec_t &exec, const void **cached, cons
 
 void destroy(vlp4d_adjoint *A) {
   if (!A) return;
+  if (A->have_plan_g2) cufftDestroy(A->plan_g2);
   if (A->g_fwd) cudaGraphExecDestroy(A->g_fwd);
   if (A->g_bwd) cudaGraphExecDestroy(A->g_bwd);
   for (void *p : A->ckpt) cudaFree(p);
