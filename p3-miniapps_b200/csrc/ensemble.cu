@@ -486,7 +486,48 @@ __device__ void ens_planes11(const EnsArgs &a, const EnsRun &R, const float *fin
         *reinterpret_cast<float4 *>(b1 + row + ix0) = make_float4(out[0], out[1], out[2], out[3]);
       }
       __syncthreads();
-      for (int it = threadIdx.x; it < items; it += blockDim.x) {
+      if ((ny & 1) == 0) {
+        // Y11 of two rows per item (iy, iy + 1 of one column quad): twelve
+        // row loads and eleven differences serve both outputs, each computed
+        // exactly as by the one-row items below.
+        const int nq2 = nqp >> 1;
+        const float inv_nq2 = 1.f / (float)nq2;
+        const int items2 = np * nq2;
+        for (int it = threadIdx.x; it < items2; it += blockDim.x) {
+          const int p = div_small(it, nq2, inv_nq2);
+          const int qi = it - p * nq2;
+          const int iyp = div_small(qi, nq, inv_nq);
+          const int ix0 = (qi - iyp * nq) << 2;
+          const int iy = 2 * iyp;
+          const float *pl = b1 + p * nxy + ix0;
+          int j = iy + my;
+          j = j >= ny ? j - ny : j;
+          float2 y[12][2];
+#pragma unroll
+          for (int k = 0; k < 12; ++k) {
+            const float4 v = *reinterpret_cast<const float4 *>(pl + j * nx);
+            y[k][0] = make_float2(v.x, v.y);
+            y[k][1] = make_float2(v.z, v.w);
+            if (++j == ny) j = 0;
+          }
+          float2 o2[2][2];
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            float2 d[11];
+#pragma unroll
+            for (int k = 0; k < 11; ++k) d[k] = sub2(y[k + 1][h], y[k][h]);
+            o2[0][h] = ens_interp11(uy, y[5][h], d);
+            o2[1][h] = ens_interp11(uy, y[6][h], d + 1);
+          }
+#pragma unroll
+          for (int r = 0; r < 2; ++r) {
+            const int cell = p * nxy + (iy + r) * nx + ix0;
+            const float4 o4 = make_float4(o2[r][0].x, o2[r][0].y, o2[r][1].x, o2[r][1].y);
+            *reinterpret_cast<float4 *>(fout + gbase + cell) = o4;
+            *reinterpret_cast<float4 *>(b0 + cell) = o4;
+          }
+        }
+      } else for (int it = threadIdx.x; it < items; it += blockDim.x) {
         const int p = div_small(it, nqp, inv_nqp);
         const int qi = it - p * nqp;
         const int iy = div_small(qi, nq, inv_nq);
