@@ -40,9 +40,9 @@ def _members(pkg, dims, nsteps_dt=0.1):
 
 
 # (10, 12, 16, 14): rows that are not a multiple of four floats (the scalar
-# plane sweeps).
+# plane sweeps); (16, 15, 12, 10): an odd number of rows (one-row y items).
 DIMS = [(16, 24, 32, 16), (24, 16, 16, 32), (32, 32, 24, 24), (16, 16, 16, 16), (48, 24, 16, 24),
-        (24, 48, 48, 16), (8, 12, 20, 10), (40, 16, 24, 36), (10, 12, 16, 14)]
+        (24, 48, 48, 16), (8, 12, 20, 10), (40, 16, 24, 36), (10, 12, 16, 14), (16, 15, 12, 10)]
 
 
 def test_members_match_single_runs(pkg, cuda):
