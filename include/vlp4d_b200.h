@@ -275,8 +275,10 @@ int vlp4d_energy_grad(vlp4d_adjoint *adj, const void *f, double *J, void *lam, v
 
 /* ---- Batched ensemble.  No reference counterpart (the reference runs one
  * domain per process).  Many independent runs of uneven grids, each the
- * vlp4d step of timestep.hpp:14-67 with FP32 f and FP64 fields from the
- * Landau initial condition f0 = M(vx) M(vy) (1 + amp (cos k x + cos k y)),
+ * vlp4d time loop of timestep.hpp:14-67 with FP32 f and FP64 fields (the
+ * closing x/y half step of one step and the opening one of the next joined
+ * as in vlp4d_steps) from the Landau initial condition
+ * f0 = M(vx) M(vy) (1 + amp (cos k x + cos k y)),
  * advance in ONE persistent kernel launch that a CUDA graph replays (with
  * the initial condition and the scheduler reset).  Members need
  * nx, ny, nvx <= 64.  The energy history of each member (nsteps + 1 values,
