@@ -300,12 +300,10 @@ def gpu_arm(args, ranks):
 
     # End to end through the C ABI with host buffers (vlp4d_run): H2D of the
     # initial f from pinned memory, the initial solve, K steps, D2H of the
-    # diagnostic history and of the final f.  Also yields the FP32 vs FP64 error.
+    # diagnostic history and of the final f.
     e2e = None
     err = {}
     if not args.no_e2e and not args.only_f32:
-        finals = {}
-        histories = {}
         e2e_vals = {}
         for dtype in ("f32", "f64"):
             tdt = torch.float32 if dtype == "f32" else torch.float64
@@ -319,13 +317,11 @@ def gpu_arm(args, ranks):
                 ranks.barrier()
                 e0, e1 = _events(torch)
                 e0.record(stream)
-                nrj, mass = ctx.run(h0, K, fa, fb, f_out_host=hout)
+                ctx.run(h0, K, fa, fb, f_out_host=hout)
                 e1.record(stream)
                 torch.cuda.synchronize()
                 secs = ranks.max(e0.elapsed_time(e1) / 1e3)
                 e2e_vals[dtype] = cells * K * ranks.world / secs / 1e9
-                histories[dtype] = nrj
-                finals[dtype] = fa.double() if dtype == "f64" else fa.clone()
                 fbytes = cells * h0.element_size()
                 if dtype == "f32":
                     e2e = {"value": e2e_vals["f32"], "unit": METRIC,
@@ -333,18 +329,8 @@ def gpu_arm(args, ranks):
                            "seconds": secs, "api": "vlp4d_run (C ABI, pinned host buffers)"}
                 del fa, fb, h0, hout
                 torch.cuda.empty_cache()
-        import numpy as np
-
-        w32 = np.exp(2 * histories["f32"])
-        w64 = np.exp(2 * histories["f64"])
-        rel = np.abs(w32 - w64) / w64
-        df = (finals["f32"].double() - finals["f64"]).abs().max().item()
-        err = {"steps": K, "energy_rel_max": float(rel.max()), "energy_rel_final": float(rel[-1]),
-               "energy_abs_max_over_wmax": float(np.abs(w32 - w64).max() / w64.max()),
-               "f_maxabs": df, "f_max": finals["f64"].abs().max().item(),
-               "e2e_f64": e2e_vals["f64"]}
-        del finals
-        torch.cuda.empty_cache()
+        err = error_arm(pkg, torch, n)
+        err["e2e_f64"] = e2e_vals["f64"]
 
     adjoint = None if args.only_f32 else adjoint_arm(pkg, torch, stream)
     ensemble = None if args.only_f32 else ensemble_arm(pkg, torch, stream, peak)
@@ -370,6 +356,46 @@ def gpu_arm(args, ranks):
         "ensemble": ensemble,
     }
     return line
+
+
+ERROR_STEPS = 100
+
+
+def error_arm(pkg, torch, n, nsteps=ERROR_STEPS):
+    """FP32-storage error against the FP64 path over the configuration's own
+    100 steps, whatever --steps is: the same initial condition and solve,
+    then vlp4d_steps (the timed time loop; in FP32 its joined k_plane_xyxy
+    passes) for nsteps steps in each precision, untimed.  Relative
+    electric-energy error max_t |W32 - W64| / W64 (W = exp(2 nrj), the
+    history of Diags::compute) and the max-norm difference of the final f."""
+    import numpy as np
+
+    v = pkg.vlp4d
+    dom = pkg.landau_domain(n, dt=DT, nbiter=nsteps, L=L_BOX, vmax=VMAX)
+    hist, final = {}, {}
+    for dtype in ("f64", "f32"):
+        with pkg.Context(dom, dtype) as ctx:
+            fa, fb = ctx.empty_f(), ctx.empty_f()
+            ctx.init_case(fa, v.IC_LANDAU_SUM, 0.05, 0.5)
+            ctx.field_rho(fa)
+            ctx.field_poisson()
+            ctx.diags_compute(0)
+            ctx.steps(fa, fb, 1, nsteps)
+            hist[dtype] = ctx.diags_read(nsteps + 1)[0]
+            final[dtype] = fb.double()
+            del fa, fb
+        torch.cuda.empty_cache()
+    w32, w64 = np.exp(2 * hist["f32"]), np.exp(2 * hist["f64"])
+    rel = np.abs(w32 - w64) / w64
+    df = (final["f32"] - final["f64"]).abs().max().item()
+    out = {"steps": nsteps, "api": "vlp4d_steps in both precisions",
+           "energy_rel_max": float(rel.max()), "energy_rel_argmax_step": int(rel.argmax()),
+           "energy_rel_final": float(rel[-1]),
+           "energy_abs_max_over_wmax": float(np.abs(w32 - w64).max() / w64.max()),
+           "f_maxabs": df, "f_max": final["f64"].abs().max().item()}
+    del final
+    torch.cuda.empty_cache()
+    return out
 
 
 def ensemble_arm(pkg, torch, stream, peak, nruns=256, nsteps=50, autotune=True):

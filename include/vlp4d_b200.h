@@ -214,8 +214,10 @@ int vlp4d_print_fxvx(vlp4d_ctx *ctx, const void *fn, const char *path);
  * fixed 4 MiB array built into the library (present on every GPU that loads
  * it, until exit), so nx*ny may not exceed 524288 (larger grids return
  * VLP4D_ERR_INVALID_ARG).  The first call on each device, with that device
- * current, looks up the array's device address once; make that first call
- * before any stream capture.  All calls share the array: calls whose kernels
+ * current, looks up the array's device address once and keeps it for the
+ * life of the process; make that first call before any stream capture, and
+ * do not call this entry point after a cudaDeviceReset of that device (the
+ * kept address would be stale).  All calls share the array: calls whose kernels
  * overlap on the GPU race, so issue them on one stream or otherwise in
  * order. */
 int vlp4d_field_rho_noalloc(const void *fn, int dtype, int nx, int ny, int nvx, int nvy, double dvx, double dvy,

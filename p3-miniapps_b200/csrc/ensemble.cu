@@ -1037,6 +1037,25 @@ int ens_check(vlp4d_ensemble *E) {
   return VLP4D_OK;
 }
 
+// Makes the ensemble's device current for the duration of an API call and
+// restores the caller's device afterwards, so that graph capture, launches
+// and synchronisation always target the device the ensemble lives on.
+struct EnsDeviceScope {
+  int prev = -1;
+  bool ok = false;
+  explicit EnsDeviceScope(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    ok = prev == dev || cudaSetDevice(dev) == cudaSuccess;
+    if (!ok) cudaGetLastError();
+  }
+  ~EnsDeviceScope() {
+    if (ok && prev >= 0) cudaSetDevice(prev);
+  }
+};
+
 }  // namespace
 }  // namespace vlp4d
 
@@ -1161,6 +1180,8 @@ int vlp4d_ensemble_get_tiles(const vlp4d_ensemble *ens, int *threads, int *cols_
 
 int vlp4d_ensemble_run(vlp4d_ensemble *ens, void *stream) {
   if (!ens) return fail_msg(VLP4D_ERR_INVALID_ARG, "ens is NULL");
+  EnsDeviceScope dev_scope(ens->device);
+  if (!dev_scope.ok) return fail_msg(VLP4D_ERR_CUDA, "ensemble: cannot make its device current");
   vlp4d_ensemble *E = ens;
   cudaStream_t s = (cudaStream_t)stream;
   int rc;
@@ -1196,12 +1217,16 @@ int vlp4d_ensemble_run(vlp4d_ensemble *ens, void *stream) {
 
 int vlp4d_ensemble_check(vlp4d_ensemble *ens) {
   if (!ens) return fail_msg(VLP4D_ERR_INVALID_ARG, "ens is NULL");
+  EnsDeviceScope dev_scope(ens->device);
+  if (!dev_scope.ok) return fail_msg(VLP4D_ERR_CUDA, "ensemble: cannot make its device current");
   VLP4D_CUDA_TRY(cudaDeviceSynchronize());
   return ens_check(ens);
 }
 
 int vlp4d_ensemble_read(vlp4d_ensemble *ens, int run, void *f_out, double *nrj, void *stream) {
   if (!ens) return fail_msg(VLP4D_ERR_INVALID_ARG, "ens is NULL");
+  EnsDeviceScope dev_scope(ens->device);
+  if (!dev_scope.ok) return fail_msg(VLP4D_ERR_CUDA, "ensemble: cannot make its device current");
   if (run < 0 || run >= ens->nruns) return fail_msg(VLP4D_ERR_INVALID_ARG, "run index out of range");
   const EnsRun &R = ens->host_runs[run];
   cudaStream_t s = (cudaStream_t)stream;
@@ -1225,6 +1250,8 @@ long long vlp4d_ensemble_cells(const vlp4d_ensemble *ens) { return ens ? ens->to
 // configuration to csv_path (when not NULL) and keeps the fastest.
 int vlp4d_ensemble_autotune(vlp4d_ensemble *ens, int steps, const char *csv_path, void *stream) {
   if (!ens) return fail_msg(VLP4D_ERR_INVALID_ARG, "ens is NULL");
+  EnsDeviceScope dev_scope(ens->device);
+  if (!dev_scope.ok) return fail_msg(VLP4D_ERR_CUDA, "ensemble: cannot make its device current");
   if (steps < 1 || steps > ens->nsteps) steps = ens->nsteps > 0 ? ens->nsteps : 1;
   vlp4d_ensemble *E = ens;
   cudaStream_t s = (cudaStream_t)stream;

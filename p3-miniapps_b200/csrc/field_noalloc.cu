@@ -20,8 +20,12 @@
 // Host code cannot pass `g_rho_scratch` to a kernel: in host code the name
 // is a host-side stand-in, not a device address.  The first call on each
 // device, with that device current, looks the address up once with
-// cudaGetSymbolAddress and caches it; that first call should come before
-// any stream capture on that device.
+// cudaGetSymbolAddress and caches it for the life of the process; that
+// first call should come before any stream capture on that device.  The
+// cache assumes the device's primary context lives as long as the process:
+// after cudaDeviceReset (or anything else that destroys the primary context
+// and reloads this module) the cached address is stale, so such callers
+// must not use this entry point after a reset.
 #include <mutex>
 
 #include "internal.cuh"

@@ -444,8 +444,17 @@ def field_rho_noalloc(f, rho, nxmax, dvx, dvy, stream=None):
     without a context and without allocating device memory."""
     import torch
 
-    dtype = F64 if f.dtype == torch.float64 else F32
     nx, ny, nvx, nvy = (int(v) for v in nxmax)
+    # The C side sees only pointers: check here what it cannot.
+    if not (f.is_cuda and f.is_contiguous() and f.dtype in (torch.float64, torch.float32)):
+        raise ValueError("f must be a contiguous CUDA float64 or float32 tensor")
+    if f.numel() != nx * ny * nvx * nvy:
+        raise ValueError(f"f has {f.numel()} elements; nxmax {tuple(nxmax)} needs {nx * ny * nvx * nvy}")
+    if not (rho.is_cuda and rho.is_contiguous() and rho.dtype == torch.float64 and rho.numel() == nx * ny):
+        raise ValueError(f"rho must be a contiguous CUDA float64 tensor of nx*ny = {nx * ny} elements")
+    if f.device != rho.device:
+        raise ValueError("f and rho must be on the same device")
+    dtype = F64 if f.dtype == torch.float64 else F32
     _check(lib().vlp4d_field_rho_noalloc(C.c_void_p(f.data_ptr()), dtype, nx, ny, nvx, nvy, float(dvx), float(dvy),
                                          C.c_void_p(rho.data_ptr()), _stream_ptr(stream)))
 
