@@ -11,10 +11,13 @@ than the 126 MB L2, so no flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-One process per GPU; N > 1 runs N independent replicas (a single run does
-not shard) timed as the max over ranks.  `--impl reference` times the
-reference's own OpenMP CPU build (oracle/_ref) on the host cores instead.
-Rank 0 prints one JSON line.
+One process per GPU.  N > 1 cuts the same 128^4 run into N vy slabs
+(distrib.SlabRun: NCCL send/recv of the halo planes and an all-reduce of
+rho per step; strong scaling, timed as the max over ranks), and splits the
+batched ensemble's members over the ranks (no communication); `--replicas`
+runs N independent copies of the single-GPU workload instead.
+`--impl reference` times the reference's own OpenMP CPU build (oracle/_ref)
+on the host cores instead.  Rank 0 prints one JSON line.
 """
 from __future__ import annotations
 
@@ -51,6 +54,11 @@ def parse_args(argv=None):
                     help="profiling cases: the reverse-mode, the ensemble or the vlp4d_mpi arm alone "
                          "(--steps steps, --members members, default tiles; --n for mpi), one JSON line")
     ap.add_argument("--members", type=int, default=256, help="ensemble members for --case ensemble")
+    ap.add_argument("--replicas", action="store_true",
+                    help="N > 1: independent copies of the single-GPU workload instead of one run cut into vy slabs")
+    ap.add_argument("--halo", type=int, default=4, help="vy halo planes per side of a slab (N > 1)")
+    ap.add_argument("--slab", action="store_true",
+                    help="run the vy-slab path even on one GPU (one slab, its halos filled from itself)")
     return ap.parse_args(argv)
 
 
@@ -68,6 +76,10 @@ class Ranks:
 
             import torch.distributed as dist
 
+            if backend == "nccl":
+                import torch
+
+                torch.cuda.set_device(self.local_rank)
             dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
             self.dist = dist
         self.backend = backend
@@ -87,6 +99,13 @@ class Ranks:
             return float(x)
         t = self._tensor(x)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if not self.dist:
+            return float(x)
+        t = self._tensor(x)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
         return float(t.item())
 
     def close(self):
@@ -358,6 +377,95 @@ def gpu_arm(args, ranks):
     return line
 
 
+def slab_arm(args, ranks):
+    """N > 1: the 128^4 FP32 run cut into N vy slabs, one per GPU
+    (distrib.SlabRun on slab contexts; per step an NCCL all-reduce of the
+    nx*ny FP64 rho and NCCL send/recv of `--halo` vy planes on each side).
+    Strong scaling: the whole job advances N^4 cells per step.  `value` is
+    device-timed with CUDA events over K steps on buffers already on the
+    GPUs (max over ranks); `e2e` adds, per rank, the H2D copy of its owned
+    planes of f0 from pinned memory, the initial solve, and the D2H copy of
+    its final planes and of the diagnostic history."""
+    import importlib
+
+    import torch
+
+    import __graft_entry__ as ge
+
+    pkg = ge.load_package()
+    v = pkg.vlp4d
+    d = importlib.import_module(pkg.__name__ + ".distrib")
+    torch.cuda.set_device(ranks.local_rank)
+    dev = torch.device("cuda", ranks.local_rank)
+    stream = torch.cuda.current_stream(dev)
+    K, W = args.steps, max(args.warmup, 3)
+    n = args.n
+    dom = pkg.landau_domain(n, dt=DT, nbiter=W + 2 * K + 2, L=L_BOX, vmax=VMAX)
+    ivy0, nloc = d.partition_vy(n, ranks.world)[ranks.rank]
+    ctx = pkg.Context(dom, "f32", slab=(ivy0, nloc, args.halo))
+    run = d.SlabRun(ctx, DT)
+    comm = d.TorchComm()
+    sampler = ClockSampler(ranks.local_rank)
+    sampler.start()
+    ctx.init_case(run.state, v.IC_LANDAU_SUM, 0.05, 0.5)
+    d.run_distributed(run, comm, W, iter0=1)  # initial field + warm-up steps
+    torch.cuda.synchronize()
+    ranks.barrier()
+    torch.cuda.synchronize()
+    launches0 = v.kernel_launches()
+    halo0 = comm.halo_bytes
+    e0, e1 = _events(torch)
+    e0.record(stream)
+    d.run_distributed(run, comm, K, iter0=W + 1, start=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = v.kernel_launches() - launches0
+    halo_bytes = (comm.halo_bytes - halo0) / K
+    ctx.check()
+    secs = ranks.max(e0.elapsed_time(e1) / 1e3)
+    ranks.barrier()
+    # End to end: this rank's planes of f0 from pinned host memory in, the
+    # final planes and the diagnostic history out.
+    own = ctx.owned(run.state)
+    h0 = torch.empty(own.shape, dtype=torch.float32, pin_memory=True)
+    h0.copy_(own)
+    hout = torch.empty_like(h0, pin_memory=True)
+    torch.cuda.synchronize()
+    ranks.barrier()
+    e0.record(stream)
+    ctx.owned(run.state).copy_(h0, non_blocking=True)
+    d.run_distributed(run, comm, K, iter0=1)
+    hout.copy_(ctx.owned(run.state), non_blocking=True)
+    nrj, _ = ctx.diags_read(K + 1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_secs = ranks.max(e0.elapsed_time(e1) / 1e3)
+    clocks = sampler.stop()
+    cells = dom.cells
+    fbytes = h0.numel() * 4
+    ensemble = ensemble_arm(pkg, torch, stream, measured_hbm_peak()[0], ranks=ranks, autotune=False)
+    line = {
+        "metric": METRIC, "value": cells * K / secs / 1e9, "unit": METRIC, "n_gpus": ranks.world, "steps": K,
+        "warmup": W, "ms_per_step": secs * 1e3 / K, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "api": "distrib.SlabRun over vlp4d slab contexts (C ABI), NCCL exchanges",
+        "dtype": "f32", "data": "synthetic (Landau initial condition computed on the device)",
+        "config": {"workload": WORKLOAD, "grid": [n] * 4, "dt": DT, "storage": "f32 f, f64 fields/diagnostics",
+                   "parallelism": f"vy slabs x{ranks.world}: {nloc} planes on rank {ranks.rank}, halo "
+                                  f"{args.halo} planes per side (NCCL send/recv), rho all-reduce (NCCL)",
+                   "l2": "f slab (%.2f GB per GPU) larger than L2, no flush" % (cells / ranks.world * 4 / 1e9)},
+        "halo_bytes_per_step_per_rank": halo_bytes,
+        "e2e": {"value": cells * K / e2e_secs / 1e9, "unit": METRIC, "h2d_bytes_per_step": fbytes / K,
+                "d2h_bytes_per_step": (fbytes + 8 * (K + 1)) / K, "seconds": e2e_secs,
+                "api": "distrib.SlabRun (C ABI, pinned host buffers, per rank)"},
+        "gpu_launches": launches, "clocks": clocks,
+        "energy_first_last": [float(nrj[0]), float(nrj[-1])],
+        "ensemble": ensemble,
+    }
+    del own, h0, hout
+    ctx.close()
+    return line
+
+
 ERROR_STEPS = 100
 
 
@@ -398,7 +506,7 @@ def error_arm(pkg, torch, n, nsteps=ERROR_STEPS):
     return out
 
 
-def ensemble_arm(pkg, torch, stream, peak, nruns=256, nsteps=50, autotune=True):
+def ensemble_arm(pkg, torch, stream, peak, nruns=256, nsteps=50, autotune=True, ranks=None):
     """The batched-ensemble configuration: 256 Landau members, N per dimension
     drawn from {16, 24, 32, 48}, amp ~ U[0.01, 0.1], k in {0.3, 0.5}, 50 steps
     of dt 0.1, FP32 f, in one persistent launch replayed from a CUDA graph.
@@ -406,23 +514,40 @@ def ensemble_arm(pkg, torch, stream, peak, nruns=256, nsteps=50, autotune=True):
     per cell of a run: the moment of f0 reads f once (4 B), each step's x/y
     pass (the first one alone, later ones joined with the previous step's
     closing half step) and vx/vy pass read and write it (16 B per step), and
-    the closing x/y pass of the last step reads and writes it (8 B)."""
+    the closing x/y pass of the last step reads and writes it (8 B).
+
+    With ranks over several GPUs the members are split over them
+    (distrib.partition_members, no communication); the time is the slowest
+    rank's and the cells are summed over the ranks."""
+    import importlib
+
     v = pkg.vlp4d
     members = v.landau_ensemble_members(nruns)
+    world = ranks.world if ranks is not None else 1
+    if world > 1:
+        d = importlib.import_module(pkg.__name__ + ".distrib")
+        mine = d.partition_members([m.n for m in members], world)[ranks.rank]
+        members = [members[i] for i in mine]
     with v.Ensemble(members, nsteps) as ens:
         tiles = ens.autotune(3) if autotune else ens.tiles()
         ens.run()  # capture
         ens.check()
+        if world > 1:
+            ranks.barrier()
         t = time_calls(torch, stream, lambda: ens.run(stream), 3)
         ens.check()
         cells = ens.cells
+        if world > 1:
+            t = ranks.max(t)
+            cells = int(ranks.sum(cells))
         run_bytes = (16.0 * nsteps + 12.0) * cells
         gbs = run_bytes / t / 1e9
         return {"config": {"members": nruns, "sizes": [16, 24, 32, 48], "steps": nsteps, "dt": 0.1,
-                           "amp": [0.01, 0.1], "k": [0.3, 0.5], "storage": "f32 f, f64 fields"},
+                           "amp": [0.01, 0.1], "k": [0.3, 0.5], "storage": "f32 f, f64 fields",
+                           "ranks": world, "members_this_rank": len(members)},
                 "cells": cells, "ms": t * 1e3, "value": cells * nsteps / t / 1e9, "unit": METRIC,
                 "tiles": {"threads": tiles[0], "cols_per_tile": tiles[1], "ctas_per_sm": tiles[2]},
-                "hbm": {"achieved_gbs": gbs, "frac": gbs / peak, "bytes_per_run": run_bytes},
+                "hbm": {"achieved_gbs": gbs, "frac": gbs / (peak * world), "bytes_per_run": run_bytes},
                 "launches_per_run": 3}
 
 
@@ -665,8 +790,9 @@ def main(argv=None):
         return 0
     ranks = Ranks(world)
     try:
-        line = gpu_arm(args, ranks)
-        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        use_slabs = (world > 1 and not args.replicas) or args.slab
+        line = slab_arm(args, ranks) if use_slabs else gpu_arm(args, ranks)
+        if rank == 0 and world == 1 and not args.no_cpu_baseline and not use_slabs:
             _set_omp_env()
             line["cpu_baseline"] = reference_cpu(args.n, 3, 20.0) or {
                 "value": None, "unit": METRIC, "cores": 0, "kind": "reference", "sample": "oracle/_ref absent"}

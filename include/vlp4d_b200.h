@@ -95,6 +95,46 @@ int vlp4d_read_deck(const char *path, vlp4d_domain *out);
  * (diags.cpp:6-11). */
 int vlp4d_ctx_create(const vlp4d_domain *dom, int dtype, vlp4d_ctx **out);
 int vlp4d_ctx_destroy(vlp4d_ctx *ctx);
+
+/* ---- vy-slab decomposition of one run over several processes (one GPU
+ * each).  Stands in for the reference's domain decomposition of vlp4d_mpi:
+ * Distrib::createDecomposition (miniapps/vlp4d_mpi/thrust/Communication.cpp:10-124),
+ * Distrib::exchangeHalo with its pack/unpack (Communication.cpp:471-562)
+ * and field_reduce's MPI_Allreduce of rho (miniapps/vlp4d_mpi/thrust/Field.cpp:31-40).
+ * Here the run is cut along vy only: a rank owns the global vy planes
+ * [ivy0, ivy0 + nvy_local), and an f buffer of its context holds `halo`
+ * extra planes on each side, nx*ny*nvx*(nvy_local + 2*halo) elements
+ * (vlp4d_f_size), owned planes from plane `halo` on.  Because vy is the
+ * slowest index of layout_left, each side's halo is ONE contiguous block
+ * that the caller's transport (NCCL send/recv) writes in place: no packing.
+ *
+ * On a slab context every entry point that takes f reads and writes the
+ * owned planes of the buffers given, except the vy sweeps
+ * (vlp4d_advect_vy, vlp4d_advect_vxvy), which read the owned AND halo
+ * planes of the input (the caller fills the halos from the neighbouring
+ * ranks' owned planes first) and write the owned planes of the output.
+ * vlp4d_field_rho, vlp4d_advect_xy_moment and vlp4d_advect_xyxy leave in rho
+ * the moment of the owned planes only: the caller sums rho over the ranks
+ * (an all-reduce of nx*ny doubles) before vlp4d_field_poisson, after which
+ * every rank holds the same rho/phi, Ex, Ey and diagnostics.  A vy shift
+ * that needs planes beyond the halo sets an error that vlp4d_check
+ * reports as VLP4D_ERR_RANGE (nothing outside the buffer is read).
+ * vlp4d_step, vlp4d_steps, vlp4d_run, vlp4d_print_fxvx, vlp4d_diags_l2norm,
+ * the reverse mode and the vlp4d_mpi entry points return
+ * VLP4D_ERR_UNSUPPORTED on slab contexts.
+ *
+ * dom is the whole run; halo >= 3 (the least any vy shift needs: a shift
+ * by d cells reads at most floor(|d|) + 3 planes beyond the owned ones, on
+ * the side it comes from) and halo <= nvy_local (halos come from the two
+ * neighbouring ranks only). */
+int vlp4d_ctx_create_slab(const vlp4d_domain *dom, int dtype, int ivy0, int nvy_local, int halo,
+                          vlp4d_ctx **out);
+/* Elements of one f buffer of this context (nx*ny*nvx*nvy for an ordinary
+ * context, nx*ny*nvx*(nvy_local + 2*halo) for a slab); 0 for NULL. */
+size_t vlp4d_f_size(const vlp4d_ctx *ctx);
+/* The slab's first owned global plane, owned plane count and halo width
+ * (0, nvy, 0 for an ordinary context); any pointer may be NULL. */
+int vlp4d_slab_info(const vlp4d_ctx *ctx, int *ivy0, int *nvy_local, int *halo);
 const char *vlp4d_last_error(void);
 int vlp4d_ctx_dtype(const vlp4d_ctx *ctx);
 /* Number of this library's own kernel launches so far in the process
@@ -123,6 +163,11 @@ int vlp4d_advect_vy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void 
  * advect_1D_vy in one pass.  Equal to the 1D sequence up to FP rounding. */
 int vlp4d_advect_xy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream);
 int vlp4d_advect_vxvy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream);
+/* vlp4d_advect_xy followed by field_rho of its result (timestep.hpp:17-31:
+ * advect_1D_x, advect_1D_y, field_rho) in one pass: the moment is summed in
+ * the pass's epilogue into the context's rho (FP64, fixed summation order),
+ * so f is not read a second time. */
+int vlp4d_advect_xy_moment(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream);
 /* Two x/y shifts by dt in one pass followed by the moment of the result
  * into the context's rho: the last x/y half step of one Strang step and the
  * first of the next (timestep.hpp:50-58 then :17-28 with dt/2 each), the

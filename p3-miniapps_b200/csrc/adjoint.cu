@@ -753,6 +753,7 @@ int vlp4d_adjoint_create(vlp4d_ctx *ctx, int nsteps, int every, vlp4d_adjoint **
   if (!out) return fail_msg(VLP4D_ERR_INVALID_ARG, "out is NULL");
   *out = nullptr;
   if (!ctx) return fail_msg(VLP4D_ERR_INVALID_ARG, "ctx is NULL");
+  if (ctx->slab) return fail_msg(VLP4D_ERR_UNSUPPORTED, "adjoint_create: not available on a vy-slab context");
   if (nsteps < 1) return fail_msg(VLP4D_ERR_INVALID_ARG, "nsteps must be at least 1");
   if (every < 1) return fail_msg(VLP4D_ERR_INVALID_ARG, "the checkpoint interval must be at least 1");
   if (every > nsteps) every = nsteps;

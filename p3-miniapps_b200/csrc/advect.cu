@@ -123,6 +123,62 @@ __global__ void k_advect_pair_generic(const T *__restrict__ fn, T *__restrict__ 
   }
 }
 
+// Slab contexts: vy sweep (after the vx sweep when DVX) of the owned planes,
+// one thread per output cell.  Input plane j of the buffer is global plane
+// ivy0 - halo + j; output (owned) plane i reads input planes
+// i + halo + o + q, q = 0..5, o the column's signed vy offset (the global
+// taps (ivy + o + q) mod nvy, which the filled halo makes contiguous).
+template <typename T, bool DVX>
+__global__ void k_vy_slab_generic(const T *__restrict__ fin, T *__restrict__ fout, int nx, int ny, int nvx,
+                                  int nloc, int halo, int nvy_glob, StencilTable tvx, StencilTable tvy,
+                                  int *err) {
+  const long long nxy = (long long)nx * ny;
+  const long long total = nxy * nvx * nloc;
+  const long long ystride = nxy * nvx;
+  const int nin = nloc + 2 * halo;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long ixy = idx % nxy;
+    long long r = idx / nxy;
+    const int ivx = (int)(r % nvx);
+    const int ivy = (int)(r / nvx);
+    int o = tvy.m[ixy];
+    if (o > nvy_glob / 2) o -= nvy_glob;
+    int j = ivy + halo + o;
+    if (j < 0 || j + 5 >= nin) {  // halo too narrow for this column's shift
+      atomicOr(err, kErrSlabHalo);
+      fout[idx] = T(0);
+      continue;
+    }
+    T wy[6], row[6];
+    load_weights(WeightsOf<T>::get(tvy), ixy, wy);
+    T wx[6];
+    int jx0 = ivx;
+    if (DVX) {
+      load_weights(WeightsOf<T>::get(tvx), ixy, wx);
+      jx0 += tvx.m[ixy];
+      if (jx0 >= nvx) jx0 -= nvx;
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q, ++j) {
+      const T *plane = fin + (long long)j * ystride + ixy;
+      if (DVX) {
+        T tap[6];
+        int jx = jx0;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          tap[k] = plane[(long long)jx * nxy];
+          if (++jx == nvx) jx = 0;
+        }
+        row[q] = interp6(wx, tap[0], tap[1], tap[2], tap[3], tap[4], tap[5]);
+      } else {
+        row[q] = plane[(long long)ivx * nxy];
+      }
+    }
+    fout[idx] = interp6(wy, row[0], row[1], row[2], row[3], row[4], row[5]);
+  }
+}
+
 }  // namespace
 
 void free_table(StencilTable &t) {
@@ -178,13 +234,15 @@ int ensure_xy_table(vlp4d_ctx *c, int dim, double dt, StencilTable **out, cudaSt
   t->valid = false;
   const int vdim = dim == 0 ? 2 : 3;
   const int lines = c->g.n[vdim];
+  // Slab contexts hold the vy lines ivy0 .. ivy0 + lines - 1 of the run.
+  const int l0 = vdim == 3 ? c->ivy0 : 0;
   int rc = alloc_table(*t, lines);
   if (rc) return rc;
   std::vector<int> hm(lines);
   std::vector<double> hw(6 * (size_t)lines);
   std::vector<float> hwf(6 * (size_t)lines);
   for (int l = 0; l < lines; ++l) {
-    const double v = c->g.minp[vdim] + l * c->g.dx[vdim];
+    const double v = c->g.minp[vdim] + (l0 + l) * c->g.dx[vdim];
     const double disp = dt * v;
     const LineStencil st = line_stencil(disp, c->g.minp[dim], c->g.maxp[dim], c->g.n[dim]);
     hm[l] = st.m;
@@ -216,13 +274,14 @@ int ensure_xy11_table(vlp4d_ctx *c, int dim, double dt, StencilTable **out, cuda
   t->valid = false;
   const int vdim = dim == 0 ? 2 : 3;
   const int lines = c->g.n[vdim], n = c->g.n[dim];
+  const int l0 = vdim == 3 ? c->ivy0 : 0;  // slab contexts: global vy lines
   int rc = alloc_table(*t, lines, 11);
   if (rc) return rc;
   std::vector<int> hm(lines);
   std::vector<double> hw(11 * (size_t)lines);
   std::vector<float> hwf(11 * (size_t)lines);
   for (int l = 0; l < lines; ++l) {
-    const double v = c->g.minp[vdim] + l * c->g.dx[vdim];
+    const double v = c->g.minp[vdim] + (l0 + l) * c->g.dx[vdim];
     const LineStencil st = line_stencil(dt * v, c->g.minp[dim], c->g.maxp[dim], n);
     // out[i] = sum_k w_k sum_j w_j f[i + m + k + m + j] = sum_q W_q f[i + 2m + q].
     double W[11] = {0.};
@@ -271,7 +330,8 @@ int build_v_tables(vlp4d_ctx *c, double dt, bool vx, bool vy, cudaStream_t s) {
   if (vy) {
     int rc = alloc_table(c->tab_vy, lines);
     if (rc) return rc;
-    jobs[njobs++] = {c->ey, c->g.minp[3], c->g.maxp[3], c->g.n[3], c->tab_vy.m, c->tab_vy.w, c->tab_vy.wf};
+    // The vy geometry of the whole run (slab contexts own part of its planes).
+    jobs[njobs++] = {c->ey, c->g.minp[3], c->g.maxp[3], c->nvy_glob, c->tab_vy.m, c->tab_vy.w, c->tab_vy.wf};
   }
   if (!njobs) return VLP4D_OK;
   k_build_vtable<<<dim3((unsigned)blocks, (unsigned)njobs), threads, 0, s>>>(jobs[0], jobs[njobs - 1], lines, dt);
@@ -320,6 +380,27 @@ int launch_advect_pair_generic(vlp4d_ctx *c, bool v, const void *fn, void *fnp1,
     if (v) k_advect_pair_generic<float, true><<<blocks, threads, 0, s>>>((const float *)fn, (float *)fnp1, n[0], n[1], n[2], n[3], *ta, *tb);
     else k_advect_pair_generic<float, false><<<blocks, threads, 0, s>>>((const float *)fn, (float *)fnp1, n[0], n[1], n[2], n[3], *ta, *tb);
   }
+  VLP4D_LAUNCH_CHECK();
+  return VLP4D_OK;
+}
+
+int launch_vy_slab_generic(vlp4d_ctx *c, const void *fn_ext, void *fnp1_owned, const StencilTable *tvx,
+                           const StencilTable *tvy, cudaStream_t s) {
+  const int threads = 256;
+  const int blocks = grid_for(c->g.cells(), threads, c->num_sms);
+  const int *n = c->g.n;
+  StencilTable tx = tvx ? *tvx : StencilTable{};
+#define VLP4D_VYS(T, DVX)                                                                                 \
+  k_vy_slab_generic<T, DVX><<<blocks, threads, 0, s>>>((const T *)fn_ext, (T *)fnp1_owned, n[0], n[1], n[2], \
+                                                      n[3], c->halo, c->nvy_glob, tx, *tvy, c->d_err)
+  if (c->dtype == VLP4D_F64) {
+    if (tvx) VLP4D_VYS(double, true);
+    else VLP4D_VYS(double, false);
+  } else {
+    if (tvx) VLP4D_VYS(float, true);
+    else VLP4D_VYS(float, false);
+  }
+#undef VLP4D_VYS
   VLP4D_LAUNCH_CHECK();
   return VLP4D_OK;
 }

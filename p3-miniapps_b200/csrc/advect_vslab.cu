@@ -36,7 +36,12 @@ static_assert(8 * kMaxStages + 4 * kMaxStages + 4 <= kBarBytes, "slab header ove
 
 struct VslabArgs {
   void *fout;
-  int nxy, nvx, nvy;
+  int nxy, nvx;
+  int nvy;    // period of the vy offsets (the run's nvy; for slab contexts the global one)
+  // Input rows: row0 < 0, periodic rows (start + t) mod nvy; row0 >= 0 (slab
+  // contexts), rows start + t + row0 of an input of nin planes (the owned
+  // planes and `row0` halo planes on each side), never wrapped.
+  int row0, nin;
   int C;      // columns per chunk
   int Q;      // output vy rows per item (divides nvy)
   int nseg;   // nvy / Q
@@ -112,8 +117,17 @@ template <typename T>
 __device__ __forceinline__ void issue_slab(const CUtensorMap *tin, const VslabArgs &a, const SlabCursor &c,
                                            T *slabs, uint64_t *bars, int slot, size_t slab_elems,
                                            uint32_t slab_bytes) {
-  int row = (c.start + c.t) % a.nvy;
-  if (row < 0) row += a.nvy;
+  int row = c.start + c.t;
+  if (a.row0 < 0) {
+    row %= a.nvy;
+    if (row < 0) row += a.nvy;
+  } else {
+    row += a.row0;
+    if (row < 0 || row >= a.nin) {  // the halo is too narrow for this column's shift
+      atomicOr(a.err, kErrSlabHalo);
+      row = row < 0 ? 0 : a.nin - 1;
+    }
+  }
   mbar_arrive_expect_tx(&bars[slot], slab_bytes);
   tensor_load_3d(slabs + (size_t)slot * slab_elems, tin, c.cc * a.C, 0, row, &bars[slot]);
 }
@@ -449,9 +463,14 @@ int launch_advect_vxvy_tables(vlp4d_ctx *c, const void *fn, void *fnp1, const St
   const size_t elem = c->elem;
   const int nchunks = (int)(nxy / cfg.C);
   if (do_vy && nchunks > c->vspan_cap) return VLP4D_ERR_UNSUPPORTED;
+  // Slab contexts with a vy sweep read the whole input buffer (owned planes
+  // and both halos) and write the owned planes; everything else reads and
+  // writes nvy planes.
+  const bool slab_in = c->slab && do_vy;
+  const int nin = slab_in ? nvy + 2 * c->halo : nvy;
 
   CUtensorMap map;
-  cuuint64_t dims[3] = {(cuuint64_t)nxy, (cuuint64_t)nvx, (cuuint64_t)nvy};
+  cuuint64_t dims[3] = {(cuuint64_t)nxy, (cuuint64_t)nvx, (cuuint64_t)nin};
   cuuint64_t strides[2] = {(cuuint64_t)(nxy * elem), (cuuint64_t)(nxy * nvx * elem)};
   cuuint32_t box[3] = {(cuuint32_t)cfg.C, (cuuint32_t)nvx, 1};
   cuuint32_t estr[3] = {1, 1, 1};
@@ -462,14 +481,16 @@ int launch_advect_vxvy_tables(vlp4d_ctx *c, const void *fn, void *fnp1, const St
   if (r != CUDA_SUCCESS) return VLP4D_ERR_UNSUPPORTED;
 
   if (do_vy) {
-    k_vspan<<<(nchunks + 127) / 128, 128, 0, s>>>(tvy->m, nchunks, cfg.C, nvy, c->vspan);
+    k_vspan<<<(nchunks + 127) / 128, 128, 0, s>>>(tvy->m, nchunks, cfg.C, c->nvy_glob, c->vspan);
     VLP4D_LAUNCH_CHECK();
   }
   VslabArgs a;
   a.fout = fnp1;
   a.nxy = (int)nxy;
   a.nvx = nvx;
-  a.nvy = nvy;
+  a.nvy = slab_in ? c->nvy_glob : nvy;
+  a.row0 = slab_in ? c->halo : -1;
+  a.nin = nin;
   a.C = cfg.C;
   a.Q = cfg.Q;
   a.nseg = nvy / cfg.Q;

@@ -65,6 +65,17 @@ int check_pair(const void *a, const void *b) {
   return VLP4D_OK;
 }
 
+// Entry points that advance or read a whole run on their own (time loops,
+// the reverse mode, the vlp4d_mpi arrays) need every vy plane: slab contexts
+// advance through the stage entry points, with the caller's exchanges
+// between them.
+int reject_slab(const vlp4d_ctx *c, const char *what) {
+  if (c->slab)
+    return fail(VLP4D_ERR_UNSUPPORTED, std::string(what) + ": not available on a vy-slab context (use the stage "
+                                                         "entry points and exchange the halo and rho between ranks)");
+  return VLP4D_OK;
+}
+
 void free_ctx(vlp4d_ctx *c) {
   if (!c) return;
   if (c->plans) {
@@ -160,6 +171,7 @@ int vlp4d_ctx_create(const vlp4d_domain *dom, int dtype, vlp4d_ctx **out) {
     c->g.maxp[i] = dom->max_phy[i];
     c->g.dx[i] = (dom->max_phy[i] - dom->min_phy[i]) / dom->nxmax[i];  // init.cpp:77-79
   }
+  c->nvy_glob = c->g.n[3];
   auto bail = [&](int code) {
     free_ctx(c);
     return code;
@@ -251,6 +263,55 @@ int vlp4d_ctx_create(const vlp4d_domain *dom, int dtype, vlp4d_ctx **out) {
   return VLP4D_OK;
 }
 
+int vlp4d_ctx_create_slab(const vlp4d_domain *dom, int dtype, int ivy0, int nvy_local, int halo, vlp4d_ctx **out) {
+  if (!out) return fail(VLP4D_ERR_INVALID_ARG, "out is NULL");
+  *out = nullptr;
+  int rc = validate_domain(dom);
+  if (rc) return rc;
+  const int nvy = dom->nxmax[3];
+  if (nvy_local < 1 || ivy0 < 0 || (long long)ivy0 + nvy_local > nvy)
+    return fail(VLP4D_ERR_INVALID_ARG, "slab planes [ivy0, ivy0 + nvy_local) must lie in [0, nvy)");
+  // Three halo planes are the least any vy shift needs: a shift by d cells,
+  // |d| < 1, reads the six planes from ivy-3 (d > 0) or ivy-2 (d <= 0) on.
+  // In general a shift by d reads at most floor(|d|) + 3 planes beyond the
+  // owned ones, on the side it comes from.
+  if (halo < 3) return fail(VLP4D_ERR_INVALID_ARG, "halo must be at least 3 planes");
+  if (halo > nvy_local) return fail(VLP4D_ERR_INVALID_ARG, "halo wider than the slab (neighbours' planes only)");
+  if (halo > nvy) return fail(VLP4D_ERR_INVALID_ARG, "halo wider than the run");
+  vlp4d_domain local = *dom;
+  local.nxmax[3] = nvy_local;
+  long long ext = (long long)dom->nxmax[0] * dom->nxmax[1] * dom->nxmax[2] * (nvy_local + 2LL * halo);
+  if (ext > (1LL << 40)) return fail(VLP4D_ERR_INVALID_ARG, "grid too large");
+  vlp4d_ctx *c = nullptr;
+  if ((rc = vlp4d_ctx_create(&local, dtype, &c))) return rc;
+  c->dom = *dom;
+  c->slab = true;
+  c->ivy0 = ivy0;
+  c->halo = halo;
+  c->nvy_glob = nvy;
+  // The vy geometry of the whole run: coordinates and tables of the owned
+  // planes use their global index.
+  c->g.minp[3] = dom->min_phy[3];
+  c->g.maxp[3] = dom->max_phy[3];
+  c->g.dx[3] = (dom->max_phy[3] - dom->min_phy[3]) / nvy;
+  *out = c;
+  return VLP4D_OK;
+}
+
+size_t vlp4d_f_size(const vlp4d_ctx *ctx) {
+  if (!ctx) return 0;
+  return vy_plane_elems(ctx) * (size_t)(ctx->g.n[3] + 2 * ctx->halo);
+}
+
+int vlp4d_slab_info(const vlp4d_ctx *ctx, int *ivy0, int *nvy_local, int *halo) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (ivy0) *ivy0 = ctx->ivy0;
+  if (nvy_local) *nvy_local = ctx->g.n[3];
+  if (halo) *halo = ctx->halo;
+  return VLP4D_OK;
+}
+
 int vlp4d_ctx_destroy(vlp4d_ctx *ctx) {
   if (!ctx) return VLP4D_OK;
   free_ctx(ctx);
@@ -281,15 +342,30 @@ int vlp4d_init_case(vlp4d_ctx *ctx, void *f, int ic, double amp, double k, doubl
     case VLP4D_IC_LANDAU_SUM: case VLP4D_IC_TWO_STREAM: break;
     default: return fail(VLP4D_ERR_INVALID_ARG, "unknown initial condition");  // init.cpp:135-138 aborts
   }
-  return launch_init_case(ctx, f, ic, amp, k, u, as_stream(stream));
+  return launch_init_case(ctx, owned_planes(ctx, f), ic, amp, k, u, as_stream(stream));
 }
 
-static int advect_1d(vlp4d_ctx *ctx, int dim, const void *fn, void *fnp1, double dt, void *stream) {
+static int advect_vxvy_impl(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, cudaStream_t s);
+
+// The vy sweep (after the vx sweep when do_vx) of a slab context: reads the
+// whole input buffer fn_ext (owned planes and filled halos), writes the
+// owned planes of fnp1_owned.
+static int slab_vy(vlp4d_ctx *ctx, const void *fn_ext, void *fnp1_owned, bool do_vx, cudaStream_t s) {
+  int rc = launch_advect_vxvy_tables(ctx, fn_ext, fnp1_owned, do_vx ? &ctx->tab_vx : nullptr, &ctx->tab_vy, s);
+  if (rc != VLP4D_ERR_UNSUPPORTED) return rc;
+  if ((rc = fused_declined(ctx))) return rc;
+  return launch_vy_slab_generic(ctx, fn_ext, fnp1_owned, do_vx ? &ctx->tab_vx : nullptr, &ctx->tab_vy, s);
+}
+
+static int advect_1d(vlp4d_ctx *ctx, int dim, const void *fn_buf, void *fnp1_buf, double dt, void *stream) {
   int rc = check_ctx(ctx);
   if (rc) return rc;
-  if ((rc = check_pair(fn, fnp1))) return rc;
+  if ((rc = check_pair(fn_buf, fnp1_buf))) return rc;
   if (!std::isfinite(dt)) return fail(VLP4D_ERR_INVALID_ARG, "dt is not finite");
   cudaStream_t s = as_stream(stream);
+  // Owned planes of slab buffers (the buffers themselves otherwise).
+  const void *fn = owned_planes(ctx, fn_buf);
+  void *fnp1 = owned_planes(ctx, fnp1_buf);
   StencilTable *t = nullptr;
   if (dim < 2) {
     if ((rc = ensure_xy_table(ctx, dim, dt, &t, s))) return rc;
@@ -300,6 +376,7 @@ static int advect_1d(vlp4d_ctx *ctx, int dim, const void *fn, void *fnp1, double
     return launch_advect_generic(ctx, dim, fn, fnp1, t, s);
   }
   if ((rc = build_v_tables(ctx, dt, dim == 2, dim == 3, s))) return rc;
+  if (dim == 3 && ctx->slab) return slab_vy(ctx, fn_buf, fnp1, false, s);
   rc = launch_advect_vxvy(ctx, fn, fnp1, dim == 2, dim == 3, s);
   if (rc != VLP4D_ERR_UNSUPPORTED) return rc;
   if ((rc = fused_declined(ctx))) return rc;
@@ -331,9 +408,11 @@ static int advect_xy_impl(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt,
   return with_rho ? launch_field_rho(ctx, fnp1, s) : VLP4D_OK;
 }
 
+// Slab contexts: fn is the whole input buffer, fnp1 the owned output planes.
 static int advect_vxvy_impl(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, cudaStream_t s) {
   int rc;
   if ((rc = build_v_tables(ctx, dt, true, true, s))) return rc;
+  if (ctx->slab) return slab_vy(ctx, fn, fnp1, true, s);
   rc = launch_advect_vxvy(ctx, fn, fnp1, true, true, s);
   if (rc != VLP4D_ERR_UNSUPPORTED) return rc;
   if ((rc = fused_declined(ctx))) return rc;
@@ -345,7 +424,15 @@ int vlp4d_advect_xy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void 
   if (rc) return rc;
   if ((rc = check_pair(fn, fnp1))) return rc;
   if (!std::isfinite(dt)) return fail(VLP4D_ERR_INVALID_ARG, "dt is not finite");
-  return advect_xy_impl(ctx, fn, fnp1, dt, false, as_stream(stream));
+  return advect_xy_impl(ctx, owned_planes(ctx, fn), owned_planes(ctx, fnp1), dt, false, as_stream(stream));
+}
+
+int vlp4d_advect_xy_moment(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if ((rc = check_pair(fn, fnp1))) return rc;
+  if (!std::isfinite(dt)) return fail(VLP4D_ERR_INVALID_ARG, "dt is not finite");
+  return advect_xy_impl(ctx, owned_planes(ctx, fn), owned_planes(ctx, fnp1), dt, true, as_stream(stream));
 }
 
 int vlp4d_advect_xyxy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, void *stream) {
@@ -357,7 +444,7 @@ int vlp4d_advect_xyxy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, voi
   StencilTable *tx = nullptr, *ty = nullptr;
   if ((rc = ensure_xy_table(ctx, 0, dt, &tx, s))) return rc;
   if ((rc = ensure_xy_table(ctx, 1, dt, &ty, s))) return rc;
-  rc = launch_advect_xyxy(ctx, fn, fnp1, tx, ty, s);
+  rc = launch_advect_xyxy(ctx, owned_planes(ctx, fn), owned_planes(ctx, fnp1), tx, ty, s);
   if (rc == VLP4D_ERR_UNSUPPORTED)
     return fail(rc, "advect_xyxy: the one-pass kernel does not fit this shape, these buffers or VLP4D_KERNELS; "
                     "call vlp4d_advect_xy twice");
@@ -369,14 +456,15 @@ int vlp4d_advect_vxvy(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, voi
   if (rc) return rc;
   if ((rc = check_pair(fn, fnp1))) return rc;
   if (!std::isfinite(dt)) return fail(VLP4D_ERR_INVALID_ARG, "dt is not finite");
-  return advect_vxvy_impl(ctx, fn, fnp1, dt, as_stream(stream));
+  // Slab contexts: the whole input buffer (halos filled), the owned output planes.
+  return advect_vxvy_impl(ctx, fn, owned_planes(ctx, fnp1), dt, as_stream(stream));
 }
 
 int vlp4d_field_rho(vlp4d_ctx *ctx, const void *fn, void *stream) {
   int rc = check_ctx(ctx);
   if (rc) return rc;
   if (!fn) return fail(VLP4D_ERR_INVALID_ARG, "fn is NULL");
-  return launch_field_rho(ctx, fn, as_stream(stream));
+  return launch_field_rho(ctx, owned_planes(ctx, fn), as_stream(stream));
 }
 
 int vlp4d_field_poisson(vlp4d_ctx *ctx, void *stream) {
@@ -401,7 +489,9 @@ int vlp4d_check(vlp4d_ctx *ctx) {
   VLP4D_CUDA_TRY(cudaMemcpy(&flag, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (flag) {
     VLP4D_CUDA_TRY(cudaMemset(ctx->d_err, 0, sizeof(int)));
-    if (flag & 1) return fail(VLP4D_ERR_TIMEOUT, "an asynchronous copy did not complete within its time limit");
+    if (flag & kErrTimeout) return fail(VLP4D_ERR_TIMEOUT, "an asynchronous copy did not complete within its time limit");
+    if (flag & kErrSlabHalo)
+      return fail(VLP4D_ERR_RANGE, "a vy shift needed planes beyond the slab's halo (create the slab with a wider halo)");
     return fail(VLP4D_ERR_RANGE, "a foot left the interpolation range (the reference stops: time step is too large)");
   }
   return VLP4D_OK;
@@ -422,6 +512,7 @@ int vlp4d_diags_l2norm(vlp4d_ctx *ctx, const void *fn, int iter, void *stream) {
   if (rc) return rc;
   if (!fn) return fail(VLP4D_ERR_INVALID_ARG, "fn is NULL");
   if (iter < 0 || iter >= ctx->hist_len) return fail(VLP4D_ERR_INVALID_ARG, "iter outside [0, nbiter]");
+  if ((rc = reject_slab(ctx, "diags_l2norm"))) return rc;
   return launch_l2norm(ctx, fn, iter, as_stream(stream));
 }
 
@@ -520,6 +611,7 @@ int vlp4d_step(vlp4d_ctx *ctx, void *f_state, void *f_next, int iter, void *stre
   if (rc) return rc;
   if ((rc = check_pair(f_state, f_next))) return rc;
   if (iter < 0 || iter >= ctx->hist_len) return fail(VLP4D_ERR_INVALID_ARG, "iter outside [0, nbiter]");
+  if ((rc = reject_slab(ctx, "step"))) return rc;
   return step_impl(ctx, f_state, f_next, f_state, iter, as_stream(stream));
 }
 
@@ -532,6 +624,7 @@ int vlp4d_steps(vlp4d_ctx *ctx, void *f_state, void *f_next, int iter0, int nste
   if (nsteps < 1) return fail(VLP4D_ERR_INVALID_ARG, "nsteps must be at least 1");
   if (iter0 < 0 || (long long)iter0 + nsteps - 1 >= ctx->hist_len)
     return fail(VLP4D_ERR_INVALID_ARG, "iterations outside [0, nbiter]");
+  if ((rc = reject_slab(ctx, "steps"))) return rc;
   cudaStream_t s = as_stream(stream);
   const double dt = ctx->dom.dt;
   StencilTable *tx = nullptr, *ty = nullptr;
@@ -580,6 +673,7 @@ int vlp4d_run(vlp4d_ctx *ctx, const void *f0_host, void *f_out_host, int nsteps,
   if ((rc = check_pair(fn, fnp1))) return rc;
   if (!f0_host) return fail(VLP4D_ERR_INVALID_ARG, "f0_host is NULL");
   if (nsteps < 0 || nsteps >= ctx->hist_len) return fail(VLP4D_ERR_INVALID_ARG, "nsteps outside [0, nbiter]");
+  if ((rc = reject_slab(ctx, "run"))) return rc;
   cudaStream_t s = as_stream(stream);
   const size_t bytes = (size_t)ctx->g.cells() * ctx->elem;
   VLP4D_CUDA_TRY(cudaMemcpyAsync(fn, f0_host, bytes, cudaMemcpyHostToDevice, s));
@@ -612,6 +706,7 @@ int vlp4d_print_fxvx(vlp4d_ctx *ctx, const void *fn, const char *path) {
   int rc = check_ctx(ctx);
   if (rc) return rc;
   if (!fn || !path) return fail(VLP4D_ERR_INVALID_ARG, "NULL argument");
+  if ((rc = reject_slab(ctx, "print_fxvx"))) return rc;
   const int nx = ctx->g.n[0], nvx = ctx->g.n[2];
   const int ivy = ctx->g.n[3] / 2;  // advection.hpp:394-395
   const size_t e = ctx->elem;

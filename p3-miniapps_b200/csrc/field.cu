@@ -224,7 +224,7 @@ __global__ void k_l2_finish(const double *__restrict__ part, int blocks, double 
 
 // ---- initcase.
 template <typename T>
-__global__ void k_init_case(T *__restrict__ f, Grid g, int ic, double amp, double k, double u) {
+__global__ void k_init_case(T *__restrict__ f, Grid g, int ivy0, int ic, double amp, double k, double u) {
   const long long total = g.cells();
   const double PI = 3.14159265358979323846;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
@@ -238,7 +238,7 @@ __global__ void k_init_case(T *__restrict__ f, Grid g, int ic, double amp, doubl
     const double x = g.minp[0] + ix * g.dx[0];
     const double y = g.minp[1] + iy * g.dx[1];
     const double vx = g.minp[2] + ivx * g.dx[2];
-    const double vy = g.minp[3] + ivy * g.dx[3];
+    const double vy = g.minp[3] + (ivy0 + ivy) * g.dx[3];  // ivy0: first owned plane of a slab
     double val = 0.;
     if (ic == VLP4D_IC_SLD10) {  // init.cpp:234-256
       val = (1. / (2 * PI)) * exp(-0.5 * (vx * vx + vy * vy)) * (1 + 0.05 * (cos(0.5 * x) * cos(0.5 * y)));
@@ -368,9 +368,9 @@ int launch_init_case(vlp4d_ctx *c, void *f, int ic, double amp, double k, double
   long long blocks = (c->g.cells() + threads - 1) / threads;
   if (blocks > (long long)c->num_sms * 32) blocks = (long long)c->num_sms * 32;
   if (c->dtype == VLP4D_F64)
-    k_init_case<double><<<(unsigned)blocks, threads, 0, s>>>((double *)f, c->g, ic, amp, k, u);
+    k_init_case<double><<<(unsigned)blocks, threads, 0, s>>>((double *)f, c->g, c->ivy0, ic, amp, k, u);
   else
-    k_init_case<float><<<(unsigned)blocks, threads, 0, s>>>((float *)f, c->g, ic, amp, k, u);
+    k_init_case<float><<<(unsigned)blocks, threads, 0, s>>>((float *)f, c->g, c->ivy0, ic, amp, k, u);
   VLP4D_LAUNCH_CHECK();
   return VLP4D_OK;
 }

@@ -143,9 +143,35 @@ struct vlp4d_ctx {
   // pass (mpi.cu), mpi_part_cap pairs.
   double *mpi_part = nullptr;
   int mpi_part_cap = 0;
+
+  // vy-slab contexts (vlp4d_ctx_create_slab): this context owns the global
+  // vy planes [ivy0, ivy0 + g.n[3]) of a run with nvy_glob planes.  g holds
+  // the local extents (g.n[3] = owned planes) with the GLOBAL vy geometry
+  // (minp/maxp/dx[3]), so tables and coordinates use global indices.  An f
+  // buffer of a slab context holds `halo` planes on each side of the owned
+  // ones: nx*ny*nvx*(g.n[3] + 2*halo) elements, owned planes from plane
+  // `halo` on.  For ordinary contexts slab = false, ivy0 = halo = 0 and
+  // nvy_glob = g.n[3].
+  bool slab = false;
+  int ivy0 = 0, halo = 0, nvy_glob = 0;
 };
 
 namespace vlp4d {
+
+// Error-word bits (vlp4d_check): a bounded wait ran out; a vlp4d_mpi foot
+// left its interpolation range; a slab's vy sweep needed planes beyond its
+// halo.
+constexpr int kErrTimeout = 1, kErrMpiRange = 2, kErrSlabHalo = 4;
+
+// Planes of one (ivx, ivy) plane times nvx: elements between consecutive ivy.
+inline size_t vy_plane_elems(const vlp4d_ctx *c) { return (size_t)c->g.nxy() * c->g.n[2]; }
+// The owned planes of an f buffer (the buffer itself for ordinary contexts).
+inline const void *owned_planes(const vlp4d_ctx *c, const void *f) {
+  return static_cast<const char *>(f) + (size_t)c->halo * vy_plane_elems(c) * c->elem;
+}
+inline void *owned_planes(const vlp4d_ctx *c, void *f) {
+  return static_cast<char *>(f) + (size_t)c->halo * vy_plane_elems(c) * c->elem;
+}
 
 // advect.cu
 int alloc_table(StencilTable &t, int lines, int taps = 6);
@@ -159,6 +185,12 @@ int launch_advect_generic(vlp4d_ctx *c, int dim, const void *fn, void *fnp1, con
                           cudaStream_t s);
 int launch_advect_pair_generic(vlp4d_ctx *c, bool v, const void *fn, void *fnp1, const StencilTable *ta,
                                const StencilTable *tb, cudaStream_t s);
+// Slab contexts: the vy sweep (with the vx sweep first when tvx is given) of
+// the owned planes from an input buffer whose halo planes are filled; one
+// thread per output cell, any shape.  fn_ext is the whole input buffer,
+// fnp1_owned the owned planes of the output.
+int launch_vy_slab_generic(vlp4d_ctx *c, const void *fn_ext, void *fnp1_owned, const StencilTable *tvx,
+                           const StencilTable *tvy, cudaStream_t s);
 // advect_plane.cu / advect_vslab.cu: VLP4D_ERR_UNSUPPORTED (nothing
 // launched) when the shape or buffers do not fit; callers then use the
 // generic kernels.
@@ -194,6 +226,7 @@ int launch_rho_finish(vlp4d_ctx *c, int groups, cudaStream_t s);
 int launch_field_poisson(vlp4d_ctx *c, cudaStream_t s);
 int launch_diags(vlp4d_ctx *c, int iter, cudaStream_t s);
 int launch_l2norm(vlp4d_ctx *c, const void *fn, int iter, cudaStream_t s);
+// f: the owned planes (slab contexts use the global vy index ivy0 + ivy).
 int launch_init_case(vlp4d_ctx *c, void *f, int ic, double amp, double k, double u, cudaStream_t s);
 int launch_transpose(const void *in, void *out, int rows, int cols, int elem, cudaStream_t s);
 int launch_wait_selftest(vlp4d_ctx *c, long long limit, cudaStream_t s);

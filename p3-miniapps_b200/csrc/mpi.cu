@@ -1030,6 +1030,8 @@ namespace {
 
 int mpi_check(const vlp4d_ctx *c, const char *what) {
   if (!c) return fail_msg(VLP4D_ERR_INVALID_ARG, std::string(what) + ": context is NULL");
+  if (c->slab)
+    return fail_msg(VLP4D_ERR_UNSUPPORTED, std::string(what) + ": the vlp4d_mpi arrays need an ordinary context");
   if (c->dtype != VLP4D_F64)
     return fail_msg(VLP4D_ERR_UNSUPPORTED, std::string(what) + ": the vlp4d_mpi path is FP64 (as the reference)");
   for (int k = 0; k < 4; ++k)

@@ -40,6 +40,7 @@ EXPORTS = (
     "vlp4d_ensemble_autotune", "vlp4d_selftest_wait_timeout", "vlp4d_diags_l2norm", "vlp4d_diags_read_ext",
     "vlp4d_mpi_size", "vlp4d_mpi_init_case", "vlp4d_mpi_halo_fill", "vlp4d_mpi_spline_xy", "vlp4d_mpi_spline_vxvy", "vlp4d_mpi_advect_2d",
     "vlp4d_mpi_advect_4d", "vlp4d_mpi_field", "vlp4d_mpi_l2norm", "vlp4d_mpi_step",
+    "vlp4d_ctx_create_slab", "vlp4d_f_size", "vlp4d_slab_info", "vlp4d_advect_xy_moment",
 )
 HALO = 3  # HALO_PTS of the vlp4d_mpi halo-extended arrays
 
@@ -98,8 +99,11 @@ def lib() -> C.CDLL:
         L.vlp4d_ctx_dtype.argtypes = [vp]
         L.vlp4d_field_ptr.argtypes = [vp, i, C.POINTER(vp)]
         L.vlp4d_init_case.argtypes = [vp, vp, i, d, d, d, vp]
+        L.vlp4d_ctx_create_slab.argtypes = [C.POINTER(CDomain), i, i, i, i, C.POINTER(vp)]
+        L.vlp4d_f_size.argtypes = [vp]
+        L.vlp4d_slab_info.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
         for n in ("vlp4d_advect_x", "vlp4d_advect_y", "vlp4d_advect_vx", "vlp4d_advect_vy", "vlp4d_advect_xy",
-                  "vlp4d_advect_vxvy", "vlp4d_advect_xyxy"):
+                  "vlp4d_advect_vxvy", "vlp4d_advect_xyxy", "vlp4d_advect_xy_moment"):
             getattr(L, n).argtypes = [vp, vp, vp, d, vp]
         L.vlp4d_field_rho.argtypes = [vp, vp, vp]
         L.vlp4d_field_poisson.argtypes = [vp, vp]
@@ -141,9 +145,11 @@ def lib() -> C.CDLL:
         L.vlp4d_mpi_l2norm.argtypes = [vp, vp, i, vp]
         L.vlp4d_mpi_step.argtypes = [vp, vp, vp, i, vp]
         for n in EXPORTS:
-            if n not in ("vlp4d_last_error", "vlp4d_kernel_launches", "vlp4d_ensemble_cells", "vlp4d_mpi_size"):
+            if n not in ("vlp4d_last_error", "vlp4d_kernel_launches", "vlp4d_ensemble_cells", "vlp4d_mpi_size",
+                         "vlp4d_f_size"):
                 getattr(L, n).restype = C.c_int
         L.vlp4d_mpi_size.restype = C.c_size_t
+        L.vlp4d_f_size.restype = C.c_size_t
         L.vlp4d_ensemble_cells.restype = C.c_longlong
         L.vlp4d_kernel_launches.restype = C.c_ulonglong
         _lib = L
@@ -231,9 +237,14 @@ def _stream_ptr(stream) -> Optional[int]:
 
 
 class Context:
-    """A vlp4d_ctx: the Efield + Diags state of one run on the current device."""
+    """A vlp4d_ctx: the Efield + Diags state of one run on the current device.
 
-    def __init__(self, dom: Domain, dtype: str = "f64"):
+    slab=(ivy0, nvy_local, halo) makes a vy-slab context of the run `dom`
+    (vlp4d_ctx_create_slab): it owns the global vy planes
+    [ivy0, ivy0 + nvy_local), and its f buffers (empty_f) hold `halo` more
+    planes on each side, shape (nvy_local + 2*halo, nvx, ny, nx)."""
+
+    def __init__(self, dom: Domain, dtype: str = "f64", slab=None):
         import torch
 
         self.dom = dom
@@ -241,8 +252,22 @@ class Context:
         self.torch_dtype = torch.float64 if self.dtype_code == F64 else torch.float32
         self._c = dom.to_c()
         h = C.c_void_p()
-        _check(lib().vlp4d_ctx_create(C.byref(self._c), self.dtype_code, C.byref(h)))
+        if slab is None:
+            _check(lib().vlp4d_ctx_create(C.byref(self._c), self.dtype_code, C.byref(h)))
+            self.ivy0, self.nvy_local, self.halo = 0, dom.nxmax[3], 0
+        else:
+            ivy0, nloc, halo = (int(v) for v in slab)
+            _check(lib().vlp4d_ctx_create_slab(C.byref(self._c), self.dtype_code, ivy0, nloc, halo, C.byref(h)))
+            self.ivy0, self.nvy_local, self.halo = ivy0, nloc, halo
         self.h = h
+        self.is_slab = slab is not None
+        nx, ny, nvx, _ = dom.nxmax
+        self.f_shape = (self.nvy_local + 2 * self.halo, nvx, ny, nx)
+        self.f_size = int(lib().vlp4d_f_size(self.h))
+
+    def owned(self, f):
+        """View of the owned planes of an f buffer of this context."""
+        return f[self.halo:self.halo + self.nvy_local]
 
     def close(self):
         if getattr(self, "h", None):
@@ -265,13 +290,11 @@ class Context:
     def empty_f(self):
         import torch
 
-        return torch.empty(self.dom.shape4, dtype=self.torch_dtype, device="cuda")
+        return torch.empty(self.f_shape, dtype=self.torch_dtype, device="cuda")
 
     def _f(self, t):
-        import torch
-
-        if not (t.is_cuda and t.dtype == self.torch_dtype and t.is_contiguous() and t.numel() == self.dom.cells):
-            raise ValueError(f"f must be a contiguous CUDA {self.torch_dtype} tensor of {self.dom.cells} elements")
+        if not (t.is_cuda and t.dtype == self.torch_dtype and t.is_contiguous() and t.numel() == self.f_size):
+            raise ValueError(f"f must be a contiguous CUDA {self.torch_dtype} tensor of {self.f_size} elements")
         return C.c_void_p(t.data_ptr())
 
     def field(self, which: int):
@@ -308,6 +331,9 @@ class Context:
     def advect_xyxy(self, fn, fnp1, dt, stream=None):
         """Two x/y shifts by dt in one pass, then the moment of fnp1 into rho."""
         _check(lib().vlp4d_advect_xyxy(self.h, self._f(fn), self._f(fnp1), dt, _stream_ptr(stream)))
+
+    def advect_xy_moment(self, fn, fnp1, dt, stream=None):
+        _check(lib().vlp4d_advect_xy_moment(self.h, self._f(fn), self._f(fnp1), dt, _stream_ptr(stream)))
 
     def advect_vxvy(self, fn, fnp1, dt, stream=None):
         _check(lib().vlp4d_advect_vxvy(self.h, self._f(fn), self._f(fnp1), dt, _stream_ptr(stream)))
