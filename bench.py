@@ -503,6 +503,40 @@ def error_arm(pkg, torch, n, nsteps=ERROR_STEPS):
            "f_maxabs": df, "f_max": final["f64"].abs().max().item()}
     del final
     torch.cuda.empty_cache()
+    out["two_stream"] = two_stream_error(pkg, torch)
+    return out
+
+
+def two_stream_error(pkg, torch, nsteps=400):
+    """The two-stream configuration (64 x 64 x 128 x 128, x, y in
+    [0, 10 pi), v in [-8, 8), dt 0.05, 400 steps, f0 = (1 + 0.001 cos 0.2x +
+    0.001 cos 0.2y) 1/2 [M(vx - 2.4) + M(vx + 2.4)] M(vy)): FP32 f against
+    FP64 f over the whole run, vlp4d_steps in both, untimed."""
+    import numpy as np
+
+    v = pkg.vlp4d
+    L = 10 * math.pi
+    dom = pkg.Domain([64, 64, 128, 128], [0.0, 0.0, -8.0, -8.0], [L, L, 8.0, 8.0], 0.05, nsteps, 120)
+    hist, final = {}, {}
+    for dtype in ("f64", "f32"):
+        with pkg.Context(dom, dtype) as ctx:
+            fa, fb = ctx.empty_f(), ctx.empty_f()
+            ctx.init_case(fa, v.IC_TWO_STREAM, 0.001, 0.2, 2.4)
+            ctx.field_rho(fa)
+            ctx.field_poisson()
+            ctx.diags_compute(0)
+            ctx.steps(fa, fb, 1, nsteps)
+            hist[dtype] = ctx.diags_read(nsteps + 1)[0]
+            final[dtype] = fb.double()
+            del fa, fb
+    w32, w64 = np.exp(2 * hist["f32"]), np.exp(2 * hist["f64"])
+    rel = np.abs(w32 - w64) / w64
+    out = {"grid": [64, 64, 128, 128], "steps": nsteps, "dt": 0.05,
+           "energy_rel_max": float(rel.max()), "energy_rel_final": float(rel[-1]),
+           "energy_growth": float(w64[-1] / w64[0]),
+           "f_maxabs_over_fmax": float((final["f32"] - final["f64"]).abs().max() / final["f64"].abs().max())}
+    del final
+    torch.cuda.empty_cache()
     return out
 
 

@@ -358,6 +358,12 @@ long long vlp4d_ensemble_cells(const vlp4d_ensemble *ens);
 int vlp4d_ensemble_set_tiles(vlp4d_ensemble *ens, int threads, int cols_per_tile, int ctas_per_sm);
 int vlp4d_ensemble_get_tiles(const vlp4d_ensemble *ens, int *threads, int *cols_per_tile, int *ctas_per_sm);
 int vlp4d_ensemble_autotune(vlp4d_ensemble *ens, int steps, const char *csv_path, void *stream);
+/* How long (clock cycles) a CTA of the persistent kernel looks for a free
+ * tile in vain before it flags VLP4D_ERR_TIMEOUT (vlp4d_ensemble_check)
+ * and leaves; 0 restores the default and maximum, 4e9 (about two seconds).
+ * The CTAs that keep finding work finish the run, so its results stay
+ * valid; the flag says that some CTA gave up.  No reference counterpart. */
+int vlp4d_ensemble_set_idle_limit(vlp4d_ensemble *ens, long long cycles);
 
 /* ---- vlp4d_mpi, one process (miniapps/vlp4d_mpi, cubic-spline scheme).
  *

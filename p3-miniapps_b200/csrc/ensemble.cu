@@ -63,6 +63,10 @@ struct EnsRun {
   long long d_off;  // diagnostic history: nsteps + 1 doubles
 };
 
+// Default and largest idle limit of a CTA of k_ensemble: about two seconds
+// at 1.9 GHz.
+constexpr long long kEnsIdleLimit = 4000000000LL;
+
 struct EnsArgs {
   const EnsRun *runs;
   int nruns, nsteps;
@@ -964,6 +968,9 @@ struct vlp4d_ensemble {
   // Tile configuration (vlp4d_ensemble_set_tiles / _autotune).
   int threads = 256, cc = 32, ctas_per_sm = 0;  // 0: as many as fit
   size_t smem = 0;
+  // Cycles a CTA may look for work in vain before it flags a timeout and
+  // leaves (vlp4d_ensemble_set_idle_limit).
+  long long idle_limit = vlp4d::kEnsIdleLimit;
   cudaGraphExec_t graph = nullptr;
 };
 
@@ -993,7 +1000,7 @@ EnsArgs ens_args(vlp4d_ensemble *E, int nsteps) {
   a.err = E->err;
   a.cc = E->cc;
   a.maxnxy = E->maxnxy;
-  a.idle_limit = 4000000000LL;  // about two seconds at 1.9 GHz
+  a.idle_limit = E->idle_limit;
   return a;
 }
 
@@ -1164,6 +1171,18 @@ int vlp4d_ensemble_set_tiles(vlp4d_ensemble *ens, int threads, int cols_per_tile
   ens->cc = cols_per_tile;
   ens->ctas_per_sm = ctas_per_sm;
   if (ens->graph) {
+    cudaGraphExecDestroy(ens->graph);
+    ens->graph = nullptr;
+  }
+  return VLP4D_OK;
+}
+
+int vlp4d_ensemble_set_idle_limit(vlp4d_ensemble *ens, long long cycles) {
+  if (!ens) return fail_msg(VLP4D_ERR_INVALID_ARG, "ens is NULL");
+  if (cycles < 0 || cycles > kEnsIdleLimit)
+    return fail_msg(VLP4D_ERR_INVALID_ARG, "idle limit: 0 (default) or 1 .. 4e9 cycles");
+  ens->idle_limit = cycles ? cycles : kEnsIdleLimit;
+  if (ens->graph) {  // the graph holds the kernel's arguments: capture again
     cudaGraphExecDestroy(ens->graph);
     ens->graph = nullptr;
   }

@@ -41,6 +41,7 @@ EXPORTS = (
     "vlp4d_mpi_size", "vlp4d_mpi_init_case", "vlp4d_mpi_halo_fill", "vlp4d_mpi_spline_xy", "vlp4d_mpi_spline_vxvy", "vlp4d_mpi_advect_2d",
     "vlp4d_mpi_advect_4d", "vlp4d_mpi_field", "vlp4d_mpi_l2norm", "vlp4d_mpi_step",
     "vlp4d_ctx_create_slab", "vlp4d_f_size", "vlp4d_slab_info", "vlp4d_advect_xy_moment",
+    "vlp4d_ensemble_set_idle_limit",
 )
 HALO = 3  # HALO_PTS of the vlp4d_mpi halo-extended arrays
 
@@ -133,6 +134,7 @@ def lib() -> C.CDLL:
         L.vlp4d_ensemble_set_tiles.argtypes = [vp, i, i, i]
         L.vlp4d_ensemble_get_tiles.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
         L.vlp4d_ensemble_autotune.argtypes = [vp, i, C.c_char_p, vp]
+        L.vlp4d_ensemble_set_idle_limit.argtypes = [vp, C.c_longlong]
         L.vlp4d_selftest_wait_timeout.argtypes = [vp, C.c_longlong, vp]
         L.vlp4d_diags_l2norm.argtypes = [vp, vp, i, vp]
         L.vlp4d_diags_read_ext.argtypes = [vp, dp, dp, dp, i]
@@ -632,6 +634,10 @@ class Ensemble:
         _check(lib().vlp4d_ensemble_read(self.h, int(i), C.c_void_p(f.data_ptr()),
                                          nrj.ctypes.data_as(C.POINTER(C.c_double)), _stream_ptr(stream)))
         return f, nrj
+
+    def set_idle_limit(self, cycles: int):
+        """Cycles a CTA may find no free tile before it flags a timeout (0: default)."""
+        _check(lib().vlp4d_ensemble_set_idle_limit(self.h, int(cycles)))
 
     def set_tiles(self, threads: int, cols_per_tile: int, ctas_per_sm: int = 0):
         _check(lib().vlp4d_ensemble_set_tiles(self.h, threads, cols_per_tile, ctas_per_sm))

@@ -106,3 +106,36 @@ def test_batched_ensemble_configuration(pkg, cuda):
             f_ref, nrj_ref = _single_run(pkg, torch, members[int(i)], nsteps)
             assert float((f - f_ref).abs().max()) <= 1e-5 * float(f_ref.abs().max())
             assert np.abs(nrj - nrj_ref).max() < 1e-5
+
+
+def test_idle_limit_runs_out_then_ensemble_recovers(pkg, cuda):
+    """The persistent kernel's wait for work, made to run out: with a limit
+    of one cycle, every CTA that finds no free tile on its first look flags
+    the timeout and leaves (there is always such a CTA: at the end, while
+    the last member finishes).  The CTAs that kept finding work complete the
+    run, vlp4d_ensemble_check reports VLP4D_ERR_TIMEOUT, and a run with the
+    default limit then gives results bit-identical to a fresh ensemble's."""
+    torch = cuda
+    members = _members(pkg, DIMS[:4])
+    nsteps = 3
+    with pkg.Ensemble(members, nsteps) as ens:
+        ens.set_idle_limit(1)
+        ens.run()
+        with pytest.raises(pkg.vlp4d.Vlp4dError) as e:
+            ens.check()
+        assert e.value.code == pkg.vlp4d.ERR_TIMEOUT
+        ens.set_idle_limit(0)
+        ens.run()
+        ens.check()
+        after = [ens.read(i) for i in range(len(members))]
+    with pkg.Ensemble(members, nsteps) as fresh:
+        fresh.run()
+        fresh.check()
+        for i in range(len(members)):
+            f, nrj = fresh.read(i)
+            assert torch.equal(f, after[i][0])
+            assert np.array_equal(nrj, after[i][1])
+    with pkg.Ensemble(members, nsteps) as ens:
+        for bad in (-1, 4_000_000_001):
+            with pytest.raises(pkg.vlp4d.Vlp4dError):
+                ens.set_idle_limit(bad)
