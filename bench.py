@@ -49,6 +49,8 @@ def parse_args(argv=None):
     ap.add_argument("--n", type=int, default=N_GRID, help="cells per dimension (default 128)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end runs")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip timing the reference CPU build")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own CUDA build (baseline/_ref) on this GPU")
     ap.add_argument("--only-f32", action="store_true", help="FP32 storage only (no FP64 run, no e2e): profiling")
     ap.add_argument("--case", choices=["main", "adjoint", "ensemble", "mpi"], default="main",
                     help="profiling cases: the reverse-mode, the ensemble or the vlp4d_mpi arm alone "
@@ -772,6 +774,69 @@ def reference_cpu(n, max_steps, budget_s):
                       f"reference OpenMP build miniapps/vlp4d/openmp, FP64, OMP_NUM_THREADS={threads}"}
 
 
+REF_DECK = """grid points along x : {n}
+grid points along y : {n}
+grid points along vx : {n}
+grid points along vy : {n}
+lower bound of x : 0.
+upper bound of x : {L!r}
+lower bound of y : 0.
+upper bound of y : {L!r}
+lower bound of vx : {vmin!r}
+upper bound of vx : {vmax!r}
+lower bound of vy : {vmin!r}
+upper bound of vy : {vmax!r}
+test case : 10
+time step : {dt!r}
+number of steps : {steps}
+diagnostic frequency : 1
+write fxvx slices : 0
+"""
+
+
+def reference_gpu(n, steps, timeout_s=240):
+    """The reference's own CUDA variant (miniapps/vlp4d/thrust, built for
+    sm_100a by baseline/Makefile) on this GPU: its main() on an n^4 deck of
+    the benchmark geometry (x, y in [0, 4 pi), v in [-6, 6), dt 0.1, its
+    SLD10 initial condition, `steps` steps, FP64).  Throughput from its own
+    MainLoop timer (host clock around each onetimestep, which synchronises
+    after every stage), as the reference measures itself; its stage timers
+    as ms per call."""
+    import tempfile
+
+    exe = ROOT / "baseline" / "_ref" / "vlp4d_ref_cuda"
+    if not exe.exists():
+        return {"unavailable": "baseline/_ref/vlp4d_ref_cuda (the reference's CUDA build) is absent"}
+    with tempfile.TemporaryDirectory() as tmp:
+        deck = Path(tmp) / "landau.dat"
+        deck.write_text(REF_DECK.format(n=n, L=L_BOX, vmin=-VMAX, vmax=VMAX, dt=DT, steps=steps))
+        try:
+            out = subprocess.run([str(exe), str(deck)], cwd=tmp, capture_output=True, text=True, timeout=timeout_s)
+        except subprocess.TimeoutExpired:
+            return {"unavailable": f"the reference's CUDA build did not finish {steps} steps within {timeout_s} s"}
+        if out.returncode != 0:
+            return {"unavailable": f"the reference's CUDA build exited with {out.returncode}: {out.stderr[-300:]}"}
+        timers = {}
+        for line in out.stdout.splitlines():
+            parts = line.split()
+            if len(parts) >= 5 and parts[2] == "[s]," and parts[4] == "calls":
+                timers[parts[0]] = (float(parts[1]), int(parts[3]))
+        nrj = []
+        nrj_path = Path(tmp) / "nrj.out"
+        if nrj_path.exists():
+            nrj = [float(l.split()[1]) for l in nrj_path.read_text().splitlines() if l.strip()]
+    if "MainLoop" not in timers or timers["MainLoop"][1] == 0:
+        return {"unavailable": "the reference's CUDA build printed no MainLoop timer"}
+    secs, calls = timers["MainLoop"]
+    return {"value": n ** 4 * calls / secs / 1e9, "unit": METRIC, "ms_per_step": secs * 1e3 / calls,
+            "steps": calls, "dtype": "f64",
+            "kind": "reference CUDA variant miniapps/vlp4d/thrust (ENABLE_CUDA, Impl::for_each kernels, "
+                    "thrust reductions, cuFFT), compiled from its sources for sm_100a",
+            "timing": "the reference's own MainLoop timer (host clock, cudaDeviceSynchronize after each stage)",
+            "stages_ms_per_call": {k: v[0] * 1e3 / v[1] for k, v in timers.items() if v[1] > 0},
+            "nrj_first_last": [nrj[0], nrj[-1]] if nrj else None}
+
+
 def _set_omp_env():
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
     os.environ.setdefault("OMP_PROC_BIND", "true")
@@ -830,6 +895,12 @@ def main(argv=None):
             _set_omp_env()
             line["cpu_baseline"] = reference_cpu(args.n, 3, 20.0) or {
                 "value": None, "unit": METRIC, "cores": 0, "kind": "reference", "sample": "oracle/_ref absent"}
+        if rank == 0 and world == 1 and not args.no_reference_gpu and not use_slabs:
+            ref = reference_gpu(args.n, 10)
+            if "value" in ref:
+                ref["f64_over_reference"] = line["f64"]["value"] / ref["value"] if line.get("f64") else None
+                ref["f32_over_reference"] = line["value"] / ref["value"]
+            line["reference_gpu"] = ref
         if rank == 0:
             print(json.dumps(line), flush=True)
     finally:
