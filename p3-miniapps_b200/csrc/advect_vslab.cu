@@ -388,9 +388,12 @@ struct VslabCfg {
 // halo slabs of its vy segment (4% at Q = 128, 8% at 64), so Q is the
 // tallest segment that still leaves six items per SM (at 128^4: 64 in FP32,
 // 128 in FP64, whose chunks are half as wide).  Stages as measured best at
-// 128^4 (8 FP32, 4 FP64).  VLP4D_VSLAB_Q and VLP4D_VSLAB_STAGES override
-// for tuning sweeps.
-bool vslab_config(const vlp4d_ctx *c, VslabCfg &cfg) {
+// 128^4: 8 for the FP32 vx+vy pass (one 512-thread CTA per SM, by
+// registers), 4 for a single FP32 direction (lighter threads: four stages
+// leave room for several CTAs per SM; 0.46 -> 0.38 ms for vx, 0.50 -> 0.41
+// ms for vy), 4 in FP64.  VLP4D_VSLAB_Q and VLP4D_VSLAB_STAGES override for
+// tuning sweeps.
+bool vslab_config(const vlp4d_ctx *c, bool both, VslabCfg &cfg) {
   const long long nxy = c->g.nxy();
   const int nvx = c->g.n[2], nvy = c->g.n[3];
   const bool f32 = c->dtype == VLP4D_F32;
@@ -422,7 +425,7 @@ bool vslab_config(const vlp4d_ctx *c, VslabCfg &cfg) {
   if (Q > nvy) Q = nvy;
   while (Q > 1 && nvy % Q) --Q;
   cfg.Q = Q;
-  cfg.stages = env_int("VLP4D_VSLAB_STAGES", f32 ? 8 : 4);
+  cfg.stages = env_int("VLP4D_VSLAB_STAGES", f32 && both ? 8 : 4);
   if (cfg.stages < 2 || cfg.stages > kMaxStages) return false;
   cfg.smem = 128 + kBarBytes + (size_t)cfg.stages * cfg.C * nvx * c->elem;
   return cfg.smem <= 200 * 1024;
@@ -455,7 +458,7 @@ int launch_advect_vxvy_tables(vlp4d_ctx *c, const void *fn, void *fnp1, const St
   if (((uintptr_t)fn & 15) || ((uintptr_t)fnp1 & 15)) return VLP4D_ERR_UNSUPPORTED;
   if (!do_vx && !do_vy) return VLP4D_ERR_UNSUPPORTED;
   VslabCfg cfg;
-  if (!vslab_config(c, cfg)) return VLP4D_ERR_UNSUPPORTED;
+  if (!vslab_config(c, do_vx && do_vy, cfg)) return VLP4D_ERR_UNSUPPORTED;
   PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
   if (!encode) return VLP4D_ERR_UNSUPPORTED;
   const long long nxy = c->g.nxy();
