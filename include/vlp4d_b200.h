@@ -227,15 +227,21 @@ int vlp4d_step(vlp4d_ctx *ctx, void *f_state, void *f_next, int iter, void *stre
 
 /* `nsteps` consecutive steps, iterations iter0 .. iter0+nsteps-1 (the time
  * loop of miniapps/vlp4d/thrust/vlp4d.cpp:63-72): the same steps, field
- * solves and diagnostics as nsteps calls of vlp4d_step.  In FP32 contexts
- * (VLP4D_XYXY=1/0 at context creation forces it on/off) the last x/y half
- * step of each step and the first of the next (consecutive, with no field
- * solve between them) run as one pass (vlp4d_advect_xyxy's), so the state
- * between steps is never written to memory: 2*nsteps + 1 passes over f
- * instead of 3*nsteps, equal to nsteps vlp4d_step calls to rounding.  With
- * the joining off the result is bit-identical to them.  Reads f_state,
- * writes the final state into f_next; f_state is scratch. */
+ * solves and diagnostics as nsteps calls of vlp4d_step.  Where
+ * vlp4d_steps_joins_xy says so (FP32 contexts, and FP64 contexts whose
+ * nx/4 divides 32; VLP4D_XYXY=1/0 at context creation forces it on/off)
+ * the last x/y half step of each step and the first of the next
+ * (consecutive, with no field solve between them) run as one pass
+ * (vlp4d_advect_xyxy's), so the state between steps is never written to
+ * memory: 2*nsteps + 1 passes over f instead of 3*nsteps, equal to nsteps
+ * vlp4d_step calls to rounding.  With the joining off the result is
+ * bit-identical to them.  Reads f_state, writes the final state into
+ * f_next; f_state is scratch. */
 int vlp4d_steps(vlp4d_ctx *ctx, void *f_state, void *f_next, int iter0, int nsteps, void *stream);
+/* 1 when vlp4d_steps joins consecutive x/y half steps on this context (as
+ * above), else 0 (also for NULL).  No reference counterpart: lets a caller
+ * that runs the stages itself (a vy-slab driver) follow the same schedule. */
+int vlp4d_steps_joins_xy(const vlp4d_ctx *ctx);
 
 /* The time loop of main() (miniapps/vlp4d/thrust/vlp4d.cpp:55-73) with host
  * buffers: copies f0 (host, nx*ny*nvx*nvy elements of the context's dtype)

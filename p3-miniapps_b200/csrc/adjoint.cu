@@ -65,6 +65,10 @@ struct vlp4d_adjoint {
   bool have_plan_g2 = false;
   bool field_linear = true;  // false for the analytic-field cases 2 and 6
   StencilTable tab_x_adj, tab_y_adj, tab_vx_adj, tab_vy_adj;
+  // The transposed x/y half step applied twice as 11-tap lines: the last
+  // x/y pass of one reverse step and the first of the step before it in one
+  // k_plane_xyxy pass (valid = false: two x/y passes instead).
+  StencilTable tab_x11_adj, tab_y11_adj;
   double *dw_vx = nullptr, *dw_vy = nullptr;  // dw/dE per v line (6 each, FP64)
   bool have_forward = false;
   double J = 0.0;
@@ -543,11 +547,11 @@ int energy_grad(vlp4d_adjoint *A, const void *f, void *lam, cudaStream_t s) {
   return launch_columns(A, lam, false, c->g.dx[2] * c->g.dx[3], s);
 }
 
-// lam_out = (d step / d f)^T lam_next at the state f_state.
-// The reverse step from the stored stage input a (= XY f) and its field E:
-// lam_out = (d step/d f)^T lam_next.
-int step_adjoint_stored(vlp4d_adjoint *A, const void *a, const double *e, const void *lam_next, void *lam_out,
-                        cudaStream_t s) {
+// The middle of a reverse step, from lb = XY^T lam_next (in lb) to
+// la = VXVY^T lb + dvx dvy broadcast(dJ/drho) (into la): the v tables and
+// their E-derivatives from the stored field e of the step (NULL: the
+// context's Ex, Ey), dJ/dE from the stored stage input a, dJ/drho.
+int reverse_core(vlp4d_adjoint *A, const void *a, const double *e, const void *lb, void *la, cudaStream_t s) {
   vlp4d_ctx *c = A->ctx;
   const double dt = c->dom.dt;
   const long long n2 = c->g.nxy();
@@ -565,21 +569,30 @@ int step_adjoint_stored(vlp4d_adjoint *A, const void *a, const double *e, const 
   k_build_vtable_adj<<<blocks, threads, 0, s>>>(c->ey, lines, dt, c->g.minp[3], c->g.maxp[3], c->g.n[3],
                                                 A->tab_vy_adj.m, A->tab_vy_adj.w, A->tab_vy_adj.wf, A->dw_vy);
   VLP4D_LAUNCH_CHECK();
-  // lb = XY^T lam_next.
-  if ((rc = advect_xy_any(c, lam_next, A->W[1], &A->tab_x_adj, &A->tab_y_adj, s))) return rc;
   // dJ/dE, then dJ/drho.
-  if ((rc = launch_vgrad(A, a, A->W[1], s))) return rc;
+  if ((rc = launch_vgrad(A, a, lb, s))) return rc;
   if ((rc = field_transpose(A, s))) return rc;
   // la = VXVY^T lb + dvx dvy broadcast(dJ/drho), the broadcast folded into
-  // the v-slab pass where it runs; lambda = XY^T la.
+  // the v-slab pass where it runs.
   const double scale = c->g.dx[2] * c->g.dx[3];
-  rc = launch_advect_vxvy_tables(c, A->W[1], A->W[0], &A->tab_vx_adj, &A->tab_vy_adj, s, A->lam_rho, scale);
+  rc = launch_advect_vxvy_tables(c, lb, la, &A->tab_vx_adj, &A->tab_vy_adj, s, A->lam_rho, scale);
   if (rc == VLP4D_ERR_UNSUPPORTED) {
-    if ((rc = advect_vxvy_any(c, A->W[1], A->W[0], &A->tab_vx_adj, &A->tab_vy_adj, s))) return rc;
-    if ((rc = launch_columns(A, A->W[0], true, scale, s))) return rc;
+    if ((rc = advect_vxvy_any(c, lb, la, &A->tab_vx_adj, &A->tab_vy_adj, s))) return rc;
+    if ((rc = launch_columns(A, la, true, scale, s))) return rc;
   } else if (rc) {
     return rc;
   }
+  return VLP4D_OK;
+}
+
+// The reverse step from the stored stage input a (= XY f) and its field E:
+// lam_out = (d step/d f)^T lam_next = XY^T (reverse_core(XY^T lam_next)).
+int step_adjoint_stored(vlp4d_adjoint *A, const void *a, const double *e, const void *lam_next, void *lam_out,
+                        cudaStream_t s) {
+  vlp4d_ctx *c = A->ctx;
+  int rc;
+  if ((rc = advect_xy_any(c, lam_next, A->W[1], &A->tab_x_adj, &A->tab_y_adj, s))) return rc;
+  if ((rc = reverse_core(A, a, e, A->W[1], A->W[0], s))) return rc;
   return advect_xy_any(c, A->W[0], lam_out, &A->tab_x_adj, &A->tab_y_adj, s);
 }
 
@@ -671,10 +684,28 @@ int backward_body(vlp4d_adjoint *A, void *grad, cudaStream_t s) {
       if ((rc = launch_field_poisson(c, s))) return rc;
       save_field(A, j, s);
     }
+    // The reverse steps of the segment, last first.  Between two of them
+    // the closing XY^T of one and the opening XY^T of the next are one pass
+    // of the transposed 11-tap lines (as the forward sweep joins its x/y
+    // half steps), so the adjoint state is materialised only at the
+    // segment's start.  W[1] holds lb of the step, W[0] its la.
+    if ((rc = advect_xy_any(c, A->L[cur], A->W[1], &A->tab_x_adj, &A->tab_y_adj, s))) return rc;
     for (int j = len - 1; j >= 0; --j) {
-      void *dst = (sg == 0 && j == 0) ? grad : A->L[cur ^ 1];
-      if ((rc = step_adjoint_stored(A, A->seg[j], A->seg_e + 2 * n2 * j, A->L[cur], dst, s))) return rc;
-      cur ^= 1;
+      if ((rc = reverse_core(A, A->seg[j], A->seg_e + 2 * n2 * j, A->W[1], A->W[0], s))) return rc;
+      if (j > 0) {
+        rc = A->tab_x11_adj.valid
+                 ? launch_advect_xyxy_tables(c, A->W[0], A->W[1], &A->tab_x11_adj, &A->tab_y11_adj, false, s)
+                 : VLP4D_ERR_UNSUPPORTED;
+        if (rc == VLP4D_ERR_UNSUPPORTED) {
+          if ((rc = advect_xy_any(c, A->W[0], A->L[cur ^ 1], &A->tab_x_adj, &A->tab_y_adj, s))) return rc;
+          rc = advect_xy_any(c, A->L[cur ^ 1], A->W[1], &A->tab_x_adj, &A->tab_y_adj, s);
+        }
+        if (rc) return rc;
+      } else {
+        void *dst = sg == 0 ? grad : A->L[cur ^ 1];
+        if ((rc = advect_xy_any(c, A->W[0], dst, &A->tab_x_adj, &A->tab_y_adj, s))) return rc;
+        cur ^= 1;
+      }
     }
   }
   return VLP4D_OK;
@@ -734,6 +765,8 @@ void destroy(vlp4d_adjoint *A) {
   free_table(A->tab_y_adj);
   free_table(A->tab_vx_adj);
   free_table(A->tab_vy_adj);
+  free_table(A->tab_x11_adj);
+  free_table(A->tab_y11_adj);
   if (A->own) cudaStreamDestroy(A->own);
   delete A;
 }
@@ -809,6 +842,10 @@ int vlp4d_adjoint_create(vlp4d_ctx *ctx, int nsteps, int every, vlp4d_adjoint **
   cudaStream_t s = A->own;
   if ((rc = build_xy_adj(ctx, 0, 0.5 * ctx->dom.dt, A->tab_x_adj, s))) return bail(rc);
   if ((rc = build_xy_adj(ctx, 1, 0.5 * ctx->dom.dt, A->tab_y_adj, s))) return bail(rc);
+  if (xyxy_join(ctx)) {  // the joined reverse pass where the forward sweep joins too
+    if ((rc = build_xy11_table(ctx, 0, 0.5 * ctx->dom.dt, true, A->tab_x11_adj, s))) return bail(rc);
+    if ((rc = build_xy11_table(ctx, 1, 0.5 * ctx->dom.dt, true, A->tab_y11_adj, s))) return bail(rc);
+  }
   if ((rc = alloc_table(A->tab_vx_adj, (int)n2))) return bail(rc);
   if ((rc = alloc_table(A->tab_vy_adj, (int)n2))) return bail(rc);
   A->tab_vx_adj.valid = A->tab_vy_adj.valid = true;

@@ -265,54 +265,66 @@ int ensure_xy_table(vlp4d_ctx *c, int dim, double dt, StencilTable **out, cudaSt
   return VLP4D_OK;
 }
 
-int ensure_xy11_table(vlp4d_ctx *c, int dim, double dt, StencilTable **out, cudaStream_t s) {
-  StencilTable *t = dim == 0 ? &c->tab_x11 : &c->tab_y11;
-  if (t->valid && t->dt == dt) {
-    *out = t;
-    return VLP4D_OK;
+void line11(const LineStencil &st, int n, int *m, double W[11], float u[10]) {
+  // out[i] = sum_k w_k sum_j w_j f[i + m + k + m + j] = sum_q W_q f[i + 2m + q].
+  for (int q = 0; q < 11; ++q) W[q] = 0.;
+  for (int k = 0; k < 6; ++k)
+    for (int j = 0; j < 6; ++j) W[k + j] += st.w[k] * st.w[j];
+  *m = (int)((2LL * st.m) % n);
+  // FP32 difference form about tap 5 (the weights sum to one):
+  // out = f5 + sum_j u_j (f_{j+1} - f_j), u_j = -(W_0+..+W_j) for j < 5,
+  // u_j = W_{j+1}+..+W_10 for j >= 5.
+  double acc = 0.;
+  for (int j = 0; j < 5; ++j) {
+    acc += W[j];
+    u[j] = (float)-acc;
   }
-  t->valid = false;
+  acc = 0.;
+  for (int j = 9; j >= 5; --j) {
+    acc += W[j + 1];
+    u[j] = (float)acc;
+  }
+}
+
+int build_xy11_table(vlp4d_ctx *c, int dim, double dt, bool transposed, StencilTable &t, cudaStream_t s) {
+  t.valid = false;
   const int vdim = dim == 0 ? 2 : 3;
   const int lines = c->g.n[vdim], n = c->g.n[dim];
   const int l0 = vdim == 3 ? c->ivy0 : 0;  // slab contexts: global vy lines
-  int rc = alloc_table(*t, lines, 11);
+  int rc = alloc_table(t, lines, 11);
   if (rc) return rc;
   std::vector<int> hm(lines);
   std::vector<double> hw(11 * (size_t)lines);
   std::vector<float> hwf(11 * (size_t)lines);
   for (int l = 0; l < lines; ++l) {
     const double v = c->g.minp[vdim] + (l0 + l) * c->g.dx[vdim];
-    const LineStencil st = line_stencil(dt * v, c->g.minp[dim], c->g.maxp[dim], n);
-    // out[i] = sum_k w_k sum_j w_j f[i + m + k + m + j] = sum_q W_q f[i + 2m + q].
-    double W[11] = {0.};
-    for (int k = 0; k < 6; ++k)
-      for (int j = 0; j < 6; ++j) W[k + j] += st.w[k] * st.w[j];
-    hm[l] = (int)((2LL * st.m) % n);
-    // FP32 difference form about tap 5 (the weights sum to one):
-    // out = f5 + sum_j u_j (f_{j+1} - f_j), u_j = -(W_0+..+W_j) for j < 5,
-    // u_j = W_{j+1}+..+W_10 for j >= 5.
-    double u[10];
-    double acc = 0.;
-    for (int j = 0; j < 5; ++j) {
-      acc += W[j];
-      u[j] = -acc;
-    }
-    acc = 0.;
-    for (int j = 9; j >= 5; --j) {
-      acc += W[j + 1];
-      u[j] = acc;
-    }
+    LineStencil st = line_stencil(dt * v, c->g.minp[dim], c->g.maxp[dim], n);
+    if (transposed) st = adjoint_stencil(st, n);
+    double W[11];
+    float u[10];
+    line11(st, n, &hm[l], W, u);
     for (int k = 0; k < 11; ++k) {
       hw[11 * l + k] = W[k];
-      hwf[11 * l + k] = k < 10 ? (float)u[k] : 0.f;
+      hwf[11 * l + k] = k < 10 ? u[k] : 0.f;
     }
   }
-  VLP4D_CUDA_TRY(cudaMemcpyAsync(t->m, hm.data(), sizeof(int) * lines, cudaMemcpyHostToDevice, s));
-  VLP4D_CUDA_TRY(cudaMemcpyAsync(t->w, hw.data(), sizeof(double) * 11 * lines, cudaMemcpyHostToDevice, s));
-  VLP4D_CUDA_TRY(cudaMemcpyAsync(t->wf, hwf.data(), sizeof(float) * 11 * lines, cudaMemcpyHostToDevice, s));
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(t.m, hm.data(), sizeof(int) * lines, cudaMemcpyHostToDevice, s));
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(t.w, hw.data(), sizeof(double) * 11 * lines, cudaMemcpyHostToDevice, s));
+  VLP4D_CUDA_TRY(cudaMemcpyAsync(t.wf, hwf.data(), sizeof(float) * 11 * lines, cudaMemcpyHostToDevice, s));
   VLP4D_CUDA_TRY(cudaStreamSynchronize(s));
-  t->dt = dt;
-  t->valid = true;
+  t.dt = dt;
+  t.valid = true;
+  return VLP4D_OK;
+}
+
+int ensure_xy11_table(vlp4d_ctx *c, int dim, double dt, StencilTable **out, cudaStream_t s) {
+  StencilTable *t = dim == 0 ? &c->tab_x11 : &c->tab_y11;
+  if (t->valid && t->dt == dt) {
+    *out = t;
+    return VLP4D_OK;
+  }
+  int rc = build_xy11_table(c, dim, dt, false, *t, s);
+  if (rc) return rc;
   *out = t;
   return VLP4D_OK;
 }

@@ -538,7 +538,9 @@ __device__ __forceinline__ void sweep_x11(const T (&t)[20], int r, const W11<T> 
 // to eight different bank groups, and keeps the Y11 stores (eight
 // consecutive chunks per phase) conflict-free.
 __device__ __forceinline__ int xyxy_swz(int chunk) { return chunk ^ ((chunk >> 3) & 1); }
-template <typename T, int NX, int RT, bool X8 = false>
+// RHO = false: no moment (the reverse mode's joined pass of transposed
+// stencils has no use for one).
+template <typename T, int NX, int RT, bool X8 = false, bool RHO = true>
 __global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int nx = NX ? NX : a.nx;
@@ -655,10 +657,12 @@ __global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
         const float lo[4] = {out[0], out[1], out[2], out[3]}, hi[4] = {out[4], out[5], out[6], out[7]};
         store4(outp + (size_t)(r8 + i) * nx + c8, lo);
         store4(outp + (size_t)(r8 + i) * nx + c8 + 4, hi);
+        if constexpr (RHO) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          racc[2 * i][q] += (double)lo[q];
-          racc[2 * i + 1][q] += (double)hi[q];
+          for (int q = 0; q < 4; ++q) {
+            racc[2 * i][q] += (double)lo[q];
+            racc[2 * i + 1][q] += (double)hi[q];
+          }
         }
       }
     } else {  // X11 of the thread's rows, the moment.
@@ -688,8 +692,10 @@ __global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
         T out[4];
         sweep_x11(t, rr, wx, out);
         store4(outp + (size_t)(r0 + i) * nx + c0, out);
+        if constexpr (RHO) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) racc[i][q] += (double)out[q];
+          for (int q = 0; q < 4; ++q) racc[i][q] += (double)out[q];
+        }
       }
     }
     ivx += gdx;
@@ -703,7 +709,9 @@ __global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
       parity ^= 1u;
     }
   }
-  if constexpr (X8) {
+  if constexpr (!RHO) {
+    return;
+  } else if constexpr (X8) {
     double *rdst = a.rho_part + (long long)g * plane_elems + ((long long)chunk * R + r8) * nx + c8;
 #pragma unroll
     for (int i = 0; i < 2; ++i)
@@ -714,6 +722,189 @@ __global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
         p2[1] = make_double2(racc[2 * i + h][2], racc[2 * i + h][3]);
       }
   } else {
+    double *rdst = a.rho_part + (long long)g * plane_elems + ((long long)chunk * R + r0) * nx + c0;
+#pragma unroll
+    for (int i = 0; i < RT; ++i) {
+      reinterpret_cast<double2 *>(rdst + (size_t)i * nx)[0] = make_double2(racc[i][0], racc[i][1]);
+      reinterpret_cast<double2 *>(rdst + (size_t)i * nx)[1] = make_double2(racc[i][2], racc[i][3]);
+    }
+  }
+}
+
+// FP64 form of the two-half-step pass for row widths a warp holds whole
+// (nx/4 divides 32).  With 1 KB rows the FP32 structure (staged rows, a Y11
+// tile, X11) leaves one CTA per SM; here, as in k_plane's in-place FP64
+// pass, the staged slot is swept in place:
+//   X11: each warp sweeps whole staged rows (all R + 10 of them) and writes
+//        the x-swept row back over itself after every lane has read it;
+//   one CTA barrier;
+//   Y11: thread (quad cg, row group rg) streams its RT + 10 x-swept rows
+//        down the slot and accumulates each row into the RT outputs it
+//        belongs to (out_i = sum_k W_k row_{i+k}), so only RT accumulators
+//        and one row are live; each finished output goes to global memory
+//        and into the FP64 moment.
+// X11 then Y11 applies the same two composed stencils as Y11 then X11 (they
+// commute), at the cost of X11 on the 10 halo rows.  The slot of item it is
+// read until Y11(it) ends, so it is refilled at the barrier of item it + 1
+// (two stages keep two CTAs per SM at 128^4).  Weights plain (FP64 sums
+// w * w of the per-line Lagrange weights, as k_plane_xyxy<double>).
+template <int NX, int RT, bool RHO = true>
+__global__ void __launch_bounds__(512) k_plane_xyxy64(PlaneArgs a) {
+  using T = double;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int nx = NX ? NX : a.nx;
+  const int ny = a.ny, R = a.R, S = a.stages;
+  const int vrows = R + 10;
+  const int ncg = nx >> 2;
+  const size_t slot_elems = (size_t)vrows * nx;
+  const uint32_t slot_bytes = (uint32_t)(slot_elems * sizeof(T));
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+  LineRec11<T> *xrec = reinterpret_cast<LineRec11<T> *>(smem + kBarBytes);
+  LineRec11<T> *yrec = xrec + a.nvx;
+  T *slots = reinterpret_cast<T *>(yrec + a.nvy);
+
+  const int cg = threadIdx.x % ncg;
+  const int rg = threadIdx.x / ncg;
+  const int RG = blockDim.x / ncg;  // row groups; R == RG * RT
+  const int c0 = cg * 4;
+  const int r0 = rg * RT;
+  const int chunk = blockIdx.x % a.cpp;
+  const int G = gridDim.x / a.cpp;
+  const int g = blockIdx.x / a.cpp;
+  const long long planes = (long long)a.nvx * a.nvy;
+  const long long n_items = g < planes ? (planes - g + G - 1) / G : 0;
+  const long long plane_elems = (long long)nx * ny;
+
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < S; ++st) mbar_init(&bars[st], 1);
+    mbar_fence_init();
+  }
+  stage_lines11<T>(a.tx, a.nvx, xrec);
+  stage_lines11<T>(a.ty, a.nvy, yrec);
+  __syncthreads();
+
+  auto issue = [&](long long it) {
+    const long long p = g + it * G;
+    int phys = (chunk * R + yrec[(int)(p / a.nvx)].m) % ny;
+    uint64_t *bar = &bars[it % S];
+    mbar_arrive_expect_tx(bar, slot_bytes);
+    const T *src = static_cast<const T *>(a.fin) + p * plane_elems;
+    T *dst = slots + (size_t)(it % S) * slot_elems;
+    int remaining = vrows;
+    while (remaining > 0) {
+      const int len = remaining < ny - phys ? remaining : ny - phys;
+      bulk_load(dst, src + (long long)phys * nx, (uint32_t)((size_t)len * nx * sizeof(T)), bar);
+      dst += (size_t)len * nx;
+      remaining -= len;
+      phys = 0;
+    }
+  };
+  if (threadIdx.x == 0) {
+    const long long pre = n_items < S ? n_items : S;
+    for (long long it = 0; it < pre; ++it) issue(it);
+  }
+
+  double racc[RT][4];
+#pragma unroll
+  for (int i = 0; i < RT; ++i)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) racc[i][q] = 0.0;
+
+  // Trip count of the warp's first row group in the X11 phase, so that every
+  // lane reaches each __syncwarp; the lanes this warp has.
+  const int rgw = (int)((threadIdx.x & ~31u) / (unsigned)ncg);
+  const int trips = (vrows - rgw + RG - 1) / RG;
+  const unsigned wl = blockDim.x - (threadIdx.x & ~31u);
+  const unsigned wmask = wl >= 32 ? 0xffffffffu : (1u << wl) - 1u;
+
+  const int gdx = G % a.nvx, gdy = G / a.nvx;
+  int ivx = g % a.nvx, ivy = g / a.nvx;
+  int slot = 0;
+  uint32_t parity = 0;
+  for (long long it = 0; it < n_items; ++it) {
+    const bool ok = mbar_wait_bounded(&bars[slot], parity);
+    const long long p = g + it * G;
+    T *in = slots + (size_t)slot * slot_elems;
+    T *outp = static_cast<T *>(a.fout) + p * plane_elems + (long long)chunk * R * nx;
+    {  // X11 in place on the staged rows rg, rg + RG, ... (this warp's rows).
+      W11<T> wx;
+      int base = c0 + read_line11(xrec[ivx], wx);
+      base = base % nx;
+      const int rr = base & 3;
+      int o[5];
+      o[0] = base - rr;
+#pragma unroll
+      for (int k = 1; k < 5; ++k) {
+        o[k] = o[k - 1] + 4;
+        if (o[k] >= nx) o[k] -= nx;
+      }
+      for (int k = 0; k < trips; ++k) {
+        const int v = rg + k * RG;
+        T *row = in + (size_t)v * nx;
+        T t[20], q4[4], out[4];
+        if (v < vrows) {
+#pragma unroll
+          for (int j = 0; j < 5; ++j) {
+            load4(row + o[j], q4);
+            t[4 * j] = q4[0];
+            t[4 * j + 1] = q4[1];
+            t[4 * j + 2] = q4[2];
+            t[4 * j + 3] = q4[3];
+          }
+          sweep_x11(t, rr, wx, out);
+        }
+        __syncwarp(wmask);  // every lane has read the row
+        if (v < vrows) store4(row + c0, out);
+      }
+      // These generic writes precede the slot's next bulk copy.
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    // The x-swept rows are complete; every thread is done with item it - 1,
+    // whose slot now takes item it - 1 + S.
+    const long long issued_end = it == 0 ? (long long)S : it - 1 + S;
+    if (__syncthreads_or(!ok)) {
+      plane_abort(a, bars, it, n_items, S, issued_end);
+      return;
+    }
+    if (threadIdx.x == 0 && it > 0 && it - 1 + S < n_items) issue(it - 1 + S);
+    {  // Y11 of rows r0 .. r0+RT-1, quad c0, streamed down the slot.
+      W11<T> wy;
+      read_line11(yrec[ivy], wy);
+      const T *src = in + (size_t)r0 * nx + c0;
+      T acc[RT][4];
+#pragma unroll
+      for (int j = 0; j < RT + 10; ++j) {
+        T y[4];
+        load4(src + (size_t)j * nx, y);
+#pragma unroll
+        for (int i = 0; i < RT; ++i) {
+          const int k = j - i;
+          if (k < 0 || k > 10) continue;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[i][q] = k == 0 ? wy.w[0] * y[q] : fma(wy.w[k], y[q], acc[i][q]);
+        }
+        if (j >= 10) {
+          const int i = j - 10;
+          store4(outp + (size_t)(r0 + i) * nx + c0, acc[i]);
+          if constexpr (RHO) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) racc[i][q] += acc[i][q];
+          }
+        }
+      }
+    }
+    ivx += gdx;
+    ivy += gdy;
+    if (ivx >= a.nvx) {
+      ivx -= a.nvx;
+      ++ivy;
+    }
+    if (++slot == S) {
+      slot = 0;
+      parity ^= 1u;
+    }
+  }
+  if constexpr (RHO) {
     double *rdst = a.rho_part + (long long)g * plane_elems + ((long long)chunk * R + r0) * nx + c0;
 #pragma unroll
     for (int i = 0; i < RT; ++i) {
@@ -915,10 +1106,10 @@ bool xyxy_x8(int nx) {
 }
 
 template <typename T, int NX, int RT>
-int run_xyxy(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, cudaStream_t s) {
+int run_xyxy(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, bool rho, cudaStream_t s) {
   auto kern = k_plane_xyxy<T, NX, RT>;
   if constexpr (sizeof(T) == 4 && RT == 4) {
-    if (xyxy_x8(args.nx)) kern = k_plane_xyxy<T, NX, RT, true>;
+    if (xyxy_x8(args.nx)) kern = rho ? k_plane_xyxy<T, NX, RT, true> : k_plane_xyxy<T, NX, RT, true, false>;
   }
   VLP4D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
   int per_sm = 0;
@@ -938,19 +1129,106 @@ int run_xyxy(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, cudaStream_t s)
 }
 
 template <typename T, int RT>
-int run_xyxy_nx(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, cudaStream_t s) {
+int run_xyxy_nx(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, bool rho, cudaStream_t s) {
   switch (args.nx) {
-    case 64: return run_xyxy<T, 64, RT>(c, args, cfg, s);
-    case 128: return run_xyxy<T, 128, RT>(c, args, cfg, s);
-    case 256: return run_xyxy<T, 256, RT>(c, args, cfg, s);
-    default: return run_xyxy<T, 0, RT>(c, args, cfg, s);
+    case 64: return run_xyxy<T, 64, RT>(c, args, cfg, rho, s);
+    case 128: return run_xyxy<T, 128, RT>(c, args, cfg, rho, s);
+    case 256: return run_xyxy<T, 256, RT>(c, args, cfg, rho, s);
+    default: return run_xyxy<T, 0, RT>(c, args, cfg, rho, s);
   }
 }
 
-int run_xyxy_any(vlp4d_ctx *c, const PlaneArgs &a, PlaneCfg &cfg, cudaStream_t s) {
+// k_plane_xyxy64: FP64, row widths a warp holds whole.  Chunk height: the
+// tallest divisor of ny up to 32 whose block fits, four rows per thread
+// when it divides, else one; two stages (three when two CTAs per SM are out
+// of reach anyway).  VLP4D_XYXY64=0 turns it off (the FP64 form of
+// k_plane_xyxy then runs); VLP4D_XYXY_STAGES overrides the depth.
+size_t xyxy64_smem(int R, int nx, int stages, int nvx, int nvy) {
+  return kBarBytes + sizeof(LineRec11<double>) * (size_t)(nvx + nvy) + (size_t)stages * (R + 10) * nx * 8;
+}
+
+}  // namespace
+
+bool xyxy64_available(const vlp4d_ctx *c) {
+  const int nx = c->g.n[0];
+  return c->fused && c->dtype == VLP4D_F64 && nx % 4 == 0 && 32 % (nx / 4) == 0 && env_int("VLP4D_XYXY64", 1) != 0;
+}
+
+namespace {
+
+bool xyxy64_config(const vlp4d_ctx *c, PlaneCfg &cfg) {
+  const int nx = c->g.n[0], ny = c->g.n[1];
+  if (c->dtype != VLP4D_F64 || nx % 4 != 0 || 32 % (nx / 4) != 0) return false;
+  if (env_int("VLP4D_XYXY64", 1) == 0) return false;
+  const int ncg = nx / 4;
+  const int forced = env_int("VLP4D_XYXY_STAGES", 0);
+  if (forced && (forced < 2 || forced > kMaxStages)) return false;
+  for (int r = ny < 32 ? ny : 32; r >= 1; --r) {
+    if (ny % r) continue;
+    const int t = r % 4 == 0 ? 4 : 1;
+    const int threads = ncg * (r / t);
+    if (threads > 512) continue;
+    int st = forced ? forced : 2;
+    if (!forced && xyxy64_smem(r, nx, 2, c->g.n[2], c->g.n[3]) > 112 * 1024) st = 3;
+    const size_t smem = xyxy64_smem(r, nx, st, c->g.n[2], c->g.n[3]);
+    if (smem > 224 * 1024) continue;
+    cfg.R = r;
+    cfg.rt = t;
+    cfg.stages = st;
+    cfg.cpp = ny / r;
+    cfg.threads = threads;
+    cfg.smem = smem;
+    return true;
+  }
+  return false;
+}
+
+template <int NX, int RT>
+int run_xyxy64(vlp4d_ctx *c, PlaneArgs args, PlaneCfg &cfg, bool rho, cudaStream_t s) {
+  auto kern = rho ? k_plane_xyxy64<NX, RT, true> : k_plane_xyxy64<NX, RT, false>;
+  VLP4D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
+  int per_sm = 0;
+  VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, cfg.threads, cfg.smem));
+  if (per_sm < 1) return VLP4D_ERR_UNSUPPORTED;
+  cfg.per_sm = per_sm;
+  args.R = cfg.R;
+  args.cpp = cfg.cpp;
+  args.stages = cfg.stages;
+  const long long planes = (long long)args.nvx * args.nvy;
+  long long G = ((long long)per_sm * c->num_sms) / cfg.cpp;
+  if (G < 1) G = 1;
+  if (G > planes) G = planes;
+  if (G > c->rho_part_groups) G = c->rho_part_groups;
+  cfg.G = (int)G;
+  cfg.grid = (int)G * cfg.cpp;
+  kern<<<cfg.grid, cfg.threads, cfg.smem, s>>>(args);
+  VLP4D_LAUNCH_CHECK();
+  return VLP4D_OK;
+}
+
+template <int RT>
+int run_xyxy64_nx(vlp4d_ctx *c, const PlaneArgs &a, PlaneCfg &cfg, bool rho, cudaStream_t s) {
+  switch (a.nx) {
+    case 64: return run_xyxy64<64, RT>(c, a, cfg, rho, s);
+    case 128: return run_xyxy64<128, RT>(c, a, cfg, rho, s);
+    default: return run_xyxy64<0, RT>(c, a, cfg, rho, s);
+  }
+}
+
+int run_xyxy_any(vlp4d_ctx *c, const PlaneArgs &a, PlaneCfg &cfg, bool rho, cudaStream_t s) {
+  if (c->dtype == VLP4D_F64) {
+    PlaneCfg c64;
+    if (xyxy64_config(c, c64)) {
+      const int rc = c64.rt == 4 ? run_xyxy64_nx<4>(c, a, c64, rho, s) : run_xyxy64_nx<1>(c, a, c64, rho, s);
+      if (rc != VLP4D_ERR_UNSUPPORTED) {
+        cfg = c64;
+        return rc;
+      }
+    }
+  }
   if (c->dtype == VLP4D_F64)
-    return cfg.rt == 4 ? run_xyxy_nx<double, 4>(c, a, cfg, s) : run_xyxy_nx<double, 1>(c, a, cfg, s);
-  return cfg.rt == 4 ? run_xyxy_nx<float, 4>(c, a, cfg, s) : run_xyxy_nx<float, 1>(c, a, cfg, s);
+    return cfg.rt == 4 ? run_xyxy_nx<double, 4>(c, a, cfg, rho, s) : run_xyxy_nx<double, 1>(c, a, cfg, rho, s);
+  return cfg.rt == 4 ? run_xyxy_nx<float, 4>(c, a, cfg, rho, s) : run_xyxy_nx<float, 1>(c, a, cfg, rho, s);
 }
 
 
@@ -1001,11 +1279,20 @@ int launch_advect_xyxy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTa
   int rc0;
   if ((rc0 = ensure_xy11_table(c, 0, tx->dt, &x11, s))) return rc0;
   if ((rc0 = ensure_xy11_table(c, 1, ty->dt, &y11, s))) return rc0;
+  return launch_advect_xyxy_tables(c, fn, fnp1, x11, y11, true, s);
+}
+
+int launch_advect_xyxy_tables(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *x11,
+                              const StencilTable *y11, bool with_rho, cudaStream_t s) {
+  if (!c->fused) return VLP4D_ERR_UNSUPPORTED;
+  if (((uintptr_t)fn & 15) || ((uintptr_t)fnp1 & 15)) return VLP4D_ERR_UNSUPPORTED;
+  PlaneCfg cfg;
+  if (!xyxy_config(c, cfg)) return VLP4D_ERR_UNSUPPORTED;
   PlaneArgs a = plane_args(c, fn, fnp1, cfg, 10);
   a.tx = *x11;
   a.ty = *y11;
-  int rc = run_xyxy_any(c, a, cfg, s);
-  if (rc) return rc;
+  int rc = run_xyxy_any(c, a, cfg, with_rho, s);
+  if (rc || !with_rho) return rc;
   return launch_rho_finish(c, cfg.G, s);
 }
 

@@ -320,6 +320,8 @@ int vlp4d_ctx_destroy(vlp4d_ctx *ctx) {
 
 int vlp4d_ctx_dtype(const vlp4d_ctx *ctx) { return ctx ? ctx->dtype : -1; }
 
+int vlp4d_steps_joins_xy(const vlp4d_ctx *ctx) { return ctx && xyxy_join(ctx) ? 1 : 0; }
+
 int vlp4d_field_ptr(vlp4d_ctx *ctx, int which, double **dev_ptr) {
   int rc = check_ctx(ctx);
   if (rc) return rc;
@@ -592,14 +594,16 @@ int advect_vxvy_any(vlp4d_ctx *ctx, const void *fn, void *fnp1, const StencilTab
 
 int fail_msg(int code, const std::string &msg) { return fail(code, msg); }
 
-// Whether the x/y half steps of consecutive steps run as one k_plane_xyxy
-// pass.  That pass does the arithmetic of two passes for the HBM traffic of
-// one: it pays off in FP32, while in FP64 its shared-memory footprint leaves
-// one CTA per SM and two k_plane passes are faster.  VLP4D_XYXY=0/1 at
-// context creation overrides.
+// Whether the x/y half steps of consecutive steps run as one joined pass.
+// That pass does the arithmetic of two passes for the HBM traffic of one:
+// in FP32 (k_plane_xyxy, 0.50 ms against 2 x 0.41 ms at 128^4) and in FP64
+// where k_plane_xyxy64 runs (1.48 ms against 2 x 1.11 ms), not for the FP64
+// widths only the generic FP64 form covers (its 1 KB rows leave one CTA per
+// SM: slower than two k_plane passes).  VLP4D_XYXY=0/1 at context creation
+// overrides.
 bool xyxy_join(const vlp4d_ctx *ctx) {
   if (ctx->xyxy_mode >= 0) return ctx->xyxy_mode == 1;
-  return ctx->dtype == VLP4D_F32;
+  return ctx->dtype == VLP4D_F32 || xyxy64_available(ctx);
 }
 
 }  // namespace vlp4d

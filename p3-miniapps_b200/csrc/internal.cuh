@@ -180,6 +180,12 @@ int ensure_xy_table(vlp4d_ctx *c, int dim, double dt, StencilTable **out, cudaSt
 // The composed 11-tap table of two x (dim 0) or y (dim 1) shifts by dt:
 // per line m and 11 FP64 weights; for FP32, 10 difference weights about tap 5.
 int ensure_xy11_table(vlp4d_ctx *c, int dim, double dt, StencilTable **out, cudaStream_t s);
+// The 11-tap line of two applications of the 6-tap line st on n points:
+// offset 2m mod n, FP64 weights W = w * w, FP32 difference weights u.
+void line11(const LineStencil &st, int n, int *m, double W[11], float u[10]);
+// An 11-tap x (dim 0) or y (dim 1) table for two shifts by dt, of the
+// transposed lines when `transposed` (the reverse mode's joined pass).
+int build_xy11_table(vlp4d_ctx *c, int dim, double dt, bool transposed, StencilTable &t, cudaStream_t s);
 int build_v_tables(vlp4d_ctx *c, double dt, bool vx, bool vy, cudaStream_t s);
 int launch_advect_generic(vlp4d_ctx *c, int dim, const void *fn, void *fnp1, const StencilTable *t,
                           cudaStream_t s);
@@ -204,6 +210,14 @@ int launch_advect_vxvy_tables(vlp4d_ctx *c, const void *fn, void *fnp1, const St
                               double bias_scale = 0.0);
 int launch_advect_xyxy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *tx, const StencilTable *ty,
                        cudaStream_t s);
+// Whether the FP64 form of the joined pass (k_plane_xyxy64, row widths a
+// warp holds whole) runs for this context.
+bool xyxy64_available(const vlp4d_ctx *c);
+// The same pass with explicit 11-tap tables.  with_rho false leaves the
+// context's rho alone (the kernels without a moment-free form still write
+// their partial moments into the context's scratch).
+int launch_advect_xyxy_tables(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *x11,
+                              const StencilTable *y11, bool with_rho, cudaStream_t s);
 
 // api.cu: one Strang step f_in -> f_out through scratch (diagnostic slot
 // `iter`, none when negative); x/y and vx/vy passes with explicit tables,

@@ -196,11 +196,10 @@ class SlabRun:
         self.dt = float(dt)
         self.nloc = ctx.nvy_local
         self.halo = ctx.halo
-        # As vlp4d_steps: join the x/y half steps of consecutive steps in FP32
-        # (one pass instead of two for the same bytes), not in FP64 (where two
-        # k_plane passes are faster).
+        # As vlp4d_steps: join the x/y half steps of consecutive steps where
+        # the library does (vlp4d_steps_joins_xy).
         if join_xy is None:
-            join_xy = getattr(ctx, "dtype_code", 0) == 1  # VLP4D_F32
+            join_xy = bool(getattr(ctx, "joins_xy", False))
         self.join_xy = join_xy
         self.fa = ctx.empty_f()
         self.fb = ctx.empty_f()

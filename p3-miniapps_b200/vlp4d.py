@@ -41,7 +41,7 @@ EXPORTS = (
     "vlp4d_mpi_size", "vlp4d_mpi_init_case", "vlp4d_mpi_halo_fill", "vlp4d_mpi_spline_xy", "vlp4d_mpi_spline_vxvy", "vlp4d_mpi_advect_2d",
     "vlp4d_mpi_advect_4d", "vlp4d_mpi_field", "vlp4d_mpi_l2norm", "vlp4d_mpi_step",
     "vlp4d_ctx_create_slab", "vlp4d_f_size", "vlp4d_slab_info", "vlp4d_advect_xy_moment",
-    "vlp4d_ensemble_set_idle_limit",
+    "vlp4d_ensemble_set_idle_limit", "vlp4d_steps_joins_xy",
 )
 HALO = 3  # HALO_PTS of the vlp4d_mpi halo-extended arrays
 
@@ -102,6 +102,7 @@ def lib() -> C.CDLL:
         L.vlp4d_init_case.argtypes = [vp, vp, i, d, d, d, vp]
         L.vlp4d_ctx_create_slab.argtypes = [C.POINTER(CDomain), i, i, i, i, C.POINTER(vp)]
         L.vlp4d_f_size.argtypes = [vp]
+        L.vlp4d_steps_joins_xy.argtypes = [vp]
         L.vlp4d_slab_info.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
         for n in ("vlp4d_advect_x", "vlp4d_advect_y", "vlp4d_advect_vx", "vlp4d_advect_vy", "vlp4d_advect_xy",
                   "vlp4d_advect_vxvy", "vlp4d_advect_xyxy", "vlp4d_advect_xy_moment"):
@@ -266,6 +267,8 @@ class Context:
         nx, ny, nvx, _ = dom.nxmax
         self.f_shape = (self.nvy_local + 2 * self.halo, nvx, ny, nx)
         self.f_size = int(lib().vlp4d_f_size(self.h))
+        # Whether vlp4d_steps joins consecutive x/y half steps on this context.
+        self.joins_xy = bool(lib().vlp4d_steps_joins_xy(self.h))
 
     def owned(self, f):
         """View of the owned planes of an f buffer of this context."""

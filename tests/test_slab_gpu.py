@@ -158,8 +158,6 @@ def test_slab_stage_entry_points_match_ordinary_context(pkg, cuda, dtype):
         out_f, out_g = full.empty_f(), sl.empty_f()
         for name, dt in (("advect_x", 0.3), ("advect_y", 0.3), ("advect_vx", 0.5), ("advect_vy", 0.5),
                          ("advect_xy", 0.3), ("advect_vxvy", 0.5), ("advect_xyxy", 0.3)):
-            if name == "advect_xyxy" and dtype == "f64":
-                continue  # the joined pass is an FP32 time-loop form
             getattr(full, name)(f, out_f, dt)
             getattr(sl, name)(g, out_g, dt)
             torch.cuda.synchronize()
