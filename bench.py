@@ -52,9 +52,16 @@ def parse_args(argv=None):
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own CUDA build (baseline/_ref) on this GPU")
     ap.add_argument("--only-f32", action="store_true", help="FP32 storage only (no FP64 run, no e2e): profiling")
-    ap.add_argument("--case", choices=["main", "adjoint", "ensemble", "mpi"], default="main",
+    ap.add_argument("--only-f64", action="store_true",
+                    help="the FP64 time loop and stage timings only (one JSON line): profiling")
+    ap.add_argument("--case", choices=["main", "adjoint", "ensemble", "mpi", "stage"], default="main",
                     help="profiling cases: the reverse-mode, the ensemble or the vlp4d_mpi arm alone "
-                         "(--steps steps, --members members, default tiles; --n for mpi), one JSON line")
+                         "(--steps steps, --members members, default tiles; --n for mpi), or one stage entry "
+                         "point (--stage, --dtype, --n; --steps calls after one field solve), one JSON line")
+    ap.add_argument("--stage", default="advect_xyxy",
+                    choices=["advect_x", "advect_y", "advect_vx", "advect_vy", "advect_xy", "advect_vxvy",
+                             "advect_xyxy", "field_rho"], help="stage entry point for --case stage")
+    ap.add_argument("--dtype", choices=["f32", "f64"], default="f32", help="storage for --case stage")
     ap.add_argument("--members", type=int, default=256, help="ensemble members for --case ensemble")
     ap.add_argument("--replicas", action="store_true",
                     help="N > 1: independent copies of the single-GPU workload instead of one run cut into vy slabs")
@@ -235,7 +242,7 @@ def gpu_arm(args, ranks):
     sampler.start()
 
     per_dtype = {}
-    for dtype in (("f32",) if args.only_f32 else ("f32", "f64")):
+    for dtype in (("f32",) if args.only_f32 else ("f64",) if args.only_f64 else ("f32", "f64")):
         with pkg.Context(dom, dtype) as ctx:
             fa, fb = ctx.empty_f(), ctx.empty_f()
             ctx.init_case(fa, v.IC_LANDAU_SUM, 0.05, 0.5)
@@ -298,6 +305,12 @@ def gpu_arm(args, ranks):
             torch.cuda.empty_cache()
 
     clocks = sampler.stop()
+    if args.only_f64:
+        rec = per_dtype["f64"]
+        return {"metric": METRIC, "value": rec["value"], "unit": METRIC, "n_gpus": ranks.world, "steps": K,
+                "warmup": W, "ms_per_step": rec["ms_per_step"], "higher_is_better": True, "dtype": "f64",
+                "profiling": "FP64 arm only", "config": {"workload": WORKLOAD, "grid": [n] * 4, "dt": DT},
+                "stages": rec["stages"], "gpu_launches": rec["launches"], "clocks": clocks}
 
     # Roofline of the dominant kernel of the time loop.  Each step between
     # the first and the last runs one k_plane_xyxy pass (two x/y half steps)
@@ -466,6 +479,28 @@ def slab_arm(args, ranks):
     del own, h0, hout
     ctx.close()
     return line
+
+
+def stage_arm(pkg, torch, stream, stage, dtype, n, calls):
+    """One stage entry point on the Landau n^4 state after one field solve
+    (the x/y shifts by dt/2, the v shifts by dt, as in a step), `calls`
+    calls: a short, self-contained command for profiling one kernel."""
+    v = pkg.vlp4d
+    dom = pkg.landau_domain(n, dt=DT, nbiter=4, L=L_BOX, vmax=VMAX)
+    with pkg.Context(dom, dtype) as ctx:
+        a, b = ctx.empty_f(), ctx.empty_f()
+        ctx.init_case(a, v.IC_LANDAU_SUM, 0.05, 0.5)
+        ctx.field_rho(a)
+        ctx.field_poisson()
+        fn = getattr(ctx, stage)
+        dt = DT if stage in ("advect_vx", "advect_vy", "advect_vxvy") else 0.5 * DT
+        call = (lambda: fn(a)) if stage == "field_rho" else (lambda: fn(a, b, dt))
+        t = time_calls(torch, stream, call, max(calls, 1))
+        ctx.check()
+    elem = 4 if dtype == "f32" else 8
+    moved = (1 if stage == "field_rho" else 2) * dom.cells * elem
+    return {"stage": stage, "dtype": dtype, "grid": [n] * 4, "calls": calls, "ms": t * 1e3,
+            "gbs": moved / t / 1e9}
 
 
 ERROR_STEPS = 100
@@ -883,6 +918,8 @@ def main(argv=None):
             if not args.no_cpu_baseline:
                 _set_omp_env()
                 out["cpu_baseline"] = mpi_reference_cpu(32)
+        elif args.case == "stage":
+            out = stage_arm(pkg, torch, stream, args.stage, args.dtype, args.n, args.steps)
         else:
             out = ensemble_arm(pkg, torch, stream, peak, nruns=args.members, nsteps=args.steps, autotune=False)
         print(json.dumps({"case": args.case, **out}), flush=True)
