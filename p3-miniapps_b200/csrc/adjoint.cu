@@ -480,16 +480,6 @@ int launch_vgrad(vlp4d_adjoint *A, const void *a, const void *lb, cudaStream_t s
   if (nseg > A->gsegs) nseg = A->gsegs;
   const int Q = (nvy + nseg - 1) / nseg;
   nseg = (nvy + Q - 1) / Q;
-  {  // The slab pipeline where the shape fits.
-    int ns = 0;
-    const int rc = launch_vgrad_slab(c, a, lb, &c->tab_vx, &c->tab_vy, A->dw_vx, A->dw_vy, A->gpart, A->gsegs, &ns, s);
-    if (rc == VLP4D_OK) {
-      k_vgrad_finish<<<(nxy + 255) / 256, 256, 0, s>>>(A->gpart, ns, nxy, A->gex, A->gey);
-      VLP4D_LAUNCH_CHECK();
-      return VLP4D_OK;
-    }
-    if (rc != VLP4D_ERR_UNSUPPORTED) return rc;
-  }
   // Shared-tap kernel: V vx rows per thread (4 in FP32, 2 in FP64), nvx/V
   // threads per column, as many columns per block as fit 512 threads.
   const int V = c->dtype == VLP4D_F32 ? 4 : 2;

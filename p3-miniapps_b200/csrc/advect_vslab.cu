@@ -350,203 +350,6 @@ __global__ void k_vspan(const int *__restrict__ mvy, int nchunks, int C, int nvy
   span[cc] = make_int2(lo, hi);
 }
 
-// The reverse mode's field gradient through the vx/vy pass, from its input
-// a and the adjoint lb of its output: for every column ixy
-//   gEx = sum_{ivx, ivy} lb(ivx, ivy) sum_k wy_k B(ivx, ivy + oy + k),
-//   gEy = sum_{ivx, ivy} lb(ivx, ivy) sum_k dwy_k A(ivx, ivy + oy + k),
-// A the vx sweep of a (weights wx), B its derivative in Ex (weights dwx),
-// dwy the vy weights' derivative in Ey.  The slabs of a stream through the
-// same TMA ring, cursor and per-warp release as k_vslab's (items: C columns
-// x Q output vy rows); each thread owns one column and V consecutive vx,
-// takes its V + 5 vx taps of a slab from shared memory, keeps six rows of A
-// and B, and for every output row multiplies with lb, whose values it loads
-// two slabs ahead.  Stencil sums in the element type, the products with lb
-// and the accumulation in FP64; at the end of an item the vx groups of each
-// column are added in a fixed order into the item's partial (one per vy
-// segment and column), which k_vgrad_finish adds in segment order.
-struct VgradArgs {
-  VslabArgs v;  // ring, items, span, tables (v.tvx, v.tvy: the forward v tables)
-  const void *lb;
-  const double *dwx, *dwy;
-  double *part;
-};
-
-template <typename T, int V>
-__global__ void __launch_bounds__(512) k_vgrad_slab(const __grid_constant__ CUtensorMap tin, VgradArgs g) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  unsigned char *smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
-  const VslabArgs &a = g.v;
-  const int C = a.C, nvx = a.nvx, S = a.stages;
-  const size_t slab_elems = (size_t)C * nvx;
-  const uint32_t slab_bytes = (uint32_t)(slab_elems * sizeof(T));
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
-  int *released = reinterpret_cast<int *>(smem + 8 * kMaxStages);
-  int *issued = released + kMaxStages;
-  T *slabs = reinterpret_cast<T *>(smem + kBarBytes);
-  double *red = reinterpret_cast<double *>(slabs + (size_t)S * slab_elems);  // [2][groups][C]
-  const int col = threadIdx.x % C;
-  const int grp = threadIdx.x / C;
-  const int groups = blockDim.x / C;
-  const int vx0 = grp * V;
-  const int lane = threadIdx.x & 31;
-  const int nwarps = blockDim.x >> 5;
-
-  if (threadIdx.x == 0) {
-    for (int st = 0; st < S; ++st) {
-      mbar_init(&bars[st], 1);
-      released[st] = 0;
-    }
-    mbar_fence_init();
-  }
-  __syncthreads();
-
-  SlabCursor ahead;
-  ahead.item = blockIdx.x;
-  ahead.t = 0;
-  cursor_item<true>(a, ahead);
-  if (threadIdx.x == 0) {
-    int n = 0;
-    for (; n < S && ahead.item < a.nitems; ++n) {
-      issue_slab(&tin, a, ahead, slabs, bars, n, slab_elems, slab_bytes);
-      cursor_next<true>(a, ahead);
-    }
-    *issued = n;
-  } else {
-    for (int n = 0; n < S && ahead.item < a.nitems; ++n) cursor_next<true>(a, ahead);
-  }
-
-  const long long vstride = a.nxy, ystride = vstride * nvx;
-  const T *lbp = static_cast<const T *>(g.lb);
-  long long k = 0;
-  int slot = 0;
-  uint32_t parity = 0;
-  for (long long item = blockIdx.x; item < a.nitems; item += gridDim.x) {
-    SlabCursor cur;
-    cur.item = item;
-    cur.t = 0;
-    cursor_item<true>(a, cur);
-    const int cnt = cur.cnt, cc = cur.cc;
-    const int sg = (int)(item % a.nseg);
-    const long long ixy = (long long)cc * C + col;
-    T wx[6], dx[6], wy[6], dy[6];
-#pragma unroll
-    for (int q = 0; q < 6; ++q) {
-      wx[q] = (T)__ldg(a.tvx.w + 6 * ixy + q);
-      dx[q] = (T)__ldg(g.dwx + 6 * ixy + q);
-      wy[q] = (T)__ldg(a.tvy.w + 6 * ixy + q);
-      dy[q] = (T)__ldg(g.dwy + 6 * ixy + q);
-    }
-    int off[V + 5];
-    {
-      int j = vx0 + __ldg(a.tvx.m + ixy);
-      if (j >= nvx) j -= nvx;
-#pragma unroll
-      for (int q = 0; q < V + 5; ++q) {
-        off[q] = j * C + col;
-        if (++j == nvx) j = 0;
-      }
-    }
-    const int lag0 = 5 + signed_offset(__ldg(a.tvy.m + ixy), a.nvy) - a.span[cc].x;
-    // lb of this thread's output row e (slab t = e + lag0) sits in lq[t % 3];
-    // it is loaded two slabs ahead.
-    const T *lcol = lbp + ixy + vstride * vx0 + ystride * (long long)sg * a.Q;
-    T lq[3][V];
-    auto load_lb = [&](int t, T (&dst)[V]) {
-      const int e = t - lag0;
-      if (e >= 0 && e < a.Q) {
-        const T *pl = lcol + ystride * e;
-#pragma unroll
-        for (int i = 0; i < V; ++i) dst[i] = __ldg(pl + vstride * i);
-      }
-    };
-    load_lb(0, lq[0]);
-    load_lb(1, lq[1]);
-    T A[6][V], B[6][V];
-#pragma unroll
-    for (int j = 0; j < 6; ++j)
-#pragma unroll
-      for (int i = 0; i < V; ++i) A[j][i] = B[j][i] = T(0);
-    double gx = 0., gy = 0.;
-
-    for (int t0 = 0; t0 < cnt; t0 += 6) {
-#pragma unroll
-      for (int u = 0; u < 6; ++u) {
-        const int t = t0 + u;
-        if (t >= cnt) break;  // uniform over the CTA
-        if (!mbar_wait_bounded(&bars[slot], parity)) {
-          vslab_abort(a, bars, issued, k, S);
-          return;
-        }
-        const T *sl = slabs + (size_t)slot * slab_elems;
-        {
-          T tap[V + 5];
-#pragma unroll
-          for (int q = 0; q < V + 5; ++q) tap[q] = sl[off[q]];
-#pragma unroll
-          for (int i = 0; i < V; ++i) {
-            T sa = wx[0] * tap[i], sb = dx[0] * tap[i];
-#pragma unroll
-            for (int q = 1; q < 6; ++q) {
-              sa = fma(wx[q], tap[i + q], sa);
-              sb = fma(dx[q], tap[i + q], sb);
-            }
-            A[u][i] = sa;
-            B[u][i] = sb;
-          }
-        }
-        __syncwarp();
-        if (lane == 0) {
-          __threadfence_block();
-          if (atomicAdd(&released[slot], 1) == nwarps - 1) {
-            released[slot] = 0;
-            __threadfence_block();
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            if (ahead.item < a.nitems) {
-              issue_slab(&tin, a, ahead, slabs, bars, slot, slab_elems, slab_bytes);
-              atomicAdd(issued, 1);
-            }
-          }
-        }
-        cursor_next<true>(a, ahead);
-        load_lb(t + 2, lq[(u + 2) % 3]);
-        const int e = t - lag0;
-        if (e >= 0 && e < a.Q) {  // rows t-5 .. t sit in slots u+1 .. u+6 (mod 6)
-#pragma unroll
-          for (int i = 0; i < V; ++i) {
-            T sx = wy[0] * B[(u + 1) % 6][i], sy = dy[0] * A[(u + 1) % 6][i];
-#pragma unroll
-            for (int q = 1; q < 6; ++q) {
-              sx = fma(wy[q], B[(u + 1 + q) % 6][i], sx);
-              sy = fma(dy[q], A[(u + 1 + q) % 6][i], sy);
-            }
-            gx = fma((double)lq[u % 3][i], (double)sx, gx);
-            gy = fma((double)lq[u % 3][i], (double)sy, gy);
-          }
-        }
-        ++k;
-        if (++slot == S) {
-          slot = 0;
-          parity ^= 1u;
-        }
-      }
-    }
-    // The vx groups of each column in a fixed order.
-    red[grp * C + col] = gx;
-    red[(groups + grp) * C + col] = gy;
-    __syncthreads();
-    if (grp == 0) {
-      double sx = 0., sy = 0.;
-      for (int q = 0; q < groups; ++q) {
-        sx += red[q * C + col];
-        sy += red[(groups + q) * C + col];
-      }
-      g.part[(2LL * sg) * a.nxy + ixy] = sx;
-      g.part[(2LL * sg + 1) * a.nxy + ixy] = sy;
-    }
-    __syncthreads();
-  }
-}
-
 }  // namespace
 }  // namespace vlp4d
 
@@ -723,94 +526,6 @@ int launch_advect_vxvy_tables(vlp4d_ctx *c, const void *fn, void *fnp1, const St
     VLP4D_VS(float, false, true, 8);
   }
 #undef VLP4D_VS
-}
-
-// The field-gradient pass (k_vgrad_slab) for the reverse mode: partials of
-// gEx, gEy per vy segment into part ([2 * seg + {0, 1}][nxy]); *nseg_out
-// receives the segment count (at most max_segs).  VLP4D_ERR_UNSUPPORTED
-// (nothing launched) when the shape does not fit the slab configuration.
-int launch_vgrad_slab(vlp4d_ctx *c, const void *a, const void *lb, const StencilTable *tvx, const StencilTable *tvy,
-                      const double *dwx, const double *dwy, double *part, int max_segs, int *nseg_out,
-                      cudaStream_t s) {
-  if (!c->fused || c->slab) return VLP4D_ERR_UNSUPPORTED;
-  if (((uintptr_t)a & 15) || ((uintptr_t)lb & 15)) return VLP4D_ERR_UNSUPPORTED;
-  if (env_int("VLP4D_VGRAD_SLAB", 1) == 0) return VLP4D_ERR_UNSUPPORTED;
-  PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
-  if (!encode) return VLP4D_ERR_UNSUPPORTED;
-  const long long nxy = c->g.nxy();
-  const int nvx = c->g.n[2], nvy = c->g.n[3];
-  const bool f32 = c->dtype == VLP4D_F32;
-  const size_t elem = c->elem;
-  // V vx outputs per thread: 2 in FP32, 1 in FP64 (a thread keeps 6 x V
-  // rows of A and of B, its V + 5 taps and 24 weights in registers).
-  const int V = f32 ? 2 : 1;
-  if (nvx % V || nvx < 8) return VLP4D_ERR_UNSUPPORTED;
-  // Columns per chunk: 128 bytes of a slab row, fewer while the block would
-  // exceed 512 threads (16 bytes at least, the tensor copy's granule).
-  int C = (int)(128 / elem);
-  while (C * (nvx / V) > 512 && C * elem > 16) C /= 2;
-  const int threads = C * (nvx / V);
-  if (threads > 512 || threads % 32 || nxy % C) return VLP4D_ERR_UNSUPPORTED;
-  const int nchunks = (int)(nxy / C);
-  if (nchunks > c->vspan_cap) return VLP4D_ERR_UNSUPPORTED;
-  // vy segments: enough items to give every SM at least two, each item
-  // re-reading the five halo slabs of its segment.
-  int nseg = 1;
-  while (nseg < max_segs && nseg < nvy && (long long)nchunks * nseg < 2LL * c->num_sms) ++nseg;
-  int Q = (nvy + nseg - 1) / nseg;
-  while (nvy % Q) ++Q;  // Q divides nvy
-  nseg = nvy / Q;
-  if (nseg > max_segs) return VLP4D_ERR_UNSUPPORTED;
-  int stages = env_int("VLP4D_VGRAD_STAGES", 8);
-  if (stages < 2 || stages > kMaxStages) return VLP4D_ERR_UNSUPPORTED;
-  const size_t smem = 128 + kBarBytes + (size_t)stages * C * nvx * elem + 2 * sizeof(double) * threads;
-  if (smem > 200 * 1024) return VLP4D_ERR_UNSUPPORTED;
-
-  CUtensorMap map;
-  cuuint64_t dims[3] = {(cuuint64_t)nxy, (cuuint64_t)nvx, (cuuint64_t)nvy};
-  cuuint64_t strides[2] = {(cuuint64_t)(nxy * elem), (cuuint64_t)(nxy * nvx * elem)};
-  cuuint32_t box[3] = {(cuuint32_t)C, (cuuint32_t)nvx, 1};
-  cuuint32_t estr[3] = {1, 1, 1};
-  CUresult r = encode(&map, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
-                      const_cast<void *>(a), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return VLP4D_ERR_UNSUPPORTED;
-  k_vspan<<<(nchunks + 127) / 128, 128, 0, s>>>(tvy->m, nchunks, C, nvy, c->vspan);
-  VLP4D_LAUNCH_CHECK();
-  VgradArgs g;
-  VslabArgs &v = g.v;
-  v.fout = nullptr;
-  v.nxy = (int)nxy;
-  v.nvx = nvx;
-  v.nvy = nvy;
-  v.row0 = -1;
-  v.nin = nvy;
-  v.C = C;
-  v.Q = Q;
-  v.nseg = nseg;
-  v.nitems = (long long)nchunks * nseg;
-  v.stages = stages;
-  v.tvx = *tvx;
-  v.tvy = *tvy;
-  v.span = c->vspan;
-  v.err = c->d_err;
-  v.bias = nullptr;
-  v.bias_scale = 0.;
-  g.lb = lb;
-  g.dwx = dwx;
-  g.dwy = dwy;
-  g.part = part;
-  auto kern = f32 ? k_vgrad_slab<float, 2> : k_vgrad_slab<double, 1>;
-  VLP4D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int per_sm = 0;
-  VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
-  if (per_sm < 1) return VLP4D_ERR_UNSUPPORTED;
-  long long grid = (long long)per_sm * c->num_sms;
-  if (grid > v.nitems) grid = v.nitems;
-  kern<<<(unsigned)grid, threads, smem, s>>>(map, g);
-  VLP4D_LAUNCH_CHECK();
-  *nseg_out = nseg;
-  return VLP4D_OK;
 }
 
 }  // namespace vlp4d

@@ -210,13 +210,6 @@ int launch_advect_vxvy_tables(vlp4d_ctx *c, const void *fn, void *fnp1, const St
                               double bias_scale = 0.0);
 int launch_advect_xyxy(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *tx, const StencilTable *ty,
                        cudaStream_t s);
-// The reverse mode's field gradient through the vx/vy pass (k_vgrad_slab):
-// per vy segment, partials of gEx and gEy into part[(2 seg + {0,1}) nxy];
-// the segment count into *nseg_out.  VLP4D_ERR_UNSUPPORTED when the shape
-// does not fit (the caller then runs its gather kernel).
-int launch_vgrad_slab(vlp4d_ctx *c, const void *a, const void *lb, const StencilTable *tvx, const StencilTable *tvy,
-                      const double *dwx, const double *dwy, double *part, int max_segs, int *nseg_out,
-                      cudaStream_t s);
 // Whether the FP64 form of the joined pass (k_plane_xyxy64, row widths a
 // warp holds whole) runs for this context.
 bool xyxy64_available(const vlp4d_ctx *c);
