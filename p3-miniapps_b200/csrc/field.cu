@@ -7,6 +7,7 @@
 // Diags::compute (diags.cpp:13-55), initcase (init.cpp:118-285),
 // Impl::Transpose (lib/Cuda_Transpose.hpp:18-136).
 #include "internal.cuh"
+#include "moment.cuh"
 #include "tma.cuh"
 
 namespace vlp4d {
@@ -30,23 +31,10 @@ __global__ void k_rho_partial(const T *__restrict__ f, double *__restrict__ part
   part[(long long)g * nxy + ixy] = s;
 }
 
-__global__ void k_rho_finish(const double *__restrict__ part, double *__restrict__ rho, long long nxy, int groups,
-                             double dvx, double dvy) {
-  const long long ixy = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (ixy >= nxy) return;
-  // Groups added in order; the loads of 16 groups are issued before their
-  // adds so that their latencies overlap.
-  double s = 0.0;
-  int g = 0;
-  for (; g + 16 <= groups; g += 16) {
-    double v[16];
-#pragma unroll
-    for (int k = 0; k < 16; ++k) v[k] = part[(long long)(g + k) * nxy + ixy];
-#pragma unroll
-    for (int k = 0; k < 16; ++k) s += v[k];
-  }
-  for (; g < groups; ++g) s += part[(long long)g * nxy + ixy];
-  rho[ixy] = s * dvx * dvy;  // field.cpp:23 (sum * dvx * dvy)
+__global__ void __launch_bounds__(kMomentCells * kMomentSlices)
+    k_rho_finish(const double *__restrict__ part, double *__restrict__ rho, long long nxy, int groups, double dvx,
+                 double dvy) {
+  moment_finish(part, rho, nxy, groups, dvx, dvy);
 }
 
 // ---- field_poisson pieces.
@@ -301,9 +289,8 @@ int launch_field_rho(vlp4d_ctx *c, const void *fn, cudaStream_t s) {
 
 int launch_rho_finish(vlp4d_ctx *c, int groups, cudaStream_t s) {
   const long long nxy = c->g.nxy();
-  const int threads = 256;
-  k_rho_finish<<<(unsigned)((nxy + threads - 1) / threads), threads, 0, s>>>(c->rho_part, c->rho, nxy, groups,
-                                                                              c->g.dx[2], c->g.dx[3]);
+  k_rho_finish<<<(unsigned)((nxy + kMomentCells - 1) / kMomentCells), kMomentCells * kMomentSlices, 0, s>>>(
+      c->rho_part, c->rho, nxy, groups, c->g.dx[2], c->g.dx[3]);
   VLP4D_LAUNCH_CHECK();
   return VLP4D_OK;
 }

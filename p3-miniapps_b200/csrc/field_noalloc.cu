@@ -29,6 +29,7 @@
 #include <mutex>
 
 #include "internal.cuh"
+#include "moment.cuh"
 
 namespace vlp4d {
 
@@ -84,13 +85,11 @@ __global__ void k_noalloc_rho_partial(const T *__restrict__ f, double *__restric
   part[(long long)g * nxy + ixy] = s;
 }
 
-__global__ void k_noalloc_rho_finish(const double *__restrict__ part, double *__restrict__ rho, long long nxy,
-                                     int groups, double dvx, double dvy) {
-  const long long ixy = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (ixy >= nxy) return;
-  double s = 0.0;
-  for (int g = 0; g < groups; ++g) s += part[(long long)g * nxy + ixy];
-  rho[ixy] = s * dvx * dvy;
+// The same fixed-order second stage as the context's (moment.cuh).
+__global__ void __launch_bounds__(kMomentCells * kMomentSlices)
+    k_noalloc_rho_finish(const double *__restrict__ part, double *__restrict__ rho, long long nxy, int groups,
+                         double dvx, double dvy) {
+  moment_finish(part, rho, nxy, groups, dvx, dvy);
 }
 
 }  // namespace
@@ -142,8 +141,8 @@ extern "C" int vlp4d_field_rho_noalloc(const void *fn, int dtype, int nx, int ny
   else
     k_noalloc_rho_partial<float><<<grid, threads, 0, s>>>((const float *)fn, part, nxy, nv, (int)groups);
   VLP4D_LAUNCH_CHECK();
-  k_noalloc_rho_finish<<<(unsigned)((nxy + threads - 1) / threads), threads, 0, s>>>(part, rho, nxy, (int)groups,
-                                                                                      dvx, dvy);
+  k_noalloc_rho_finish<<<(unsigned)((nxy + kMomentCells - 1) / kMomentCells), kMomentCells * kMomentSlices, 0, s>>>(
+      part, rho, nxy, (int)groups, dvx, dvy);
   VLP4D_LAUNCH_CHECK();
   return VLP4D_OK;
 }
