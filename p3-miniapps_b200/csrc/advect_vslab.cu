@@ -113,12 +113,15 @@ __device__ __forceinline__ void cursor_next(const VslabArgs &a, SlabCursor &c) {
   }
 }
 
-template <typename T>
+// SLAB: the input rows of a slab context (owned planes and halos, never
+// wrapped); otherwise periodic rows.  A separate instantiation, so that the
+// periodic kernels carry none of the slab arithmetic.
+template <typename T, bool SLAB = false>
 __device__ __forceinline__ void issue_slab(const CUtensorMap *tin, const VslabArgs &a, const SlabCursor &c,
                                            T *slabs, uint64_t *bars, int slot, size_t slab_elems,
                                            uint32_t slab_bytes) {
   int row = c.start + c.t;
-  if (a.row0 < 0) {
+  if constexpr (!SLAB) {
     row %= a.nvy;
     if (row < 0) row += a.nvy;
   } else {
@@ -134,7 +137,7 @@ __device__ __forceinline__ void issue_slab(const CUtensorMap *tin, const VslabAr
 
 // NXY: compile-time nx*ny (0 = read a.nxy at run time); with it the V output
 // stores of a thread use immediate offsets.
-template <typename T, bool DVX, bool DVY, int V, int NXY, bool BIAS = false>
+template <typename T, bool DVX, bool DVY, int V, int NXY, bool BIAS = false, bool SLAB = false>
 __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorMap tin, VslabArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // Tensor-copy destinations on a 128-byte boundary whatever the base
@@ -169,7 +172,7 @@ __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorM
   if (threadIdx.x == 0) {
     int n = 0;
     for (; n < S && ahead.item < a.nitems; ++n) {
-      issue_slab(&tin, a, ahead, slabs, bars, n, slab_elems, slab_bytes);
+      issue_slab<T, SLAB>(&tin, a, ahead, slabs, bars, n, slab_elems, slab_bytes);
       cursor_next<DVY>(a, ahead);
     }
     *issued = n;
@@ -281,7 +284,7 @@ __global__ void __launch_bounds__(512) k_vslab(const __grid_constant__ CUtensorM
             __threadfence_block();
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             if (ahead.item < a.nitems) {
-              issue_slab(&tin, a, ahead, slabs, bars, slot, slab_elems, slab_bytes);
+              issue_slab<T, SLAB>(&tin, a, ahead, slabs, bars, slot, slab_elems, slab_bytes);
               atomicAdd(issued, 1);
             }
           }
@@ -431,9 +434,9 @@ bool vslab_config(const vlp4d_ctx *c, bool both, VslabCfg &cfg) {
   return cfg.smem <= 200 * 1024;
 }
 
-template <typename T, bool DVX, bool DVY, int V, int NXY, bool BIAS = false>
+template <typename T, bool DVX, bool DVY, int V, int NXY, bool BIAS = false, bool SLAB = false>
 int run_vslab(vlp4d_ctx *c, const CUtensorMap &map, const VslabArgs &args, const VslabCfg &cfg, cudaStream_t s) {
-  auto kern = k_vslab<T, DVX, DVY, V, NXY, BIAS>;
+  auto kern = k_vslab<T, DVX, DVY, V, NXY, BIAS, SLAB>;
   VLP4D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
   int per_sm = 0;
   VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, cfg.threads, cfg.smem));
@@ -510,6 +513,15 @@ int launch_advect_vxvy_tables(vlp4d_ctx *c, const void *fn, void *fnp1, const St
     case 16384: return run_vslab<T, DVX, DVY, V, 16384>(c, map, a, cfg, s);      \
     case 4096: return run_vslab<T, DVX, DVY, V, 4096>(c, map, a, cfg, s);        \
     default: return run_vslab<T, DVX, DVY, V, 0>(c, map, a, cfg, s);             \
+  }
+  if (slab_in) {  // slab contexts: rows of the owned planes and halos
+    if (bias) return VLP4D_ERR_UNSUPPORTED;
+    if (c->dtype == VLP4D_F64) {
+      if (do_vx) return run_vslab<double, true, true, 4, 0, false, true>(c, map, a, cfg, s);
+      return run_vslab<double, false, true, 4, 0, false, true>(c, map, a, cfg, s);
+    }
+    if (do_vx) return run_vslab<float, true, true, 8, 0, false, true>(c, map, a, cfg, s);
+    return run_vslab<float, false, true, 8, 0, false, true>(c, map, a, cfg, s);
   }
   if (bias) {  // the reverse mode's vx+vy pass with the per-column term
     if (!(do_vx && do_vy)) return VLP4D_ERR_UNSUPPORTED;
