@@ -488,10 +488,27 @@ int launch_vgrad(vlp4d_adjoint *A, const void *a, const void *lb, cudaStream_t s
     int cw = 512 / gy;
     if (cw > 32) cw = 32;
     const int bxv = (nxy + cw - 1) / cw;
-    int ns = (2 * c->num_sms + bxv - 1) / bxv;
-    if (ns < 1) ns = 1;
-    if (ns > nvy) ns = nvy;
-    if (ns > A->gsegs) ns = A->gsegs;
+    // vy segments: a block streams Qv + 5 rows of its segment, one block per
+    // SM at a time, so the pass takes about ceil(blocks / SMs) * (Qv + 5)
+    // row times; the segment count minimises that among those that give
+    // every SM a block (VLP4D_VGRAD_SEGS overrides).
+    int ns = 0;
+    {
+      long long best = -1;
+      const int forced = getenv("VLP4D_VGRAD_SEGS") ? atoi(getenv("VLP4D_VGRAD_SEGS")) : 0;
+      for (int k = 1; k <= nvy && k <= A->gsegs; ++k) {
+        const int q = (nvy + k - 1) / k;
+        if ((nvy + q - 1) / q != k) continue;  // the same segments as a smaller count
+        const long long blocks = (long long)bxv * k;
+        if (forced ? k != forced : (blocks < c->num_sms && k < nvy && k < A->gsegs)) continue;
+        const long long cost = (blocks + c->num_sms - 1) / c->num_sms * (q + 5);
+        if (best < 0 || cost < best) {
+          best = cost;
+          ns = k;
+        }
+      }
+      if (!ns) ns = 1;
+    }
     const int Qv = (nvy + ns - 1) / ns;
     ns = (nvy + Qv - 1) / Qv;
     dim3 gridv(bxv, ns), blockv(cw, gy);

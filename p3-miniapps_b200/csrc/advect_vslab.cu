@@ -387,16 +387,17 @@ struct VslabCfg {
 };
 
 // C*elem = 128 bytes per slab row (64 when nvx > 128), V vx per thread,
-// 512 threads.  Q output rows per item: each item re-reads the 5 + spread
-// halo slabs of its vy segment (4% at Q = 128, 8% at 64), so Q is the
-// tallest segment that still leaves six items per SM (at 128^4: 64 in FP32,
-// 128 in FP64, whose chunks are half as wide).  Stages as measured best at
+// 512 threads.  Q output rows per item (the segment height, below): each
+// item re-reads the 5 + spread halo slabs of its vy segment (4% at Q = 128,
+// 8% at 64; at 128^4: 64 in FP32, 128 in FP64, whose chunks are half as
+// wide).  Stages as measured best at
 // 128^4: 8 for the FP32 vx+vy pass (one 512-thread CTA per SM, by
 // registers), 4 for a single FP32 direction (lighter threads: four stages
 // leave room for several CTAs per SM; 0.46 -> 0.38 ms for vx, 0.50 -> 0.41
 // ms for vy), 4 in FP64.  VLP4D_VSLAB_Q and VLP4D_VSLAB_STAGES override for
 // tuning sweeps.
-bool vslab_config(const vlp4d_ctx *c, bool both, VslabCfg &cfg) {
+bool vslab_config(const vlp4d_ctx *c, bool do_vx, bool do_vy, VslabCfg &cfg) {
+  const bool both = do_vx && do_vy;
   const long long nxy = c->g.nxy();
   const int nvx = c->g.n[2], nvy = c->g.n[3];
   const bool f32 = c->dtype == VLP4D_F32;
@@ -413,17 +414,30 @@ bool vslab_config(const vlp4d_ctx *c, bool both, VslabCfg &cfg) {
   // Whole warps only: every warp releases each slab once, and the last of
   // blockDim/32 releases refills it.
   if (cfg.threads > 512 || cfg.threads < 32 || cfg.threads % 32) return false;
-  // Q: the tallest vy segment (fewest halo re-reads) that still leaves at
-  // least six items per SM.
+  // Q: the vy segment height.  A CTA streams its items one after another,
+  // each item Q output rows plus (with a vy sweep) the five halo rows and
+  // the chunk's offset spread, about Q + 6 slabs; with one CTA per SM the
+  // pass takes about ceil(items / SMs) * (Q + 6) slab times.  Q minimises
+  // that among the divisors of nvy up to 128 that still give every SM an
+  // item (the smallest Q when none does).  128^4 FP32: Q = 64 (1024 items,
+  // 7 per SM); 64^4 FP32: Q = 32 (60.8 -> 47.6 us for vx+vy against Q = 8).
   const long long nchunks = nxy / cfg.C;
   int Q = env_int("VLP4D_VSLAB_Q", 0);
   if (Q <= 0) {
-    Q = 1;
-    for (int q = nvy < 128 ? nvy : 128; q >= 1; --q)
-      if (nvy % q == 0 && (nchunks * (nvy / q) >= 6LL * c->num_sms || q == 1)) {
+    Q = 0;
+    long long best = -1;
+    const int halo = do_vy ? 6 : 0;
+    for (int q = nvy < 128 ? nvy : 128; q >= 1; --q) {
+      if (nvy % q) continue;
+      const long long items = nchunks * (nvy / q);
+      if (items < c->num_sms && q != 1) continue;
+      const long long cost = (items + c->num_sms - 1) / c->num_sms * (q + halo);
+      if (best < 0 || cost < best) {
+        best = cost;
         Q = q;
-        break;
       }
+    }
+    if (!Q) Q = 1;
   }
   if (Q > nvy) Q = nvy;
   while (Q > 1 && nvy % Q) --Q;
@@ -461,7 +475,7 @@ int launch_advect_vxvy_tables(vlp4d_ctx *c, const void *fn, void *fnp1, const St
   if (((uintptr_t)fn & 15) || ((uintptr_t)fnp1 & 15)) return VLP4D_ERR_UNSUPPORTED;
   if (!do_vx && !do_vy) return VLP4D_ERR_UNSUPPORTED;
   VslabCfg cfg;
-  if (!vslab_config(c, do_vx && do_vy, cfg)) return VLP4D_ERR_UNSUPPORTED;
+  if (!vslab_config(c, do_vx, do_vy, cfg)) return VLP4D_ERR_UNSUPPORTED;
   PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
   if (!encode) return VLP4D_ERR_UNSUPPORTED;
   const long long nxy = c->g.nxy();
