@@ -100,6 +100,9 @@ void free_ctx(vlp4d_ctx *c) {
     cudaFree(t->wf);
   }
   if (c->h_diag) cudaFreeHost(c->h_diag);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->side) cudaStreamDestroy(c->side);
   delete c;
 }
 
@@ -259,6 +262,10 @@ int vlp4d_ctx_create(const vlp4d_domain *dom, int dtype, vlp4d_ctx **out) {
   c->plans = true;
   if (cudaMallocHost(&c->h_diag, sizeof(double) * 2 * c->hist_len) != cudaSuccess)
     return bail(fail(VLP4D_ERR_CUDA, "cudaMallocHost failed"));
+  if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess)
+    return bail(fail(VLP4D_ERR_CUDA, "stream/event creation failed"));
   *out = c;
   return VLP4D_OK;
 }
@@ -563,13 +570,15 @@ int step_impl(vlp4d_ctx *ctx, const void *f_in, void *f_out, void *scratch, int 
   int rc;
   // timestep.hpp:17-28: x(dt/2), y(dt/2) and the moment of the result.
   if ((rc = advect_xy_impl(ctx, f_in, f_out, 0.5 * dt, true, s))) return rc;
-  // timestep.hpp:30-38: field solve and the mid-step diagnostic.
+  // timestep.hpp:30-38: field solve and the mid-step diagnostic (beside
+  // the v pass, on the side stream).
   if ((rc = launch_field_poisson(ctx, s))) return rc;
-  if (iter >= 0 && (rc = launch_diags(ctx, iter, s))) return rc;
+  if (iter >= 0 && (rc = diags_async(ctx, iter, s))) return rc;
   // timestep.hpp:40-48: vx(dt), vy(dt).
   if ((rc = advect_vxvy_impl(ctx, f_out, scratch, dt, s))) return rc;
   // timestep.hpp:50-58: x(dt/2), y(dt/2).
-  return advect_xy_impl(ctx, scratch, f_out, 0.5 * dt, false, s);
+  if ((rc = advect_xy_impl(ctx, scratch, f_out, 0.5 * dt, false, s))) return rc;
+  return iter >= 0 ? diags_join(ctx, s) : VLP4D_OK;
 }
 
 int advect_xy_moment(vlp4d_ctx *ctx, const void *fn, void *fnp1, double dt, cudaStream_t s) {
@@ -639,11 +648,15 @@ int vlp4d_steps(vlp4d_ctx *ctx, void *f_state, void *f_next, int iter0, int nste
   if ((rc = advect_xy_impl(ctx, cur, oth, 0.5 * dt, true, s))) return rc;
   std::swap(cur, oth);
   for (int k = 0; k < nsteps; ++k) {
-    // timestep.hpp:30-48: field solve, diagnostic, vx/vy full step.
+    // timestep.hpp:30-48: field solve, diagnostic (on the side stream,
+    // beside the v pass), vx/vy full step.
     if ((rc = launch_field_poisson(ctx, s))) return rc;
-    if ((rc = launch_diags(ctx, iter0 + k, s))) return rc;
+    if ((rc = diags_async(ctx, iter0 + k, s))) return rc;
     if ((rc = advect_vxvy_impl(ctx, cur, oth, dt, s))) return rc;
     std::swap(cur, oth);
+    // The diagnostic has read rho and the field before the next pass
+    // writes rho (or before the call returns).
+    if ((rc = diags_join(ctx, s))) return rc;
     if (k + 1 == nsteps) break;
     // timestep.hpp:50-58 of step k, then :17-28 of step k+1, in one pass
     // where that pass is the faster choice.

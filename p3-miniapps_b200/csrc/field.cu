@@ -336,6 +336,20 @@ int launch_diags(vlp4d_ctx *c, int iter, cudaStream_t s) {
   return VLP4D_OK;
 }
 
+int diags_async(vlp4d_ctx *c, int iter, cudaStream_t s) {
+  VLP4D_CUDA_TRY(cudaEventRecord(c->ev_fork, s));
+  VLP4D_CUDA_TRY(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+  int rc = launch_diags(c, iter, c->side);
+  if (rc) return rc;
+  VLP4D_CUDA_TRY(cudaEventRecord(c->ev_join, c->side));
+  return VLP4D_OK;
+}
+
+int diags_join(vlp4d_ctx *c, cudaStream_t s) {
+  VLP4D_CUDA_TRY(cudaStreamWaitEvent(s, c->ev_join, 0));
+  return VLP4D_OK;
+}
+
 int launch_l2norm(vlp4d_ctx *c, const void *fn, int iter, cudaStream_t s) {
   const long long n = c->g.cells();
   if ((uintptr_t)fn % 16) return fail_msg(VLP4D_ERR_INVALID_ARG, "diags_l2norm: f must be 16-byte aligned");

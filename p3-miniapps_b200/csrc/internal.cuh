@@ -154,6 +154,14 @@ struct vlp4d_ctx {
   // nvy_glob = g.n[3].
   bool slab = false;
   int ivy0 = 0, halo = 0, nvy_glob = 0;
+
+  // The energy/mass diagnostic of a time step reads only the solved field
+  // and nothing on the step's critical path reads its result, so the time
+  // loops run it on this side stream (forked after the field solve, joined
+  // before rho is next written), overlapping the v-table build and the vx/vy
+  // pass.
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 namespace vlp4d {
@@ -239,6 +247,10 @@ int launch_field_rho(vlp4d_ctx *c, const void *fn, cudaStream_t s);
 int launch_rho_finish(vlp4d_ctx *c, int groups, cudaStream_t s);
 int launch_field_poisson(vlp4d_ctx *c, cudaStream_t s);
 int launch_diags(vlp4d_ctx *c, int iter, cudaStream_t s);
+// launch_diags on the context's side stream after the work queued on s so
+// far; diags_join makes s wait for it (before anything writes rho, Ex, Ey).
+int diags_async(vlp4d_ctx *c, int iter, cudaStream_t s);
+int diags_join(vlp4d_ctx *c, cudaStream_t s);
 int launch_l2norm(vlp4d_ctx *c, const void *fn, int iter, cudaStream_t s);
 // f: the owned planes (slab contexts use the global vy index ivy0 + ivy).
 int launch_init_case(vlp4d_ctx *c, void *f, int ic, double amp, double k, double u, cudaStream_t s);
