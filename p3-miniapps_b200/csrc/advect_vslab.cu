@@ -416,11 +416,13 @@ bool vslab_config(const vlp4d_ctx *c, bool do_vx, bool do_vy, VslabCfg &cfg) {
   if (cfg.threads > 512 || cfg.threads < 32 || cfg.threads % 32) return false;
   // Q: the vy segment height.  A CTA streams its items one after another,
   // each item Q output rows plus (with a vy sweep) the five halo rows and
-  // the chunk's offset spread, about Q + 6 slabs; with one CTA per SM the
-  // pass takes about ceil(items / SMs) * (Q + 6) slab times.  Q minimises
-  // that among the divisors of nvy up to 128 that still give every SM an
-  // item (the smallest Q when none does).  128^4 FP32: Q = 64 (1024 items,
-  // 7 per SM); 64^4 FP32: Q = 32 (60.8 -> 47.6 us for vx+vy against Q = 8).
+  // the chunk's offset spread, about Q + 6 slabs, and about four slab times
+  // of start-up (tables, the pipeline refilling); with one CTA per SM the
+  // pass takes about ceil(items / SMs) * (Q + halo + 4) slab times.  Q
+  // minimises that among the divisors of nvy up to 128 that still give
+  // every SM an item (the smallest Q when none does).  128^4 FP32: Q = 64
+  // (1024 items, 7 per SM); 64^4 FP32: Q = 32 (60.8 -> 47.6 us for vx+vy
+  // against Q = 8).
   const long long nchunks = nxy / cfg.C;
   int Q = env_int("VLP4D_VSLAB_Q", 0);
   if (Q <= 0) {
@@ -431,7 +433,7 @@ bool vslab_config(const vlp4d_ctx *c, bool do_vx, bool do_vy, VslabCfg &cfg) {
       if (nvy % q) continue;
       const long long items = nchunks * (nvy / q);
       if (items < c->num_sms && q != 1) continue;
-      const long long cost = (items + c->num_sms - 1) / c->num_sms * (q + halo);
+      const long long cost = (items + c->num_sms - 1) / c->num_sms * (q + halo + 4);
       if (best < 0 || cost < best) {
         best = cost;
         Q = q;
