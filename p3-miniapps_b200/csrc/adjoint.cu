@@ -188,19 +188,47 @@ __global__ void __launch_bounds__(256) k_vgrad(const T *__restrict__ a, const T 
   }
 }
 
+// Asynchronous 4- or 8-byte global-to-shared copies (through L1), in
+// commit groups per thread.
+template <int BYTES>
+__device__ __forceinline__ void cp_async_small(void *dst, const void *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (BYTES == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_group() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_groups() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 // The same sums with the vx taps shared: thread (cw, g) of a block owns
 // column ixy = blockIdx.x*CW + cw and the V consecutive output vx rows
 // g*V .. g*V+V-1 (blockDim = CW x nvx/V), so one input row costs V+5 loads
 // for V outputs.  The stencil sums run in the element type, the products
 // with lb and the accumulation in FP64.  Ring slot of row r: r mod 6,
 // static after unrolling by six.
-template <typename T, int V>
+//
+// Loads: each thread copies its own V+5 taps and V adjoint values of a row
+// into its private slots of a shared-memory ring of S rows with cp.async,
+// S-1 rows ahead of the row it computes (one commit group per row; the
+// slot written is the one read a row earlier, so no copy lands in a slot
+// still being read).  Slots are laid out [slot][element][thread]: a warp's
+// accesses are consecutive words.  Nothing is shared between threads
+// until the final reduction.
+template <typename T, int V, int S>
 __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const T *__restrict__ lb, int nxy,
                                                  int nvx, int nvy, int Q, StencilTable tvx, StencilTable tvy,
                                                  const double *__restrict__ dwx, const double *__restrict__ dwy,
                                                  double *__restrict__ part) {
+  static_assert(6 % S == 0, "ring slots are static after unrolling by six");
+  constexpr int NE = V + 5 + V;  // elements of one row per thread
+  constexpr int D = S - 1;       // rows in flight ahead of the computed one
+  extern __shared__ __align__(16) unsigned char vg_smem[];
   const int CW = blockDim.x;
+  const int G = blockDim.y;
   const int cw = threadIdx.x, g = threadIdx.y;
+  const int nth = CW * G, tid = g * CW + cw;
+  T *ring = reinterpret_cast<T *>(vg_smem);                               // [S][NE][nth]
+  double *red = reinterpret_cast<double *>(vg_smem + sizeof(T) * S * NE * nth);  // [2][G][CW]
   const int ixy = blockIdx.x * CW + cw;
   const int seg = blockIdx.y;
   const int ivy0 = seg * Q;
@@ -233,33 +261,39 @@ __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const 
     const int my = tvy.m[ixy];
     const T *lcol = lb + (long long)vx0 * vstride + ixy;
     T A[6][V], B[6][V];
-    int row = (ivy0 + my) % nvy;
     const int nrows = q + 5;
-    // Loads run one row ahead: the taps of row r+1 and the adjoint values
-    // of the output row r+1-5 are in flight while row r is computed.
-    T t[V + 5], l[V];
-    {
-      const T *p = a + (long long)row * ystride + ixy;
+    int lrow = (ivy0 + my) % nvy;  // the a row of the next row to load
+    // Row rr of the segment into ring slot rr mod S (an empty group past
+    // the last row, so that every row has one commit group).
+    auto issue = [&](int rr) {
+      if (rr < nrows) {
+        T *dst = ring + (size_t)(rr % S) * NE * nth + tid;
+        const T *p = a + (long long)lrow * ystride + ixy;
 #pragma unroll
-      for (int k = 0; k < V + 5; ++k) t[k] = __ldg(p + (long long)toff[k] * vstride);
-    }
+        for (int k = 0; k < V + 5; ++k) cp_async_small<sizeof(T)>(dst + k * nth, p + (long long)toff[k] * vstride);
+        if (rr >= 5) {
+          const T *lp = lcol + (long long)(ivy0 + rr - 5) * ystride;
+#pragma unroll
+          for (int i = 0; i < V; ++i) cp_async_small<sizeof(T)>(dst + (V + 5 + i) * nth, lp + (long long)i * vstride);
+        }
+        if (++lrow == nvy) lrow = 0;
+      }
+      cp_async_commit_group();
+    };
+#pragma unroll
+    for (int rr = 0; rr < D; ++rr) issue(rr);
     for (int r0 = 0; r0 < nrows; r0 += 6) {
 #pragma unroll
       for (int u = 0; u < 6; ++u) {
         const int r = r0 + u;
         if (r >= nrows) break;
-        if (++row == nvy) row = 0;
-        T tn[V + 5], ln[V];
-        if (r + 1 < nrows) {
-          const T *p = a + (long long)row * ystride + ixy;
+        // Rows up to r have landed (D groups committed after row r's).
+        cp_async_wait_groups<D - 1>();
+        issue(r + D);  // into slot (r + D) mod S = (r - 1) mod S, read a row ago
+        const T *src = ring + (size_t)(u % S) * NE * nth + tid;
+        T t[V + 5];
 #pragma unroll
-          for (int k = 0; k < V + 5; ++k) tn[k] = __ldg(p + (long long)toff[k] * vstride);
-          if (r + 1 >= 5) {
-            const T *lp = lcol + (long long)(ivy0 + r - 4) * ystride;
-#pragma unroll
-            for (int i = 0; i < V; ++i) ln[i] = __ldg(lp + (long long)i * vstride);
-          }
-        }
+        for (int k = 0; k < V + 5; ++k) t[k] = src[k * nth];
 #pragma unroll
         for (int i = 0; i < V; ++i) {
           T sa = wx[0] * t[i], sb = dx[0] * t[i];
@@ -274,26 +308,22 @@ __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const 
         if (r >= 5) {
 #pragma unroll
           for (int i = 0; i < V; ++i) {
+            const T l = src[(V + 5 + i) * nth];
             T sx = wy[0] * B[(u + 1) % 6][i], sy = dy[0] * A[(u + 1) % 6][i];
 #pragma unroll
             for (int k = 1; k < 6; ++k) {
               sx = fma(wy[k], B[(u + 1 + k) % 6][i], sx);
               sy = fma(dy[k], A[(u + 1 + k) % 6][i], sy);
             }
-            gx = fma((double)l[i], (double)sx, gx);
-            gy = fma((double)l[i], (double)sy, gy);
+            gx = fma((double)l, (double)sx, gx);
+            gy = fma((double)l, (double)sy, gy);
           }
         }
-#pragma unroll
-        for (int k = 0; k < V + 5; ++k) t[k] = tn[k];
-#pragma unroll
-        for (int i = 0; i < V; ++i) l[i] = ln[i];
       }
     }
+    cp_async_wait_groups<0>();
   }
   // Sum the vx groups of each column in a fixed order.
-  extern __shared__ double red[];  // [2][blockDim.y][CW]
-  const int G = blockDim.y;
   red[g * CW + cw] = gx;
   red[(G + g) * CW + cw] = gy;
   __syncthreads();
@@ -306,6 +336,17 @@ __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const 
     part[(2LL * seg) * nxy + ixy] = ax;
     part[(2LL * seg + 1) * nxy + ixy] = ay;
   }
+}
+
+// Ring rows of k_vgrad_v (two rows in flight; six spill registers in FP32),
+// and its shared memory.
+template <typename T>
+constexpr int vgrad_slots() {
+  return 3;
+}
+template <typename T, int V>
+size_t vgrad_smem(int nth, int gy, int cw) {
+  return sizeof(T) * vgrad_slots<T>() * (2 * V + 5) * (size_t)nth + sizeof(double) * 2 * gy * cw;
 }
 
 __global__ void k_vgrad_finish(const double *__restrict__ part, int nseg, int nxy, double *__restrict__ gex,
@@ -512,13 +553,19 @@ int launch_vgrad(vlp4d_adjoint *A, const void *a, const void *lb, cudaStream_t s
     const int Qv = (nvy + ns - 1) / ns;
     ns = (nvy + Qv - 1) / Qv;
     dim3 gridv(bxv, ns), blockv(cw, gy);
-    const size_t sm = sizeof(double) * 2 * gy * cw;
-    if (c->dtype == VLP4D_F64)
-      k_vgrad_v<double, 2><<<gridv, blockv, sm, s>>>((const double *)a, (const double *)lb, nxy, nvx, nvy, Qv,
-                                                     c->tab_vx, c->tab_vy, A->dw_vx, A->dw_vy, A->gpart);
-    else
-      k_vgrad_v<float, 4><<<gridv, blockv, sm, s>>>((const float *)a, (const float *)lb, nxy, nvx, nvy, Qv,
-                                                    c->tab_vx, c->tab_vy, A->dw_vx, A->dw_vy, A->gpart);
+    if (c->dtype == VLP4D_F64) {
+      auto kern = k_vgrad_v<double, 2, vgrad_slots<double>()>;
+      const size_t sm = vgrad_smem<double, 2>(cw * gy, gy, cw);
+      VLP4D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      kern<<<gridv, blockv, sm, s>>>((const double *)a, (const double *)lb, nxy, nvx, nvy, Qv, c->tab_vx, c->tab_vy,
+                                     A->dw_vx, A->dw_vy, A->gpart);
+    } else {
+      auto kern = k_vgrad_v<float, 4, vgrad_slots<float>()>;
+      const size_t sm = vgrad_smem<float, 4>(cw * gy, gy, cw);
+      VLP4D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      kern<<<gridv, blockv, sm, s>>>((const float *)a, (const float *)lb, nxy, nvx, nvy, Qv, c->tab_vx, c->tab_vy,
+                                     A->dw_vx, A->dw_vy, A->gpart);
+    }
     VLP4D_LAUNCH_CHECK();
     k_vgrad_finish<<<(nxy + 255) / 256, 256, 0, s>>>(A->gpart, ns, nxy, A->gex, A->gey);
     VLP4D_LAUNCH_CHECK();

@@ -11,13 +11,13 @@
 //   0: moment of f0                     tiles: nvy  (one vy row of planes each)
 //   1: field solve, diagnostic 0        tiles: 1
 //   per step t (stage 2 + 3t + sub):
-//   sub 0: x, y (dt/2) + moment         tiles: nvy
+//   sub 0: x, y (dt/2) + moment         tiles: ceil(nvy / rows) (rows vy rows each)
 //          for t > 0 joined with the closing x, y (dt/2) of step t - 1
 //          (no field solve separates them): x, y, x, y as the composed
 //          11-tap stencils, as the single-run time loop does in FP32
 //   sub 1: field solve, diagnostic t+1  tiles: 1
 //   sub 2: vx, vy (dt)                  tiles: ceil(nx*ny / cc)   (cc columns each)
-//   last:  x, y (dt/2), the closing half step of the last step   tiles: nvy
+//   last:  x, y (dt/2), the closing half step of the last step   tiles: ceil(nvy / rows)
 // A stage's tiles may start only when the member's previous stage is
 // complete; different members are independent.  Scheduling is dynamic and
 // wait-free: a CTA picks a member, atomically takes the next tile of the
@@ -42,6 +42,7 @@
 // mode 0 zeroed), and the inverse DFT keeping the real part.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "internal.cuh"
@@ -61,14 +62,21 @@ struct EnsRun {
   long long p_off;  // moment partials: nvy * nx*ny doubles
   long long e_off;  // fields: ex, ey (2 * nx*ny doubles)
   long long d_off;  // diagnostic history: nsteps + 1 doubles
+  long long l_off;  // line tables: nvx x lines then nvy y lines (dt/2 shifts)
+  int rows;         // vy rows per tile of the x/y stages
 };
 
 // Default and largest idle limit of a CTA of k_ensemble: about two seconds
 // at 1.9 GHz.
 constexpr long long kEnsIdleLimit = 4000000000LL;
 
+struct EnsLine;
+struct EnsLine11;
+
 struct EnsArgs {
   const EnsRun *runs;
+  const EnsLine *lines;      // per member at l_off: x lines by ivx, y lines by ivy
+  const EnsLine11 *lines11;  // the same lines composed with themselves (11 taps)
   int nruns, nsteps;
   float *F0, *F1;
   double *part, *fld, *nrj;
@@ -91,7 +99,7 @@ __device__ __forceinline__ int stage_tiles(const EnsRun &R, int S, int cc) {
   const int sub = (S - 2) % 3;
   if (sub == 1) return 1;
   if (sub == 2) return (R.n[0] * R.n[1] + cc - 1) / cc;
-  return R.n[3];  // sub 0 and the closing x, y stage
+  return (R.n[3] + R.rows - 1) / R.rows;  // sub 0 and the closing x, y stage
 }
 
 // Stencil record of one line: FP32 difference weights and the tap offset.
@@ -131,193 +139,17 @@ __device__ __forceinline__ int div_small(int a, int n, float inv) {
   return q;
 }
 
-// Moment of f0 (stage 0) or x/y half step (+ moment) of the vy row `ivy`.
-// The row's nvx planes are contiguous; they are processed in groups of P
-// planes (P * nx*ny <= kEnsGroupCells), streamed through a ring of
-// kEnsRing shared buffers with cp.async (two groups in flight while one is
-// swept).  Per group: the x sweep into the swept buffer, one barrier, the
-// y sweep to global memory (items: every (plane, column quad) of the
-// group, so that small planes keep all threads busy).  With the moment the
-// y sweep also leaves its output in the group's raw buffer (no longer read
-// after the barrier), and after a second barrier the thread that owns cell
-// q adds the group's planes to the cell's FP64 sum in ivx order: the sums
-// do not depend on the block size or the tile configuration.
-template <bool SWEEP, bool MOMENT>
-__device__ void ens_planes(const EnsArgs &a, const EnsRun &R, const float *fin, float *fout, int ivy,
-                           unsigned char *smem) {
-  const int nx = R.n[0], ny = R.n[1], nvx = R.n[2];
-  const int nxy = nx * ny;
+// Moment of f0 (stage 0) of the vy row `ivy`: the per-cell sum over the
+// row's nvx planes in ivx order, FP64, to the row's partial.
+__device__ void ens_moment0(const EnsArgs &a, const EnsRun &R, const float *fin, int ivy) {
+  const int nvx = R.n[2];
+  const int nxy = R.n[0] * R.n[1];
   const long long row0 = R.f_off + (long long)ivy * nvx * nxy;
-  double *acc = reinterpret_cast<double *>(smem);
-  if (!SWEEP) {
-    double *pp = a.part + R.p_off + (long long)ivy * nxy;
-    for (int q = threadIdx.x; q < nxy; q += blockDim.x) {
-      double s = 0.;
-      for (int p = 0; p < nvx; ++p) s += (double)__ldcg(fin + row0 + (long long)p * nxy + q);
-      pp[q] = s;
-    }
-    return;
-  }
-  float *raw0 = reinterpret_cast<float *>(acc + a.maxnxy);
-  float *b1 = raw0 + (size_t)kEnsRing * kEnsGroupCells;
-  EnsLine *xl = reinterpret_cast<EnsLine *>(b1 + kEnsGroupCells);
-  __shared__ EnsLine yl;
-  const double hdt = 0.5 * R.dt;
-  int P = kEnsGroupCells / nxy;
-  P = P < 1 ? 1 : (P > nvx ? nvx : P);
-  const int ngroups = (nvx + P - 1) / P;
-  for (int l = threadIdx.x; l < nvx; l += blockDim.x)
-    xl[l] = ens_line(hdt * (R.minp[2] + l * R.dx[2]), R.minp[0], R.maxp[0], nx);
-  if (threadIdx.x == 0) yl = ens_line(hdt * (R.minp[3] + ivy * R.dx[3]), R.minp[1], R.maxp[1], ny);
-  if (MOMENT)
-    for (int q = threadIdx.x; q < nxy; q += blockDim.x) acc[q] = 0.;
-  // Column quads when the rows are multiples of four floats (f_off is a
-  // multiple of 64 elements, so every plane starts 16-byte aligned).
-  const bool quad = (nx & 3) == 0;
-  auto load_group = [&](int gi) {
-    if (gi < ngroups) {
-      const int p0 = gi * P;
-      const int np = nvx - p0 < P ? nvx - p0 : P;
-      float *dst = raw0 + (size_t)(gi % kEnsRing) * kEnsGroupCells;
-      const long long gbase = row0 + (long long)p0 * nxy;
-      if (quad) {
-        const float4 *src = reinterpret_cast<const float4 *>(fin + gbase);
-        float4 *d4 = reinterpret_cast<float4 *>(dst);
-        for (int c = threadIdx.x; c < (np * nxy) >> 2; c += blockDim.x) cp_async16(d4 + c, src + c);
-      } else {
-        for (int c = threadIdx.x; c < np * nxy; c += blockDim.x) dst[c] = __ldcg(fin + gbase + c);
-      }
-    }
-    cp_async_commit();
-  };
-  __syncthreads();
-#pragma unroll
-  for (int gi = 0; gi < kEnsRing - 1; ++gi) load_group(gi);
-  const int my = yl.m;
-  for (int gi = 0; gi < ngroups; ++gi) {
-    cp_async_wait<kEnsRing - 2>();
-    // Group gi has landed (every thread's copies); every thread is done
-    // with group gi - 1, whose buffer the next load reuses.
-    __syncthreads();
-    load_group(gi + kEnsRing - 1);
-    const int p0 = gi * P;
-    const int np = nvx - p0 < P ? nvx - p0 : P;
-    float *b0 = raw0 + (size_t)(gi % kEnsRing) * kEnsGroupCells;
-    const long long gbase = row0 + (long long)p0 * nxy;
-    if (quad) {
-      const int nq = nx >> 2, nqp = nxy >> 2;
-      const float inv_nq = 1.f / (float)nq, inv_nqp = 1.f / (float)nqp;
-      const int items = np * nqp;
-      for (int it = threadIdx.x; it < items; it += blockDim.x) {
-        const int p = div_small(it, nqp, inv_nqp);
-        const int qi = it - p * nqp;
-        const int iy = div_small(qi, nq, inv_nq);
-        const int ix0 = (qi - iy * nq) << 2;
-        const int row = p * nxy + iy * nx;
-        const EnsLine &lx = xl[p0 + p];
-        int base = ix0 + lx.m;
-        base = base >= nx ? base - nx : base;
-        const int rr = base & 3;
-        int o[3];
-        o[0] = base - rr;
-        o[1] = o[0] + 4 >= nx ? o[0] + 4 - nx : o[0] + 4;
-        o[2] = o[1] + 4 >= nx ? o[1] + 4 - nx : o[1] + 4;
-        float t[12];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          const float4 v = *reinterpret_cast<const float4 *>(b0 + row + o[k]);
-          t[4 * k] = v.x;
-          t[4 * k + 1] = v.y;
-          t[4 * k + 2] = v.z;
-          t[4 * k + 3] = v.w;
-        }
-        SweepW<float> w;
-        make_sweep_w(lx.v, w);
-        float out[4];
-        sweep_x4(t, rr, w, out);
-        *reinterpret_cast<float4 *>(b1 + row + ix0) = make_float4(out[0], out[1], out[2], out[3]);
-      }
-      __syncthreads();
-      SweepW<float> wy;
-      make_sweep_w(yl.v, wy);
-      for (int it = threadIdx.x; it < items; it += blockDim.x) {
-        const int p = div_small(it, nqp, inv_nqp);
-        const int qi = it - p * nqp;
-        const int iy = div_small(qi, nq, inv_nq);
-        const int ix0 = (qi - iy * nq) << 2;
-        const float *pl = b1 + p * nxy + ix0;
-        int j = iy + my;
-        j = j >= ny ? j - ny : j;
-        float2 y[6][2];
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-          const float4 v = *reinterpret_cast<const float4 *>(pl + j * nx);
-          y[k][0] = make_float2(v.x, v.y);
-          y[k][1] = make_float2(v.z, v.w);
-          if (++j == ny) j = 0;
-        }
-        float2 o2[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-          o2[h] = interp_diff2(wy.v, y[2][h], sub2(y[1][h], y[0][h]), sub2(y[2][h], y[1][h]), sub2(y[3][h], y[2][h]),
-                               sub2(y[4][h], y[3][h]), sub2(y[5][h], y[4][h]));
-        const float4 o4 = make_float4(o2[0].x, o2[0].y, o2[1].x, o2[1].y);
-        *reinterpret_cast<float4 *>(fout + gbase + (long long)it * 4) = o4;
-        if (MOMENT) *reinterpret_cast<float4 *>(b0 + it * 4) = o4;
-      }
-    } else {
-      const float inv_nx = 1.f / (float)nx, inv_nxy = 1.f / (float)nxy;
-      const int cells = np * nxy;
-      for (int c = threadIdx.x; c < cells; c += blockDim.x) {
-        const int p = div_small(c, nxy, inv_nxy);
-        const int qc = c - p * nxy;
-        const int ix = qc - div_small(qc, nx, inv_nx) * nx;
-        const int row = c - ix;
-        const EnsLine &lx = xl[p0 + p];
-        int j = ix + lx.m;
-        j = j >= nx ? j - nx : j;
-        float t[6];
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-          t[k] = b0[row + j];
-          if (++j == nx) j = 0;
-        }
-        b1[c] = interp6(lx.v, t[0], t[1], t[2], t[3], t[4], t[5]);
-      }
-      __syncthreads();
-      const EnsLine ly = yl;
-      for (int c = threadIdx.x; c < cells; c += blockDim.x) {
-        const int p = div_small(c, nxy, inv_nxy);
-        const int qc = c - p * nxy;
-        const int iy = div_small(qc, nx, inv_nx);
-        const float *pl = b1 + p * nxy + (qc - iy * nx);
-        int j = iy + my;
-        j = j >= ny ? j - ny : j;
-        float t[6];
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-          t[k] = pl[j * nx];
-          if (++j == ny) j = 0;
-        }
-        const float o = interp6(ly.v, t[0], t[1], t[2], t[3], t[4], t[5]);
-        fout[gbase + c] = o;
-        if (MOMENT) b0[c] = o;
-      }
-    }
-    if (MOMENT) {
-      __syncthreads();  // the group's outputs are in b0
-      for (int q = threadIdx.x; q < nxy; q += blockDim.x) {
-        double s = acc[q];
-        for (int p = 0; p < np; ++p) s += (double)b0[p * nxy + q];
-        acc[q] = s;
-      }
-    }
-  }
-  cp_async_wait<0>();
-  if (MOMENT) {
-    __syncthreads();
-    double *pp = a.part + R.p_off + (long long)ivy * nxy;
-    for (int q = threadIdx.x; q < nxy; q += blockDim.x) pp[q] = acc[q];
+  double *pp = a.part + R.p_off + (long long)ivy * nxy;
+  for (int q = threadIdx.x; q < nxy; q += blockDim.x) {
+    double s = 0.;
+    for (int p = 0; p < nvx; ++p) s += (double)__ldcg(fin + row0 + (long long)p * nxy + q);
+    pp[q] = s;
   }
 }
 
@@ -392,36 +224,66 @@ __device__ __forceinline__ float ens_interp11_1(const float (&u)[10], const floa
   return t[5] + acc;
 }
 
-// x, y, x, y (dt/2 each) + moment of the vy row `ivy`: X11 then Y11 (the x
-// and y shifts commute), otherwise as ens_planes: plane groups through the
-// cp.async ring, X11 into the swept buffer, one barrier, Y11 per (plane,
-// column quad) to global memory and in place into the raw buffer, a
-// barrier, the moment in ivx order per cell.
-__device__ void ens_planes11(const EnsArgs &a, const EnsRun &R, const float *fin, float *fout, int ivy,
-                             unsigned char *smem) {
-  const int nx = R.n[0], ny = R.n[1], nvx = R.n[2];
+template <bool J11>
+struct EnsLineOf {
+  using T = EnsLine;
+};
+template <>
+struct EnsLineOf<true> {
+  using T = EnsLine11;
+};
+
+// x/y sweeps of the vy rows [tile * R.rows, tile * R.rows + R.rows) of
+// member R.  MODE 0: x, y (dt/2); 1: x, y (dt/2) + moment; 2: x, y, x, y
+// (dt/2 each) + moment, as the composed 11-tap stencils X11 then Y11 (the x
+// and y shifts commute).  The tile's rows are contiguous in f (nvx planes of
+// nx*ny cells each); each row is cut into groups of P planes (P * nx*ny <=
+// kEnsGroupCells) and the tile's groups, row after row, stream through a
+// ring of kEnsRing shared buffers with cp.async: two groups in flight while
+// one is swept, across row boundaries, so that small members pay the ring's
+// start-up once per tile of several rows.  Per group: the x sweep into the
+// swept buffer, one barrier, the y sweep to global memory (items: every
+// (plane, column quad) of the group, or two rows of a column quad in the
+// joined form, so that small planes keep all threads busy).  With the
+// moment the y sweep also leaves its output in the group's raw buffer (no
+// longer read after the barrier), and after a second barrier the thread
+// that owns cell q adds the group's planes to the cell's FP64 sum in ivx
+// order, storing the row's sum after the row's last group: the sums do not
+// depend on the block size or the tile configuration.  The lines come from
+// the member's tables (x by ivx, y by ivy), built when the ensemble is
+// created.
+template <int MODE>
+__device__ void ens_rows(const EnsArgs &a, const EnsRun &R, const float *fin, float *fout, int tile,
+                         unsigned char *smem) {
+  constexpr bool MOMENT = MODE >= 1;
+  constexpr bool J11 = MODE == 2;
+  using Line = typename EnsLineOf<J11>::T;
+  const int nx = R.n[0], ny = R.n[1], nvx = R.n[2], nvy = R.n[3];
   const int nxy = nx * ny;
-  const long long row0 = R.f_off + (long long)ivy * nvx * nxy;
+  const int y0 = tile * R.rows;
+  const int nrows = nvy - y0 < R.rows ? nvy - y0 : R.rows;
   double *acc = reinterpret_cast<double *>(smem);
   float *raw0 = reinterpret_cast<float *>(acc + a.maxnxy);
   float *b1 = raw0 + (size_t)kEnsRing * kEnsGroupCells;
-  EnsLine11 *xl = reinterpret_cast<EnsLine11 *>(b1 + kEnsGroupCells);
-  __shared__ EnsLine11 yl;
-  const double hdt = 0.5 * R.dt;
+  Line *xl = reinterpret_cast<Line *>(b1 + kEnsGroupCells);
+  const Line *tab;
+  if constexpr (J11) tab = a.lines11 + R.l_off;
+  else tab = a.lines + R.l_off;
   int P = kEnsGroupCells / nxy;
   P = P < 1 ? 1 : (P > nvx ? nvx : P);
-  const int ngroups = (nvx + P - 1) / P;
-  for (int l = threadIdx.x; l < nvx; l += blockDim.x)
-    xl[l] = ens_line11(hdt * (R.minp[2] + l * R.dx[2]), R.minp[0], R.maxp[0], nx);
-  if (threadIdx.x == 0) yl = ens_line11(hdt * (R.minp[3] + ivy * R.dx[3]), R.minp[1], R.maxp[1], ny);
-  for (int q = threadIdx.x; q < nxy; q += blockDim.x) acc[q] = 0.;
+  const int gpr = (nvx + P - 1) / P;  // groups per row
+  const int ngroups = nrows * gpr;
+  const long long tile0 = R.f_off + (long long)y0 * nvx * nxy;
+  // Column quads when the rows are multiples of four floats (f_off is a
+  // multiple of 64 elements, so every plane starts 16-byte aligned).
   const bool quad = (nx & 3) == 0;
   auto load_group = [&](int gi) {
     if (gi < ngroups) {
-      const int p0 = gi * P;
+      const int r = gi / gpr;
+      const int p0 = (gi - r * gpr) * P;
       const int np = nvx - p0 < P ? nvx - p0 : P;
       float *dst = raw0 + (size_t)(gi % kEnsRing) * kEnsGroupCells;
-      const long long gbase = row0 + (long long)p0 * nxy;
+      const long long gbase = tile0 + ((long long)r * nvx + p0) * nxy;
       if (quad) {
         const float4 *src = reinterpret_cast<const float4 *>(fin + gbase);
         float4 *d4 = reinterpret_cast<float4 *>(dst);
@@ -432,184 +294,303 @@ __device__ void ens_planes11(const EnsArgs &a, const EnsRun &R, const float *fin
     }
     cp_async_commit();
   };
-  __syncthreads();
+  // The ring's first loads go out before anything else; the previous tile
+  // of this CTA has finished with every buffer (the scheduler's barrier).
 #pragma unroll
   for (int gi = 0; gi < kEnsRing - 1; ++gi) load_group(gi);
-  const int my = yl.m;
-  float2 uy[10];
-  float uys[10];
-#pragma unroll
-  for (int k = 0; k < 10; ++k) {
-    uys[k] = yl.u[k];
-    uy[k] = make_float2(uys[k], uys[k]);
-  }
+  for (int l = threadIdx.x; l < nvx; l += blockDim.x) xl[l] = tab[l];
+  if (MOMENT)
+    for (int q = threadIdx.x; q < nxy; q += blockDim.x) acc[q] = 0.;
   for (int gi = 0; gi < ngroups; ++gi) {
     cp_async_wait<kEnsRing - 2>();
-    __syncthreads();  // group gi landed; every thread is done with group gi - 1
+    // Group gi has landed (every thread's copies); every thread is done
+    // with group gi - 1, whose buffer the next load reuses (at gi = 0: the
+    // x lines are in place).
+    __syncthreads();
     load_group(gi + kEnsRing - 1);
-    const int p0 = gi * P;
+    const int r = gi / gpr;
+    const int p0 = (gi - r * gpr) * P;
     const int np = nvx - p0 < P ? nvx - p0 : P;
     float *b0 = raw0 + (size_t)(gi % kEnsRing) * kEnsGroupCells;
-    const long long gbase = row0 + (long long)p0 * nxy;
-    if (quad) {
-      const int nq = nx >> 2, nqp = nxy >> 2;
-      const float inv_nq = 1.f / (float)nq, inv_nqp = 1.f / (float)nqp;
-      const int items = np * nqp;
-      for (int it = threadIdx.x; it < items; it += blockDim.x) {
-        const int p = div_small(it, nqp, inv_nqp);
-        const int qi = it - p * nqp;
-        const int iy = div_small(qi, nq, inv_nq);
-        const int ix0 = (qi - iy * nq) << 2;
-        const int row = p * nxy + iy * nx;
-        const EnsLine11 &lx = xl[p0 + p];
-        int base = ix0 + lx.m;
-        base = base >= nx ? base - nx : base;
-        const int rr = base & 3;
-        int o = base - rr;
-        float t[20];
+    const long long gbase = tile0 + ((long long)r * nvx + p0) * nxy;
+    const Line ly = tab[nvx + y0 + r];
+    const int my = ly.m;
+    if constexpr (!J11) {
+      if (quad) {
+        const int nq = nx >> 2, nqp = nxy >> 2;
+        const float inv_nq = 1.f / (float)nq, inv_nqp = 1.f / (float)nqp;
+        const int items = np * nqp;
+        for (int it = threadIdx.x; it < items; it += blockDim.x) {
+          const int p = div_small(it, nqp, inv_nqp);
+          const int qi = it - p * nqp;
+          const int iy = div_small(qi, nq, inv_nq);
+          const int ix0 = (qi - iy * nq) << 2;
+          const int row = p * nxy + iy * nx;
+          const EnsLine &lx = xl[p0 + p];
+          int base = ix0 + lx.m;
+          base = base >= nx ? base - nx : base;
+          const int rr = base & 3;
+          int o[3];
+          o[0] = base - rr;
+          o[1] = o[0] + 4 >= nx ? o[0] + 4 - nx : o[0] + 4;
+          o[2] = o[1] + 4 >= nx ? o[1] + 4 - nx : o[1] + 4;
+          float t[12];
 #pragma unroll
-        for (int k = 0; k < 5; ++k) {
-          const float4 v = *reinterpret_cast<const float4 *>(b0 + row + o);
-          t[4 * k] = v.x;
-          t[4 * k + 1] = v.y;
-          t[4 * k + 2] = v.z;
-          t[4 * k + 3] = v.w;
-          o += 4;
-          if (o >= nx) o -= nx;
+          for (int k = 0; k < 3; ++k) {
+            const float4 v = *reinterpret_cast<const float4 *>(b0 + row + o[k]);
+            t[4 * k] = v.x;
+            t[4 * k + 1] = v.y;
+            t[4 * k + 2] = v.z;
+            t[4 * k + 3] = v.w;
+          }
+          SweepW<float> w;
+          make_sweep_w(lx.v, w);
+          float out[4];
+          sweep_x4(t, rr, w, out);
+          *reinterpret_cast<float4 *>(b1 + row + ix0) = make_float4(out[0], out[1], out[2], out[3]);
         }
-        float2 u[10];
-#pragma unroll
-        for (int k = 0; k < 10; ++k) u[k] = make_float2(lx.u[k], lx.u[k]);
-        float out[4];
-        switch (rr) {
-          case 0: ens_x11_from<0>(t, u, out); break;
-          case 1: ens_x11_from<1>(t, u, out); break;
-          case 2: ens_x11_from<2>(t, u, out); break;
-          default: ens_x11_from<3>(t, u, out); break;
-        }
-        *reinterpret_cast<float4 *>(b1 + row + ix0) = make_float4(out[0], out[1], out[2], out[3]);
-      }
-      __syncthreads();
-      if ((ny & 1) == 0) {
-        // Y11 of two rows per item (iy, iy + 1 of one column quad): twelve
-        // row loads and eleven differences serve both outputs, each computed
-        // exactly as by the one-row items below.
-        const int nq2 = nqp >> 1;
-        const float inv_nq2 = 1.f / (float)nq2;
-        const int items2 = np * nq2;
-        for (int it = threadIdx.x; it < items2; it += blockDim.x) {
-          const int p = div_small(it, nq2, inv_nq2);
-          const int qi = it - p * nq2;
-          const int iyp = div_small(qi, nq, inv_nq);
-          const int ix0 = (qi - iyp * nq) << 2;
-          const int iy = 2 * iyp;
+        __syncthreads();
+        SweepW<float> wy;
+        make_sweep_w(ly.v, wy);
+        for (int it = threadIdx.x; it < items; it += blockDim.x) {
+          const int p = div_small(it, nqp, inv_nqp);
+          const int qi = it - p * nqp;
+          const int iy = div_small(qi, nq, inv_nq);
+          const int ix0 = (qi - iy * nq) << 2;
           const float *pl = b1 + p * nxy + ix0;
           int j = iy + my;
           j = j >= ny ? j - ny : j;
-          float2 y[12][2];
+          float2 y[6][2];
 #pragma unroll
-          for (int k = 0; k < 12; ++k) {
+          for (int k = 0; k < 6; ++k) {
             const float4 v = *reinterpret_cast<const float4 *>(pl + j * nx);
             y[k][0] = make_float2(v.x, v.y);
             y[k][1] = make_float2(v.z, v.w);
             if (++j == ny) j = 0;
           }
-          float2 o2[2][2];
+          float2 o2[2];
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            float2 d[11];
+          for (int h = 0; h < 2; ++h)
+            o2[h] = interp_diff2(wy.v, y[2][h], sub2(y[1][h], y[0][h]), sub2(y[2][h], y[1][h]), sub2(y[3][h], y[2][h]),
+                                 sub2(y[4][h], y[3][h]), sub2(y[5][h], y[4][h]));
+          const float4 o4 = make_float4(o2[0].x, o2[0].y, o2[1].x, o2[1].y);
+          *reinterpret_cast<float4 *>(fout + gbase + (long long)it * 4) = o4;
+          if (MOMENT) *reinterpret_cast<float4 *>(b0 + it * 4) = o4;
+        }
+      } else {
+        const float inv_nx = 1.f / (float)nx, inv_nxy = 1.f / (float)nxy;
+        const int cells = np * nxy;
+        for (int c = threadIdx.x; c < cells; c += blockDim.x) {
+          const int p = div_small(c, nxy, inv_nxy);
+          const int qc = c - p * nxy;
+          const int ix = qc - div_small(qc, nx, inv_nx) * nx;
+          const int row = c - ix;
+          const EnsLine &lx = xl[p0 + p];
+          int j = ix + lx.m;
+          j = j >= nx ? j - nx : j;
+          float t[6];
 #pragma unroll
-            for (int k = 0; k < 11; ++k) d[k] = sub2(y[k + 1][h], y[k][h]);
-            o2[0][h] = ens_interp11(uy, y[5][h], d);
-            o2[1][h] = ens_interp11(uy, y[6][h], d + 1);
+          for (int k = 0; k < 6; ++k) {
+            t[k] = b0[row + j];
+            if (++j == nx) j = 0;
           }
+          b1[c] = interp6(lx.v, t[0], t[1], t[2], t[3], t[4], t[5]);
+        }
+        __syncthreads();
+        for (int c = threadIdx.x; c < cells; c += blockDim.x) {
+          const int p = div_small(c, nxy, inv_nxy);
+          const int qc = c - p * nxy;
+          const int iy = div_small(qc, nx, inv_nx);
+          const float *pl = b1 + p * nxy + (qc - iy * nx);
+          int j = iy + my;
+          j = j >= ny ? j - ny : j;
+          float t[6];
 #pragma unroll
-          for (int r = 0; r < 2; ++r) {
-            const int cell = p * nxy + (iy + r) * nx + ix0;
-            const float4 o4 = make_float4(o2[r][0].x, o2[r][0].y, o2[r][1].x, o2[r][1].y);
-            *reinterpret_cast<float4 *>(fout + gbase + cell) = o4;
-            *reinterpret_cast<float4 *>(b0 + cell) = o4;
+          for (int k = 0; k < 6; ++k) {
+            t[k] = pl[j * nx];
+            if (++j == ny) j = 0;
           }
+          const float o = interp6(ly.v, t[0], t[1], t[2], t[3], t[4], t[5]);
+          fout[gbase + c] = o;
+          if (MOMENT) b0[c] = o;
         }
-      } else for (int it = threadIdx.x; it < items; it += blockDim.x) {
-        const int p = div_small(it, nqp, inv_nqp);
-        const int qi = it - p * nqp;
-        const int iy = div_small(qi, nq, inv_nq);
-        const int ix0 = (qi - iy * nq) << 2;
-        const float *pl = b1 + p * nxy + ix0;
-        int j = iy + my;
-        j = j >= ny ? j - ny : j;
-        float2 y[11][2];
-#pragma unroll
-        for (int k = 0; k < 11; ++k) {
-          const float4 v = *reinterpret_cast<const float4 *>(pl + j * nx);
-          y[k][0] = make_float2(v.x, v.y);
-          y[k][1] = make_float2(v.z, v.w);
-          if (++j == ny) j = 0;
-        }
-        float2 o2[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          float2 d[10];
-#pragma unroll
-          for (int k = 0; k < 10; ++k) d[k] = sub2(y[k + 1][h], y[k][h]);
-          o2[h] = ens_interp11(uy, y[5][h], d);
-        }
-        const float4 o4 = make_float4(o2[0].x, o2[0].y, o2[1].x, o2[1].y);
-        *reinterpret_cast<float4 *>(fout + gbase + (long long)it * 4) = o4;
-        *reinterpret_cast<float4 *>(b0 + it * 4) = o4;
       }
     } else {
-      const float inv_nx = 1.f / (float)nx, inv_nxy = 1.f / (float)nxy;
-      const int cells = np * nxy;
-      for (int c = threadIdx.x; c < cells; c += blockDim.x) {
-        const int p = div_small(c, nxy, inv_nxy);
-        const int qc = c - p * nxy;
-        const int ix = qc - div_small(qc, nx, inv_nx) * nx;
-        const int row = c - ix;
-        const EnsLine11 &lx = xl[p0 + p];
-        int j = ix + lx.m;
-        j = j >= nx ? j - nx : j;
-        float t[11], u[10];
+      float2 uy[10];
+      float uys[10];
 #pragma unroll
-        for (int k = 0; k < 11; ++k) {
-          t[k] = b0[row + j];
-          if (++j == nx) j = 0;
-        }
-#pragma unroll
-        for (int k = 0; k < 10; ++k) u[k] = lx.u[k];
-        b1[c] = ens_interp11_1(u, t);
+      for (int k = 0; k < 10; ++k) {
+        uys[k] = ly.u[k];
+        uy[k] = make_float2(uys[k], uys[k]);
       }
-      __syncthreads();
-      for (int c = threadIdx.x; c < cells; c += blockDim.x) {
-        const int p = div_small(c, nxy, inv_nxy);
-        const int qc = c - p * nxy;
-        const int iy = div_small(qc, nx, inv_nx);
-        const float *pl = b1 + p * nxy + (qc - iy * nx);
-        int j = iy + my;
-        j = j >= ny ? j - ny : j;
-        float t[11];
+      if (quad) {
+        const int nq = nx >> 2, nqp = nxy >> 2;
+        const float inv_nq = 1.f / (float)nq, inv_nqp = 1.f / (float)nqp;
+        const int items = np * nqp;
+        for (int it = threadIdx.x; it < items; it += blockDim.x) {
+          const int p = div_small(it, nqp, inv_nqp);
+          const int qi = it - p * nqp;
+          const int iy = div_small(qi, nq, inv_nq);
+          const int ix0 = (qi - iy * nq) << 2;
+          const int row = p * nxy + iy * nx;
+          const EnsLine11 &lx = xl[p0 + p];
+          int base = ix0 + lx.m;
+          base = base >= nx ? base - nx : base;
+          const int rr = base & 3;
+          int o = base - rr;
+          float t[20];
 #pragma unroll
-        for (int k = 0; k < 11; ++k) {
-          t[k] = pl[j * nx];
-          if (++j == ny) j = 0;
+          for (int k = 0; k < 5; ++k) {
+            const float4 v = *reinterpret_cast<const float4 *>(b0 + row + o);
+            t[4 * k] = v.x;
+            t[4 * k + 1] = v.y;
+            t[4 * k + 2] = v.z;
+            t[4 * k + 3] = v.w;
+            o += 4;
+            if (o >= nx) o -= nx;
+          }
+          float2 u[10];
+#pragma unroll
+          for (int k = 0; k < 10; ++k) u[k] = make_float2(lx.u[k], lx.u[k]);
+          float out[4];
+          switch (rr) {
+            case 0: ens_x11_from<0>(t, u, out); break;
+            case 1: ens_x11_from<1>(t, u, out); break;
+            case 2: ens_x11_from<2>(t, u, out); break;
+            default: ens_x11_from<3>(t, u, out); break;
+          }
+          *reinterpret_cast<float4 *>(b1 + row + ix0) = make_float4(out[0], out[1], out[2], out[3]);
         }
-        const float o = ens_interp11_1(uys, t);
-        fout[gbase + c] = o;
-        b0[c] = o;
+        __syncthreads();
+        if ((ny & 1) == 0) {
+          // Y11 of two rows per item (iy, iy + 1 of one column quad): twelve
+          // row loads and eleven differences serve both outputs, each computed
+          // exactly as by the one-row items below.
+          const int nq2 = nqp >> 1;
+          const float inv_nq2 = 1.f / (float)nq2;
+          const int items2 = np * nq2;
+          for (int it = threadIdx.x; it < items2; it += blockDim.x) {
+            const int p = div_small(it, nq2, inv_nq2);
+            const int qi = it - p * nq2;
+            const int iyp = div_small(qi, nq, inv_nq);
+            const int ix0 = (qi - iyp * nq) << 2;
+            const int iy = 2 * iyp;
+            const float *pl = b1 + p * nxy + ix0;
+            int j = iy + my;
+            j = j >= ny ? j - ny : j;
+            float2 y[12][2];
+#pragma unroll
+            for (int k = 0; k < 12; ++k) {
+              const float4 v = *reinterpret_cast<const float4 *>(pl + j * nx);
+              y[k][0] = make_float2(v.x, v.y);
+              y[k][1] = make_float2(v.z, v.w);
+              if (++j == ny) j = 0;
+            }
+            float2 o2[2][2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              float2 d[11];
+#pragma unroll
+              for (int k = 0; k < 11; ++k) d[k] = sub2(y[k + 1][h], y[k][h]);
+              o2[0][h] = ens_interp11(uy, y[5][h], d);
+              o2[1][h] = ens_interp11(uy, y[6][h], d + 1);
+            }
+#pragma unroll
+            for (int rw = 0; rw < 2; ++rw) {
+              const int cell = p * nxy + (iy + rw) * nx + ix0;
+              const float4 o4 = make_float4(o2[rw][0].x, o2[rw][0].y, o2[rw][1].x, o2[rw][1].y);
+              *reinterpret_cast<float4 *>(fout + gbase + cell) = o4;
+              *reinterpret_cast<float4 *>(b0 + cell) = o4;
+            }
+          }
+        } else {
+          for (int it = threadIdx.x; it < items; it += blockDim.x) {
+            const int p = div_small(it, nqp, inv_nqp);
+            const int qi = it - p * nqp;
+            const int iy = div_small(qi, nq, inv_nq);
+            const int ix0 = (qi - iy * nq) << 2;
+            const float *pl = b1 + p * nxy + ix0;
+            int j = iy + my;
+            j = j >= ny ? j - ny : j;
+            float2 y[11][2];
+#pragma unroll
+            for (int k = 0; k < 11; ++k) {
+              const float4 v = *reinterpret_cast<const float4 *>(pl + j * nx);
+              y[k][0] = make_float2(v.x, v.y);
+              y[k][1] = make_float2(v.z, v.w);
+              if (++j == ny) j = 0;
+            }
+            float2 o2[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              float2 d[10];
+#pragma unroll
+              for (int k = 0; k < 10; ++k) d[k] = sub2(y[k + 1][h], y[k][h]);
+              o2[h] = ens_interp11(uy, y[5][h], d);
+            }
+            const float4 o4 = make_float4(o2[0].x, o2[0].y, o2[1].x, o2[1].y);
+            *reinterpret_cast<float4 *>(fout + gbase + (long long)it * 4) = o4;
+            *reinterpret_cast<float4 *>(b0 + it * 4) = o4;
+          }
+        }
+      } else {
+        const float inv_nx = 1.f / (float)nx, inv_nxy = 1.f / (float)nxy;
+        const int cells = np * nxy;
+        for (int c = threadIdx.x; c < cells; c += blockDim.x) {
+          const int p = div_small(c, nxy, inv_nxy);
+          const int qc = c - p * nxy;
+          const int ix = qc - div_small(qc, nx, inv_nx) * nx;
+          const int row = c - ix;
+          const EnsLine11 &lx = xl[p0 + p];
+          int j = ix + lx.m;
+          j = j >= nx ? j - nx : j;
+          float t[11], u[10];
+#pragma unroll
+          for (int k = 0; k < 11; ++k) {
+            t[k] = b0[row + j];
+            if (++j == nx) j = 0;
+          }
+#pragma unroll
+          for (int k = 0; k < 10; ++k) u[k] = lx.u[k];
+          b1[c] = ens_interp11_1(u, t);
+        }
+        __syncthreads();
+        for (int c = threadIdx.x; c < cells; c += blockDim.x) {
+          const int p = div_small(c, nxy, inv_nxy);
+          const int qc = c - p * nxy;
+          const int iy = div_small(qc, nx, inv_nx);
+          const float *pl = b1 + p * nxy + (qc - iy * nx);
+          int j = iy + my;
+          j = j >= ny ? j - ny : j;
+          float t[11];
+#pragma unroll
+          for (int k = 0; k < 11; ++k) {
+            t[k] = pl[j * nx];
+            if (++j == ny) j = 0;
+          }
+          const float o = ens_interp11_1(uys, t);
+          fout[gbase + c] = o;
+          b0[c] = o;
+        }
       }
     }
-    __syncthreads();  // the group's outputs are in b0
-    for (int q = threadIdx.x; q < nxy; q += blockDim.x) {
-      double s = acc[q];
-      for (int p = 0; p < np; ++p) s += (double)b0[p * nxy + q];
-      acc[q] = s;
+    if (MOMENT) {
+      __syncthreads();  // the group's outputs are in b0
+      const bool last = p0 + np == nvx;
+      double *pp = a.part + R.p_off + (long long)(y0 + r) * nxy;
+      for (int q = threadIdx.x; q < nxy; q += blockDim.x) {
+        double s = acc[q];
+        for (int p = 0; p < np; ++p) s += (double)b0[p * nxy + q];
+        if (last) {
+          pp[q] = s;  // the row's sum; cell q's next row starts from zero
+          acc[q] = 0.;
+        } else {
+          acc[q] = s;
+        }
+      }
     }
   }
   cp_async_wait<0>();
-  __syncthreads();
-  double *pp = a.part + R.p_off + (long long)ivy * nxy;
-  for (int q = threadIdx.x; q < nxy; q += blockDim.x) pp[q] = acc[q];
 }
 
 // vx then vy (dt) of the columns [tile*cc, tile*cc + cc).  Thread (col, g)
@@ -883,17 +864,17 @@ __global__ void __launch_bounds__(512) k_ensemble(EnsArgs a) {
       const EnsRun &R = a.runs[run];
       const int S = s_stage, tile = s_tile;
       if (S == 0) {
-        ens_planes<false, true>(a, R, a.F0, nullptr, tile, smem);
+        ens_moment0(a, R, a.F0, tile);
       } else if (S == 1) {
         ens_field(a, R, 0, smem);
       } else if (S + 1 == total_stages) {
-        ens_planes<true, false>(a, R, a.F0, a.F1, tile, smem);  // closing half step
+        ens_rows<0>(a, R, a.F0, a.F1, tile, smem);  // closing half step
       } else {
         // The state lives in F0 between steps; sub 0 writes F1, vx/vy F0.
         const int t = (S - 2) / 3, sub = (S - 2) % 3;
         if (sub == 0) {
-          if (t == 0) ens_planes<true, true>(a, R, a.F0, a.F1, tile, smem);
-          else ens_planes11(a, R, a.F0, a.F1, tile, smem);
+          if (t == 0) ens_rows<1>(a, R, a.F0, a.F1, tile, smem);
+          else ens_rows<2>(a, R, a.F0, a.F1, tile, smem);
         } else if (sub == 1) {
           ens_field(a, R, t + 1, smem);
         } else {
@@ -938,6 +919,28 @@ __global__ void k_ens_init(EnsArgs a) {
   }
 }
 
+// Line tables of every member (one block each): the dt/2 shifts of the x/y
+// stages, x lines by ivx (displacement dt/2 * vx) and y lines by ivy
+// (dt/2 * vy), as single lines and composed with themselves.  Built once
+// per ensemble: they depend only on the member's grid and dt.
+__global__ void k_ens_lines(const EnsRun *runs, EnsLine *lines, EnsLine11 *lines11) {
+  const EnsRun &R = runs[blockIdx.x];
+  const double hdt = 0.5 * R.dt;
+  const int nx = R.n[0], ny = R.n[1], nvx = R.n[2], nvy = R.n[3];
+  EnsLine *l1 = lines + R.l_off;
+  EnsLine11 *l2 = lines11 + R.l_off;
+  for (int l = threadIdx.x; l < nvx; l += blockDim.x) {
+    const double disp = hdt * (R.minp[2] + l * R.dx[2]);
+    l1[l] = ens_line(disp, R.minp[0], R.maxp[0], nx);
+    l2[l] = ens_line11(disp, R.minp[0], R.maxp[0], nx);
+  }
+  for (int l = threadIdx.x; l < nvy; l += blockDim.x) {
+    const double disp = hdt * (R.minp[3] + l * R.dx[3]);
+    l1[nvx + l] = ens_line(disp, R.minp[1], R.maxp[1], ny);
+    l2[nvx + l] = ens_line11(disp, R.minp[1], R.maxp[1], ny);
+  }
+}
+
 __global__ void k_ens_reset(EnsArgs a) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r < a.nruns) {
@@ -958,6 +961,8 @@ struct vlp4d_ensemble {
   int nruns = 0, nsteps = 0;
   std::vector<vlp4d::EnsRun> host_runs;
   vlp4d::EnsRun *runs = nullptr;
+  vlp4d::EnsLine *lines = nullptr;
+  vlp4d::EnsLine11 *lines11 = nullptr;
   float *F[2] = {nullptr, nullptr};
   double *part = nullptr, *fld = nullptr, *nrj = nullptr;
   unsigned long long *word = nullptr;
@@ -987,6 +992,8 @@ size_t ens_smem(int maxnxy) {
 EnsArgs ens_args(vlp4d_ensemble *E, int nsteps) {
   EnsArgs a;
   a.runs = E->runs;
+  a.lines = E->lines;
+  a.lines11 = E->lines11;
   a.nruns = E->nruns;
   a.nsteps = nsteps;
   a.F0 = E->F[0];
@@ -1026,6 +1033,8 @@ void ens_free(vlp4d_ensemble *E) {
   if (!E) return;
   if (E->graph) cudaGraphExecDestroy(E->graph);
   cudaFree(E->runs);
+  cudaFree(E->lines);
+  cudaFree(E->lines11);
   cudaFree(E->F[0]);
   cudaFree(E->F[1]);
   cudaFree(E->part);
@@ -1086,7 +1095,12 @@ int vlp4d_ensemble_create(const vlp4d_ens_member *members, int nruns, int nsteps
   VLP4D_CUDA_TRY(cudaDeviceGetAttribute(&E->num_sms, cudaDevAttrMultiProcessorCount, dev));
   E->nruns = nruns;
   E->nsteps = nsteps;
-  long long foff = 0, poff = 0, eoff = 0, doff = 0;
+  long long foff = 0, poff = 0, eoff = 0, doff = 0, loff = 0;
+  // Cells per tile of the x/y stages: the vy rows of small members are
+  // batched into tiles of about this many cells (one row at least), so that
+  // the plane-group ring's start-up is paid once per tile.
+  long long tile_cells = 131072;
+  if (const char *env = getenv("VLP4D_ENS_TILE_CELLS")) tile_cells = atoll(env) > 0 ? atoll(env) : 1;
   for (int r = 0; r < nruns; ++r) {
     const vlp4d_ens_member &m = members[r];
     EnsRun R;
@@ -1121,6 +1135,15 @@ int vlp4d_ensemble_create(const vlp4d_ens_member *members, int nruns, int nsteps
     eoff += 2 * nxy;
     R.d_off = doff;
     doff += nsteps + 1;
+    R.l_off = loff;
+    loff += R.n[2] + R.n[3];
+    {
+      const long long row_cells = nxy * R.n[2];
+      long long per = tile_cells / row_cells;
+      per = per < 1 ? 1 : (per > R.n[3] ? R.n[3] : per);
+      const long long tiles = (R.n[3] + per - 1) / per;
+      R.rows = (int)((R.n[3] + tiles - 1) / tiles);  // balanced tiles
+    }
     E->total_cells += cells;
     if (cells > E->max_cells) E->max_cells = cells;
     if (nxy > E->maxnxy) E->maxnxy = (int)nxy;
@@ -1136,7 +1159,9 @@ int vlp4d_ensemble_create(const vlp4d_ens_member *members, int nruns, int nsteps
             cudaMalloc(&E->nrj, sizeof(double) * doff) == cudaSuccess &&
             cudaMalloc(&E->word, sizeof(unsigned long long) * nruns) == cudaSuccess &&
             cudaMalloc(&E->done, sizeof(unsigned int) * nruns) == cudaSuccess &&
-            cudaMalloc(&E->remaining, sizeof(int) * 2) == cudaSuccess;
+            cudaMalloc(&E->remaining, sizeof(int) * 2) == cudaSuccess &&
+            cudaMalloc(&E->lines, sizeof(EnsLine) * loff) == cudaSuccess &&
+            cudaMalloc(&E->lines11, sizeof(EnsLine11) * loff) == cudaSuccess;
   if (!ok) {
     cudaGetLastError();
     ens_free(E);
@@ -1149,6 +1174,12 @@ int vlp4d_ensemble_create(const vlp4d_ens_member *members, int nruns, int nsteps
     cudaGetLastError();
     ens_free(E);
     return fail_msg(VLP4D_ERR_CUDA, "ensemble upload failed");
+  }
+  k_ens_lines<<<nruns, 64>>>(E->runs, E->lines, E->lines11);
+  if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+    cudaGetLastError();
+    ens_free(E);
+    return fail_msg(VLP4D_ERR_CUDA, "ensemble line tables failed");
   }
   *out = E;
   return VLP4D_OK;
