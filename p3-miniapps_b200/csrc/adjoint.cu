@@ -203,9 +203,9 @@ __device__ __forceinline__ void cp_async_wait_groups() { asm volatile("cp.async.
 // The same sums with the vx taps shared: thread (cw, g) of a block owns
 // column ixy = blockIdx.x*CW + cw and the V consecutive output vx rows
 // g*V .. g*V+V-1 (blockDim = CW x nvx/V), so one input row costs V+5 loads
-// for V outputs.  The stencil sums run in the element type, the products
-// with lb and the accumulation in FP64.  Ring slot of row r: r mod 6,
-// static after unrolling by six.
+// for V outputs.  The stencil sums and the row's products with lb run in
+// the element type, the accumulation over rows in FP64.  Register ring of
+// the vx-swept rows: slot r mod 6, static after unrolling by six.
 //
 // Loads: each thread copies its own V+5 taps and V adjoint values of a row
 // into its private slots of a shared-memory ring of S rows with cp.async,
@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const 
                                                  int nvx, int nvy, int Q, StencilTable tvx, StencilTable tvy,
                                                  const double *__restrict__ dwx, const double *__restrict__ dwy,
                                                  double *__restrict__ part) {
-  static_assert(6 % S == 0, "ring slots are static after unrolling by six");
+  static_assert(S >= 2, "at least one row in flight");
   constexpr int NE = V + 5 + V;  // elements of one row per thread
   constexpr int D = S - 1;       // rows in flight ahead of the computed one
   extern __shared__ __align__(16) unsigned char vg_smem[];
@@ -263,11 +263,12 @@ __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const 
     T A[6][V], B[6][V];
     const int nrows = q + 5;
     int lrow = (ivy0 + my) % nvy;  // the a row of the next row to load
+    int wslot = 0, rslot = 0;      // ring slots of the next row to load / to compute
     // Row rr of the segment into ring slot rr mod S (an empty group past
     // the last row, so that every row has one commit group).
     auto issue = [&](int rr) {
       if (rr < nrows) {
-        T *dst = ring + (size_t)(rr % S) * NE * nth + tid;
+        T *dst = ring + (size_t)wslot * NE * nth + tid;
         const T *p = a + (long long)lrow * ystride + ixy;
 #pragma unroll
         for (int k = 0; k < V + 5; ++k) cp_async_small<sizeof(T)>(dst + k * nth, p + (long long)toff[k] * vstride);
@@ -278,6 +279,7 @@ __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const 
         }
         if (++lrow == nvy) lrow = 0;
       }
+      if (++wslot == S) wslot = 0;
       cp_async_commit_group();
     };
 #pragma unroll
@@ -290,7 +292,8 @@ __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const 
         // Rows up to r have landed (D groups committed after row r's).
         cp_async_wait_groups<D - 1>();
         issue(r + D);  // into slot (r + D) mod S = (r - 1) mod S, read a row ago
-        const T *src = ring + (size_t)(u % S) * NE * nth + tid;
+        const T *src = ring + (size_t)rslot * NE * nth + tid;
+        if (++rslot == S) rslot = 0;
         T t[V + 5];
 #pragma unroll
         for (int k = 0; k < V + 5; ++k) t[k] = src[k * nth];
@@ -306,6 +309,9 @@ __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const 
           B[u][i] = sb;
         }
         if (r >= 5) {
+          // The row's V products with lb summed in the element type, then
+          // added to the FP64 sums (two conversions per row, not 3V).
+          T px = 0, py = 0;
 #pragma unroll
           for (int i = 0; i < V; ++i) {
             const T l = src[(V + 5 + i) * nth];
@@ -315,9 +321,11 @@ __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const 
               sx = fma(wy[k], B[(u + 1 + k) % 6][i], sx);
               sy = fma(dy[k], A[(u + 1 + k) % 6][i], sy);
             }
-            gx = fma((double)l, (double)sx, gx);
-            gy = fma((double)l, (double)sy, gy);
+            px = fma(l, sx, px);
+            py = fma(l, sy, py);
           }
+          gx += (double)px;
+          gy += (double)py;
         }
       }
     }
@@ -338,15 +346,16 @@ __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const 
   }
 }
 
-// Ring rows of k_vgrad_v (two rows in flight; six spill registers in FP32),
-// and its shared memory.
-template <typename T>
+// Ring rows of k_vgrad_v: two rows in flight (three to five rows measured
+// no faster; V = 2 with five rows in flight slower, 72.8 against 63.1 us at
+// 64^4), and its shared memory.
+template <typename T, int V>
 constexpr int vgrad_slots() {
   return 3;
 }
 template <typename T, int V>
 size_t vgrad_smem(int nth, int gy, int cw) {
-  return sizeof(T) * vgrad_slots<T>() * (2 * V + 5) * (size_t)nth + sizeof(double) * 2 * gy * cw;
+  return sizeof(T) * vgrad_slots<T, V>() * (2 * V + 5) * (size_t)nth + sizeof(double) * 2 * gy * cw;
 }
 
 __global__ void k_vgrad_finish(const double *__restrict__ part, int nseg, int nxy, double *__restrict__ gex,
@@ -554,13 +563,13 @@ int launch_vgrad(vlp4d_adjoint *A, const void *a, const void *lb, cudaStream_t s
     ns = (nvy + Qv - 1) / Qv;
     dim3 gridv(bxv, ns), blockv(cw, gy);
     if (c->dtype == VLP4D_F64) {
-      auto kern = k_vgrad_v<double, 2, vgrad_slots<double>()>;
+      auto kern = k_vgrad_v<double, 2, vgrad_slots<double, 2>()>;
       const size_t sm = vgrad_smem<double, 2>(cw * gy, gy, cw);
       VLP4D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
       kern<<<gridv, blockv, sm, s>>>((const double *)a, (const double *)lb, nxy, nvx, nvy, Qv, c->tab_vx, c->tab_vy,
                                      A->dw_vx, A->dw_vy, A->gpart);
     } else {
-      auto kern = k_vgrad_v<float, 4, vgrad_slots<float>()>;
+      auto kern = k_vgrad_v<float, 4, vgrad_slots<float, 4>()>;
       const size_t sm = vgrad_smem<float, 4>(cw * gy, gy, cw);
       VLP4D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
       kern<<<gridv, blockv, sm, s>>>((const float *)a, (const float *)lb, nxy, nvx, nvy, Qv, c->tab_vx, c->tab_vy,
