@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const 
   const int G = blockDim.y;
   const int cw = threadIdx.x, g = threadIdx.y;
   const int nth = CW * G, tid = g * CW + cw;
-  T *ring = reinterpret_cast<T *>(vg_smem);                               // [S][NE][nth]
+  T *ring = reinterpret_cast<T *>(vg_smem);                               // [S][nth][NE]
   double *red = reinterpret_cast<double *>(vg_smem + sizeof(T) * S * NE * nth);  // [2][G][CW]
   const int ixy = blockIdx.x * CW + cw;
   const int seg = blockIdx.y;
@@ -248,38 +248,52 @@ __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const 
       wy[k] = (T)tvy.w[6 * (long long)ixy + k];
       dy[k] = (T)dwy[6 * (long long)ixy + k];
     }
-    int toff[V + 5];  // vx tap rows of this thread
+    // Element offsets within a vy row of this thread's vx tap rows
+    // (nvx * nxy < 2^31) and of its lb rows.
+    int toff[V + 5];
     {
       int j = vx0 + tvx.m[ixy];
       if (j >= nvx) j -= nvx;
 #pragma unroll
       for (int k = 0; k < V + 5; ++k) {
-        toff[k] = j;
+        toff[k] = j * nxy;
         if (++j == nvx) j = 0;
       }
     }
     const int my = tvy.m[ixy];
-    const T *lcol = lb + (long long)vx0 * vstride + ixy;
     T A[6][V], B[6][V];
     const int nrows = q + 5;
-    int lrow = (ivy0 + my) % nvy;  // the a row of the next row to load
-    int wslot = 0, rslot = 0;      // ring slots of the next row to load / to compute
-    // Row rr of the segment into ring slot rr mod S (an empty group past
-    // the last row, so that every row has one commit group).
+    // Running pointers: the a row of the next row to load (periodic in vy),
+    // the lb row it brings (from row 5 on), the ring slots of the next row
+    // to load and to compute.  The ring is [slot][thread][element]: element
+    // offsets are immediates, and the odd (FP32) or 18-word (FP64) thread
+    // stride keeps a warp's accesses on distinct banks.
+    int lrow = (ivy0 + my) % nvy;
+    const T *arow = a + (long long)lrow * ystride + ixy;
+    const T *lnext = lb + (long long)ivy0 * ystride + (long long)vx0 * vstride + ixy;
+    T *const ring0 = ring + (size_t)tid * NE;
+    const size_t slot_elems = (size_t)nth * NE;
+    T *wptr = ring0;
+    const T *rptr = ring0;
+    // Row rr of the segment into the next slot (an empty group past the
+    // last row, so that every row has one commit group).
     auto issue = [&](int rr) {
       if (rr < nrows) {
-        T *dst = ring + (size_t)wslot * NE * nth + tid;
-        const T *p = a + (long long)lrow * ystride + ixy;
 #pragma unroll
-        for (int k = 0; k < V + 5; ++k) cp_async_small<sizeof(T)>(dst + k * nth, p + (long long)toff[k] * vstride);
+        for (int k = 0; k < V + 5; ++k) cp_async_small<sizeof(T)>(wptr + k, arow + toff[k]);
         if (rr >= 5) {
-          const T *lp = lcol + (long long)(ivy0 + rr - 5) * ystride;
 #pragma unroll
-          for (int i = 0; i < V; ++i) cp_async_small<sizeof(T)>(dst + (V + 5 + i) * nth, lp + (long long)i * vstride);
+          for (int i = 0; i < V; ++i) cp_async_small<sizeof(T)>(wptr + V + 5 + i, lnext + i * nxy);
+          lnext += ystride;
         }
-        if (++lrow == nvy) lrow = 0;
+        if (++lrow == nvy) {
+          lrow = 0;
+          arow = a + ixy;
+        } else {
+          arow += ystride;
+        }
       }
-      if (++wslot == S) wslot = 0;
+      wptr = wptr + slot_elems == ring0 + S * slot_elems ? ring0 : wptr + slot_elems;
       cp_async_commit_group();
     };
 #pragma unroll
@@ -292,11 +306,11 @@ __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const 
         // Rows up to r have landed (D groups committed after row r's).
         cp_async_wait_groups<D - 1>();
         issue(r + D);  // into slot (r + D) mod S = (r - 1) mod S, read a row ago
-        const T *src = ring + (size_t)rslot * NE * nth + tid;
-        if (++rslot == S) rslot = 0;
+        const T *src = rptr;
+        rptr = rptr + slot_elems == ring0 + S * slot_elems ? ring0 : rptr + slot_elems;
         T t[V + 5];
 #pragma unroll
-        for (int k = 0; k < V + 5; ++k) t[k] = src[k * nth];
+        for (int k = 0; k < V + 5; ++k) t[k] = src[k];
 #pragma unroll
         for (int i = 0; i < V; ++i) {
           T sa = wx[0] * t[i], sb = dx[0] * t[i];
@@ -314,7 +328,7 @@ __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const 
           T px = 0, py = 0;
 #pragma unroll
           for (int i = 0; i < V; ++i) {
-            const T l = src[(V + 5 + i) * nth];
+            const T l = src[V + 5 + i];
             T sx = wy[0] * B[(u + 1) % 6][i], sy = dy[0] * A[(u + 1) % 6][i];
 #pragma unroll
             for (int k = 1; k < 6; ++k) {
