@@ -77,25 +77,38 @@ struct vlp4d_adjoint {
 namespace vlp4d {
 namespace {
 
-// Transposed v tables and the weight derivatives of one direction, from E.
-__global__ void k_build_vtable_adj(const double *__restrict__ e, int lines, double dt, double hmin, double hmax,
-                                   int n, int *__restrict__ m, double *__restrict__ w, float *__restrict__ wf,
-                                   double *__restrict__ dw) {
+// The v tables of one direction of a reverse step, from E: the forward
+// stencils (into the context's tables), the transposed ones and the weight
+// derivatives, from one line_stencil per line.  grid.y selects the
+// direction (vx, vy): one launch for all six tables.
+struct VtableAdjJob {
+  const double *e;
+  double hmin, hmax;
+  int n;
+  StencilTable fwd, adj;
+  double *dw;
+};
+__global__ void k_build_vtables_rev(VtableAdjJob jx, VtableAdjJob jy, int lines, double dt) {
   const int line = blockIdx.x * blockDim.x + threadIdx.x;
   if (line >= lines) return;
-  const LineStencil s = line_stencil(__dmul_rn(dt, e[line]), hmin, hmax, n);
-  const LineStencil t = adjoint_stencil(s, n);
-  m[line] = t.m;
-  float f[6];
-  weights_to_f32(t.w, f);
+  const VtableAdjJob &j = blockIdx.y ? jy : jx;
+  const LineStencil s = line_stencil(__dmul_rn(dt, j.e[line]), j.hmin, j.hmax, j.n);
+  const LineStencil t = adjoint_stencil(s, j.n);
+  float f[6], fa[6];
+  weights_to_f32(s.w, f);
+  weights_to_f32(t.w, fa);
+  j.fwd.m[line] = s.m;
+  j.adj.m[line] = t.m;
   double dc[6];
   lag_basis5_deriv(s.d, dc);
-  const double scale = -dt / ((hmax - hmin) / (double)n);
+  const double scale = -dt / ((j.hmax - j.hmin) / (double)j.n);
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
-    w[6 * line + k] = t.w[k];
-    wf[6 * line + k] = f[k];
-    dw[6 * line + k] = dc[k] * scale;
+    j.fwd.w[6 * line + k] = s.w[k];
+    j.fwd.wf[6 * line + k] = f[k];
+    j.adj.w[6 * line + k] = t.w[k];
+    j.adj.wf[6 * line + k] = fa[k];
+    j.dw[6 * line + k] = dc[k] * scale;
   }
 }
 
@@ -648,14 +661,13 @@ int reverse_core(vlp4d_adjoint *A, const void *a, const double *e, const void *l
     VLP4D_CUDA_TRY(cudaMemcpyAsync(c->ex, e, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
     VLP4D_CUDA_TRY(cudaMemcpyAsync(c->ey, e + n2, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
   }
-  if ((rc = build_v_tables(c, dt, true, true, s))) return rc;
+  if ((rc = alloc_table(c->tab_vx, lines)) || (rc = alloc_table(c->tab_vy, lines))) return rc;
   const int threads = 256, blocks = (lines + threads - 1) / threads;
-  k_build_vtable_adj<<<blocks, threads, 0, s>>>(c->ex, lines, dt, c->g.minp[2], c->g.maxp[2], c->g.n[2],
-                                                A->tab_vx_adj.m, A->tab_vx_adj.w, A->tab_vx_adj.wf, A->dw_vx);
+  const VtableAdjJob jx = {c->ex, c->g.minp[2], c->g.maxp[2], c->g.n[2], c->tab_vx, A->tab_vx_adj, A->dw_vx};
+  const VtableAdjJob jy = {c->ey, c->g.minp[3], c->g.maxp[3], c->g.n[3], c->tab_vy, A->tab_vy_adj, A->dw_vy};
+  k_build_vtables_rev<<<dim3((unsigned)blocks, 2u), threads, 0, s>>>(jx, jy, lines, dt);
   VLP4D_LAUNCH_CHECK();
-  k_build_vtable_adj<<<blocks, threads, 0, s>>>(c->ey, lines, dt, c->g.minp[3], c->g.maxp[3], c->g.n[3],
-                                                A->tab_vy_adj.m, A->tab_vy_adj.w, A->tab_vy_adj.wf, A->dw_vy);
-  VLP4D_LAUNCH_CHECK();
+  c->tab_vx.valid = c->tab_vy.valid = true;
   // dJ/dE, then dJ/drho.
   if ((rc = launch_vgrad(A, a, lb, s))) return rc;
   if ((rc = field_transpose(A, s))) return rc;
