@@ -8,6 +8,7 @@
 // Impl::Transpose (lib/Cuda_Transpose.hpp:18-136).
 #include "internal.cuh"
 #include "moment.cuh"
+#include "poisson.cuh"
 #include "tma.cuh"
 
 namespace vlp4d {
@@ -58,42 +59,20 @@ __global__ void k_analytic_field(double *__restrict__ ex, double *__restrict__ e
   }
 }
 
-// efield.cpp:68-99 with the filter of efield.cpp:27-33: for every (kx, ky)
-//   ex_hat = -i kx/k^2 rho_hat / (nx*ny), ey_hat = -i ky/k^2 rho_hat / (nx*ny),
-//   rho_hat = rho_hat / k^2 / (nx*ny);  ky = 0 uses filter(kx) (0 at kx = 0),
-//   ky takes the negative branch for ix2 >= ny/2+1.
+// efield.cpp:68-99: the mode-wise solve (poisson.cuh) of every mode of the
+// half spectrum, in place for phi_hat.
 __global__ void k_poisson_solve(cufftDoubleComplex *__restrict__ rho_hat, cufftDoubleComplex *__restrict__ ex_hat,
                                 cufftDoubleComplex *__restrict__ ey_hat, int nx1h, int nx2, double kx0,
                                 double ky0, double normcoeff) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nx1h * nx2) return;
   const int ix1 = i % nx1h, ix2 = i / nx1h;
-  const int nx2h = nx2 / 2 + 1;
-  const double kx = ix1 * kx0;
   const cufftDoubleComplex r = rho_hat[i];
-  cufftDoubleComplex e1, e2, r1;
-  if (ix2 == 0) {
-    const double filt = ix1 == 0 ? 0. : 1. / (kx * kx);
-    e1.x = __dmul_rn(__dmul_rn(__dmul_rn(kx, r.y), filt), normcoeff);
-    e1.y = __dmul_rn(__dmul_rn(__dmul_rn(-kx, r.x), filt), normcoeff);
-    e2.x = 0.;
-    e2.y = 0.;
-    r1.x = __dmul_rn(__dmul_rn(r.x, filt), normcoeff);
-    r1.y = __dmul_rn(__dmul_rn(r.y, filt), normcoeff);
-  } else {
-    const double ky = (ix2 < nx2h ? ix2 : ix2 - nx2) * ky0;
-    const double k2 = __dadd_rn(__dmul_rn(kx, kx), __dmul_rn(ky, ky));
-    const double cx = -(kx / k2), cy = -(ky / k2);
-    e1.x = __dmul_rn(-cx * r.y, normcoeff);
-    e1.y = __dmul_rn(cx * r.x, normcoeff);
-    e2.x = __dmul_rn(-cy * r.y, normcoeff);
-    e2.y = __dmul_rn(cy * r.x, normcoeff);
-    r1.x = __dmul_rn(r.x / k2, normcoeff);
-    r1.y = __dmul_rn(r.y / k2, normcoeff);
-  }
-  ex_hat[i] = e1;
-  ey_hat[i] = e2;
-  rho_hat[i] = r1;
+  double2 e1, e2, r1;
+  poisson_mode(ix1, ix2, nx2, make_double2(r.x, r.y), kx0, ky0, normcoeff, e1, e2, r1);
+  ex_hat[i] = make_cuDoubleComplex(e1.x, e1.y);
+  ey_hat[i] = make_cuDoubleComplex(e2.x, e2.y);
+  rho_hat[i] = make_cuDoubleComplex(r1.x, r1.y);
 }
 
 // ---- Diags::compute: Kahan-compensated FP64 sums of rho and |E|^2 in one
@@ -306,7 +285,10 @@ int launch_field_poisson(vlp4d_ctx *c, cudaStream_t s) {
     VLP4D_LAUNCH_CHECK();
     return VLP4D_OK;
   }
-  if (idcase == 10 || idcase == 20) {
+  // Cases 10 and 20 solve for rho - 1 (field.cpp:65-72).
+  const bool minus_one = idcase == 10 || idcase == 20;
+  if (field_cluster_available(c)) return launch_field_cluster(c, minus_one ? 1. : 0., s);
+  if (minus_one) {
     k_rho_minus_one<<<(unsigned)((n2 + threads - 1) / threads), threads, 0, s>>>(c->rho, n2);
     VLP4D_LAUNCH_CHECK();
   }

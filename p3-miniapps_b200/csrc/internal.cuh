@@ -93,6 +93,10 @@ struct vlp4d_ctx {
   cufftHandle plan_bwd3 = 0;
   size_t fstride = 0, hstride = 0;
   bool plans = false;
+  // The cluster field solve (k_field_cluster) instead of the cuFFT plans:
+  // -1 not yet decided, 0 no (shape, VLP4D_FIELD=cufft, or no cluster
+  // fits), else the cluster size (8 or 16).
+  int field_cluster = -1;
 
   // Diagnostics history (nbiter+1 entries each) and the reduction scratch.
   double *nrj = nullptr, *mass = nullptr;
@@ -246,6 +250,10 @@ bool xyxy_join(const vlp4d_ctx *ctx);
 int launch_field_rho(vlp4d_ctx *c, const void *fn, cudaStream_t s);
 int launch_rho_finish(vlp4d_ctx *c, int groups, cudaStream_t s);
 int launch_field_poisson(vlp4d_ctx *c, cudaStream_t s);
+// The cluster field solve (field_cluster.cu): whether it serves this
+// context, and its launch (rho - offset -> phi in rho, ex, ey).
+bool field_cluster_available(vlp4d_ctx *c);
+int launch_field_cluster(vlp4d_ctx *c, double offset, cudaStream_t s);
 int launch_diags(vlp4d_ctx *c, int iter, cudaStream_t s);
 // launch_diags on the context's side stream after the work queued on s so
 // far; diags_join makes s wait for it (before anything writes rho, Ex, Ey).
