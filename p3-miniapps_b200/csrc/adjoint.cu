@@ -213,6 +213,26 @@ __device__ __forceinline__ void cp_async_commit_group() { asm volatile("cp.async
 template <int N>
 __device__ __forceinline__ void cp_async_wait_groups() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+// Element pairs of k_vgrad_v: two independent sums advanced by one packed
+// instruction in FP32 (fma.rn.f32x2 / mul.rn.f32x2: per-lane results equal
+// to the scalar fmaf / multiply), component-wise in FP64.
+template <typename T>
+struct VgPair;
+template <>
+struct VgPair<float> {
+  using P = float2;
+  static __device__ __forceinline__ P mk(float a, float b) { return make_float2(a, b); }
+  static __device__ __forceinline__ P mul(P a, P b) { return __fmul2_rn(a, b); }
+  static __device__ __forceinline__ P fma2(P a, P b, P c) { return __ffma2_rn(a, b, c); }
+};
+template <>
+struct VgPair<double> {
+  using P = double2;
+  static __device__ __forceinline__ P mk(double a, double b) { return make_double2(a, b); }
+  static __device__ __forceinline__ P mul(P a, P b) { return make_double2(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)); }
+  static __device__ __forceinline__ P fma2(P a, P b, P c) { return make_double2(fma(a.x, b.x, c.x), fma(a.y, b.y, c.y)); }
+};
+
 // The same sums with the vx taps shared: thread (cw, g) of a block owns
 // column ixy = blockIdx.x*CW + cw and the V consecutive output vx rows
 // g*V .. g*V+V-1 (blockDim = CW x nvx/V), so one input row costs V+5 loads
@@ -253,13 +273,15 @@ __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const 
     // Stencil sums in the element type (FP32 sums of FP32 data are
     // accurate to ~1e-7 for a gradient); products with lb and the
     // accumulation in FP64.
-    T wx[6], dx[6], wy[6], dy[6];
+    // Weight pairs: (dwx, wx) for the vx sums (B, A) of a row, (wy, dwy) for
+    // the vy sums (sx, sy) = (sum wy B, sum dwy A).
+    using VP = VgPair<T>;
+    using P = typename VP::P;
+    P wdx[6], wdy[6];
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-      wx[k] = (T)tvx.w[6 * (long long)ixy + k];
-      dx[k] = (T)dwx[6 * (long long)ixy + k];
-      wy[k] = (T)tvy.w[6 * (long long)ixy + k];
-      dy[k] = (T)dwy[6 * (long long)ixy + k];
+      wdx[k] = VP::mk((T)dwx[6 * (long long)ixy + k], (T)tvx.w[6 * (long long)ixy + k]);
+      wdy[k] = VP::mk((T)tvy.w[6 * (long long)ixy + k], (T)dwy[6 * (long long)ixy + k]);
     }
     // Element offsets within a vy row of this thread's vx tap rows
     // (nvx * nxy < 2^31) and of its lb rows.
@@ -274,7 +296,7 @@ __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const 
       }
     }
     const int my = tvy.m[ixy];
-    T A[6][V], B[6][V];
+    P BA[6][V];  // ring of the vx-swept rows: (B, A) = (sum dwx t, sum wx t)
     const int nrows = q + 5;
     // Running pointers: the a row of the next row to load (periodic in vy),
     // the lb row it brings (from row 5 on), the ring slots of the next row
@@ -326,33 +348,25 @@ __global__ void __launch_bounds__(512) k_vgrad_v(const T *__restrict__ a, const 
         for (int k = 0; k < V + 5; ++k) t[k] = src[k];
 #pragma unroll
         for (int i = 0; i < V; ++i) {
-          T sa = wx[0] * t[i], sb = dx[0] * t[i];
+          P ba = VP::mul(wdx[0], VP::mk(t[i], t[i]));
 #pragma unroll
-          for (int k = 1; k < 6; ++k) {
-            sa = fma(wx[k], t[i + k], sa);
-            sb = fma(dx[k], t[i + k], sb);
-          }
-          A[u][i] = sa;
-          B[u][i] = sb;
+          for (int k = 1; k < 6; ++k) ba = VP::fma2(wdx[k], VP::mk(t[i + k], t[i + k]), ba);
+          BA[u][i] = ba;
         }
         if (r >= 5) {
           // The row's V products with lb summed in the element type, then
           // added to the FP64 sums (two conversions per row, not 3V).
-          T px = 0, py = 0;
+          P pxy = VP::mk(0, 0);
 #pragma unroll
           for (int i = 0; i < V; ++i) {
             const T l = src[V + 5 + i];
-            T sx = wy[0] * B[(u + 1) % 6][i], sy = dy[0] * A[(u + 1) % 6][i];
+            P sxy = VP::mul(wdy[0], BA[(u + 1) % 6][i]);
 #pragma unroll
-            for (int k = 1; k < 6; ++k) {
-              sx = fma(wy[k], B[(u + 1 + k) % 6][i], sx);
-              sy = fma(dy[k], A[(u + 1 + k) % 6][i], sy);
-            }
-            px = fma(l, sx, px);
-            py = fma(l, sy, py);
+            for (int k = 1; k < 6; ++k) sxy = VP::fma2(wdy[k], BA[(u + 1 + k) % 6][i], sxy);
+            pxy = VP::fma2(VP::mk(l, l), sxy, pxy);
           }
-          gx += (double)px;
-          gy += (double)py;
+          gx += (double)pxy.x;
+          gy += (double)pxy.y;
         }
       }
     }
