@@ -60,7 +60,7 @@ def parse_args(argv=None):
                          "point (--stage, --dtype, --n; --steps calls after one field solve), one JSON line")
     ap.add_argument("--stage", default="advect_xyxy",
                     choices=["advect_x", "advect_y", "advect_vx", "advect_vy", "advect_xy", "advect_vxvy",
-                             "advect_xyxy", "field_rho"], help="stage entry point for --case stage")
+                             "advect_xyxy", "field_rho", "field_poisson"], help="stage entry point for --case stage")
     ap.add_argument("--dtype", choices=["f32", "f64"], default="f32", help="storage for --case stage")
     ap.add_argument("--members", type=int, default=256, help="ensemble members for --case ensemble")
     ap.add_argument("--replicas", action="store_true",
@@ -494,11 +494,19 @@ def stage_arm(pkg, torch, stream, stage, dtype, n, calls):
         ctx.field_poisson()
         fn = getattr(ctx, stage)
         dt = DT if stage in ("advect_vx", "advect_vy", "advect_vxvy") else 0.5 * DT
-        call = (lambda: fn(a)) if stage == "field_rho" else (lambda: fn(a, b, dt))
+        if stage == "field_poisson":
+            call = fn
+        elif stage == "field_rho":
+            call = lambda: fn(a)
+        else:
+            call = lambda: fn(a, b, dt)
         t = time_calls(torch, stream, call, max(calls, 1))
         ctx.check()
     elem = 4 if dtype == "f32" else 8
-    moved = (1 if stage == "field_rho" else 2) * dom.cells * elem
+    if stage == "field_poisson":  # rho in; phi, Ex, Ey out (FP64 planes)
+        moved = 4 * n * n * 8
+    else:
+        moved = (1 if stage == "field_rho" else 2) * dom.cells * elem
     return {"stage": stage, "dtype": dtype, "grid": [n] * 4, "calls": calls, "ms": t * 1e3,
             "gbs": moved / t / 1e9}
 
