@@ -766,7 +766,8 @@ __global__ void __launch_bounds__(512) k_plane_xyxy64(PlaneArgs a) {
   const int cg = threadIdx.x % ncg;
   const int rg = threadIdx.x / ncg;
   const int RG = blockDim.x / ncg;  // row groups; R == RG * RT
-  const int c0 = cg * 4;
+  const int c0 = cg * 4;  // X11: the column quad c0 .. c0+3
+  const int yc = cg * 2;  // Y11 and the moment: columns yc, yc+1 and yc+nx/2, yc+nx/2+1
   const int r0 = rg * RT;
   const int chunk = blockIdx.x % a.cpp;
   const int G = gridDim.x / a.cpp;
@@ -867,15 +868,24 @@ __global__ void __launch_bounds__(512) k_plane_xyxy64(PlaneArgs a) {
       return;
     }
     if (threadIdx.x == 0 && it > 0 && it - 1 + S < n_items) issue(it - 1 + S);
-    {  // Y11 of rows r0 .. r0+RT-1, quad c0, streamed down the slot.
+    {  // Y11 of rows r0 .. r0+RT-1, columns yc, yc+1, yc+nx/2, yc+nx/2+1,
+       // streamed down the slot (16-byte accesses, consecutive across the
+       // lanes: no bank conflicts).
       W11<T> wy;
       read_line11(yrec[ivy], wy);
-      const T *src = in + (size_t)r0 * nx + c0;
+      const T *src = in + (size_t)r0 * nx + yc;
       T acc[RT][4];
 #pragma unroll
       for (int j = 0; j < RT + 10; ++j) {
         T y[4];
-        load4(src + (size_t)j * nx, y);
+        {
+          const double2 lo = *reinterpret_cast<const double2 *>(src + (size_t)j * nx);
+          const double2 hi = *reinterpret_cast<const double2 *>(src + (size_t)j * nx + nx / 2);
+          y[0] = lo.x;
+          y[1] = lo.y;
+          y[2] = hi.x;
+          y[3] = hi.y;
+        }
 #pragma unroll
         for (int i = 0; i < RT; ++i) {
           const int k = j - i;
@@ -885,7 +895,9 @@ __global__ void __launch_bounds__(512) k_plane_xyxy64(PlaneArgs a) {
         }
         if (j >= 10) {
           const int i = j - 10;
-          store4(outp + (size_t)(r0 + i) * nx + c0, acc[i]);
+          T *orow = outp + (size_t)(r0 + i) * nx + yc;
+          *reinterpret_cast<double2 *>(orow) = make_double2(acc[i][0], acc[i][1]);
+          *reinterpret_cast<double2 *>(orow + nx / 2) = make_double2(acc[i][2], acc[i][3]);
           if constexpr (RHO) {
 #pragma unroll
             for (int q = 0; q < 4; ++q) racc[i][q] += acc[i][q];
@@ -905,11 +917,11 @@ __global__ void __launch_bounds__(512) k_plane_xyxy64(PlaneArgs a) {
     }
   }
   if constexpr (RHO) {
-    double *rdst = a.rho_part + (long long)g * plane_elems + ((long long)chunk * R + r0) * nx + c0;
+    double *rdst = a.rho_part + (long long)g * plane_elems + ((long long)chunk * R + r0) * nx + yc;
 #pragma unroll
     for (int i = 0; i < RT; ++i) {
-      reinterpret_cast<double2 *>(rdst + (size_t)i * nx)[0] = make_double2(racc[i][0], racc[i][1]);
-      reinterpret_cast<double2 *>(rdst + (size_t)i * nx)[1] = make_double2(racc[i][2], racc[i][3]);
+      *reinterpret_cast<double2 *>(rdst + (size_t)i * nx) = make_double2(racc[i][0], racc[i][1]);
+      *reinterpret_cast<double2 *>(rdst + (size_t)i * nx + nx / 2) = make_double2(racc[i][2], racc[i][3]);
     }
   }
 }
