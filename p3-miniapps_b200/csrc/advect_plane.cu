@@ -748,6 +748,36 @@ __global__ void __launch_bounds__(512) k_plane_xyxy(PlaneArgs a) {
 // read until Y11(it) ends, so it is refilled at the barrier of item it + 1
 // (two stages keep two CTAs per SM at 128^4).  Weights plain (FP64 sums
 // w * w of the per-line Lagrange weights, as k_plane_xyxy<double>).
+// X11 of the output pair (c, c + 1) of an FP64 row, from the fourteen
+// values at the even column a0 = (c + mx) - r, a0 + 1, ... (periodic; the
+// row width is even): output q uses t[r+q .. r+q+10], each computed as
+// x11_from<double> computes it.
+template <int R_>
+__device__ __forceinline__ void x11_pair_from(const double (&t)[14], const W11<double> &w, double (&o)[2]) {
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    double acc = w.w[0] * t[R_ + q];
+#pragma unroll
+    for (int k = 1; k < 11; ++k) acc = fma(w.w[k], t[R_ + q + k], acc);
+    o[q] = acc;
+  }
+}
+__device__ __forceinline__ void x11_pair_row(const double *row, int a0, int nx, int r, const W11<double> &w,
+                                             double (&o)[2]) {
+  double t[14];
+  int c = a0;
+#pragma unroll
+  for (int j = 0; j < 7; ++j) {
+    const double2 v = *reinterpret_cast<const double2 *>(row + c);
+    t[2 * j] = v.x;
+    t[2 * j + 1] = v.y;
+    c += 2;
+    if (c >= nx) c -= nx;
+  }
+  if (r) x11_pair_from<1>(t, w, o);
+  else x11_pair_from<0>(t, w, o);
+}
+
 template <int NX, int RT, bool RHO = true>
 __global__ void __launch_bounds__(512) k_plane_xyxy64(PlaneArgs a) {
   using T = double;
@@ -827,35 +857,27 @@ __global__ void __launch_bounds__(512) k_plane_xyxy64(PlaneArgs a) {
     const long long p = g + it * G;
     T *in = slots + (size_t)slot * slot_elems;
     T *outp = static_cast<T *>(a.fout) + p * plane_elems + (long long)chunk * R * nx;
-    {  // X11 in place on the staged rows rg, rg + RG, ... (this warp's rows).
+    {  // X11 in place on the staged rows rg, rg + RG, ... (this warp's rows),
+       // output pairs at columns yc and yc + nx/2 (16-byte accesses,
+       // consecutive across the lanes).
       W11<T> wx;
-      int base = c0 + read_line11(xrec[ivx], wx);
-      base = base % nx;
-      const int rr = base & 3;
-      int o[5];
-      o[0] = base - rr;
-#pragma unroll
-      for (int k = 1; k < 5; ++k) {
-        o[k] = o[k - 1] + 4;
-        if (o[k] >= nx) o[k] -= nx;
-      }
+      int ba = (yc + read_line11(xrec[ivx], wx)) % nx;  // first tap of the pair at yc
+      const int rr = ba & 1;                            // the same for both pairs (nx/2 is even)
+      ba -= rr;
+      const int bb = ba + nx / 2 >= nx ? ba - nx / 2 : ba + nx / 2;
       for (int k = 0; k < trips; ++k) {
         const int v = rg + k * RG;
         T *row = in + (size_t)v * nx;
-        T t[20], q4[4], out[4];
+        T outa[2], outb[2];
         if (v < vrows) {
-#pragma unroll
-          for (int j = 0; j < 5; ++j) {
-            load4(row + o[j], q4);
-            t[4 * j] = q4[0];
-            t[4 * j + 1] = q4[1];
-            t[4 * j + 2] = q4[2];
-            t[4 * j + 3] = q4[3];
-          }
-          sweep_x11(t, rr, wx, out);
+          x11_pair_row(row, ba, nx, rr, wx, outa);
+          x11_pair_row(row, bb, nx, rr, wx, outb);
         }
         __syncwarp(wmask);  // every lane has read the row
-        if (v < vrows) store4(row + c0, out);
+        if (v < vrows) {
+          *reinterpret_cast<double2 *>(row + yc) = make_double2(outa[0], outa[1]);
+          *reinterpret_cast<double2 *>(row + yc + nx / 2) = make_double2(outb[0], outb[1]);
+        }
       }
       // These generic writes precede the slot's next bulk copy.
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
