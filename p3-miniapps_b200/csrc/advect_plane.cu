@@ -147,6 +147,55 @@ __device__ __noinline__ void plane_abort(const PlaneArgs &a, uint64_t *bars, lon
 // of item it - 1 is refilled at the barrier of item it (one item later than
 // with the separate tile).  Without the two x-swept tiles an FP64 pass at
 // 128^4 fits two CTAs per SM.
+// FP64 pair mapping of k_plane.  x6_pair_row: the x-swept outputs (c, c + 1)
+// of a row from the eight values at the even column a0 = (c + mx) - r, a0
+// + 1, ... (periodic; the row width is even); output q uses t[r+q ..
+// r+q+5], computed as x4_from<double> computes it.  sweep_y_pairs: phase Y
+// of the columns (c, c + 1, c + h, c + h + 1) from RT + 5 rows, each output
+// as sweep_y<double> computes it.
+template <int R_>
+__device__ __forceinline__ void x6_pair_from(const double (&t)[8], const SweepW<double> &w, double (&o)[2]) {
+#pragma unroll
+  for (int q = 0; q < 2; ++q)
+    o[q] = interp6(w.w, t[R_ + q], t[R_ + q + 1], t[R_ + q + 2], t[R_ + q + 3], t[R_ + q + 4], t[R_ + q + 5]);
+}
+__device__ __forceinline__ void x6_pair_row(const double *row, int a0, int nx, int r, const SweepW<double> &w,
+                                            double (&o)[2]) {
+  double t[8];
+  int c = a0;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const double2 v = *reinterpret_cast<const double2 *>(row + c);
+    t[2 * j] = v.x;
+    t[2 * j + 1] = v.y;
+    c += 2;
+    if (c >= nx) c -= nx;
+  }
+  if (r) x6_pair_from<1>(t, w, o);
+  else x6_pair_from<0>(t, w, o);
+}
+template <int RT, typename Emit>
+__device__ __forceinline__ void sweep_y_pairs(const double *src, int nx, int h, const SweepW<double> &w, Emit emit) {
+  double y[RT + 5][4];
+#pragma unroll
+  for (int j = 0; j < RT + 5; ++j) {
+    const double2 lo = *reinterpret_cast<const double2 *>(src + (size_t)j * nx);
+    const double2 hi = *reinterpret_cast<const double2 *>(src + (size_t)j * nx + h);
+    y[j][0] = lo.x;
+    y[j][1] = lo.y;
+    y[j][2] = hi.x;
+    y[j][3] = hi.y;
+    if (j >= 5) {
+      const int i = j - 5;
+      double o[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        o[q] = interp6(w.w, y[i][q], y[i + 1][q], y[i + 2][q], y[i + 3][q], y[i + 4][q], y[j][q]);
+      emit(i, o);
+    }
+  }
+}
+
 // Thread t owns column quad c0 = 4*(t % (nx/4)) and row group t / (nx/4)
 // for the whole kernel; blockDim = (nx/4) * (R/RT).
 template <typename T, int NX, int RT, bool DX, bool DY, bool RHO, bool INPLACE = false>
@@ -171,6 +220,13 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
   const int rg = threadIdx.x / ncg;
   const int RG = blockDim.x / ncg;  // row groups; R == RG * RT
   const int c0 = cg * 4;
+  // FP64: the thread's four columns are the pairs (yc, yc + 1) and
+  // (yc + nx/2, yc + nx/2 + 1), so that a warp's 16-byte shared-memory
+  // accesses are consecutive (a quad of doubles per lane would put two
+  // lanes of each quarter-warp phase on the same banks).
+  constexpr bool PAIRS = sizeof(T) == 8;
+  const int yc = cg * 2;
+  const int hx = nx >> 1;
   const int r0 = rg * RT;
 
   const int chunk = blockIdx.x % a.cpp;
@@ -234,13 +290,47 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
 
     if (DX) {  // Phase X: staged rows rg, rg+RG, ...; this thread's column quad.
       T wl[6];
-      int base = c0 + read_line(xrec[ivx], wl);
+      const int mx = read_line(xrec[ivx], wl);
+      int base = c0 + mx;
       SweepW<T> wx;
       make_sweep_w(wl, wx);
       base = wrap_col<NX>(base, nx);
       const int rr = base & 3;
       const int o0 = base - rr, o1 = wrap_col<NX>(o0 + 4, nx), o2 = wrap_col<NX>(o0 + 8, nx);
-      if constexpr (INPLACE) {
+      // Pair mapping: the tap windows of the pairs at yc and yc + nx/2
+      // start at the even columns pa and pb, offset pr within them.
+      int pa = wrap_col<NX>(yc + mx, nx);
+      const int pr = pa & 1;
+      pa -= pr;
+      const int pb = pa + hx >= nx ? pa - hx : pa + hx;
+      if constexpr (PAIRS) {
+        const int rgw = (int)((threadIdx.x & ~31u) / (unsigned)ncg);
+        const int trips = INPLACE ? (vrows - rgw + RG - 1) / RG : 0;
+        const unsigned wlane = blockDim.x - (threadIdx.x & ~31u);
+        const unsigned wmask = wlane >= 32 ? 0xffffffffu : (1u << wlane) - 1u;
+        const int nv = INPLACE ? trips : (vrows - rg + RG - 1) / RG;
+        for (int k = 0; k < nv; ++k) {
+          const int v = rg + k * RG;
+          T *row = const_cast<T *>(in) + (size_t)v * nx;
+          double oa[2], ob[2];
+          if (v < vrows) {
+            x6_pair_row(row, pa, nx, pr, wx, oa);
+            x6_pair_row(row, pb, nx, pr, wx, ob);
+          }
+          T *dst;
+          if constexpr (INPLACE) {
+            __syncwarp(wmask);  // the row is read by all its lanes
+            dst = row;
+          } else {
+            dst = (DY ? xs : outp) + (size_t)v * nx;
+          }
+          if (v < vrows) {
+            *reinterpret_cast<double2 *>(dst + yc) = make_double2(oa[0], oa[1]);
+            *reinterpret_cast<double2 *>(dst + yc + hx) = make_double2(ob[0], ob[1]);
+          }
+        }
+        if constexpr (INPLACE) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      } else if constexpr (INPLACE) {
         // Trip count of the warp's first row group, so that every lane
         // reaches each __syncwarp.
         const int rgw = (int)((threadIdx.x & ~31u) / (unsigned)ncg);
@@ -310,15 +400,28 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
       read_line(yrec[ivy], wl);
       SweepW<T> wy;
       make_sweep_w(wl, wy);
-      const T *src = ((DX && !INPLACE) ? xs : in) + (size_t)r0 * nx + c0;
-      T *dst = outp + (size_t)r0 * nx + c0;
-      sweep_y<RT>(src, nx, wy, [&](int i, const T (&o)[4]) {
-        store4(dst + (size_t)i * nx, o);
-        if (RHO) {
+      if constexpr (PAIRS) {
+        const double *src = ((DX && !INPLACE) ? xs : in) + (size_t)r0 * nx + yc;
+        T *dst = outp + (size_t)r0 * nx + yc;
+        sweep_y_pairs<RT>(src, nx, hx, wy, [&](int i, const double (&o)[4]) {
+          *reinterpret_cast<double2 *>(dst + (size_t)i * nx) = make_double2(o[0], o[1]);
+          *reinterpret_cast<double2 *>(dst + (size_t)i * nx + hx) = make_double2(o[2], o[3]);
+          if (RHO) {
 #pragma unroll
-          for (int q = 0; q < 4; ++q) racc[i][q] += (double)o[q];
-        }
-      });
+            for (int q = 0; q < 4; ++q) racc[i][q] += o[q];
+          }
+        });
+      } else {
+        const T *src = ((DX && !INPLACE) ? xs : in) + (size_t)r0 * nx + c0;
+        T *dst = outp + (size_t)r0 * nx + c0;
+        sweep_y<RT>(src, nx, wy, [&](int i, const T (&o)[4]) {
+          store4(dst + (size_t)i * nx, o);
+          if (RHO) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) racc[i][q] += (double)o[q];
+          }
+        });
+      }
     }
     ivx += gdx;
     ivy += gdy;
@@ -339,11 +442,12 @@ __global__ void __launch_bounds__(512) k_plane(PlaneArgs a) {
     if (threadIdx.x == 0 && it + S < n_items) issue(it + S);
   }
   if (RHO) {
-    double *dst = a.rho_part + (long long)g * plane_elems + ((long long)chunk * R + r0) * nx + c0;
+    double *dst = a.rho_part + (long long)g * plane_elems + ((long long)chunk * R + r0) * nx + (PAIRS ? yc : c0);
+    const int second = PAIRS ? hx : 2;  // element offset of the second double pair
 #pragma unroll
     for (int i = 0; i < RT; ++i) {
-      reinterpret_cast<double2 *>(dst + (size_t)i * nx)[0] = make_double2(racc[i][0], racc[i][1]);
-      reinterpret_cast<double2 *>(dst + (size_t)i * nx)[1] = make_double2(racc[i][2], racc[i][3]);
+      *reinterpret_cast<double2 *>(dst + (size_t)i * nx) = make_double2(racc[i][0], racc[i][1]);
+      *reinterpret_cast<double2 *>(dst + (size_t)i * nx + second) = make_double2(racc[i][2], racc[i][3]);
     }
   }
 }
