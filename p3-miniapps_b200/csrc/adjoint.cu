@@ -549,6 +549,8 @@ int field_transpose(vlp4d_adjoint *A, cudaStream_t s) {
     VLP4D_CUDA_TRY(cudaMemsetAsync(A->lam_rho, 0, sizeof(double) * c->g.nxy(), s));
     return VLP4D_OK;
   }
+  if (field_cluster_t_available(c))
+    return launch_field_transpose_cluster(c, A->gex, A->gey, A->hx_hat, A->hy_hat, A->lam_rho, s);
   VLP4D_CUFFT_TRY(cufftSetStream(A->plan_g2, s));
   VLP4D_CUFFT_TRY(cufftSetStream(c->plan_bwd, s));
   VLP4D_CUFFT_TRY(cufftExecD2Z(A->plan_g2, A->gex, c->ex_hat));  // gex, gey -> ex_hat, ey_hat

@@ -257,6 +257,109 @@ __global__ void __launch_bounds__(kFieldThreads) k_field_cluster(FieldArgs a) {
   cluster_barrier();
 }
 
+
+// The transpose of the field solve (the reverse mode's lam_rho = D^T (gex,
+// gey)), with the same decomposition: rows of gex and gey along x; --
+// cluster barrier --; own columns of both along y, the mode-wise
+// lam_hat = (conj(hx_hat) gx_hat + conj(hy_hat) gy_hat) / (nx*ny) with the
+// impulse-response spectra hx_hat, hy_hat (half-spectrum layout of the
+// forward D2Z, ky * (nx/2+1) + kx), the inverse along y; -- cluster barrier
+// --; own rows of lam_hat: Hermitian extension, inverse along x, real part
+// into lam_rho; -- cluster barrier --.
+struct FieldTArgs {
+  const double *gex, *gey;
+  const double2 *hx, *hy;
+  double *lam;
+  int nx, ny;
+  double norm;
+};
+
+// Shared memory of k_field_cluster_t: four row buffers (gex and gey rows
+// and their pass partners), four column buffers, the twiddles.
+__host__ __device__ inline size_t field_t_bytes(int nx, int ny, int ctas) {
+  const FieldSmem L(nx, ny, ctas);
+  return sizeof(double2) * (4 * L.rows_elems + 4 * (size_t)L.Kc * ny + nx + ny);
+}
+
+template <int kFieldCtas>
+__global__ void __launch_bounds__(kFieldThreads) k_field_cluster_t(FieldTArgs a) {
+  extern __shared__ __align__(16) unsigned char fsm[];
+  const int nx = a.nx, ny = a.ny, nxh = nx / 2 + 1;
+  const FieldSmem L(nx, ny, kFieldCtas);
+  const int R = L.R, Kc = L.Kc;
+  const size_t ce = (size_t)Kc * ny;
+  double2 *rx = reinterpret_cast<double2 *>(fsm);
+  double2 *rxt = rx + L.rows_elems;
+  double2 *ry = rxt + L.rows_elems;
+  double2 *ryt = ry + L.rows_elems;
+  double2 *cx = ryt + L.rows_elems;
+  double2 *cxt = cx + ce;
+  double2 *cy = cxt + ce;
+  double2 *cyt = cy + ce;
+  double2 *twx = cyt + ce;
+  double2 *twy = twx + nx;
+  const unsigned c = cluster_rank();
+  for (int m = threadIdx.x; m < nx; m += blockDim.x) {
+    double sn, cs;
+    sincospi(2.0 * m / nx, &sn, &cs);
+    twx[m] = make_double2(cs, sn);
+  }
+  for (int m = threadIdx.x; m < ny; m += blockDim.x) {
+    double sn, cs;
+    sincospi(2.0 * m / ny, &sn, &cs);
+    twy[m] = make_double2(cs, sn);
+  }
+  const int iy0 = (int)c * R;
+  for (int i = threadIdx.x; i < R * nx; i += blockDim.x) {
+    rx[i] = make_double2(a.gex[(size_t)iy0 * nx + i], 0.);
+    ry[i] = make_double2(a.gey[(size_t)iy0 * nx + i], 0.);
+  }
+  __syncthreads();
+  const double2 *rowsx = line_dft(rx, rxt, R, nx, twx, false);
+  const double2 *rowsy = line_dft(ry, ryt, R, nx, twx, false);
+  cluster_barrier();
+  int nq = 0;
+  for (int kx = (int)c; kx < nxh; kx += kFieldCtas) ++nq;
+  for (int i = threadIdx.x; i < nq * ny; i += blockDim.x) {
+    const int q = i / ny, iy = i - q * ny;
+    const int kx = (int)c + q * kFieldCtas;
+    const size_t off = (size_t)(iy % R) * nx + kx;
+    const unsigned owner = (unsigned)(iy / R);
+    cx[i] = ld_cluster(rowsx + off, owner);
+    cy[i] = ld_cluster(rowsy + off, owner);
+  }
+  __syncthreads();
+  const double2 *gxh = line_dft(cx, cxt, nq, ny, twy, false);
+  const double2 *gyh = line_dft(cy, cyt, nq, ny, twy, false);
+  // lam_hat of the own columns into a buffer neither spectrum occupies.
+  double2 *lam = gxh == cx ? cxt : cx;
+  double2 *lamt = gyh == cy ? cyt : cy;
+  for (int i = threadIdx.x; i < nq * ny; i += blockDim.x) {
+    const int q = i / ny, iy = i - q * ny;
+    const int kx = (int)c + q * kFieldCtas;
+    const double2 g1 = gxh[i], g2 = gyh[i];
+    const double2 p = a.hx[(size_t)iy * nxh + kx], r = a.hy[(size_t)iy * nxh + kx];
+    lam[i] = make_double2((p.x * g1.x + p.y * g1.y + r.x * g2.x + r.y * g2.y) * a.norm,
+                          (p.x * g1.y - p.y * g1.x + r.x * g2.y - r.y * g2.x) * a.norm);
+  }
+  __syncthreads();
+  const double2 *cols = line_dft(lam, lamt, nq, ny, twy, true);
+  cluster_barrier();
+  for (int i = threadIdx.x; i < R * nxh; i += blockDim.x) {
+    const int r = i / nxh, kx = i - r * nxh;
+    rx[(size_t)r * nx + kx] = ld_cluster(cols + (size_t)(kx / kFieldCtas) * ny + iy0 + r, (unsigned)(kx % kFieldCtas));
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < R * (nx - nxh); i += blockDim.x) {
+    const int r = i / (nx - nxh), kx = nxh + (i - r * (nx - nxh));
+    const double2 v = rx[(size_t)r * nx + (nx - kx)];
+    rx[(size_t)r * nx + kx] = make_double2(v.x, -v.y);
+  }
+  __syncthreads();
+  const double2 *out = line_dft(rx, rxt, R, nx, twx, true);
+  for (int i = threadIdx.x; i < R * nx; i += blockDim.x) a.lam[(size_t)iy0 * nx + i] = out[i].x;
+  cluster_barrier();
+}
 }  // namespace
 
 namespace {
@@ -309,6 +412,56 @@ bool field_cluster_available(vlp4d_ctx *c) {
   if (want == 16 && cluster_fits<16>(nx, ny)) c->field_cluster = 16;
   else if (cluster_fits<8>(nx, ny)) c->field_cluster = 8;
   return c->field_cluster > 0;
+}
+
+// The transposed solve on the cluster size the forward solve uses; false
+// (cuFFT path) if it does not fit.
+bool field_cluster_t_available(vlp4d_ctx *c) {
+  if (!field_cluster_available(c)) return false;
+  if (c->field_cluster_t >= 0) return c->field_cluster_t > 0;
+  c->field_cluster_t = 0;
+  const int nx = c->g.n[0], ny = c->g.n[1], C = c->field_cluster;
+  const size_t smem = field_t_bytes(nx, ny, C);
+  cudaError_t e = C == 16 ? cudaFuncSetAttribute(k_field_cluster_t<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                          : cudaFuncSetAttribute(k_field_cluster_t<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess && C == 16)
+    e = cudaFuncSetAttribute(k_field_cluster_t<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  cudaLaunchAttribute attr;
+  cudaLaunchConfig_t cfg = field_config(nx, ny, C, &attr, 0);
+  cfg.dynamicSmemBytes = smem;
+  int clusters = 0;
+  e = C == 16 ? cudaOccupancyMaxActiveClusters(&clusters, k_field_cluster_t<16>, &cfg)
+              : cudaOccupancyMaxActiveClusters(&clusters, k_field_cluster_t<8>, &cfg);
+  if (e != cudaSuccess || clusters < 1) {
+    cudaGetLastError();
+    return false;
+  }
+  c->field_cluster_t = 1;
+  return true;
+}
+
+int launch_field_transpose_cluster(vlp4d_ctx *c, const double *gex, const double *gey, const void *hx_hat,
+                                   const void *hy_hat, double *lam_rho, cudaStream_t s) {
+  const int nx = c->g.n[0], ny = c->g.n[1];
+  FieldTArgs a;
+  a.gex = gex;
+  a.gey = gey;
+  a.hx = static_cast<const double2 *>(hx_hat);
+  a.hy = static_cast<const double2 *>(hy_hat);
+  a.lam = lam_rho;
+  a.nx = nx;
+  a.ny = ny;
+  a.norm = 1.0 / ((double)nx * ny);
+  cudaLaunchAttribute attr;
+  cudaLaunchConfig_t cfg = field_config(nx, ny, c->field_cluster, &attr, s);
+  cfg.dynamicSmemBytes = field_t_bytes(nx, ny, c->field_cluster);
+  if (c->field_cluster == 16) VLP4D_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_field_cluster_t<16>, a));
+  else VLP4D_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_field_cluster_t<8>, a));
+  return VLP4D_OK;
 }
 
 int launch_field_cluster(vlp4d_ctx *c, double offset, cudaStream_t s) {

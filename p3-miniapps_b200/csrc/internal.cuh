@@ -97,6 +97,7 @@ struct vlp4d_ctx {
   // -1 not yet decided, 0 no (shape, VLP4D_FIELD=cufft, or no cluster
   // fits), else the cluster size (8 or 16).
   int field_cluster = -1;
+  int field_cluster_t = -1;  // the same for the transposed solve (reverse mode)
 
   // Diagnostics history (nbiter+1 entries each) and the reduction scratch.
   double *nrj = nullptr, *mass = nullptr;
@@ -254,6 +255,11 @@ int launch_field_poisson(vlp4d_ctx *c, cudaStream_t s);
 // context, and its launch (rho - offset -> phi in rho, ex, ey).
 bool field_cluster_available(vlp4d_ctx *c);
 int launch_field_cluster(vlp4d_ctx *c, double offset, cudaStream_t s);
+// The transposed solve lam_rho = D^T (gex, gey) from the impulse-response
+// spectra (half-spectrum layout of the forward D2Z).
+bool field_cluster_t_available(vlp4d_ctx *c);
+int launch_field_transpose_cluster(vlp4d_ctx *c, const double *gex, const double *gey, const void *hx_hat,
+                                   const void *hy_hat, double *lam_rho, cudaStream_t s);
 int launch_diags(vlp4d_ctx *c, int iter, cudaStream_t s);
 // launch_diags on the context's side stream after the work queued on s so
 // far; diags_join makes s wait for it (before anything writes rho, Ex, Ey).
