@@ -85,31 +85,38 @@ struct VtableAdjJob {
   const double *e;
   double hmin, hmax;
   int n;
-  StencilTable fwd, adj;
+  StencilTable fwd, adj;  // span / span_C set: also the chunk spans (the vy direction)
   double *dw;
 };
 __global__ void k_build_vtables_rev(VtableAdjJob jx, VtableAdjJob jy, int lines, double dt) {
   const int line = blockIdx.x * blockDim.x + threadIdx.x;
-  if (line >= lines) return;
+  const bool on = line < lines;
   const VtableAdjJob &j = blockIdx.y ? jy : jx;
-  const LineStencil s = line_stencil(__dmul_rn(dt, j.e[line]), j.hmin, j.hmax, j.n);
-  const LineStencil t = adjoint_stencil(s, j.n);
-  float f[6], fa[6];
-  weights_to_f32(s.w, f);
-  weights_to_f32(t.w, fa);
-  j.fwd.m[line] = s.m;
-  j.adj.m[line] = t.m;
-  double dc[6];
-  lag_basis5_deriv(s.d, dc);
-  const double scale = -dt / ((j.hmax - j.hmin) / (double)j.n);
+  int ms = 0, mt = 0;
+  if (on) {
+    const LineStencil s = line_stencil(__dmul_rn(dt, j.e[line]), j.hmin, j.hmax, j.n);
+    const LineStencil t = adjoint_stencil(s, j.n);
+    float f[6], fa[6];
+    weights_to_f32(s.w, f);
+    weights_to_f32(t.w, fa);
+    j.fwd.m[line] = s.m;
+    j.adj.m[line] = t.m;
+    ms = s.m;
+    mt = t.m;
+    double dc[6];
+    lag_basis5_deriv(s.d, dc);
+    const double scale = -dt / ((j.hmax - j.hmin) / (double)j.n);
 #pragma unroll
-  for (int k = 0; k < 6; ++k) {
-    j.fwd.w[6 * line + k] = s.w[k];
-    j.fwd.wf[6 * line + k] = f[k];
-    j.adj.w[6 * line + k] = t.w[k];
-    j.adj.wf[6 * line + k] = fa[k];
-    j.dw[6 * line + k] = dc[k] * scale;
+    for (int k = 0; k < 6; ++k) {
+      j.fwd.w[6 * line + k] = s.w[k];
+      j.fwd.wf[6 * line + k] = f[k];
+      j.adj.w[6 * line + k] = t.w[k];
+      j.adj.wf[6 * line + k] = fa[k];
+      j.dw[6 * line + k] = dc[k] * scale;
+    }
   }
+  if (j.fwd.span_C) chunk_span(on, signed_offset(ms, j.n), line, j.fwd.span_C, j.fwd.span);
+  if (j.adj.span_C) chunk_span(on, signed_offset(mt, j.n), line, j.adj.span_C, j.adj.span);
 }
 
 // gE partial sums.  Block (32 columns) x (GY vx groups); grid (column
@@ -678,6 +685,13 @@ int reverse_core(vlp4d_adjoint *A, const void *a, const double *e, const void *l
     VLP4D_CUDA_TRY(cudaMemcpyAsync(c->ey, e + n2, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
   }
   if ((rc = alloc_table(c->tab_vx, lines)) || (rc = alloc_table(c->tab_vy, lines))) return rc;
+  // The vy chunk spans of the v-slab pass (forward and transposed tables)
+  // where it runs on this shape.
+  const int C = vslab_chunk_cols(c);
+  c->tab_vy.span_C = A->tab_vy_adj.span_C = 0;
+  if (C && alloc_span(c->tab_vy, C) == VLP4D_OK && alloc_span(A->tab_vy_adj, C) == VLP4D_OK)
+    c->tab_vy.span_C = A->tab_vy_adj.span_C = C;
+  c->tab_vx.span_C = A->tab_vx_adj.span_C = 0;
   const int threads = 256, blocks = (lines + threads - 1) / threads;
   const VtableAdjJob jx = {c->ex, c->g.minp[2], c->g.maxp[2], c->g.n[2], c->tab_vx, A->tab_vx_adj, A->dw_vx};
   const VtableAdjJob jy = {c->ey, c->g.minp[3], c->g.maxp[3], c->g.n[3], c->tab_vy, A->tab_vy_adj, A->dw_vy};

@@ -25,20 +25,27 @@ struct VtableJob {
   int *m;
   double *w;
   float *wf;
+  int2 *span;  // non-null: also the chunk spans of the signed offsets (chunks of C lines)
+  int C;
 };
 __global__ void k_build_vtable(VtableJob j0, VtableJob j1, int lines, double dt) {
   const int line = blockIdx.x * blockDim.x + threadIdx.x;
-  if (line >= lines) return;
+  const bool on = line < lines;
   const VtableJob j = blockIdx.y ? j1 : j0;
-  const LineStencil s = line_stencil(__dmul_rn(dt, j.e[line]), j.hmin, j.hmax, j.n);
-  j.m[line] = s.m;
-  float f[6];
-  weights_to_f32(s.w, f);
+  int m = 0;
+  if (on) {
+    const LineStencil s = line_stencil(__dmul_rn(dt, j.e[line]), j.hmin, j.hmax, j.n);
+    m = s.m;
+    j.m[line] = s.m;
+    float f[6];
+    weights_to_f32(s.w, f);
 #pragma unroll
-  for (int k = 0; k < 6; ++k) {
-    j.w[6 * line + k] = s.w[k];
-    j.wf[6 * line + k] = f[k];
+    for (int k = 0; k < 6; ++k) {
+      j.w[6 * line + k] = s.w[k];
+      j.wf[6 * line + k] = f[k];
+    }
   }
+  if (j.span) chunk_span(on, signed_offset(m, j.n), line, j.C, j.span);
 }
 
 // Generic 1D sweep along dimension DIM: one thread per output cell, taps
@@ -185,11 +192,21 @@ void free_table(StencilTable &t) {
   cudaFree(t.m);
   cudaFree(t.w);
   cudaFree(t.wf);
+  cudaFree(t.span);
   t.m = nullptr;
   t.w = nullptr;
   t.wf = nullptr;
+  t.span = nullptr;
+  t.span_C = 0;
   t.lines = 0;
   t.valid = false;
+}
+
+int alloc_span(StencilTable &t, int C) {
+  if (C < 8 || 32 % C) return VLP4D_ERR_UNSUPPORTED;
+  // Room for the smallest chunk width, 8 lines.
+  if (!t.span) VLP4D_CUDA_TRY(cudaMalloc(&t.span, sizeof(int2) * ((size_t)t.lines / 8 + 1)));
+  return VLP4D_OK;
 }
 
 int alloc_table(StencilTable &t, int lines, int taps) {
@@ -197,7 +214,10 @@ int alloc_table(StencilTable &t, int lines, int taps) {
   cudaFree(t.m);
   cudaFree(t.w);
   cudaFree(t.wf);
+  cudaFree(t.span);
   t.m = nullptr; t.w = nullptr; t.wf = nullptr;
+  t.span = nullptr;
+  t.span_C = 0;
   VLP4D_CUDA_TRY(cudaMalloc(&t.m, sizeof(int) * lines));
   VLP4D_CUDA_TRY(cudaMalloc(&t.w, sizeof(double) * taps * lines));
   VLP4D_CUDA_TRY(cudaMalloc(&t.wf, sizeof(float) * taps * lines));
@@ -337,13 +357,18 @@ int build_v_tables(vlp4d_ctx *c, double dt, bool vx, bool vy, cudaStream_t s) {
   if (vx) {
     int rc = alloc_table(c->tab_vx, lines);
     if (rc) return rc;
-    jobs[njobs++] = {c->ex, c->g.minp[2], c->g.maxp[2], c->g.n[2], c->tab_vx.m, c->tab_vx.w, c->tab_vx.wf};
+    jobs[njobs++] = {c->ex, c->g.minp[2], c->g.maxp[2], c->g.n[2], c->tab_vx.m, c->tab_vx.w, c->tab_vx.wf, nullptr, 0};
   }
   if (vy) {
     int rc = alloc_table(c->tab_vy, lines);
     if (rc) return rc;
+    // With the chunk spans of the v-slab pass when it runs on this shape.
+    const int C = vslab_chunk_cols(c);
+    c->tab_vy.span_C = 0;
+    if (C && threads % 32 == 0 && (rc = alloc_span(c->tab_vy, C)) == VLP4D_OK) c->tab_vy.span_C = C;
     // The vy geometry of the whole run (slab contexts own part of its planes).
-    jobs[njobs++] = {c->ey, c->g.minp[3], c->g.maxp[3], c->nvy_glob, c->tab_vy.m, c->tab_vy.w, c->tab_vy.wf};
+    jobs[njobs++] = {c->ey, c->g.minp[3], c->g.maxp[3], c->nvy_glob, c->tab_vy.m, c->tab_vy.w, c->tab_vy.wf,
+                     c->tab_vy.span_C ? c->tab_vy.span : nullptr, c->tab_vy.span_C};
   }
   if (!njobs) return VLP4D_OK;
   k_build_vtable<<<dim3((unsigned)blocks, (unsigned)njobs), threads, 0, s>>>(jobs[0], jobs[njobs - 1], lines, dt);

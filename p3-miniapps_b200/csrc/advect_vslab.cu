@@ -56,8 +56,6 @@ struct VslabArgs {
   double bias_scale;
 };
 
-// Signed form of a tap offset m in [0, n): the shift in cells, in (-n/2, n/2].
-__device__ __forceinline__ int signed_offset(int m, int n) { return m > n / 2 ? m - n : m; }
 
 // Error exit of one warp after a copy timed out: flag it, let the copies
 // already issued for slabs k .. issued-1 land (bounded waits), then leave.
@@ -402,14 +400,9 @@ bool vslab_config(const vlp4d_ctx *c, bool do_vx, bool do_vy, VslabCfg &cfg) {
   const int nvx = c->g.n[2], nvy = c->g.n[3];
   const bool f32 = c->dtype == VLP4D_F32;
   if (nvx < 8 || nvx > 256) return false;
-  if (f32) {
-    cfg.V = 8;
-    cfg.C = nvx <= 128 ? 32 : 16;
-  } else {
-    cfg.V = 4;
-    cfg.C = nvx <= 128 ? 16 : 8;
-  }
-  if (nvx % cfg.V || nxy % cfg.C) return false;
+  cfg.V = f32 ? 8 : 4;
+  cfg.C = vslab_chunk_cols(c);
+  if (!cfg.C || nvx % cfg.V || nxy % cfg.C) return false;
   cfg.threads = cfg.C * (nvx / cfg.V);
   // Whole warps only: every warp releases each slab once, and the last of
   // blockDim/32 releases refills it.
@@ -470,6 +463,13 @@ int launch_advect_vxvy(vlp4d_ctx *c, const void *fn, void *fnp1, bool do_vx, boo
   return launch_advect_vxvy_tables(c, fn, fnp1, do_vx ? &c->tab_vx : nullptr, do_vy ? &c->tab_vy : nullptr, s);
 }
 
+int vslab_chunk_cols(const vlp4d_ctx *c) {
+  const int nvx = c->g.n[2];
+  if (nvx < 8 || nvx > 256) return 0;
+  const int C = c->dtype == VLP4D_F32 ? (nvx <= 128 ? 32 : 16) : (nvx <= 128 ? 16 : 8);
+  return c->g.nxy() % C ? 0 : C;
+}
+
 int launch_advect_vxvy_tables(vlp4d_ctx *c, const void *fn, void *fnp1, const StencilTable *tvx,
                               const StencilTable *tvy, cudaStream_t s, const double *bias, double bias_scale) {
   const bool do_vx = tvx != nullptr, do_vy = tvy != nullptr;
@@ -502,7 +502,12 @@ int launch_advect_vxvy_tables(vlp4d_ctx *c, const void *fn, void *fnp1, const St
                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return VLP4D_ERR_UNSUPPORTED;
 
-  if (do_vy) {
+  // The chunks' vy spans: from the table when its builder made them for
+  // this chunk width, else here.
+  const int2 *span = c->vspan;
+  if (do_vy && tvy->span && tvy->span_C == cfg.C) {
+    span = tvy->span;
+  } else if (do_vy) {
     k_vspan<<<(nchunks + 127) / 128, 128, 0, s>>>(tvy->m, nchunks, cfg.C, c->nvy_glob, c->vspan);
     VLP4D_LAUNCH_CHECK();
   }
@@ -520,7 +525,7 @@ int launch_advect_vxvy_tables(vlp4d_ctx *c, const void *fn, void *fnp1, const St
   a.stages = cfg.stages;
   if (do_vx) a.tvx = *tvx;
   if (do_vy) a.tvy = *tvy;
-  a.span = c->vspan;
+  a.span = span;
   a.err = c->d_err;
   a.bias = bias;
   a.bias_scale = bias_scale;

@@ -606,7 +606,7 @@ int fail_msg(int code, const std::string &msg) { return fail(code, msg); }
 // Whether the x/y half steps of consecutive steps run as one joined pass.
 // That pass does the arithmetic of two passes for the HBM traffic of one:
 // in FP32 (k_plane_xyxy, 0.50 ms against 2 x 0.41 ms at 128^4) and in FP64
-// where k_plane_xyxy64 runs (1.48 ms against 2 x 1.11 ms), not for the FP64
+// where k_plane_xyxy64 runs (1.08 ms against 2 x 0.84 ms), not for the FP64
 // widths only the generic FP64 form covers (its 1 KB rows leave one CTA per
 // SM: slower than two k_plane passes).  VLP4D_XYXY=0/1 at context creation
 // overrides.

@@ -64,6 +64,11 @@ struct Grid {
 //   wf[6*line + j] : FP32 difference weights (stencil.cuh), j < 5.
 struct StencilTable {
   int *m = nullptr;
+  // vy tables built for the v-slab pass: per chunk of span_C consecutive
+  // lines the smallest and largest signed offset (span_C = 0: none; the
+  // pass then computes them).
+  int2 *span = nullptr;
+  int span_C = 0;
   double *w = nullptr;
   float *wf = nullptr;
   int lines = 0;
@@ -188,6 +193,26 @@ inline void *owned_planes(const vlp4d_ctx *c, void *f) {
 
 // advect.cu
 int alloc_table(StencilTable &t, int lines, int taps = 6);
+// The span buffer of a vy table for chunks of C lines (lines / C entries).
+int alloc_span(StencilTable &t, int C);
+// Columns per chunk of the v-slab pass of this context (0: the pass does
+// not run on this shape).
+int vslab_chunk_cols(const vlp4d_ctx *c);
+// Signed form of a tap offset m in [0, n): the shift in cells, in (-n/2, n/2].
+__host__ __device__ __forceinline__ int signed_offset(int m, int n) { return m > n / 2 ? m - n : m; }
+// Per chunk of C consecutive lines (C divides 32; lines and lanes
+// consecutive, chunks aligned to warps): lane `line % C == 0` stores the
+// smallest and largest o of its chunk.  Every lane of the warp calls it;
+// `on` false for lanes past the last line.
+__device__ __forceinline__ void chunk_span(bool on, int o, int line, int C, int2 *span) {
+  int lo = on ? o : (1 << 30), hi = on ? o : -(1 << 30);
+  for (int d = C >> 1; d > 0; d >>= 1) {
+    const int l2 = __shfl_xor_sync(0xffffffffu, lo, d), h2 = __shfl_xor_sync(0xffffffffu, hi, d);
+    lo = l2 < lo ? l2 : lo;
+    hi = h2 > hi ? h2 : hi;
+  }
+  if (on && line % C == 0) span[line / C] = make_int2(lo, hi);
+}
 void free_table(StencilTable &t);
 int ensure_xy_table(vlp4d_ctx *c, int dim, double dt, StencilTable **out, cudaStream_t s);
 // The composed 11-tap table of two x (dim 0) or y (dim 1) shifts by dt:
