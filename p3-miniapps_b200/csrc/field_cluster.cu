@@ -170,8 +170,11 @@ struct FieldSmem {
     rows_elems = (size_t)R * nx;
     cols_elems = (size_t)3 * Kc * ny;
   }
+  // The forward solve: two row buffers of three fields' rows each (the
+  // inverse x transforms of phi, Ex, Ey run as one batch), two column
+  // buffers, the twiddles.
   __host__ __device__ size_t bytes(int nx, int ny) const {
-    return sizeof(double2) * (2 * rows_elems + 2 * cols_elems + nx + ny);
+    return sizeof(double2) * (6 * rows_elems + 2 * cols_elems + nx + ny);
   }
 };
 
@@ -182,8 +185,8 @@ __global__ void __launch_bounds__(kFieldThreads) k_field_cluster(FieldArgs a) {
   const FieldSmem L(nx, ny, kFieldCtas);
   const int R = L.R, Kc = L.Kc;
   double2 *rowA = reinterpret_cast<double2 *>(fsm);
-  double2 *rowB = rowA + L.rows_elems;
-  double2 *colA = rowB + L.rows_elems;
+  double2 *rowB = rowA + 3 * L.rows_elems;
+  double2 *colA = rowB + 3 * L.rows_elems;
   double2 *colB = colA + L.cols_elems;
   double2 *twx = colB + L.cols_elems;
   double2 *twy = twx + nx;
@@ -234,25 +237,25 @@ __global__ void __launch_bounds__(kFieldThreads) k_field_cluster(FieldArgs a) {
   // slots are contiguous; their values are never read).
   const double2 *cols = line_dft(spec, spare, 3 * Kc, ny, twy, true);
   cluster_barrier();
-  // 5. Own rows per field: half spectrum from the column owners, Hermitian
-  // extension, inverse along x, real part.
-  for (int f = 0; f < 3; ++f) {
-    for (int i = threadIdx.x; i < R * nxh; i += blockDim.x) {
-      const int r = i / nxh, kx = i - r * nxh;
-      const int owner = kx % kFieldCtas, q = kx / kFieldCtas;
-      rowA[(size_t)r * nx + kx] = ld_cluster(cols + (size_t)(f * Kc + q) * ny + iy0 + r, (unsigned)owner);
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < R * (nx - nxh); i += blockDim.x) {
-      const int r = i / (nx - nxh), kx = nxh + (i - r * (nx - nxh));
-      const double2 v = rowA[(size_t)r * nx + (nx - kx)];
-      rowA[(size_t)r * nx + kx] = make_double2(v.x, -v.y);
-    }
-    __syncthreads();
-    const double2 *out = line_dft(rowA, rowB, R, nx, twx, true);
-    double *dst = a.rho + f * a.fstride + (size_t)iy0 * nx;
-    for (int i = threadIdx.x; i < R * nx; i += blockDim.x) dst[i] = out[i].x;
-    __syncthreads();  // rowA and rowB are reused by the next field
+  // 5. Own rows of the three fields (line f * R + r): half spectra from the
+  // column owners, Hermitian extension, inverse along x, real part.
+  for (int i = threadIdx.x; i < 3 * R * nxh; i += blockDim.x) {
+    const int l = i / nxh, kx = i - l * nxh;
+    const int f = l / R, r = l - f * R;
+    const int owner = kx % kFieldCtas, q = kx / kFieldCtas;
+    rowA[(size_t)l * nx + kx] = ld_cluster(cols + (size_t)(f * Kc + q) * ny + iy0 + r, (unsigned)owner);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 3 * R * (nx - nxh); i += blockDim.x) {
+    const int l = i / (nx - nxh), kx = nxh + (i - l * (nx - nxh));
+    const double2 v = rowA[(size_t)l * nx + (nx - kx)];
+    rowA[(size_t)l * nx + kx] = make_double2(v.x, -v.y);
+  }
+  __syncthreads();
+  const double2 *out = line_dft(rowA, rowB, 3 * R, nx, twx, true);
+  for (int i = threadIdx.x; i < 3 * R * nx; i += blockDim.x) {
+    const int f = i / (R * nx), e = i - f * (R * nx);
+    a.rho[f * a.fstride + (size_t)iy0 * nx + e] = out[i].x;
   }
   cluster_barrier();
 }
