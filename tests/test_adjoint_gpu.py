@@ -150,3 +150,28 @@ def test_graph_and_eager_reverse_sweeps_agree(pkg, cuda, dtype):
             del os.environ["VLP4D_ADJOINT_GRAPHS"]
     assert res[0][0] == res[1][0]
     assert torch.equal(res[0][1], res[1][1])
+
+
+@pytest.mark.parametrize("n", [(32, 16, 32, 24), (16, 8, 16, 8), (64, 64, 16, 16)])
+def test_cluster_and_cufft_field_solves_give_the_same_reverse_step(pkg, cuda, n):
+    """The reverse step through the cluster solves (forward D and D^T in one
+    cluster launch each) and through the cuFFT path (VLP4D_FIELD=cufft)
+    agree to FP64 rounding of the transforms."""
+    torch = cuda
+    dom = _dom(pkg, n)
+    ora = Restatement(dom.nxmax, dom.min_phy, dom.max_phy, dom.dt, dom.idcase)
+    f1 = ora.step(ora.init_case(IC_LANDAU_SUM, 0.05, 0.5))
+    lam = np.random.default_rng(3).normal(size=ora.shape4)
+    outs = []
+    for mode in ("", "cufft"):
+        os.environ["VLP4D_FIELD"] = mode
+        try:
+            with pkg.Context(dom, "f64") as ctx, pkg.Adjoint(ctx, 1, 1) as adj:
+                out = ctx.empty_f()
+                adj.step_adjoint(torch.from_numpy(f1).cuda(), torch.from_numpy(lam).cuda(), out)
+                torch.cuda.synchronize()
+                ctx.check()
+                outs.append(out.cpu().numpy())
+        finally:
+            del os.environ["VLP4D_FIELD"]
+    assert _rel(outs[0], outs[1]) < 1e-12
