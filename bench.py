@@ -40,6 +40,24 @@ METRIC = "Gcell-updates/s"
 WORKLOAD = "Landau damping 128^4, dt 0.1, sum-form IC (amp 0.05, k 0.5), Strang step"
 
 
+def headline_config(n, world, slabs=False, halo=4, rank=0):
+    """The `config` of the headline line: the same dict for this library's
+    arm and the reference arm at the same N.  With vy slabs, `rank`'s
+    planes (rank 0 prints the line): nvy // world planes, one more on the
+    first nvy % world ranks."""
+    cells = n ** 4
+    cfg = {"workload": WORKLOAD, "grid": [n] * 4, "dt": DT, "storage": "f32 f, f64 fields/diagnostics"}
+    if slabs:
+        nloc = n // world + (1 if rank < n % world else 0)
+        cfg["parallelism"] = (f"vy slabs x{world}: {nloc} planes on rank {rank}, halo {halo} planes per side "
+                              f"(NCCL send/recv), rho all-reduce (NCCL)")
+        cfg["l2"] = "f slab (%.2f GB per GPU) larger than L2, no flush" % (cells / world * 4 / 1e9)
+    else:
+        cfg["parallelism"] = f"replicas x{world}" if world > 1 else "single GPU"
+        cfg["l2"] = "f (%.2f GB) larger than L2, no flush" % (cells * 4 / 1e9)
+    return cfg
+
+
 def parse_args(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -376,9 +394,7 @@ def gpu_arm(args, ranks):
         "api": "vlp4d_steps (time loop, K steps per call)",
         "per_step_api": rec["per_step_api"],
         "dtype": "f32", "data": "synthetic (Landau initial condition computed on the device)",
-        "config": {"workload": WORKLOAD, "grid": [n] * 4, "dt": DT, "storage": "f32 f, f64 fields/diagnostics",
-                   "parallelism": f"replicas x{ranks.world}" if ranks.world > 1 else "single GPU",
-                   "l2": "f (%.2f GB) larger than L2, no flush" % (cells * 4 / 1e9)},
+        "config": headline_config(n, ranks.world),
         "roofline": roofline, "e2e": e2e, "gpu_launches": rec["launches"], "clocks": clocks,
         "f64": ({"value": per_dtype["f64"]["value"], "ms_per_step": per_dtype["f64"]["ms_per_step"],
                  "per_step_api": per_dtype["f64"]["per_step_api"],
@@ -464,10 +480,7 @@ def slab_arm(args, ranks):
         "warmup": W, "ms_per_step": secs * 1e3 / K, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "api": "distrib.SlabRun over vlp4d slab contexts (C ABI), NCCL exchanges",
         "dtype": "f32", "data": "synthetic (Landau initial condition computed on the device)",
-        "config": {"workload": WORKLOAD, "grid": [n] * 4, "dt": DT, "storage": "f32 f, f64 fields/diagnostics",
-                   "parallelism": f"vy slabs x{ranks.world}: {nloc} planes on rank {ranks.rank}, halo "
-                                  f"{args.halo} planes per side (NCCL send/recv), rho all-reduce (NCCL)",
-                   "l2": "f slab (%.2f GB per GPU) larger than L2, no flush" % (cells / ranks.world * 4 / 1e9)},
+        "config": headline_config(n, ranks.world, slabs=True, halo=args.halo, rank=ranks.rank),
         "halo_bytes_per_step_per_rank": halo_bytes,
         "e2e": {"value": cells * K / e2e_secs / 1e9, "unit": METRIC, "h2d_bytes_per_step": fbytes / K,
                 "d2h_bytes_per_step": (fbytes + 8 * (K + 1)) / K, "seconds": e2e_secs,
@@ -786,34 +799,37 @@ def landau_f0_numpy(n):
     return out
 
 
-def reference_cpu(n, max_steps, budget_s):
+def reference_cpu(n, max_steps, budget_s, warmup=1):
     """Times the reference's own OpenMP build (oracle/_ref) on this host:
-    full Strang steps on the whole grid, one untimed step first, then up to
-    max_steps timed steps while the total stays within budget_s."""
+    full Strang steps on the whole grid, `warmup` untimed steps first (at
+    least one), then up to max_steps timed steps while the total stays
+    within budget_s."""
     sys.path.insert(0, str(ROOT))
     from oracle.oracle import Reference
 
     if not Reference.available():
         return None
+    warmup = max(int(warmup), 1)
     ref = Reference((n, n, n, n), (0.0, 0.0, -VMAX, -VMAX), (L_BOX, L_BOX, VMAX, VMAX), DT,
-                    nbiter=max_steps + 2, idcase=10)
+                    nbiter=max_steps + warmup + 1, idcase=10)
     f0 = landau_f0_numpy(n)
     ref.set_f(0, f0)
     del f0
     threads = int(ref.L.ref_max_threads())
-    ref.onetimestep(1)  # first touch of fnp1 and the FFT buffers
+    for w in range(warmup):  # the first one touches fnp1 and the FFT buffers
+        ref.onetimestep(1 + w)
     times = []
     for it in range(max_steps):
         t0 = time.perf_counter()
-        ref.onetimestep(2 + it)
+        ref.onetimestep(1 + warmup + it)
         times.append(time.perf_counter() - t0)
         if sum(times) > budget_s:
             break
     ref.close()
     secs = sum(times)
     return {"value": n ** 4 * len(times) / secs / 1e9, "unit": METRIC, "cores": threads, "kind": "reference",
-            "steps": len(times), "seconds": secs,
-            "sample": f"{len(times)} full Strang steps of the {n}^4 grid (after 1 untimed step), "
+            "steps": len(times), "warmup": warmup, "seconds": secs,
+            "sample": f"{len(times)} full Strang steps of the {n}^4 grid (after {warmup} untimed), "
                       f"reference OpenMP build miniapps/vlp4d/openmp, FP64, OMP_NUM_THREADS={threads}"}
 
 
@@ -888,16 +904,21 @@ def _set_omp_env():
 def reference_arm(args):
     _set_omp_env()
     budget = 150.0
-    res = reference_cpu(args.n, max(args.steps, 1), budget)
+    res = reference_cpu(args.n, max(args.steps, 1), budget, warmup=max(args.warmup, 1))
     if res is None:
         return {"impl": "reference", "unavailable": "oracle/_ref/libvlp4d_ref.so (the reference's OpenMP build) is absent"}
     ms = res["seconds"] * 1e3 / res["steps"]
+    world = args.gpus
+    slabs = (world > 1 and not args.replicas) or args.slab
     return {
         "impl": "reference", "metric": METRIC, "value": res["value"], "unit": METRIC, "n_gpus": args.gpus,
-        "steps": res["steps"], "warmup": 1, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "steps": res["steps"], "warmup": res["warmup"], "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "strong" if slabs else "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (Landau initial condition)",
-        "config": {"workload": WORKLOAD, "grid": [args.n] * 4, "dt": DT, "storage": "f64 (reference)",
-                   "requested_steps": args.steps},
+        # The same config as this library's arm at the same N (the reference
+        # itself is one FP64 process on the host cores: `dtype`, `cpu_baseline`).
+        "config": headline_config(args.n, world, slabs=slabs, halo=args.halo),
+        "requested_steps": args.steps,
         "cpu_baseline": res,
         "e2e": {"value": res["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
