@@ -1,8 +1,8 @@
 // Thin wrappers over the sm_90+/sm_100a asynchronous-copy PTX used by the
 // fused advection kernels: mbarrier transaction barriers, 1D bulk copies
 // (cp.async.bulk) and 3D tiled tensor copies (cp.async.bulk.tensor).  All
-// copies are global -> this CTA's shared memory, single-CTA, no cluster
-// multicast.  Every wait is bounded in time so a lost transaction turns
+// copies are global (this GPU's memory) -> this CTA's shared memory, one
+// destination CTA per copy.  Every wait is bounded in time so a lost transaction turns
 // into an error status instead of a hung GPU.
 #pragma once
 
