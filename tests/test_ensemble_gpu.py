@@ -139,3 +139,28 @@ def test_idle_limit_runs_out_then_ensemble_recovers(pkg, cuda):
         for bad in (-1, 4_000_000_001):
             with pytest.raises(pkg.vlp4d.Vlp4dError):
                 ens.set_idle_limit(bad)
+
+
+def test_rows_per_tile_do_not_change_results(pkg, cuda):
+    """The x/y stages batch the vy rows of small members into tiles of about
+    VLP4D_ENS_TILE_CELLS cells; one row per tile and the default give the
+    same f and energy history bit for bit (each row's moment is summed in
+    ivx order whatever the tile)."""
+    import os
+
+    torch = cuda
+    members = _members(pkg, DIMS)
+    res = []
+    for cells in ("1", ""):
+        if cells:
+            os.environ["VLP4D_ENS_TILE_CELLS"] = cells
+        try:
+            with pkg.Ensemble(members, 4) as ens:
+                ens.run()
+                ens.check()
+                res.append([ens.read(i) for i in range(len(members))])
+        finally:
+            os.environ.pop("VLP4D_ENS_TILE_CELLS", None)
+    for (f1, n1), (f2, n2) in zip(*res):
+        assert torch.equal(f1, f2)
+        assert np.array_equal(n1, n2)
