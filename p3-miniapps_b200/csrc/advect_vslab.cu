@@ -450,6 +450,12 @@ int run_vslab(vlp4d_ctx *c, const CUtensorMap &map, const VslabArgs &args, const
   int per_sm = 0;
   VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, cfg.threads, cfg.smem));
   if (per_sm < 1) return VLP4D_ERR_UNSUPPORTED;
+  // One CTA per SM (VLP4D_VSLAB_CTAS overrides): the pipeline is sized for
+  // it, and where registers allow a second one (the FP64 vx sweep alone,
+  // 64 registers) two CTAs per SM measured slower: 0.86 against 0.74 ms at
+  // 128^4.
+  const int cap = env_int("VLP4D_VSLAB_CTAS", 1);
+  if (cap > 0 && per_sm > cap) per_sm = cap;
   long long grid = (long long)per_sm * c->num_sms;
   if (grid > args.nitems) grid = args.nitems;
   kern<<<(unsigned)grid, cfg.threads, cfg.smem, s>>>(map, args);
