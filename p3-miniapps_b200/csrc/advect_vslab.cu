@@ -450,11 +450,11 @@ int run_vslab(vlp4d_ctx *c, const CUtensorMap &map, const VslabArgs &args, const
   int per_sm = 0;
   VLP4D_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, cfg.threads, cfg.smem));
   if (per_sm < 1) return VLP4D_ERR_UNSUPPORTED;
-  // One CTA per SM (VLP4D_VSLAB_CTAS overrides): the pipeline is sized for
-  // it, and where registers allow a second one (the FP64 vx sweep alone,
-  // 64 registers) two CTAs per SM measured slower: 0.86 against 0.74 ms at
-  // 128^4.
-  const int cap = env_int("VLP4D_VSLAB_CTAS", 1);
+  // At most 512 threads per SM (VLP4D_VSLAB_CTAS sets the CTAs per SM):
+  // where registers allow more (the FP64 vx sweep alone, 64 registers, two
+  // CTAs of 512 threads) the pass measured slower, 0.86 against 0.74 ms at
+  // 128^4; blocks of 256 threads (64^4) keep two CTAs per SM.
+  const int cap = env_int("VLP4D_VSLAB_CTAS", 512 / cfg.threads > 0 ? 512 / cfg.threads : 1);
   if (cap > 0 && per_sm > cap) per_sm = cap;
   long long grid = (long long)per_sm * c->num_sms;
   if (grid > args.nitems) grid = args.nitems;
@@ -553,7 +553,11 @@ int launch_advect_vxvy_tables(vlp4d_ctx *c, const void *fn, void *fnp1, const St
   if (bias) {  // the reverse mode's vx+vy pass with the per-column term
     if (!(do_vx && do_vy)) return VLP4D_ERR_UNSUPPORTED;
     if (c->dtype == VLP4D_F64) return run_vslab<double, true, true, 4, 0, true>(c, map, a, cfg, s);
-    return run_vslab<float, true, true, 8, 0, true>(c, map, a, cfg, s);
+    switch (a.nxy) {  // the plane sizes of the benchmark configurations, compile-time
+      case 16384: return run_vslab<float, true, true, 8, 16384, true>(c, map, a, cfg, s);
+      case 4096: return run_vslab<float, true, true, 8, 4096, true>(c, map, a, cfg, s);
+      default: return run_vslab<float, true, true, 8, 0, true>(c, map, a, cfg, s);
+    }
   }
   if (c->dtype == VLP4D_F64) {
     if (do_vx && do_vy) VLP4D_VS(double, true, true, 4);
