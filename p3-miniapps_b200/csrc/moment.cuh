@@ -13,7 +13,7 @@
 
 namespace vlp4d {
 
-constexpr int kMomentSlices = 8;
+constexpr int kMomentSlices = 16;
 constexpr int kMomentCells = 32;  // cells per block; blockDim = kMomentCells x kMomentSlices
 
 __device__ __forceinline__ void moment_finish(const double *__restrict__ part, double *__restrict__ rho,
