@@ -3,7 +3,8 @@ against the cuFFT path of the same entry point (VLP4D_FIELD=cufft): the
 mode-wise solve is shared, the transforms differ only in rounding, so phi,
 Ex and Ey agree to FP64 rounding of the transforms.  Shapes: the powers of
 two of the benchmark configurations (Stockham passes), and a row count that
-is not a power of two (direct DFT along y); cases 10 (rho - 1) and 110."""
+is not a power of two (direct DFT along y), rows and columns of lengths
+48, 96, 40 (direct DFTs along x, along both); cases 10 (rho - 1) and 110."""
 from __future__ import annotations
 
 import os
@@ -30,7 +31,7 @@ def _solve(pkg, dom, rho, use_cufft):
         os.environ.pop("VLP4D_FIELD", None)
 
 
-@pytest.mark.parametrize("nxy", [(128, 128), (64, 64), (32, 16), (16, 8), (64, 128), (32, 24)])
+@pytest.mark.parametrize("nxy", [(128, 128), (64, 64), (32, 16), (16, 8), (64, 128), (32, 24), (48, 48), (96, 64), (40, 16)])
 @pytest.mark.parametrize("idcase", [10, 110])
 def test_cluster_solve_matches_cufft(pkg, cuda, nxy, idcase):
     torch = cuda
