@@ -648,12 +648,14 @@ def adjoint_arm(pkg, torch, stream, n=64, nsteps=200, every=8):
     (200 steps), FP32 f / FP64 fields, a checkpoint every 8 steps.  Times the
     forward run with checkpoints, the reverse run (segment recomputation
     included) and, as the forward reference, the same steps through
-    vlp4d_steps; device time with CUDA events."""
+    vlp4d_steps; device time with CUDA events.  `store_all`: the same with
+    every = 0 (the forward run keeps every step's stage input and field,
+    200 x 67 MB, and the reverse run recomputes nothing)."""
     v = pkg.vlp4d
     dom = pkg.landau_domain(n, dt=0.1, nbiter=nsteps + 1, idcase=110)
     out = {"config": {"grid": [n] * 4, "dt": 0.1, "steps": nsteps, "checkpoint_every": every,
                       "storage": "f32 f, f64 fields", "objective": "dx dy sum |E(T)|^2"}}
-    with pkg.Context(dom, "f32") as ctx, v.Adjoint(ctx, nsteps, every) as adj:
+    with pkg.Context(dom, "f32") as ctx:
         f0 = ctx.empty_f()
         ctx.init_case(f0, v.IC_LANDAU_SUM, 0.05, 0.5)
         a, b = f0.clone(), ctx.empty_f()
@@ -661,21 +663,30 @@ def adjoint_arm(pkg, torch, stream, n=64, nsteps=200, every=8):
         ctx.field_poisson()
         ctx.diags_compute(0)
         grad = ctx.empty_f()
-        adj.forward(f0)  # warm-up (allocations, tables)
-        adj.backward(grad)
         fwd_steps = time_calls(torch, stream, lambda: ctx.steps(a.clone(), b, 1, nsteps), 3)
-        t_fwd = time_calls(torch, stream, lambda: adj.forward(f0), 3)
-        t_bwd = time_calls(torch, stream, lambda: adj.backward(grad), 3)
-        J = adj.forward(f0)
-        out.update({
-            "J": J,
-            "forward_steps_ms_per_step": fwd_steps * 1e3 / nsteps,
-            "forward_with_checkpoints_ms_per_step": t_fwd * 1e3 / nsteps,
-            "backward_ms_per_step": t_bwd * 1e3 / nsteps,
-            "ratio_backward_to_forward_steps": t_bwd / fwd_steps,
-            "ratio_backward_to_forward_checkpointed": t_bwd / t_fwd,
-            "grad_finite": bool(torch.isfinite(grad).all().item()),
-        })
+        out["forward_steps_ms_per_step"] = fwd_steps * 1e3 / nsteps
+        for ev, key in ((every, None), (0, "store_all")):
+            with v.Adjoint(ctx, nsteps, ev) as adj:
+                adj.forward(f0)  # warm-up (allocations, tables, graph capture)
+                adj.backward(grad)
+                t_fwd = time_calls(torch, stream, lambda: adj.forward(f0), 3)
+                t_bwd = time_calls(torch, stream, lambda: adj.backward(grad), 3)
+                J = adj.forward(f0)
+            res = {
+                "J": J,
+                ("forward_with_checkpoints_ms_per_step" if key is None else "forward_storing_ms_per_step"):
+                    t_fwd * 1e3 / nsteps,
+                "backward_ms_per_step": t_bwd * 1e3 / nsteps,
+                "ratio_backward_to_forward_steps": t_bwd / fwd_steps,
+                ("ratio_backward_to_forward_checkpointed" if key is None else "ratio_backward_to_forward_storing"):
+                    t_bwd / t_fwd,
+                "grad_finite": bool(torch.isfinite(grad).all().item()),
+            }
+            if key is None:
+                out.update(res)
+            else:
+                out[key] = res
+            torch.cuda.empty_cache()
         del a, b, grad, f0
     torch.cuda.empty_cache()
     return out

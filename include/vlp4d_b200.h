@@ -303,10 +303,14 @@ int vlp4d_selftest_wait_timeout(vlp4d_ctx *ctx, long long limit_cycles, void *st
 typedef struct vlp4d_adjoint vlp4d_adjoint;
 
 /* Allocates the reverse-mode state for runs of nsteps steps of ctx with a
- * checkpoint of f every `every` steps: ceil(nsteps/every) checkpoints, every-1
- * recompute buffers and six work buffers, each one f.  The recomputation of
- * a segment therefore holds `every` states at a time.  Runs one field solve
- * on a unit impulse (the context's rho/Ex/Ey are restored). */
+ * checkpoint of f every `every` steps: ceil(nsteps/every) checkpoints, every
+ * recompute buffers and six work buffers, each one f, plus 2*every fields.
+ * The recomputation of a segment therefore holds `every` states at a time.
+ * every = 0: no checkpoints; the forward run stores the stage input (one f)
+ * and field of each of the nsteps steps, and vlp4d_adjoint_backward
+ * recomputes nothing (nsteps + 6 f in all; results bit-identical to
+ * every = nsteps).  Runs one field solve on a unit impulse (the context's
+ * rho/Ex/Ey are restored). */
 int vlp4d_adjoint_create(vlp4d_ctx *ctx, int nsteps, int every, vlp4d_adjoint **out);
 int vlp4d_adjoint_destroy(vlp4d_adjoint *adj);
 
@@ -315,7 +319,8 @@ int vlp4d_adjoint_destroy(vlp4d_adjoint *adj);
  * the objective (host pointer, may be NULL).  Synchronises the stream. */
 int vlp4d_adjoint_forward(vlp4d_adjoint *adj, const void *f0, void *f_out, double *J, void *stream);
 /* grad = dJ/df0 for the last vlp4d_adjoint_forward; recomputes each segment
- * from its checkpoint, then runs the reverse steps.  Synchronises. */
+ * from its checkpoint (not with every = 0), then runs the reverse steps.
+ * Synchronises. */
 int vlp4d_adjoint_backward(vlp4d_adjoint *adj, void *grad, void *stream);
 
 /* One reverse step: lam_out = (d step/d f)^T lam_next, the step taken at

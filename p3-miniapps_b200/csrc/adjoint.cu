@@ -41,10 +41,16 @@ using vlp4d::StencilTable;
 struct vlp4d_adjoint {
   vlp4d_ctx *ctx = nullptr;
   int nsteps = 0, every = 0;
+  // every = 0 at creation: the forward sweep keeps the stage input and field
+  // of every step (seg, seg_e hold nsteps), the reverse sweep recomputes
+  // nothing; `every` is then nsteps and ckpt is empty.
+  bool store_all = false;
   size_t fbytes = 0;
   std::vector<void *> ckpt;  // f at steps 0, every, 2*every, ...
   std::vector<void *> seg;   // a = XY f of each step of a segment (every)
-  double *seg_e = nullptr;   // Ex, Ey of each step of a segment (every x 2 x nx*ny)
+  // Ex, Ey of each step of a segment, laid out as the context's fields
+  // (Ey fstride after Ex, 2 x fstride per step): one copy saves both.
+  double *seg_e = nullptr;
   void *P[2] = {nullptr, nullptr};  // forward work / final state
   void *W[2] = {nullptr, nullptr};  // reverse-step work
   void *L[2] = {nullptr, nullptr};  // adjoint states
@@ -680,10 +686,8 @@ int reverse_core(vlp4d_adjoint *A, const void *a, const double *e, const void *l
   const long long n2 = c->g.nxy();
   const int lines = (int)n2;
   int rc;
-  if (e) {
-    VLP4D_CUDA_TRY(cudaMemcpyAsync(c->ex, e, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
-    VLP4D_CUDA_TRY(cudaMemcpyAsync(c->ey, e + n2, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
-  }
+  // The step's field: stored (Ey fstride after Ex) or the context's own.
+  const double *ex = e ? e : c->ex, *ey = e ? e + c->fstride : c->ey;
   if ((rc = alloc_table(c->tab_vx, lines)) || (rc = alloc_table(c->tab_vy, lines))) return rc;
   // The vy chunk spans of the v-slab pass (forward and transposed tables)
   // where it runs on this shape.
@@ -693,8 +697,8 @@ int reverse_core(vlp4d_adjoint *A, const void *a, const double *e, const void *l
     c->tab_vy.span_C = A->tab_vy_adj.span_C = C;
   c->tab_vx.span_C = A->tab_vx_adj.span_C = 0;
   const int threads = 256, blocks = (lines + threads - 1) / threads;
-  const VtableAdjJob jx = {c->ex, c->g.minp[2], c->g.maxp[2], c->g.n[2], c->tab_vx, A->tab_vx_adj, A->dw_vx};
-  const VtableAdjJob jy = {c->ey, c->g.minp[3], c->g.maxp[3], c->g.n[3], c->tab_vy, A->tab_vy_adj, A->dw_vy};
+  const VtableAdjJob jx = {ex, c->g.minp[2], c->g.maxp[2], c->g.n[2], c->tab_vx, A->tab_vx_adj, A->dw_vx};
+  const VtableAdjJob jy = {ey, c->g.minp[3], c->g.maxp[3], c->g.n[3], c->tab_vy, A->tab_vy_adj, A->dw_vy};
   k_build_vtables_rev<<<dim3((unsigned)blocks, 2u), threads, 0, s>>>(jx, jy, lines, dt);
   VLP4D_LAUNCH_CHECK();
   c->tab_vx.valid = c->tab_vy.valid = true;
@@ -734,12 +738,13 @@ int step_adjoint(vlp4d_adjoint *A, const void *f_state, const void *lam_next, vo
   return step_adjoint_stored(A, A->P[0], nullptr, lam_next, lam_out, s);
 }
 
+// Ex and Ey of step j of the segment: one copy (Ey sits fstride after Ex in
+// both places).
 void save_field(vlp4d_adjoint *A, int j, cudaStream_t s) {
   vlp4d_ctx *c = A->ctx;
   const long long n2 = c->g.nxy();
-  double *e = A->seg_e + 2 * n2 * (long long)j;
-  cudaMemcpyAsync(e, c->ex, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s);
-  cudaMemcpyAsync(e + n2, c->ey, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s);
+  double *e = A->seg_e + 2 * (long long)c->fstride * j;
+  cudaMemcpyAsync(e, c->ex, sizeof(double) * ((long long)c->fstride + n2), cudaMemcpyDeviceToDevice, s);
 }
 
 // The closing x/y half step of one step and the opening one (with the
@@ -758,12 +763,46 @@ int xy_xy_moment(vlp4d_ctx *c, const void *in, void *out, void *tmp, cudaStream_
   return advect_xy_moment(c, tmp, out, 0.5 * c->dom.dt, s);
 }
 
+// The stage inputs a = XY f (into seg[0 .. len-1]) and fields E (seg_e) of
+// len steps from the state f: the moment pass, then per further step the
+// v pass and the joined x/y/x/y pass with the moment; the last step's v pass
+// is left to the caller.
+int store_segment(vlp4d_adjoint *A, const void *f, int len, cudaStream_t s) {
+  vlp4d_ctx *c = A->ctx;
+  const double dt = c->dom.dt;
+  int rc;
+  if ((rc = advect_xy_moment(c, f, A->seg[0], 0.5 * dt, s))) return rc;
+  if ((rc = launch_field_poisson(c, s))) return rc;
+  save_field(A, 0, s);
+  for (int j = 1; j < len; ++j) {
+    if ((rc = build_v_tables(c, dt, true, true, s))) return rc;
+    if ((rc = advect_vxvy_any(c, A->seg[j - 1], A->W[0], &c->tab_vx, &c->tab_vy, s))) return rc;
+    if ((rc = xy_xy_moment(c, A->W[0], A->seg[j], A->W[1], s))) return rc;
+    if ((rc = launch_field_poisson(c, s))) return rc;
+    save_field(A, j, s);
+  }
+  return VLP4D_OK;
+}
+
 // Forward sweep: nsteps steps from f0, each segment's final state written to
 // the next checkpoint (the last one to P[1]); J and dJ/df_N into d_J, L[0].
 int forward_body(vlp4d_adjoint *A, const void *f0, void *f_out, cudaStream_t s) {
   vlp4d_ctx *c = A->ctx;
   const double dt = c->dom.dt;
   int rc;
+  if (A->store_all) {
+    if ((rc = store_segment(A, f0, A->nsteps, s))) return rc;
+    // The last step's v pass and closing x/y half step.
+    if ((rc = build_v_tables(c, dt, true, true, s))) return rc;
+    if ((rc = advect_vxvy_any(c, A->seg[A->nsteps - 1], A->W[0], &c->tab_vx, &c->tab_vy, s))) return rc;
+    StencilTable *tx = nullptr, *ty = nullptr;
+    if ((rc = ensure_xy_table(c, 0, 0.5 * dt, &tx, s))) return rc;
+    if ((rc = ensure_xy_table(c, 1, 0.5 * dt, &ty, s))) return rc;
+    if ((rc = advect_xy_any(c, A->W[0], A->P[1], tx, ty, s))) return rc;
+    if ((rc = energy_grad(A, A->P[1], A->L[0], s))) return rc;
+    if (f_out) VLP4D_CUDA_TRY(cudaMemcpyAsync(f_out, A->P[1], A->fbytes, cudaMemcpyDeviceToDevice, s));
+    return VLP4D_OK;
+  }
   VLP4D_CUDA_TRY(cudaMemcpyAsync(A->ckpt[0], f0, A->fbytes, cudaMemcpyDeviceToDevice, s));
   const int nseg = (int)A->ckpt.size();
   for (int sg = 0; sg < nseg; ++sg) {
@@ -800,19 +839,11 @@ int backward_body(vlp4d_adjoint *A, void *grad, cudaStream_t s) {
   const long long n2 = c->g.nxy();
   int rc;
   int cur = 0;
-  const int nseg = (int)A->ckpt.size();
+  const int nseg = A->store_all ? 1 : (int)A->ckpt.size();
   for (int sg = nseg - 1; sg >= 0; --sg) {
     const int len = A->nsteps - sg * A->every < A->every ? A->nsteps - sg * A->every : A->every;
-    if ((rc = advect_xy_moment(c, A->ckpt[sg], A->seg[0], 0.5 * dt, s))) return rc;
-    if ((rc = launch_field_poisson(c, s))) return rc;
-    save_field(A, 0, s);
-    for (int j = 1; j < len; ++j) {
-      if ((rc = build_v_tables(c, dt, true, true, s))) return rc;
-      if ((rc = advect_vxvy_any(c, A->seg[j - 1], A->W[0], &c->tab_vx, &c->tab_vy, s))) return rc;
-      if ((rc = xy_xy_moment(c, A->W[0], A->seg[j], A->W[1], s))) return rc;
-      if ((rc = launch_field_poisson(c, s))) return rc;
-      save_field(A, j, s);
-    }
+    // The forward sweep stored everything when store_all.
+    if (!A->store_all && (rc = store_segment(A, A->ckpt[sg], len, s))) return rc;
     // The reverse steps of the segment, last first.  Between two of them
     // the closing XY^T of one and the opening XY^T of the next are one pass
     // of the transposed 11-tap lines (as the forward sweep joins its x/y
@@ -820,7 +851,8 @@ int backward_body(vlp4d_adjoint *A, void *grad, cudaStream_t s) {
     // segment's start.  W[1] holds lb of the step, W[0] its la.
     if ((rc = advect_xy_any(c, A->L[cur], A->W[1], &A->tab_x_adj, &A->tab_y_adj, s))) return rc;
     for (int j = len - 1; j >= 0; --j) {
-      if ((rc = reverse_core(A, A->seg[j], A->seg_e + 2 * n2 * j, A->W[1], A->W[0], s))) return rc;
+      if ((rc = reverse_core(A, A->seg[j], A->seg_e + 2 * (long long)c->fstride * j, A->W[1], A->W[0], s)))
+        return rc;
       if (j > 0) {
         rc = A->tab_x11_adj.valid
                  ? launch_advect_xyxy_tables(c, A->W[0], A->W[1], &A->tab_x11_adj, &A->tab_y11_adj, false, s)
@@ -917,13 +949,15 @@ int vlp4d_adjoint_create(vlp4d_ctx *ctx, int nsteps, int every, vlp4d_adjoint **
   if (!ctx) return fail_msg(VLP4D_ERR_INVALID_ARG, "ctx is NULL");
   if (ctx->slab) return fail_msg(VLP4D_ERR_UNSUPPORTED, "adjoint_create: not available on a vy-slab context");
   if (nsteps < 1) return fail_msg(VLP4D_ERR_INVALID_ARG, "nsteps must be at least 1");
-  if (every < 1) return fail_msg(VLP4D_ERR_INVALID_ARG, "the checkpoint interval must be at least 1");
-  if (every > nsteps) every = nsteps;
+  if (every < 0) return fail_msg(VLP4D_ERR_INVALID_ARG, "the checkpoint interval must be at least 0");
+  const bool store_all = every == 0;
+  if (store_all || every > nsteps) every = nsteps;
   VLP4D_CUDA_TRY(cudaSetDevice(ctx->device));
   vlp4d_adjoint *A = new vlp4d_adjoint();
   A->ctx = ctx;
   A->nsteps = nsteps;
   A->every = every;
+  A->store_all = store_all;
   A->fbytes = (size_t)ctx->g.cells() * ctx->elem;
   const char *g = getenv("VLP4D_ADJOINT_GRAPHS");
   if (g && *g == '0') A->use_graphs = false;
@@ -940,7 +974,7 @@ int vlp4d_adjoint_create(vlp4d_ctx *ctx, int nsteps, int every, vlp4d_adjoint **
       return bail(fail_msg(VLP4D_ERR_CUDA, "cudaMalloc failed in vlp4d_adjoint_create (" #ptr ")")); \
     }                                                                                              \
   } while (0)
-  const int nck = (nsteps + every - 1) / every;
+  const int nck = store_all ? 0 : (nsteps + every - 1) / every;
   A->ckpt.assign(nck, nullptr);
   for (auto &p : A->ckpt) ADJ_ALLOC(p, A->fbytes);
   A->seg.assign(every, nullptr);
@@ -950,7 +984,7 @@ int vlp4d_adjoint_create(vlp4d_ctx *ctx, int nsteps, int every, vlp4d_adjoint **
     ADJ_ALLOC(A->W[i], A->fbytes);
     ADJ_ALLOC(A->L[i], A->fbytes);
   }
-  ADJ_ALLOC(A->seg_e, sizeof(double) * 2 * n2 * (size_t)every);
+  ADJ_ALLOC(A->seg_e, sizeof(double) * 2 * ctx->fstride * (size_t)every);
   ADJ_ALLOC(A->gex, sizeof(double) * (6 * n2 + 1));
   A->gey = A->gex + n2;
   A->lam_rho = A->gey + n2;

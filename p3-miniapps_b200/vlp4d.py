@@ -499,7 +499,10 @@ def transpose(a, out, stream=None):
 
 class Adjoint:
     """Reverse mode of a Context (vlp4d_adjoint_*): checkpointed runs of
-    `nsteps` steps with the objective J = dx dy sum |E(f_N)|^2."""
+    `nsteps` steps with the objective J = dx dy sum |E(f_N)|^2; a checkpoint
+    of f every `every` steps, or (every = 0) every step's stage input and
+    field stored by the forward run, so that the reverse run recomputes
+    nothing."""
 
     def __init__(self, ctx: Context, nsteps: int, every: int = 8):
         self.ctx = ctx

@@ -64,8 +64,10 @@ def test_step_adjoint_matches_cpu_adjoint(pkg, cuda, n, kernels):
         ctx.check()
 
 
-@pytest.mark.parametrize("every", [1, 3, 8])
+@pytest.mark.parametrize("every", [1, 3, 8, 0])
 def test_checkpointed_run_gradient_matches_cpu_adjoint(pkg, cuda, every):
+    """every = 0: the forward run stores every step's stage input and field,
+    the reverse run recomputes nothing."""
     torch = cuda
     n, nsteps = (16, 8, 16, 12), 7
     dom = _dom(pkg, n, nbiter=nsteps)
@@ -77,6 +79,29 @@ def test_checkpointed_run_gradient_matches_cpu_adjoint(pkg, cuda, every):
         g = adj.backward().cpu().numpy()
     assert abs(J - J_ref) <= 1e-11 * J_ref
     assert _rel(g, g_ref) < 1e-10
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_store_all_run_equals_one_segment_run(pkg, cuda, dtype):
+    """every = 0 runs the forward sweep of a single checkpoint segment
+    (every = nsteps) and stores what that segment's recomputation would
+    store: J, the final state and the gradient are bit-identical."""
+    torch = cuda
+    n, nsteps = (32, 16, 32, 24), 9
+    dom = _dom(pkg, n, nbiter=nsteps)
+    res = []
+    for every in (nsteps, 0):
+        with pkg.Context(dom, dtype) as ctx, pkg.Adjoint(ctx, nsteps, every) as adj:
+            f0 = ctx.empty_f()
+            ctx.init_case(f0, IC_LANDAU_SUM, 0.05, 0.5)
+            fN = ctx.empty_f()
+            for _ in range(2):  # the second call through the cached graphs
+                J = adj.forward(f0, fN)
+                g = adj.backward()
+            res.append((J, fN.cpu(), g.cpu()))
+    assert res[0][0] == res[1][0]
+    assert torch.equal(res[0][1], res[1][1])
+    assert torch.equal(res[0][2], res[1][2])
 
 
 def _landau_eps_f0(torch, n, eps, k=0.5, vmax=6.0, dtype=None):
