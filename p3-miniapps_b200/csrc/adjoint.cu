@@ -593,11 +593,17 @@ int launch_vgrad(vlp4d_adjoint *A, const void *a, const void *lb, cudaStream_t s
     const int gy = nvx / V;
     int cw = 512 / gy;
     if (cw > 32) cw = 32;
+    if (getenv("VLP4D_VGRAD_CW")) {  // columns per block, for tuning sweeps
+      const int f = atoi(getenv("VLP4D_VGRAD_CW"));
+      if (f >= 1 && f <= cw) cw = f;
+    }
     const int bxv = (nxy + cw - 1) / cw;
     // vy segments: a block streams Qv + 5 rows of its segment, one block per
     // SM at a time, so the pass takes about ceil(blocks / SMs) * (Qv + 5)
-    // row times; the segment count minimises that among those that give
-    // every SM a block (VLP4D_VGRAD_SEGS overrides).
+    // row times; the segment count minimises that, one wave on part of the
+    // SMs included (64^4 FP32: 128 blocks of one segment, 69 row times,
+    // measured 2-3 us faster than 256 blocks of two, 2 x 37; VLP4D_VGRAD_SEGS
+    // overrides).
     int ns = 0;
     {
       long long best = -1;
@@ -606,7 +612,7 @@ int launch_vgrad(vlp4d_adjoint *A, const void *a, const void *lb, cudaStream_t s
         const int q = (nvy + k - 1) / k;
         if ((nvy + q - 1) / q != k) continue;  // the same segments as a smaller count
         const long long blocks = (long long)bxv * k;
-        if (forced ? k != forced : (blocks < c->num_sms && k < nvy && k < A->gsegs)) continue;
+        if (forced && k != forced) continue;
         const long long cost = (blocks + c->num_sms - 1) / c->num_sms * (q + 5);
         if (best < 0 || cost < best) {
           best = cost;
@@ -618,22 +624,27 @@ int launch_vgrad(vlp4d_adjoint *A, const void *a, const void *lb, cudaStream_t s
     const int Qv = (nvy + ns - 1) / ns;
     ns = (nvy + Qv - 1) / Qv;
     dim3 gridv(bxv, ns), blockv(cw, gy);
+    // One segment: its partials are gex, gey themselves (gey follows gex
+    // as the partials of a segment follow each other).
+    double *part = ns == 1 ? A->gex : A->gpart;
     if (c->dtype == VLP4D_F64) {
       auto kern = k_vgrad_v<double, 2, vgrad_slots<double, 2>()>;
       const size_t sm = vgrad_smem<double, 2>(cw * gy, gy, cw);
       VLP4D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
       kern<<<gridv, blockv, sm, s>>>((const double *)a, (const double *)lb, nxy, nvx, nvy, Qv, c->tab_vx, c->tab_vy,
-                                     A->dw_vx, A->dw_vy, A->gpart);
+                                     A->dw_vx, A->dw_vy, part);
     } else {
       auto kern = k_vgrad_v<float, 4, vgrad_slots<float, 4>()>;
       const size_t sm = vgrad_smem<float, 4>(cw * gy, gy, cw);
       VLP4D_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
       kern<<<gridv, blockv, sm, s>>>((const float *)a, (const float *)lb, nxy, nvx, nvy, Qv, c->tab_vx, c->tab_vy,
-                                     A->dw_vx, A->dw_vy, A->gpart);
+                                     A->dw_vx, A->dw_vy, part);
     }
     VLP4D_LAUNCH_CHECK();
-    k_vgrad_finish<<<(nxy + 255) / 256, 256, 0, s>>>(A->gpart, ns, nxy, A->gex, A->gey);
-    VLP4D_LAUNCH_CHECK();
+    if (ns > 1) {
+      k_vgrad_finish<<<(nxy + 255) / 256, 256, 0, s>>>(A->gpart, ns, nxy, A->gex, A->gey);
+      VLP4D_LAUNCH_CHECK();
+    }
     return VLP4D_OK;
   }
   dim3 grid(bx, nseg), block(32, 8);
