@@ -1277,10 +1277,14 @@ int run_xyxy_nx(vlp4d_ctx *c, const PlaneArgs &args, PlaneCfg &cfg, bool rho, cu
 }
 
 // k_plane_xyxy64: FP64, row widths a warp holds whole.  Chunk height: the
-// tallest divisor of ny up to 32 whose block fits, four rows per thread
-// when it divides, else one; two stages (three when two CTAs per SM are out
-// of reach anyway).  VLP4D_XYXY64=0 turns it off (the FP64 form of
-// k_plane_xyxy then runs); VLP4D_XYXY_STAGES overrides the depth.
+// tallest divisor of ny up to 64 whose block fits, four rows per thread
+// when it divides, else one (the X11 phase also sweeps the ten halo rows:
+// 16% extra at 64 rows, 31% at 32; at 128^4, 64 rows and two stages in one
+// 512-thread CTA per SM measured 1.050 against 1.080 ms for 32 rows in two
+// CTAs); two stages (three when two CTAs per SM are out of reach anyway and
+// three fit).  VLP4D_XYXY64=0 turns it off (the FP64 form of
+// k_plane_xyxy then runs); VLP4D_XYXY_STAGES overrides the depth,
+// VLP4D_XYXY64_R the chunk height.
 size_t xyxy64_smem(int R, int nx, int stages, int nvx, int nvy) {
   return kBarBytes + sizeof(LineRec11<double>) * (size_t)(nvx + nvy) + (size_t)stages * (R + 10) * nx * 8;
 }
@@ -1301,13 +1305,18 @@ bool xyxy64_config(const vlp4d_ctx *c, PlaneCfg &cfg) {
   const int ncg = nx / 4;
   const int forced = env_int("VLP4D_XYXY_STAGES", 0);
   if (forced && (forced < 2 || forced > kMaxStages)) return false;
-  for (int r = ny < 32 ? ny : 32; r >= 1; --r) {
+  const int forced_r = env_int("VLP4D_XYXY64_R", 0);  // chunk height, for tuning sweeps
+  const int rmax = forced_r > 0 ? forced_r : 64;
+  for (int r = ny < rmax ? ny : rmax; r >= 1; --r) {
     if (ny % r) continue;
+    if (forced_r && r != forced_r) continue;
     const int t = r % 4 == 0 ? 4 : 1;
     const int threads = ncg * (r / t);
     if (threads > 512) continue;
     int st = forced ? forced : 2;
-    if (!forced && xyxy64_smem(r, nx, 2, c->g.n[2], c->g.n[3]) > 112 * 1024) st = 3;
+    if (!forced && xyxy64_smem(r, nx, 2, c->g.n[2], c->g.n[3]) > 112 * 1024 &&
+        xyxy64_smem(r, nx, 3, c->g.n[2], c->g.n[3]) <= 224 * 1024)
+      st = 3;
     const size_t smem = xyxy64_smem(r, nx, st, c->g.n[2], c->g.n[3]);
     if (smem > 224 * 1024) continue;
     cfg.R = r;
