@@ -1079,9 +1079,9 @@ size_t plane_smem(int R, int halo, int nx, size_t elem, int stages, bool dx, boo
 }
 
 // Chooses the chunk height R, rows per thread RT, the pipeline depth and the
-// block size nx/4 * R/RT.  R is the tallest divisor of ny up to 32 (the
-// halo re-read is 5/R of the rows, served from L2; taller chunks were not
-// faster at 128^4); then the deepest pipeline (3, else 2 stages) that lets
+// block size nx/4 * R/RT.  R is the tallest divisor of ny up to 32, 64 for
+// the in-place FP64 x+y form (the halo re-read is 5/R of the rows, served
+// from L2); then the deepest pipeline (3, else 2 stages) that lets
 // two CTAs share an SM, else one CTA per SM with 3 stages.
 // VLP4D_PLANE_R / _STAGES / _RT override for tuning sweeps.
 bool plane_config(const vlp4d_ctx *c, bool dx, bool dy, PlaneCfg &cfg) {
@@ -1093,8 +1093,17 @@ bool plane_config(const vlp4d_ctx *c, bool dx, bool dy, PlaneCfg &cfg) {
   const int forced_r = env_int("VLP4D_PLANE_R", 0);
   const int forced_rt = env_int("VLP4D_PLANE_RT", 0);
   const int forced_s = env_int("VLP4D_PLANE_STAGES", 0);
+  // FP64 x+y: x-swept rows in place (no separate tiles) when a warp holds
+  // whole rows; VLP4D_PLANE_INPLACE=0 turns it off.
+  const bool inplace = elem == 8 && dx && dy && 32 % ncg == 0 && env_int("VLP4D_PLANE_INPLACE", 1) != 0;
+  // Chunks of up to 32 rows; up to 64 for the in-place FP64 form, whose x
+  // sweep also covers the five halo rows (7.8% extra at 64 rows, 15.6% at
+  // 32): at 128^4, 64 rows in three stages (one 512-thread CTA per SM)
+  // measured 0.768 against 0.844 ms; FP32 x+y was slower with 64 (0.430
+  // against 0.412 ms).
   int R = 0, rt = 1;
-  for (int r = ny < 32 ? ny : 32; r >= 1; --r) {
+  const int rmax = forced_r > 32 ? forced_r : (inplace ? 64 : 32);
+  for (int r = ny < rmax ? ny : rmax; r >= 1; --r) {
     if (ny % r) continue;
     if (forced_r && r != forced_r) continue;
     const int t = forced_rt ? forced_rt : (r % 4 == 0 ? 4 : 1);
@@ -1105,9 +1114,6 @@ bool plane_config(const vlp4d_ctx *c, bool dx, bool dy, PlaneCfg &cfg) {
     break;
   }
   if (!R) return false;
-  // FP64 x+y: x-swept rows in place (no separate tiles) when a warp holds
-  // whole rows; VLP4D_PLANE_INPLACE=0 turns it off.
-  const bool inplace = elem == 8 && dx && dy && 32 % ncg == 0 && env_int("VLP4D_PLANE_INPLACE", 1) != 0;
   const size_t two_per_sm = 112 * 1024, one_per_sm = 224 * 1024;
   int stages = 0;
   if (forced_s) {
